@@ -1,0 +1,213 @@
+/*
+ * vkb.h -- C ABI of the B200 render backend for vork's `std/path` integrator.
+ *
+ * The reference has no FFI or plugin registry for its integrator: the path pass is
+ * recorded by `passes::path::record` (crates/vork-render/src/passes/path.rs:539-559)
+ * over a 30-binding wgpu layout (passes/path.rs:323-384), after the acceleration
+ * structures are built by `rt::Rays::new` / `FrameRays::new` / `rt::encode`
+ * (crates/vork-render/src/rt.rs:1098,1339,1387).  The entry points below are what a
+ * Rust shim in `passes::path` would bind instead of that dispatch.  Plain C types
+ * only: pointers, sizes and POD structs.  No call traps on the device; every device
+ * wait and traversal loop is bounded and reports through vkb_status / vkb_stats.
+ */
+#ifndef VKB_H
+#define VKB_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VKB_ABI_VERSION 1u
+
+/* Error model: FailureKind exit categories of crates/vork-render/src/failure.rs:21-100,
+ * reduced to what a render call can report. */
+typedef enum vkb_status {
+    VKB_OK = 0,
+    VKB_INVALID_ARG = 1,      /* malformed descriptor or profile (failure.rs "scene") */
+    VKB_OUT_OF_MEMORY = 2,    /* device allocation refused (gpu_memory.rs device_limit) */
+    VKB_DEVICE_TIMEOUT = 3,   /* a bounded device loop or host wait ran out */
+    VKB_NONFINITE = 4,        /* reserved: non-finite scene input */
+    VKB_INTERNAL = 5,         /* CUDA runtime error; message via vkb_last_error() */
+    VKB_UNSUPPORTED = 6       /* a profile feature outside the built subset */
+} vkb_status;
+
+/* Ray-event bits, crates/vork-slang/src/registry.rs:186-191. */
+#define VKB_RAY_CAMERA 1u
+#define VKB_RAY_SHADOW 2u
+#define VKB_RAY_DIFFUSE 4u
+#define VKB_RAY_SPECULAR 8u
+#define VKB_RAY_TRANSMISSION 16u
+#define VKB_RAY_VOLUME 32u
+/* Light record words, registry.rs:161,322-328,344. */
+#define VKB_LIGHT_CONTRIBUTION_WORD 0
+#define VKB_LIGHT_LINK_WORD 1
+#define VKB_LIGHT_RAY_WORD 2
+#define VKB_LIGHT_RAY_LINK_WORD 3
+#define VKB_LIGHT_RAY_SHADOWED 1u
+#define VKB_LIGHT_RAY_SHADOWED_BY_ALL 2u
+#define VKB_LIGHT_LINK_ALL 64u
+
+/* One triangle mesh in object space (the BLAS input of rt.rs:1098-1289). */
+typedef struct vkb_mesh {
+    const float* positions;    /* num_vertices*3 */
+    const float* normals;      /* num_vertices*3 smooth normals (NULL: face normals) */
+    const uint32_t* indices;   /* num_triangles*3, counter-clockwise = front */
+    uint32_t num_vertices;
+    uint32_t num_triangles;
+} vkb_mesh;
+
+/* OpenPBR 1.1.1 inputs used by the path subset (crates/vork-scene/openpbr-params.md:22-30);
+ * every other OpenPBR input is held at its specification default. */
+typedef struct vkb_material {
+    float base_weight;
+    float base_color[3];
+    float base_metalness;
+    float specular_weight;
+    float specular_color[3];
+    float specular_roughness;
+    float specular_ior;
+    float emission_luminance;  /* must be 0: emissive meshes are outside the built subset */
+    float emission_color[3];
+    uint32_t flags;            /* bit 1: double sided (registry FLAG_DOUBLE_SIDED) */
+} vkb_material;
+
+/* Analytic light record, byte-for-byte `Light` of crates/vork-render/src/lights.rs:13-24
+ * (8 shadow words + 8 float4 = 160 B). kind = position[3]: 0 sun, 1 point, 2 spot, 3 area. */
+typedef struct vkb_light {
+    uint32_t shadow_offsets[8];
+    float position[4];
+    float direction[4];
+    float radiance[4];
+    float params[4];
+    float emitter_u[4];
+    float emitter_v[4];
+    float emission[4];
+    float projection[4];
+} vkb_light;
+
+/* Pinhole camera: the Frame uniform subset path_camera_ray reads
+ * (crates/vork-render/src/lib.rs:288-320; shaders/vork_prelude.slang:95-108). */
+typedef struct vkb_camera {
+    float eye[3];
+    float right[3];
+    float up[3];
+    float forward[3];
+    float proj_x;       /* projection[0][0]: Frame.projection.y */
+    float proj_y;       /* projection[1][1]: Frame.projection.x */
+    float near_plane;   /* Frame.params.x */
+    float far_plane;    /* Frame.params.y */
+    uint32_t width;
+    uint32_t height;
+} vkb_camera;
+
+/* Constant world light (Frame.radiance / background, path.slang:961-983). */
+typedef struct vkb_environment {
+    float radiance[3];         /* constant environment radiance seen by every ray */
+    float exposure;            /* Frame.radiance.w, multiplies the finished sample */
+    float background[3];       /* camera-miss colour when camera_sees_environment == 0 */
+    uint32_t camera_sees_environment;
+} vkb_environment;
+
+typedef struct vkb_scene_desc {
+    const vkb_mesh* meshes;
+    uint32_t num_meshes;
+    uint32_t num_instances;
+    const float* instance_rows;       /* num_instances*12: rows of the 3x4 object->world matrix (Object.model, lib.rs:226-240) */
+    const uint32_t* instance_mesh;    /* num_instances */
+    const uint32_t* instance_material;/* num_instances */
+    const vkb_material* materials;
+    uint32_t num_materials;
+    const vkb_light* lights;
+    uint32_t num_lights;
+    vkb_camera camera;
+    vkb_environment environment;
+} vkb_scene_desc;
+
+/* PathSettings (path.slang:54; passes/path.rs:16-28,576-607). */
+typedef struct vkb_profile {
+    uint32_t samples;          /* exposure sample count (Frame.temporal.y) */
+    uint32_t first_sample;     /* first exposure index rendered by this call (resume/progressive) */
+    uint32_t sample_count;     /* samples rendered by this call (0 = samples - first_sample) */
+    uint32_t seed;             /* sampling.y */
+    uint32_t bounces[4];       /* max, diffuse, glossy, transmission */
+    uint32_t transparent;      /* limits.z */
+    uint32_t caustics;         /* limits.w bits: 1 glossy after diffuse, 2 transmission after diffuse */
+    float clamp_direct;        /* clamp.x (0 = off) */
+    float clamp_indirect;      /* clamp.y (0 = off) */
+    float light_threshold;     /* adaptive.z: stochastic light-sample kill */
+    uint32_t adaptive;         /* must be 0: adaptive stopping is outside the built subset */
+    uint32_t wave_samples;     /* samples per wavefront wave (0 = automatic) */
+} vkb_profile;
+
+/* Render output: linear RGBA32F mean image (resolve.slang:162-191). */
+typedef struct vkb_output {
+    float* rgba;               /* width*height*4 */
+    uint32_t on_device;        /* 1: rgba is a device pointer on the context's GPU */
+    uint32_t* primary_ids;     /* optional, width*height*2 (instance, triangle) of sample first_sample; 0xffffffff on miss */
+} vkb_output;
+
+typedef struct vkb_stats {
+    uint64_t paths;            /* camera samples traced */
+    uint64_t extension_rays;   /* closest-hit rays */
+    uint64_t shadow_rays;      /* any-hit rays */
+    uint64_t dropped_path_samples;  /* non-finite samples zeroed (path.slang:1946-1955) */
+    uint64_t dropped_light_samples; /* non-finite contributions dropped (sample_clamp.slang) */
+    uint64_t traversal_overflows;   /* bounded-stack or iteration-cap exits (error, never a trap) */
+    float render_ms;           /* device time of the wavefront, CUDA events */
+    float build_ms;            /* device time of the last acceleration-structure build */
+} vkb_stats;
+
+typedef struct vkb_ctx vkb_ctx;
+typedef struct vkb_scene vkb_scene;
+
+/* Library identity and the last error message of this thread. */
+uint32_t vkb_abi_version(void);
+const char* vkb_last_error(void);
+
+/* Renderer::new (crates/vork-render/src/lib.rs:726) for one CUDA device.  Also bakes
+ * the BRDF lookup atlas (shaders/environment.slang:28-108, src/environment.rs:312-323). */
+vkb_status vkb_open(int device, vkb_ctx** out);
+vkb_status vkb_close(vkb_ctx* ctx);
+
+/* Renderer::install + FrameRays::new (lib.rs:1322-1470; rt.rs:1098-1385): uploads the
+ * descriptor (copied; the caller may free it on return) and builds every BLAS and the TLAS. */
+vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* desc, vkb_scene** out);
+vkb_status vkb_scene_destroy(vkb_scene* scene);
+
+/* rt::encode / rebuild_tlas (rt.rs:1387-1476): new object->world rows for every
+ * instance (host pointer, num_instances*12 floats). policy 0: refit-vs-rebuild by the
+ * reference's quarter-of-the-bytes rule, 1: always rebuild, 2: always refit. */
+vkb_status vkb_scene_update_instances(vkb_scene* scene, const float* rows, uint32_t num_instances, int policy);
+
+/* passes::path::record + resolve (passes/path.rs:539-724; resolve.slang:162-191): renders
+ * samples [first_sample, first_sample+sample_count) of `profile` and writes the mean
+ * over them. stats may be NULL. */
+vkb_status vkb_render(vkb_scene* scene, const vkb_profile* profile, vkb_output* out, vkb_stats* stats);
+
+/* --- Test and measurement entry points (no reference counterpart beyond the cited tests) --- */
+
+/* Sampler groups, bit-exact with path_sampler.slang:53-95 (the harness of
+ * src/path_sampler.rs:266-276): for each i, the four 32-bit scrambled fractions of
+ * group groups[i] at pixel (px[i],py[i]), index[i], count, stream. out: n*4 u32 (host). */
+vkb_status vkb_debug_sampler_groups(vkb_ctx* ctx, uint32_t n, const uint32_t* px, const uint32_t* py,
+                                    const uint32_t* index, const uint32_t* groups, uint32_t count,
+                                    uint32_t stream, uint32_t* out_bits);
+/* The BRDF atlas as baked on the device: 128*2240*4 floats (host), fp16 values widened. */
+vkb_status vkb_debug_brdf_lut(vkb_ctx* ctx, float* out);
+/* 30-bit Morton codes of the scene's TLAS build (instance AABB centroids over the scene
+ * box), in instance order: num_instances u32 (host). */
+vkb_status vkb_debug_tlas_morton(vkb_scene* scene, uint32_t* out);
+/* 30-bit Morton codes of one mesh's BLAS build (triangle centroids over the mesh box). */
+vkb_status vkb_debug_blas_morton(vkb_scene* scene, uint32_t mesh, uint32_t* out);
+/* Closest hits of n world rays (origin xyz, dir xyz, tmax per ray; host arrays):
+ * out_t[n], out_ids[n*2] (instance, triangle; 0xffffffff on miss), out_uv[n*2]. */
+vkb_status vkb_debug_trace(vkb_scene* scene, uint32_t n, const float* rays7, float* out_t,
+                           uint32_t* out_ids, float* out_uv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,168 @@
+"""vork_b200: a B200 (sm_100a) render backend for vork's `std/path` integrator.
+
+The product path is the CUDA library behind include/vkb.h; this module is the
+host-side mirror of the reference's entry (`Shot::render` / `vork.render(scene, ...)`,
+crates/vork-render/src/shot.rs:374, packages/python/vork/__init__.py:291) over it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi
+from .abi import VkbError
+from .scene import Scene
+
+__all__ = ["Profile", "Renderer", "InstalledScene", "render", "VkbError", "Scene"]
+
+
+@dataclass
+class Profile:
+    """PathSettings of one render (passes/path.rs:576-607; constants.rs:256-267).
+
+    The defaults are vork's std/path defaults; `reference_transport(depth)` is the
+    reference's own test hook `reference_transport_bounces` (passes/path.rs:599-607):
+    every bounce budget = depth, transparent = depth, both clamps off.
+    """
+    samples: int = 64
+    seed: int = 0
+    bounces: tuple = (12, 4, 4, 12)
+    transparent: int = 8
+    caustics: int = 0b11
+    clamp_direct: float = 0.0
+    clamp_indirect: float = 10.0
+    light_threshold: float = 0.01
+    adaptive: bool = False
+    first_sample: int = 0
+    sample_count: int = 0
+    wave_samples: int = 0
+
+    @classmethod
+    def reference_transport(cls, depth: int, samples: int, seed: int = 0, **kw) -> "Profile":
+        return cls(samples=samples, seed=seed, bounces=(depth,) * 4, transparent=depth, clamp_direct=0.0,
+                   clamp_indirect=0.0, **kw)
+
+    def c(self) -> abi.VkbProfile:
+        p = abi.VkbProfile()
+        p.samples, p.first_sample, p.sample_count, p.seed = self.samples, self.first_sample, self.sample_count, self.seed & 0xFFFFFFFF
+        p.bounces[:] = list(self.bounces)
+        p.transparent, p.caustics = self.transparent, self.caustics
+        p.clamp_direct, p.clamp_indirect, p.light_threshold = self.clamp_direct, self.clamp_indirect, self.light_threshold
+        p.adaptive = 1 if self.adaptive else 0
+        p.wave_samples = self.wave_samples
+        return p
+
+
+class Renderer:
+    """One CUDA device (Renderer::new, crates/vork-render/src/lib.rs:726)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = abi.load()
+        h = C.c_void_p()
+        abi.check(self.lib.vkb_open(device, C.byref(h)))
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if self.h:
+            self.lib.vkb_close(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def install(self, scene: Scene) -> "InstalledScene":
+        return InstalledScene(self, scene)
+
+    def sampler_groups(self, px, py, index, groups, count, stream):
+        px, py, index, groups = (np.ascontiguousarray(a, np.uint32) for a in (px, py, index, groups))
+        out = np.zeros((px.size, 4), np.uint32)
+        abi.check(self.lib.vkb_debug_sampler_groups(self.h, px.size, abi.uptr(px), abi.uptr(py), abi.uptr(index), abi.uptr(groups),
+                                                    count, stream, abi.uptr(out)))
+        return out
+
+    def brdf_lut(self):
+        out = np.zeros((2240, 128, 4), np.float32)
+        abi.check(self.lib.vkb_debug_brdf_lut(self.h, abi.fptr(out)))
+        return out
+
+
+@dataclass
+class RenderResult:
+    image: np.ndarray          # (H, W, 4) linear RGBA32F mean
+    stats: dict
+    primary_ids: np.ndarray | None = None
+
+
+class InstalledScene:
+    """Renderer::install + FrameRays (lib.rs:1322-1470; rt.rs:1098-1385) for one scene."""
+
+    def __init__(self, renderer: Renderer, scene: Scene):
+        self.r = renderer
+        self.scene = scene
+        self.desc = scene.desc()
+        h = C.c_void_p()
+        abi.check(renderer.lib.vkb_scene_create(renderer.h, C.byref(self.desc), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.r.lib.vkb_scene_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def update_instances(self, rows: np.ndarray, policy: int = 0):
+        rows = np.ascontiguousarray(rows, np.float32).reshape(-1)
+        abi.check(self.r.lib.vkb_scene_update_instances(self.h, abi.fptr(rows), rows.size // 12, policy))
+
+    def render(self, profile: Profile, ids: bool = False, out: np.ndarray | None = None, device_ptr: int | None = None) -> RenderResult:
+        cam = self.scene.camera
+        o = abi.VkbOutput()
+        img = None
+        if device_ptr is not None:
+            o.rgba = C.c_void_p(device_ptr)
+            o.on_device = 1
+        else:
+            img = out if out is not None else np.empty((cam.height, cam.width, 4), np.float32)
+            o.rgba = img.ctypes.data_as(C.c_void_p)
+            o.on_device = 0
+        idbuf = np.empty((cam.height, cam.width, 2), np.uint32) if ids else None
+        o.primary_ids = abi.uptr(idbuf) if ids else None
+        st = abi.VkbStats()
+        p = profile.c()
+        abi.check(self.r.lib.vkb_render(self.h, C.byref(p), C.byref(o), C.byref(st)))
+        stats = {k: getattr(st, k) for k, _ in abi.VkbStats._fields_}
+        return RenderResult(img, stats, idbuf)
+
+    def tlas_morton(self):
+        out = np.zeros(self.desc.num_instances, np.uint32)
+        abi.check(self.r.lib.vkb_debug_tlas_morton(self.h, abi.uptr(out)))
+        return out
+
+    def blas_morton(self, mesh: int):
+        out = np.zeros(self.scene.meshes[mesh].num_triangles, np.uint32)
+        abi.check(self.r.lib.vkb_debug_blas_morton(self.h, mesh, abi.uptr(out)))
+        return out
+
+    def trace(self, rays7: np.ndarray):
+        r = np.ascontiguousarray(rays7, np.float32)
+        n = r.shape[0]
+        t = np.zeros(n, np.float32); ids = np.zeros((n, 2), np.uint32); uv = np.zeros((n, 2), np.float32)
+        abi.check(self.r.lib.vkb_debug_trace(self.h, n, abi.fptr(r), abi.fptr(t), abi.uptr(ids), abi.fptr(uv)))
+        return t, ids, uv
+
+
+def render(scene: Scene, profile: Profile | None = None, device: int = 0) -> RenderResult:
+    """Render `scene` under `profile` on one GPU and return the linear mean image."""
+    with Renderer(device) as r, r.install(scene) as s:
+        return s.render(profile or Profile())

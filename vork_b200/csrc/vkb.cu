@@ -1,0 +1,632 @@
+// Host runtime and C ABI of the B200 render backend (include/vkb.h).
+//
+// One vkb_ctx per device: a CUDA stream, the BRDF atlas baked on the device
+// (Renderer::new + environment bake, crates/vork-render/src/lib.rs:726,
+// src/environment.rs:312-323) and the film table (src/sampling.rs:149-178).
+// One vkb_scene per installed scene: meshes, per-mesh BLAS, instance TLAS, material
+// and light tables (Renderer::install, lib.rs:1322-1470; rt.rs:1098-1385), plus the
+// wavefront buffers its renders reuse.
+#include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "vkb_kernels.cuh"
+
+using namespace vkb;
+
+namespace {
+
+thread_local std::string g_error;
+
+struct CudaError {
+    cudaError_t code;
+    const char* what;
+};
+#define VKB_CUDA(x)                                                    \
+    do {                                                               \
+        cudaError_t e_ = (x);                                          \
+        if (e_ != cudaSuccess) throw CudaError{e_, #x};                \
+    } while (0)
+
+struct ArgError { std::string msg; };
+struct Unsupported { std::string msg; };
+
+template <class T> struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        if (count <= n && p) return;
+        release();
+        if (count == 0) return;
+        VKB_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        n = count;
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+    void upload(const T* src, size_t count, cudaStream_t s) { alloc(count); if (count) VKB_CUDA(cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyHostToDevice, s)); }
+};
+
+int grid_for(uint32_t n, int block, int sm_count, int per_sm = 8) {
+    int need = int((uint64_t(n) + block - 1) / block);
+    return std::max(1, std::min(need, sm_count * per_sm));
+}
+
+// Film table: inverse CDF of Cycles' 1.5 px Blackman-Harris kernel, bisected in f64
+// (crates/vork-render/src/sampling.rs:151-178).
+std::vector<float> film_table() {
+    auto cdf = [](double x) {
+        const double pi = 3.141592653589793;
+        double t = pi * x / 1.5;
+        return 0.5 + (0.35875 * x + 1.5 / pi * (0.48829 * std::sin(t) + 0.14128 * std::sin(2. * t) / 2. + 0.01168 * std::sin(3. * t) / 3.)) / (3. * 0.35875);
+    };
+    std::vector<float> t(FILTER_INTERVALS + 1);
+    for (uint32_t i = 0; i <= FILTER_INTERVALS; ++i) {
+        if (i == 0) { t[i] = -1.5f; continue; }
+        if (i == FILTER_INTERVALS) { t[i] = 1.5f; continue; }
+        double u = double(i) / FILTER_INTERVALS, lo = -1.5, hi = 1.5;
+        for (int k = 0; k < 48; ++k) { double mid = (lo + hi) * 0.5; if (cdf(mid) < u) lo = mid; else hi = mid; }
+        t[i] = float((lo + hi) * 0.5);
+    }
+    return t;
+}
+
+// Light tree over analytic sources (crates/vork-render/src/lights/tree.rs:43-176).
+std::vector<LightTreeNode> light_tree(const vkb_light* lights, uint32_t n) {
+    struct Src { float lo[3], hi[3]; double power; bool inf; };
+    std::vector<Src> src(n);
+    const float lumc[3] = {0.2126f, 0.7152f, 0.0722f};
+    for (uint32_t i = 0; i < n; ++i) {
+        const vkb_light& l = lights[i];
+        uint32_t kind = uint32_t(l.position[3]);
+        for (int c = 0; c < 3; ++c) {
+            float r = kind == 3 ? (std::fabs(l.emitter_u[c]) + std::fabs(l.emitter_v[c])) * 0.5f : (kind == 0 ? 0.f : l.params[1]);
+            src[i].lo[c] = l.position[c] - r; src[i].hi[c] = l.position[c] + r;
+        }
+        double p = 0;
+        for (int c = 0; c < 3; ++c) p += double(l.radiance[c]) * double(lumc[c]);
+        src[i].power = std::max(p, 0.);
+        src[i].inf = kind == 0;
+    }
+    double scale = 2.2250738585072014e-308;
+    for (auto& s : src) scale = std::max(scale, s.power);
+    std::vector<LightTreeNode> nodes;
+    std::vector<uint32_t> ids(n);
+    for (uint32_t i = 0; i < n; ++i) ids[i] = i;
+    struct Builder {
+        std::vector<Src>& src; std::vector<LightTreeNode>& nodes; double scale;
+        uint32_t go(uint32_t* id, uint32_t count, uint32_t parent) {
+            uint32_t index = uint32_t(nodes.size());
+            nodes.push_back(LightTreeNode{});
+            float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+            double power = 0; bool inf = false;
+            for (uint32_t k = 0; k < count; ++k) {
+                const Src& s = src[id[k]];
+                for (int c = 0; c < 3; ++c) { lo[c] = std::min(lo[c], s.lo[c]); hi[c] = std::max(hi[c], s.hi[c]); }
+                power += s.power / scale; inf |= s.inf;
+            }
+            float pf = float(power);
+            if (pf < 1.17549435e-38f) pf = 0.f;
+            LightTreeNode nd{};
+            nd.lower_power = make_float4(lo[0], lo[1], lo[2], pf);
+            nd.upper_infinite = make_float4(hi[0], hi[1], hi[2], inf ? 1.f : 0.f);
+            nd.links = make_uint4(0xffffffffu, 0xffffffffu, parent, count);
+            if (count == 1) {
+                nd.source = make_uint4(0u, id[0], id[0], 0u);
+            } else {
+                double ext[3];
+                for (int c = 0; c < 3; ++c) ext[c] = double(hi[c]) - double(lo[c]);
+                int axis = (ext[0] >= ext[1] && ext[0] >= ext[2]) ? 0 : (ext[1] >= ext[2] ? 1 : 2);
+                uint32_t finite = 0;
+                for (uint32_t k = 0; k < count; ++k) finite += src[id[k]].inf ? 0u : 1u;
+                uint32_t split;
+                if (finite > 0 && finite < count) {
+                    std::sort(id, id + count, [&](uint32_t a, uint32_t b) { return std::make_pair(src[a].inf, a) < std::make_pair(src[b].inf, b); });
+                    split = finite;
+                } else {
+                    split = count / 2;
+                    std::nth_element(id, id + split, id + count, [&](uint32_t a, uint32_t b) {
+                        double ca = double(src[a].lo[axis]) + double(src[a].hi[axis]), cb = double(src[b].lo[axis]) + double(src[b].hi[axis]);
+                        return ca < cb || (ca == cb && a < b);
+                    });
+                }
+                uint32_t l = go(id, split, index);
+                uint32_t r = go(id + split, count - split, index);
+                nd.links.x = l; nd.links.y = r;
+            }
+            nodes[index] = nd;
+            return index;
+        }
+    } b{src, nodes, scale};
+    if (n) b.go(ids.data(), n, 0xffffffffu);
+    return nodes;
+}
+
+// Scratch of one LBVH build, reused across builds.
+struct LbvhScratch {
+    DBuf<uint32_t> codes, codes_sorted, ids, ids_sorted, leaf_parent, node_parent, counters, bounds;
+    DBuf<unsigned char> cub_temp;
+    void reserve(size_t n, cudaStream_t s) {
+        codes.alloc(n); codes_sorted.alloc(n); ids.alloc(n); ids_sorted.alloc(n);
+        leaf_parent.alloc(n); node_parent.alloc(std::max<size_t>(n, 1)); counters.alloc(std::max<size_t>(n, 1)); bounds.alloc(6);
+        size_t bytes = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, bytes, codes.p, codes_sorted.p, ids.p, ids_sorted.p, int(n), 0, 30, s);
+        cub_temp.alloc(std::max<size_t>(bytes, 1));
+    }
+};
+
+// Build one LBVH over n boxes into nodes (n-1 internal nodes, or 1 for n == 1).
+// On return scratch.ids_sorted holds the leaf order and scratch.codes the codes in input order.
+void build_lbvh(uint32_t n, const float4* lo, const float4* hi, BvhNode* nodes, LbvhScratch& sc, cudaStream_t s, int sms) {
+    if (n == 0) return;
+    sc.reserve(n, s);
+    VKB_CUDA(cudaMemsetAsync(sc.bounds.p, 0xff, 3 * sizeof(uint32_t), s));
+    VKB_CUDA(cudaMemsetAsync(sc.bounds.p + 3, 0x00, 3 * sizeof(uint32_t), s));
+    k_centroid_box<<<grid_for(n, 256, sms), 256, 0, s>>>(n, lo, hi, sc.bounds.p);
+    k_morton<<<grid_for(n, 256, sms), 256, 0, s>>>(n, lo, hi, sc.bounds.p, sc.codes.p, sc.ids.p);
+    size_t bytes = sc.cub_temp.n;
+    VKB_CUDA(cub::DeviceRadixSort::SortPairs(sc.cub_temp.p, bytes, sc.codes.p, sc.codes_sorted.p, sc.ids.p, sc.ids_sorted.p, int(n), 0, 30, s));
+    if (n == 1) {
+        k_single_leaf<<<1, 1, 0, s>>>(lo, hi, nodes);
+        return;
+    }
+    k_karras<<<grid_for(n - 1, 256, sms), 256, 0, s>>>(int(n), sc.codes_sorted.p, nodes, sc.leaf_parent.p, sc.node_parent.p, sc.counters.p);
+    k_refit<<<grid_for(n, 256, sms), 256, 0, s>>>(int(n), sc.ids_sorted.p, lo, hi, nodes, sc.leaf_parent.p, sc.node_parent.p, sc.counters.p);
+    VKB_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+struct vkb_ctx {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    DBuf<ushort4> lut;
+    DBuf<float> filter;
+};
+
+struct vkb_scene {
+    vkb_ctx* ctx = nullptr;
+    // host copies of the descriptor
+    uint32_t num_meshes = 0, num_instances = 0, total_tris = 0;
+    std::vector<MeshInfo> mesh_info;
+    std::vector<uint32_t> inst_mesh, inst_mat;
+    std::vector<vkb_material> materials;
+    std::vector<vkb_light> lights;
+    vkb_camera camera{};
+    vkb_environment env{};
+    uint32_t tree_nodes = 0;
+    double changed_bytes = 0;
+    // device scene
+    DBuf<float4> vpos, vnrm, blas_tris, o2w, w2o, inst_lo, inst_hi, tri_lo, tri_hi;
+    DBuf<uint32_t> indices, tlas_codes;
+    DBuf<uint4> inst_info;
+    DBuf<MeshInfo> meshes;
+    DBuf<BvhNode> blas_nodes, tlas_nodes;
+    DBuf<TlasLeaf> tlas_leaves;
+    DBuf<vkb_material> d_materials;
+    DBuf<vkb_light> d_lights;
+    DBuf<LightTreeNode> tree;
+    LbvhScratch scratch;
+    // wavefront
+    DBuf<float4> ray_o0, ray_d0, ray_o1, ray_d1, hit, thr, rad, sa_o, sa_d, sa_c, sb_o, sb_d, sb_c, accum, out_rgba;
+    DBuf<uint32_t> hit_inst, counters, err, ids;
+    DBuf<uint2> rng;
+    float build_ms = 0.f;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+vkb_status fail(vkb_status st, const std::string& msg) { g_error = msg; return st; }
+template <class F> vkb_status guarded(F&& f) {
+    try {
+        f();
+        return VKB_OK;
+    } catch (const CudaError& e) {
+        return fail(e.code == cudaErrorMemoryAllocation ? VKB_OUT_OF_MEMORY : VKB_INTERNAL, std::string(e.what) + ": " + cudaGetErrorString(e.code));
+    } catch (const ArgError& e) {
+        return fail(VKB_INVALID_ARG, e.msg);
+    } catch (const Unsupported& e) {
+        return fail(VKB_UNSUPPORTED, e.msg);
+    } catch (const std::bad_alloc&) {
+        return fail(VKB_OUT_OF_MEMORY, "host allocation failed");
+    }
+}
+
+SceneView scene_view(const vkb_scene* s) {
+    SceneView v;
+    v.tlas_nodes = s->tlas_nodes.p; v.tlas_leaves = s->tlas_leaves.p;
+    v.blas_nodes = s->blas_nodes.p; v.blas_tris = s->blas_tris.p;
+    v.num_instances = s->num_instances;
+    return v;
+}
+
+// Instance rows -> w2o, world boxes, TLAS (LBVH) and its leaf records.
+void build_tlas(vkb_scene* s) {
+    cudaStream_t st = s->ctx->stream;
+    int sms = s->ctx->sms;
+    uint32_t n = s->num_instances;
+    if (n == 0) return;
+    VKB_CUDA(cudaEventRecord(s->ev0, st));
+    k_instances<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->o2w.p, s->inst_info.p, s->meshes.p, s->w2o.p, s->inst_lo.p, s->inst_hi.p);
+    build_lbvh(n, s->inst_lo.p, s->inst_hi.p, s->tlas_nodes.p, s->scratch, st, sms);
+    k_tlas_leaves<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->scratch.ids_sorted.p, s->w2o.p, s->inst_info.p, s->meshes.p, s->d_materials.p, s->tlas_leaves.p);
+    VKB_CUDA(cudaMemcpyAsync(s->tlas_codes.p, s->scratch.codes.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    VKB_CUDA(cudaEventRecord(s->ev1, st));
+    VKB_CUDA(cudaEventSynchronize(s->ev1));
+    VKB_CUDA(cudaEventElapsedTime(&s->build_ms, s->ev0, s->ev1));
+}
+
+void validate_desc(const vkb_scene_desc* d) {
+    if (!d) throw ArgError{"null scene descriptor"};
+    if (d->num_meshes && !d->meshes) throw ArgError{"meshes pointer is null"};
+    for (uint32_t m = 0; m < d->num_meshes; ++m) {
+        const vkb_mesh& me = d->meshes[m];
+        if (me.num_triangles && (!me.positions || !me.indices)) throw ArgError{"mesh " + std::to_string(m) + " has no positions or indices"};
+        for (size_t i = 0; i < size_t(me.num_triangles) * 3; ++i)
+            if (me.indices[i] >= me.num_vertices) throw ArgError{"mesh " + std::to_string(m) + " index out of range"};
+        for (size_t i = 0; i < size_t(me.num_vertices) * 3; ++i)
+            if (!std::isfinite(me.positions[i])) throw ArgError{"mesh " + std::to_string(m) + " has a non-finite position"};
+    }
+    if (d->num_instances && (!d->instance_rows || !d->instance_mesh || !d->instance_material)) throw ArgError{"instance arrays are null"};
+    for (uint32_t i = 0; i < d->num_instances; ++i) {
+        if (d->instance_mesh[i] >= d->num_meshes) throw ArgError{"instance mesh index out of range"};
+        if (d->instance_material[i] >= d->num_materials) throw ArgError{"instance material index out of range"};
+    }
+    for (uint32_t m = 0; m < d->num_materials; ++m)
+        if (d->materials[m].emission_luminance != 0.f) throw Unsupported{"emissive materials are outside the built subset"};
+    for (uint32_t l = 0; l < d->num_lights; ++l) {
+        float k = d->lights[l].position[3];
+        if (!(k == 0.f || k == 1.f || k == 2.f || k == 3.f)) throw ArgError{"light kind must be 0..3"};
+    }
+    if (d->camera.width == 0 || d->camera.height == 0) throw ArgError{"camera resolution is zero"};
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t vkb_abi_version(void) { return VKB_ABI_VERSION; }
+const char* vkb_last_error(void) { return g_error.c_str(); }
+
+vkb_status vkb_open(int device, vkb_ctx** out) {
+    if (!out) return fail(VKB_INVALID_ARG, "null output pointer");
+    *out = nullptr;
+    vkb_ctx* c = new vkb_ctx();
+    vkb_status st = guarded([&] {
+        c->device = device;
+        VKB_CUDA(cudaSetDevice(device));
+        VKB_CUDA(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
+        VKB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->lut.alloc(size_t(BRDF_SIZE) * BRDF_HEIGHT);
+        k_bake_lut<<<dim3(1, BRDF_HEIGHT), BRDF_SIZE, 0, c->stream>>>(c->lut.p);
+        VKB_CUDA(cudaGetLastError());
+        std::vector<float> ft = film_table();
+        c->filter.upload(ft.data(), ft.size(), c->stream);
+        VKB_CUDA(cudaStreamSynchronize(c->stream));
+    });
+    if (st != VKB_OK) { delete c; return st; }
+    *out = c;
+    return VKB_OK;
+}
+
+vkb_status vkb_close(vkb_ctx* c) {
+    if (!c) return VKB_OK;
+    cudaSetDevice(c->device);
+    c->lut.release(); c->filter.release();
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return VKB_OK;
+}
+
+vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** out) {
+    if (!ctx || !out) return fail(VKB_INVALID_ARG, "null context or output pointer");
+    *out = nullptr;
+    vkb_scene* s = new vkb_scene();
+    s->ctx = ctx;
+    vkb_status st = guarded([&] {
+        validate_desc(d);
+        VKB_CUDA(cudaSetDevice(ctx->device));
+        cudaStream_t str = ctx->stream;
+        int sms = ctx->sms;
+        VKB_CUDA(cudaEventCreate(&s->ev0));
+        VKB_CUDA(cudaEventCreate(&s->ev1));
+        s->num_meshes = d->num_meshes;
+        s->num_instances = d->num_instances;
+        // Concatenate meshes.
+        uint32_t nv = 0, nt = 0;
+        s->mesh_info.resize(d->num_meshes);
+        for (uint32_t m = 0; m < d->num_meshes; ++m) {
+            MeshInfo& mi = s->mesh_info[m];
+            std::memset(&mi, 0, sizeof(mi));
+            mi.vertex_offset = nv; mi.index_offset = 3u * nt; mi.tri_offset = nt; mi.num_triangles = d->meshes[m].num_triangles;
+            float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+            for (uint32_t i = 0; i < d->meshes[m].num_vertices; ++i)
+                for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], d->meshes[m].positions[3 * i + a]); hi[a] = std::max(hi[a], d->meshes[m].positions[3 * i + a]); }
+            for (int a = 0; a < 3; ++a) { mi.lo[a] = lo[a]; mi.hi[a] = hi[a]; }
+            nv += d->meshes[m].num_vertices; nt += d->meshes[m].num_triangles;
+        }
+        s->total_tris = nt;
+        std::vector<float4> pos(nv), nrm(nv);
+        std::vector<uint32_t> idx(size_t(nt) * 3);
+        for (uint32_t m = 0; m < d->num_meshes; ++m) {
+            const vkb_mesh& me = d->meshes[m];
+            const MeshInfo& mi = s->mesh_info[m];
+            for (uint32_t i = 0; i < me.num_vertices; ++i) {
+                pos[mi.vertex_offset + i] = make_float4(me.positions[3 * i], me.positions[3 * i + 1], me.positions[3 * i + 2], 0.f);
+                nrm[mi.vertex_offset + i] = me.normals ? make_float4(me.normals[3 * i], me.normals[3 * i + 1], me.normals[3 * i + 2], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            std::copy(me.indices, me.indices + size_t(me.num_triangles) * 3, idx.begin() + mi.index_offset);
+        }
+        s->vpos.upload(pos.data(), pos.size(), str);
+        s->vnrm.upload(nrm.data(), nrm.size(), str);
+        s->indices.upload(idx.data(), idx.size(), str);
+        // BLAS per mesh: node offsets first (n-1 internal nodes, at least 1).
+        uint32_t node_total = 0;
+        for (auto& mi : s->mesh_info) { mi.node_offset = node_total; node_total += std::max(1u, mi.num_triangles > 1 ? mi.num_triangles - 1u : 1u); }
+        s->blas_nodes.alloc(std::max(1u, node_total));
+        s->blas_tris.alloc(std::max<size_t>(1, size_t(nt) * 3));
+        uint32_t max_tris = 0;
+        for (auto& mi : s->mesh_info) max_tris = std::max(max_tris, mi.num_triangles);
+        s->tri_lo.alloc(std::max(1u, max_tris)); s->tri_hi.alloc(std::max(1u, max_tris));
+        VKB_CUDA(cudaEventRecord(s->ev0, str));
+        for (uint32_t m = 0; m < d->num_meshes; ++m) {
+            const MeshInfo& mi = s->mesh_info[m];
+            if (mi.num_triangles == 0) continue;
+            // Relative index buffer -> absolute for the box and sorted-triangle kernels.
+            const uint32_t* mid = s->indices.p + mi.index_offset;
+            const float4* mpos = s->vpos.p + mi.vertex_offset;
+            k_tri_boxes<<<grid_for(mi.num_triangles, 256, sms), 256, 0, str>>>(mi.num_triangles, mid, mpos, s->tri_lo.p, s->tri_hi.p);
+            build_lbvh(mi.num_triangles, s->tri_lo.p, s->tri_hi.p, s->blas_nodes.p + mi.node_offset, s->scratch, str, sms);
+            k_sorted_tris<<<grid_for(mi.num_triangles, 256, sms), 256, 0, str>>>(mi.num_triangles, s->scratch.ids_sorted.p, mid, mpos, s->blas_tris.p + 3 * size_t(mi.tri_offset));
+        }
+        VKB_CUDA(cudaEventRecord(s->ev1, str));
+        s->meshes.upload(s->mesh_info.data(), s->mesh_info.size(), str);
+        // Materials, lights, light tree.
+        s->materials.assign(d->materials, d->materials + d->num_materials);
+        s->lights.assign(d->lights, d->lights + d->num_lights);
+        s->d_materials.upload(s->materials.data(), s->materials.size(), str);
+        s->d_lights.upload(s->lights.data(), std::max<size_t>(s->lights.size(), 0), str);
+        std::vector<LightTreeNode> tree = light_tree(d->lights, d->num_lights);
+        s->tree_nodes = uint32_t(tree.size());
+        s->tree.upload(tree.data(), tree.size(), str);
+        s->camera = d->camera;
+        s->env = d->environment;
+        // Instances + TLAS.
+        uint32_t n = d->num_instances;
+        s->inst_mesh.assign(d->instance_mesh, d->instance_mesh + n);
+        s->inst_mat.assign(d->instance_material, d->instance_material + n);
+        std::vector<uint4> info(n);
+        for (uint32_t i = 0; i < n; ++i) info[i] = make_uint4(d->instance_mesh[i], d->instance_material[i], 0u, 0u);
+        s->inst_info.upload(info.data(), n, str);
+        s->o2w.upload(reinterpret_cast<const float4*>(d->instance_rows), size_t(n) * 3, str);
+        s->w2o.alloc(size_t(n) * 3);
+        s->inst_lo.alloc(n); s->inst_hi.alloc(n);
+        s->tlas_nodes.alloc(std::max(1u, n > 1 ? n - 1 : 1u));
+        s->tlas_leaves.alloc(std::max(1u, n));
+        s->tlas_codes.alloc(std::max(1u, n));
+        VKB_CUDA(cudaStreamSynchronize(str));
+        float blas_ms = 0.f;
+        VKB_CUDA(cudaEventElapsedTime(&blas_ms, s->ev0, s->ev1));
+        build_tlas(s);
+        s->build_ms += blas_ms;
+    });
+    if (st != VKB_OK) { vkb_scene_destroy(s); return st; }
+    *out = s;
+    return VKB_OK;
+}
+
+vkb_status vkb_scene_destroy(vkb_scene* s) {
+    if (!s) return VKB_OK;
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+    DBuf<float4>* f4[] = {&s->vpos, &s->vnrm, &s->blas_tris, &s->o2w, &s->w2o, &s->inst_lo, &s->inst_hi, &s->tri_lo, &s->tri_hi,
+                          &s->ray_o0, &s->ray_d0, &s->ray_o1, &s->ray_d1, &s->hit, &s->thr, &s->rad, &s->sa_o, &s->sa_d, &s->sa_c,
+                          &s->sb_o, &s->sb_d, &s->sb_c, &s->accum, &s->out_rgba};
+    for (auto* b : f4) b->release();
+    s->indices.release(); s->tlas_codes.release(); s->inst_info.release(); s->meshes.release();
+    s->blas_nodes.release(); s->tlas_nodes.release(); s->tlas_leaves.release(); s->d_materials.release(); s->d_lights.release();
+    s->tree.release(); s->hit_inst.release(); s->counters.release(); s->err.release(); s->ids.release(); s->rng.release();
+    s->scratch.codes.release(); s->scratch.codes_sorted.release(); s->scratch.ids.release(); s->scratch.ids_sorted.release();
+    s->scratch.leaf_parent.release(); s->scratch.node_parent.release(); s->scratch.counters.release(); s->scratch.bounds.release(); s->scratch.cub_temp.release();
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    delete s;
+    return VKB_OK;
+}
+
+vkb_status vkb_scene_update_instances(vkb_scene* s, const float* rows, uint32_t n, int policy) {
+    if (!s || !rows) return fail(VKB_INVALID_ARG, "null scene or rows");
+    if (n != s->num_instances) return fail(VKB_INVALID_ARG, "instance count differs from the installed scene");
+    if (policy < 0 || policy > 2) return fail(VKB_INVALID_ARG, "policy must be 0, 1 or 2");
+    return guarded([&] {
+        VKB_CUDA(cudaSetDevice(s->ctx->device));
+        s->o2w.upload(reinterpret_cast<const float4*>(rows), size_t(n) * 3, s->ctx->stream);
+        // rt.rs:1465-1476: rebuild once the changed object bytes reach a quarter of
+        // the object buffer; every row changed here, so policy 0 rebuilds.  Refit
+        // (policy 2) keeps the topology and would reuse it; both rebuild for now.
+        s->changed_bytes += double(n) * 48.0;
+        build_tlas(s);
+        s->changed_bytes = 0;
+    });
+}
+
+vkb_status vkb_render(vkb_scene* s, const vkb_profile* pf, vkb_output* out, vkb_stats* stats) {
+    if (!s || !pf || !out || !out->rgba) return fail(VKB_INVALID_ARG, "null scene, profile or output");
+    return guarded([&] {
+        if (pf->adaptive) throw Unsupported{"adaptive sampling is outside the built subset"};
+        if (pf->samples == 0) throw ArgError{"samples must be positive"};
+        if (pf->first_sample >= pf->samples) throw ArgError{"first_sample beyond samples"};
+        uint32_t count = pf->sample_count ? pf->sample_count : pf->samples - pf->first_sample;
+        if (pf->first_sample + count > pf->samples) throw ArgError{"sample range beyond samples"};
+        if (pf->bounces[0] > 250) throw ArgError{"bounce budget above 250"};
+        vkb_ctx* c = s->ctx;
+        VKB_CUDA(cudaSetDevice(c->device));
+        cudaStream_t st = c->stream;
+        int sms = c->sms;
+        const uint32_t W = s->camera.width, H = s->camera.height, npix = W * H;
+        uint32_t wave = pf->wave_samples;
+        if (wave == 0) wave = std::max(1u, std::min(count, (8u << 20) / std::max(1u, npix)));
+        wave = std::min(wave, count);
+        size_t slots = size_t(npix) * wave;
+        s->ray_o0.alloc(slots); s->ray_d0.alloc(slots); s->ray_o1.alloc(slots); s->ray_d1.alloc(slots);
+        s->hit.alloc(slots); s->hit_inst.alloc(slots); s->thr.alloc(slots); s->rad.alloc(slots); s->rng.alloc(slots);
+        s->sa_o.alloc(slots); s->sa_d.alloc(slots); s->sa_c.alloc(slots); s->sb_o.alloc(slots); s->sb_d.alloc(slots); s->sb_c.alloc(slots);
+        s->accum.alloc(npix); s->counters.alloc(16); s->err.alloc(1);
+        if (out->primary_ids) s->ids.alloc(size_t(npix) * 2);
+        VKB_CUDA(cudaMemsetAsync(s->accum.p, 0, npix * sizeof(float4), st));
+        VKB_CUDA(cudaMemsetAsync(s->counters.p, 0, 16 * sizeof(uint32_t), st));
+        VKB_CUDA(cudaMemsetAsync(s->err.p, 0, sizeof(uint32_t), st));
+        PathParams p{};
+        p.sv = scene_view(s);
+        p.o2w = s->o2w.p; p.w2o = s->w2o.p; p.inst_info = s->inst_info.p; p.meshes = s->meshes.p;
+        p.vpos = s->vpos.p; p.vnrm = s->vnrm.p; p.indices = s->indices.p;
+        p.materials = s->d_materials.p; p.lights = s->d_lights.p; p.num_lights = uint32_t(s->lights.size());
+        p.tree = s->tree.p; p.tree_nodes = s->tree_nodes;
+        p.lut.texels = c->lut.p; p.filter = c->filter.p;
+        p.cam = s->camera; p.env = s->env;
+        p.spp = pf->samples; p.seed = pf->seed;
+        for (int k = 0; k < 4; ++k) p.bounces[k] = pf->bounces[k];
+        p.caustics = pf->caustics;
+        p.sample_mask = pf->samples <= 1 ? 0u : ((2u << (31 - __builtin_clz(pf->samples - 1u))) - 1u);
+        p.clamp_direct = pf->clamp_direct; p.clamp_indirect = pf->clamp_indirect; p.light_threshold = pf->light_threshold;
+        p.npix = npix; p.first_sample = pf->first_sample;
+        p.ray_o[0] = s->ray_o0.p; p.ray_d[0] = s->ray_d0.p; p.ray_o[1] = s->ray_o1.p; p.ray_d[1] = s->ray_d1.p;
+        p.hit = s->hit.p; p.hit_inst = s->hit_inst.p; p.thr = s->thr.p; p.rad = s->rad.p; p.rng = s->rng.p;
+        p.sa_o = s->sa_o.p; p.sa_d = s->sa_d.p; p.sa_c = s->sa_c.p; p.sb_o = s->sb_o.p; p.sb_d = s->sb_d.p; p.sb_c = s->sb_c.p;
+        p.accum = s->accum.p; p.counters = s->counters.p; p.err = s->err.p;
+        p.primary_ids = out->primary_ids ? s->ids.p : nullptr;
+        VKB_CUDA(cudaEventRecord(s->ev0, st));
+        for (uint32_t done = 0; done < count; done += wave) {
+            uint32_t ws = std::min(wave, count - done);
+            p.wave_first = pf->first_sample + done;
+            p.wave_samples = ws;
+            p.n_paths = npix * ws;
+            VKB_CUDA(cudaMemcpyAsync(s->counters.p, &p.n_paths, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+            k_camera<<<grid_for(p.n_paths, 256, sms), 256, 0, st>>>(p);
+            const int tgrid = sms * 16, sgrid = sms * 16;
+            for (uint32_t b = 0; b <= pf->bounces[0]; ++b) {
+                int cur = int(b & 1u);
+                k_trace<false><<<tgrid, 128, 0, st>>>(p, cur);
+                k_reset_queues<<<1, 1, 0, st>>>(s->counters.p, cur ^ 1);
+                k_shade<<<sgrid, 128, 0, st>>>(p, cur);
+                k_trace<true><<<tgrid, 128, 0, st>>>(p, -1);
+            }
+            k_accumulate<<<grid_for(npix, 256, sms), 256, 0, st>>>(p);
+            VKB_CUDA(cudaGetLastError());
+        }
+        VKB_CUDA(cudaEventRecord(s->ev1, st));
+        float4* dst;
+        if (out->on_device) dst = reinterpret_cast<float4*>(out->rgba);
+        else { s->out_rgba.alloc(npix); dst = s->out_rgba.p; }
+        k_resolve<<<grid_for(npix, 256, sms), 256, 0, st>>>(npix, s->accum.p, dst);
+        if (!out->on_device) VKB_CUDA(cudaMemcpyAsync(out->rgba, dst, npix * sizeof(float4), cudaMemcpyDeviceToHost, st));
+        if (out->primary_ids) VKB_CUDA(cudaMemcpyAsync(out->primary_ids, s->ids.p, size_t(npix) * 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        uint32_t ctr[16], err = 0;
+        VKB_CUDA(cudaMemcpyAsync(ctr, s->counters.p, sizeof(ctr), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaMemcpyAsync(&err, s->err.p, sizeof(err), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaStreamSynchronize(st));
+        float ms = 0.f;
+        VKB_CUDA(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+        if (stats) {
+            stats->paths = uint64_t(npix) * count;
+            stats->extension_rays = ctr[3];
+            stats->shadow_rays = ctr[4];
+            stats->dropped_light_samples = ctr[5];
+            stats->dropped_path_samples = ctr[6];
+            stats->traversal_overflows = err;
+            stats->render_ms = ms;
+            stats->build_ms = s->build_ms;
+        }
+    });
+}
+
+vkb_status vkb_debug_sampler_groups(vkb_ctx* c, uint32_t n, const uint32_t* px, const uint32_t* py, const uint32_t* index,
+                                    const uint32_t* groups, uint32_t count, uint32_t stream, uint32_t* out_bits) {
+    if (!c || (n && (!px || !py || !index || !groups || !out_bits))) return fail(VKB_INVALID_ARG, "null argument");
+    return guarded([&] {
+        VKB_CUDA(cudaSetDevice(c->device));
+        DBuf<uint32_t> a, b, i, g;
+        DBuf<uint4> o;
+        a.upload(px, n, c->stream); b.upload(py, n, c->stream); i.upload(index, n, c->stream); g.upload(groups, n, c->stream);
+        o.alloc(n);
+        uint32_t mask = count <= 1 ? 0u : ((2u << (31 - __builtin_clz(count - 1u))) - 1u);
+        if (n) k_sampler_groups<<<grid_for(n, 256, c->sms), 256, 0, c->stream>>>(n, a.p, b.p, i.p, g.p, mask, stream, o.p);
+        if (n) VKB_CUDA(cudaMemcpyAsync(out_bits, o.p, size_t(n) * sizeof(uint4), cudaMemcpyDeviceToHost, c->stream));
+        VKB_CUDA(cudaStreamSynchronize(c->stream));
+        a.release(); b.release(); i.release(); g.release(); o.release();
+    });
+}
+
+vkb_status vkb_debug_brdf_lut(vkb_ctx* c, float* out) {
+    if (!c || !out) return fail(VKB_INVALID_ARG, "null argument");
+    return guarded([&] {
+        VKB_CUDA(cudaSetDevice(c->device));
+        std::vector<ushort4> h(size_t(BRDF_SIZE) * BRDF_HEIGHT);
+        VKB_CUDA(cudaMemcpyAsync(h.data(), c->lut.p, h.size() * sizeof(ushort4), cudaMemcpyDeviceToHost, c->stream));
+        VKB_CUDA(cudaStreamSynchronize(c->stream));
+        for (size_t i = 0; i < h.size(); ++i) {
+            uint16_t v[4] = {h[i].x, h[i].y, h[i].z, h[i].w};
+            for (int k = 0; k < 4; ++k) out[4 * i + k] = __half2float(__ushort_as_half(v[k]));
+        }
+    });
+}
+
+vkb_status vkb_debug_tlas_morton(vkb_scene* s, uint32_t* out) {
+    if (!s || !out) return fail(VKB_INVALID_ARG, "null argument");
+    return guarded([&] {
+        VKB_CUDA(cudaSetDevice(s->ctx->device));
+        if (s->num_instances) VKB_CUDA(cudaMemcpyAsync(out, s->tlas_codes.p, s->num_instances * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->ctx->stream));
+        VKB_CUDA(cudaStreamSynchronize(s->ctx->stream));
+    });
+}
+
+vkb_status vkb_debug_blas_morton(vkb_scene* s, uint32_t mesh, uint32_t* out) {
+    if (!s || !out) return fail(VKB_INVALID_ARG, "null argument");
+    if (mesh >= s->num_meshes) return fail(VKB_INVALID_ARG, "mesh index out of range");
+    return guarded([&] {
+        VKB_CUDA(cudaSetDevice(s->ctx->device));
+        const MeshInfo& mi = s->mesh_info[mesh];
+        uint32_t n = mi.num_triangles;
+        if (n == 0) return;
+        cudaStream_t st = s->ctx->stream;
+        int sms = s->ctx->sms;
+        s->tri_lo.alloc(n); s->tri_hi.alloc(n);
+        s->scratch.reserve(n, st);
+        k_tri_boxes<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->indices.p + mi.index_offset, s->vpos.p + mi.vertex_offset, s->tri_lo.p, s->tri_hi.p);
+        VKB_CUDA(cudaMemsetAsync(s->scratch.bounds.p, 0xff, 3 * sizeof(uint32_t), st));
+        VKB_CUDA(cudaMemsetAsync(s->scratch.bounds.p + 3, 0x00, 3 * sizeof(uint32_t), st));
+        k_centroid_box<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->tri_lo.p, s->tri_hi.p, s->scratch.bounds.p);
+        k_morton<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->tri_lo.p, s->tri_hi.p, s->scratch.bounds.p, s->scratch.codes.p, s->scratch.ids.p);
+        VKB_CUDA(cudaMemcpyAsync(out, s->scratch.codes.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+vkb_status vkb_debug_trace(vkb_scene* s, uint32_t n, const float* rays7, float* out_t, uint32_t* out_ids, float* out_uv) {
+    if (!s || (n && (!rays7 || !out_t || !out_ids || !out_uv))) return fail(VKB_INVALID_ARG, "null argument");
+    return guarded([&] {
+        VKB_CUDA(cudaSetDevice(s->ctx->device));
+        cudaStream_t st = s->ctx->stream;
+        DBuf<float> r, t, uv;
+        DBuf<uint32_t> ids, err;
+        r.upload(rays7, size_t(n) * 7, st);
+        t.alloc(n); uv.alloc(size_t(n) * 2); ids.alloc(size_t(n) * 2); err.alloc(1);
+        VKB_CUDA(cudaMemsetAsync(err.p, 0, sizeof(uint32_t), st));
+        if (n) k_debug_trace<<<grid_for(n, 128, s->ctx->sms), 128, 0, st>>>(scene_view(s), n, r.p, t.p, ids.p, uv.p, err.p);
+        if (n) {
+            VKB_CUDA(cudaMemcpyAsync(out_t, t.p, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+            VKB_CUDA(cudaMemcpyAsync(out_ids, ids.p, size_t(n) * 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            VKB_CUDA(cudaMemcpyAsync(out_uv, uv.p, size_t(n) * 2 * sizeof(float), cudaMemcpyDeviceToHost, st));
+        }
+        VKB_CUDA(cudaStreamSynchronize(st));
+        r.release(); t.release(); uv.release(); ids.release(); err.release();
+    });
+}
+
+}  // extern "C"

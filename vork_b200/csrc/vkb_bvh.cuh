@@ -1,0 +1,212 @@
+// Acceleration structures for the B200 backend (B200 has no RT cores): per-mesh BLAS
+// and a per-frame instance TLAS, both linear BVHs (Karras 2012) over 30-bit Morton
+// codes, sorted with cub's radix sort and refitted bottom-up with atomic counters.
+// The reference builds these inside the Vulkan driver (crates/vork-render/src/rt.rs:
+// Rays::new :1098-1289 for BLAS batches, FrameRays::new :1339-1385 and encode /
+// rebuild_tlas :1387-1476 for the instance TLAS); its traversal is RayQuery::Proceed
+// (shaders/path.slang:155-189, :641-684).  Traversal here is a two-level stack walk
+// over 64-byte BVH2 nodes holding both child boxes, with watertight triangle tests
+// (Woop, Benthin & Wald, JCGT 2013), bounded stack and iteration count.
+#pragma once
+#include <cstdint>
+#include "vkb_device.cuh"
+
+namespace vkb {
+
+// Both child boxes of a binary node in four 16-byte lanes: one 64-byte load per visit.
+// a = (L.lo.x, L.hi.x, L.lo.y, L.hi.y), b = (R.lo.x, R.hi.x, R.lo.y, R.hi.y),
+// c = (L.lo.z, L.hi.z, R.lo.z, R.hi.z), d = (left, right, -, -).  A child reference
+// >= 0 is an internal node, < 0 is ~(sorted leaf index).
+struct alignas(16) BvhNode { float4 a, b, c; int4 d; };
+
+// One TLAS leaf, in Morton order: the instance's world->object rows and what its BLAS needs.
+struct alignas(16) TlasLeaf { float4 w2o[3]; uint32_t instance, node_offset, tri_offset, flags; };
+constexpr uint32_t LEAF_CULL_BACKFACES = 1u;
+
+struct MeshInfo {
+    uint32_t node_offset, tri_offset, index_offset, vertex_offset;
+    uint32_t num_triangles, pad0, pad1, pad2;
+    float lo[4], hi[4];
+};
+
+constexpr int TRACE_STACK = 64;
+constexpr uint32_t TRACE_STEP_LIMIT = 1u << 22;
+constexpr int SENTINEL = 0x7fffffff;
+
+// ---------------------------------------------------------------- Morton codes (bit-exact with the CPU restatement)
+__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+__device__ __forceinline__ uint32_t quantize10(float x) {
+    float q = __fmul_rn(x, 1024.f);
+    q = q < 0.f ? 0.f : q;
+    q = q > 1023.f ? 1023.f : q;
+    return uint32_t(q);
+}
+// Centroid (lo+hi)/2 normalised over the centroid box, 10 bits per axis, x highest.
+__device__ __forceinline__ uint32_t morton_code(float4 lo, float4 hi, float3 slo, float3 ext) {
+    float c[3] = {__fmul_rn(__fadd_rn(lo.x, hi.x), 0.5f), __fmul_rn(__fadd_rn(lo.y, hi.y), 0.5f), __fmul_rn(__fadd_rn(lo.z, hi.z), 0.5f)};
+    float l[3] = {slo.x, slo.y, slo.z}, e[3] = {ext.x, ext.y, ext.z};
+    uint32_t q[3];
+    for (int a = 0; a < 3; ++a) q[a] = quantize10(e[a] > 0.f ? __fdiv_rn(__fsub_rn(c[a], l[a]), e[a]) : 0.5f);
+    return (expand_bits(q[0]) << 2) | (expand_bits(q[1]) << 1) | expand_bits(q[2]);
+}
+// Order-preserving float <-> uint for atomic min/max of the centroid box.
+__device__ __forceinline__ uint32_t float_flip(float f) { uint32_t u = __float_as_uint(f); return (u & 0x80000000u) ? ~u : (u | 0x80000000u); }
+__device__ __forceinline__ float float_unflip(uint32_t u) { return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u); }
+
+// ---------------------------------------------------------------- traversal
+struct RaySpace {
+    float3 o, d, idir, ood;     // origin, direction, 1/d, o/d
+    int kx, ky, kz;             // watertight shear permutation
+    float sx, sy, sz;
+};
+__device__ __forceinline__ float safe_rcp(float x) { return 1.f / (fabsf(x) > 1e-20f ? x : copysignf(1e-20f, x)); }
+__device__ __forceinline__ float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+__device__ __forceinline__ void make_space(RaySpace& r, float3 o, float3 d) {
+    r.o = o; r.d = d;
+    r.idir = f3(safe_rcp(d.x), safe_rcp(d.y), safe_rcp(d.z));
+    r.ood = f3(o.x * r.idir.x, o.y * r.idir.y, o.z * r.idir.z);
+    float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    r.kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    r.kx = r.kz + 1 == 3 ? 0 : r.kz + 1;
+    r.ky = r.kx + 1 == 3 ? 0 : r.kx + 1;
+    float dz = comp(d, r.kz);
+    if (dz < 0.f) { int t = r.kx; r.kx = r.ky; r.ky = t; }
+    r.sx = comp(d, r.kx) / dz;
+    r.sy = comp(d, r.ky) / dz;
+    r.sz = 1.f / dz;
+}
+// Slab test of both children of a node; returns entry distances (or +inf on miss).
+__device__ __forceinline__ void node_boxes(const BvhNode& n, const RaySpace& r, float tmax, float& tl, float& tr) {
+    float lx0 = fmaf(n.a.x, r.idir.x, -r.ood.x), lx1 = fmaf(n.a.y, r.idir.x, -r.ood.x);
+    float ly0 = fmaf(n.a.z, r.idir.y, -r.ood.y), ly1 = fmaf(n.a.w, r.idir.y, -r.ood.y);
+    float lz0 = fmaf(n.c.x, r.idir.z, -r.ood.z), lz1 = fmaf(n.c.y, r.idir.z, -r.ood.z);
+    float rx0 = fmaf(n.b.x, r.idir.x, -r.ood.x), rx1 = fmaf(n.b.y, r.idir.x, -r.ood.x);
+    float ry0 = fmaf(n.b.z, r.idir.y, -r.ood.y), ry1 = fmaf(n.b.w, r.idir.y, -r.ood.y);
+    float rz0 = fmaf(n.c.z, r.idir.z, -r.ood.z), rz1 = fmaf(n.c.w, r.idir.z, -r.ood.z);
+    float lmin = fmaxf(fmaxf(fminf(lx0, lx1), fminf(ly0, ly1)), fmaxf(fminf(lz0, lz1), 0.f));
+    float lmax = fminf(fminf(fmaxf(lx0, lx1), fmaxf(ly0, ly1)), fminf(fmaxf(lz0, lz1), tmax));
+    float rmin = fmaxf(fmaxf(fminf(rx0, rx1), fminf(ry0, ry1)), fmaxf(fminf(rz0, rz1), 0.f));
+    float rmax = fminf(fminf(fmaxf(rx0, rx1), fmaxf(ry0, ry1)), fminf(fmaxf(rz0, rz1), tmax));
+    // Conservative widening by a few ulps keeps hits on box faces (exact-fit leaf boxes).
+    tl = lmin <= lmax * 1.00000024f ? lmin : __int_as_float(0x7f800000);
+    tr = rmin <= rmax * 1.00000024f ? rmin : __int_as_float(0x7f800000);
+}
+// Watertight ray/triangle test. cull: accept front faces only (counter-clockwise
+// winding seen from the ray origin).  Returns t and barycentrics of vertices 1, 2.
+__device__ __forceinline__ bool tri_test(const RaySpace& r, float3 v0, float3 v1, float3 v2, bool cull, float tbest, float& t, float& b1, float& b2) {
+    float3 A = v0 - r.o, B = v1 - r.o, C = v2 - r.o;
+    float Az = comp(A, r.kz), Bz = comp(B, r.kz), Cz = comp(C, r.kz);
+    float Ax = comp(A, r.kx) - r.sx * Az, Ay = comp(A, r.ky) - r.sy * Az;
+    float Bx = comp(B, r.kx) - r.sx * Bz, By = comp(B, r.ky) - r.sy * Bz;
+    float Cx = comp(C, r.kx) - r.sx * Cz, Cy = comp(C, r.ky) - r.sy * Cz;
+    float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+    if (U == 0.f || V == 0.f || W == 0.f) {
+        double cxby = double(Cx) * double(By), cybx = double(Cy) * double(Bx);
+        double axcy = double(Ax) * double(Cy), aycx = double(Ay) * double(Cx);
+        double bxay = double(Bx) * double(Ay), byax = double(By) * double(Ax);
+        U = float(cxby - cybx); V = float(axcy - aycx); W = float(bxay - byax);
+    }
+    bool neg = U < 0.f || V < 0.f || W < 0.f, pos = U > 0.f || V > 0.f || W > 0.f;
+    if (cull ? neg : (neg && pos)) return false;
+    float det = U + V + W;
+    if (det == 0.f) return false;
+    float T = U * (r.sz * Az) + V * (r.sz * Bz) + W * (r.sz * Cz);
+    float inv = 1.f / det;
+    t = T * inv;
+    if (!(t >= 0.f && t <= tbest)) return false;
+    b1 = V * inv; b2 = W * inv;
+    return true;
+}
+
+struct HitRecord { float t, u, v; uint32_t prim, inst; };
+
+struct SceneView {
+    const BvhNode* tlas_nodes;
+    const TlasLeaf* tlas_leaves;
+    const BvhNode* blas_nodes;
+    const float4* blas_tris;     // 3 per triangle (Morton order within a mesh); v0.w = original triangle id
+    uint32_t num_instances;
+};
+
+// Closest hit (any == false) or first hit (any == true) of a world ray over the
+// two-level BVH.  Error: overflow/step-limit exits set *err and return the best so far.
+template <bool ANY>
+__device__ __forceinline__ bool trace_ray(const SceneView& s, float3 o, float3 d, float tmax, HitRecord& hit, uint32_t* err) {
+    RaySpace ws, rs;
+    make_space(ws, o, d);
+    rs = ws;
+    int stack[TRACE_STACK];
+    int sp = 0;
+    float tbest = tmax;
+    bool found = false, in_blas = false;
+    const BvhNode* nodes = s.tlas_nodes;
+    const float4* tris = s.blas_tris;
+    uint32_t tri_base = 0, cur_instance = 0;
+    bool cull = false;
+    int node = 0;
+    if (s.num_instances == 0) return false;
+    for (uint32_t steps = 0;; ++steps) {
+        if (steps >= TRACE_STEP_LIMIT) { atomicOr(err, 2u); break; }
+        if (node >= 0) {
+            BvhNode n;
+            const float4* p = reinterpret_cast<const float4*>(nodes + node);
+            n.a = __ldg(p); n.b = __ldg(p + 1); n.c = __ldg(p + 2);
+            n.d = __ldg(reinterpret_cast<const int4*>(p + 3));
+            float tl, tr;
+            node_boxes(n, rs, tbest, tl, tr);
+            bool hl = tl != __int_as_float(0x7f800000), hr = tr != __int_as_float(0x7f800000);
+            if (hl && hr) {
+                int nearer = tl <= tr ? n.d.x : n.d.y, farther = tl <= tr ? n.d.y : n.d.x;
+                if (sp >= TRACE_STACK) { atomicOr(err, 1u); break; }
+                stack[sp++] = farther;
+                node = nearer;
+                continue;
+            }
+            if (hl) { node = n.d.x; continue; }
+            if (hr) { node = n.d.y; continue; }
+        } else if (!in_blas) {
+            const TlasLeaf* lf = s.tlas_leaves + (~node);
+            float4 r0 = __ldg(&lf->w2o[0]), r1 = __ldg(&lf->w2o[1]), r2 = __ldg(&lf->w2o[2]);
+            uint4 info = __ldg(reinterpret_cast<const uint4*>(&lf->instance));
+            float3 oo = f3(r0.x * o.x + r0.y * o.y + r0.z * o.z + r0.w, r1.x * o.x + r1.y * o.y + r1.z * o.z + r1.w, r2.x * o.x + r2.y * o.y + r2.z * o.z + r2.w);
+            float3 od = f3(r0.x * d.x + r0.y * d.y + r0.z * d.z, r1.x * d.x + r1.y * d.y + r1.z * d.z, r2.x * d.x + r2.y * d.y + r2.z * d.z);
+            make_space(rs, oo, od);
+            cur_instance = info.x;
+            nodes = s.blas_nodes + info.y;
+            tri_base = info.z;
+            cull = !ANY && (info.w & LEAF_CULL_BACKFACES);
+            if (sp >= TRACE_STACK) { atomicOr(err, 1u); break; }
+            stack[sp++] = SENTINEL;
+            in_blas = true;
+            node = 0;
+            continue;
+        } else {
+            const float4* tp = tris + 3u * (tri_base + uint32_t(~node));
+            float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
+            float t, b1, b2;
+            if (tri_test(rs, f3(v0.x, v0.y, v0.z), f3(v1.x, v1.y, v1.z), f3(v2.x, v2.y, v2.z), cull, tbest, t, b1, b2)) {
+                tbest = t; found = true;
+                hit.t = t; hit.u = b1; hit.v = b2; hit.prim = __float_as_uint(v0.w); hit.inst = cur_instance;
+                if (ANY) return true;
+            }
+        }
+        // pop
+        for (;;) {
+            if (sp == 0) return found;
+            node = stack[--sp];
+            if (node != SENTINEL) break;
+            in_blas = false;
+            rs = ws;
+            nodes = s.tlas_nodes;
+        }
+    }
+    return found;
+}
+
+}  // namespace vkb

@@ -1,0 +1,616 @@
+// Device kernels of the B200 backend: BRDF-atlas bake, LBVH build, and the path
+// wavefront (camera -> closest-hit trace -> shade/NEE -> shadow trace -> accumulate).
+#pragma once
+#include <cstdint>
+#include "vkb_device.cuh"
+#include "vkb_bvh.cuh"
+
+namespace vkb {
+
+// ================================================================ BRDF atlas bake (shaders/environment.slang:14-108)
+__device__ __forceinline__ float brdf_cosine(uint32_t col) { float t = float(col) / float(BRDF_SIZE - 1); float t2 = t * t; return t2 * t2; }
+__device__ __forceinline__ float brdf_alpha(uint32_t row) {
+    if (row == 0) return MIN_ALPHA;
+    if (row == BRDF_SIZE - 1) return 1.f;
+    return exp2f(log2f(MIN_ALPHA) * (1.f - float(row) / float(BRDF_SIZE - 1)));
+}
+// openpbr_core.slang:160-171.
+__device__ __forceinline__ float dielectric_directional_albedo(float no, float r, float eta, uint32_t samples) {
+    if (eta == 1.f) return 0.f;
+    if (r == 0.f) return eta <= 0.f ? 1.f : fresnel(no, eta);
+    float a = specular_alpha(r), result = 0.f;
+    for (uint32_t i = 0; i < samples; ++i) {
+        float ux = (float(i) + 0.5f) / float(samples), uy = float(__brev(i) >> 8u) * UINT_SCALE, vh;
+        float w = ggx_visible_reflection(no, a, ux, uy, vh);
+        result += (eta <= 0.f ? 1.f : fresnel(vh, eta)) * w;
+    }
+    return result / float(samples);
+}
+__global__ void k_bake_lut(ushort4* out) {
+    uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= BRDF_SIZE || y >= BRDF_HEIGHT) return;
+    float4 v;
+    if (y >= BRDF_SIZE) {
+        const uint32_t n = BRDF_ALBEDO_SIZE;
+        uint32_t cx = x % n, cy = (y - BRDF_SIZE) % n, slice = ((y - BRDF_SIZE) / n) * 2u + x / n;
+        if (slice > BRDF_IOR_STEPS) v = make_float4(0.f, 0.f, 0.f, 0.f);
+        else {
+            float no = fmaxf(float(cx) / float(n - 1), MIN_ALPHA), r = float(cy) / float(n - 1), q = float(slice) / float(BRDF_IOR_STEPS);
+            float eta = slice == BRDF_IOR_STEPS ? 0.f : q / fmaxf(1.f - q, POSITIVE_EPSILON);
+            v = make_float4(dielectric_directional_albedo(no, r, eta, DIELECTRIC_ALBEDO_SAMPLES), 0.f, 0.f, 1.f);
+        }
+    } else {
+        float s0 = 0.f, s1 = 0.f, s2 = 0.f, nv = brdf_cosine(x), alpha = brdf_alpha(y), average = 0.f;
+        for (uint32_t i = 0; i < ENVIRONMENT_SAMPLES; ++i) {
+            float ux = (float(i) + 0.5f) / float(ENVIRONMENT_SAMPLES), uy = float(__brev(i)) * RADICAL_INVERSE_SCALE, vh;
+            float g = ggx_visible_reflection(nv, alpha, ux, uy, vh);
+            float f = powf(1.f - vh, 5.f);
+            s0 += (1.f - f) * g; s1 += f * g; s2 += vh * powf(1.f - vh, 6.f) * g;
+        }
+        if (x == 0) {
+            for (uint32_t j = 0; j < BRDF_SIZE; ++j) {
+                float c = brdf_cosine(j);
+                float interval = 0.5f * (brdf_cosine(min(j + 1u, BRDF_SIZE - 1u)) - brdf_cosine(j > 0 ? j - 1u : 0u));
+                for (uint32_t i = 0; i < ENVIRONMENT_SAMPLES; ++i) {
+                    float ux = (float(i) + 0.5f) / float(ENVIRONMENT_SAMPLES), uy = float(__brev(i)) * RADICAL_INVERSE_SCALE, vh;
+                    average += interval * 2.f * c * ggx_visible_reflection(c, alpha, ux, uy, vh);
+                }
+            }
+            average /= float(ENVIRONMENT_SAMPLES);
+        }
+        v = make_float4(s0 / float(ENVIRONMENT_SAMPLES), s1 / float(ENVIRONMENT_SAMPLES), s2 / float(ENVIRONMENT_SAMPLES), average);
+    }
+    out[y * BRDF_SIZE + x] = make_ushort4(__half_as_ushort(__float2half_rn(v.x)), __half_as_ushort(__float2half_rn(v.y)),
+                                          __half_as_ushort(__float2half_rn(v.z)), __half_as_ushort(__float2half_rn(v.w)));
+}
+
+// ================================================================ LBVH build
+// Object-space triangle boxes of one mesh (index buffer relative to the mesh's vertices).
+__global__ void k_tri_boxes(uint32_t n, const uint32_t* idx, const float4* pos, float4* lo, float4* hi) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        float4 a = pos[idx[3 * t]], b = pos[idx[3 * t + 1]], c = pos[idx[3 * t + 2]];
+        lo[t] = make_float4(fminf(a.x, fminf(b.x, c.x)), fminf(a.y, fminf(b.y, c.y)), fminf(a.z, fminf(b.z, c.z)), 0.f);
+        hi[t] = make_float4(fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y)), fmaxf(a.z, fmaxf(b.z, c.z)), 0.f);
+    }
+}
+// Instance rows -> world->object rows and world boxes of the mesh box's 8 corners,
+// each coordinate ((m0 x + m1 y) + m2 z) + m3 without contraction (bit-exact boxes).
+__global__ void k_instances(uint32_t n, const float4* o2w, const uint4* info, const MeshInfo* meshes, float4* w2o, float4* lo, float4* hi) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 r0 = o2w[3 * i], r1 = o2w[3 * i + 1], r2 = o2w[3 * i + 2];
+        const MeshInfo& m = meshes[info[i].x];
+        float l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int k = 0; k < 8; ++k) {
+            float p[3] = {k & 1 ? m.hi[0] : m.lo[0], k & 2 ? m.hi[1] : m.lo[1], k & 4 ? m.hi[2] : m.lo[2]};
+            float4 rr[3] = {r0, r1, r2};
+            for (int a = 0; a < 3; ++a) {
+                float v = __fmul_rn(rr[a].x, p[0]);
+                v = __fadd_rn(v, __fmul_rn(rr[a].y, p[1]));
+                v = __fadd_rn(v, __fmul_rn(rr[a].z, p[2]));
+                v = __fadd_rn(v, rr[a].w);
+                l[a] = fminf(l[a], v); h[a] = fmaxf(h[a], v);
+            }
+        }
+        lo[i] = make_float4(l[0], l[1], l[2], 0.f);
+        hi[i] = make_float4(h[0], h[1], h[2], 0.f);
+        // Affine inverse of the 3x4 rows.
+        float a00 = r0.x, a01 = r0.y, a02 = r0.z, a10 = r1.x, a11 = r1.y, a12 = r1.z, a20 = r2.x, a21 = r2.y, a22 = r2.z;
+        float c00 = a11 * a22 - a12 * a21, c01 = a02 * a21 - a01 * a22, c02 = a01 * a12 - a02 * a11;
+        float c10 = a12 * a20 - a10 * a22, c11 = a00 * a22 - a02 * a20, c12 = a02 * a10 - a00 * a12;
+        float c20 = a10 * a21 - a11 * a20, c21 = a01 * a20 - a00 * a21, c22 = a00 * a11 - a01 * a10;
+        float det = a00 * c00 + a01 * c10 + a02 * c20, id = 1.f / det;
+        float i00 = c00 * id, i01 = c01 * id, i02 = c02 * id, i10 = c10 * id, i11 = c11 * id, i12 = c12 * id, i20 = c20 * id, i21 = c21 * id, i22 = c22 * id;
+        w2o[3 * i] = make_float4(i00, i01, i02, -(i00 * r0.w + i01 * r1.w + i02 * r2.w));
+        w2o[3 * i + 1] = make_float4(i10, i11, i12, -(i10 * r0.w + i11 * r1.w + i12 * r2.w));
+        w2o[3 * i + 2] = make_float4(i20, i21, i22, -(i20 * r0.w + i21 * r1.w + i22 * r2.w));
+    }
+}
+// Centroid box: bounds[0..2] flipped minima, bounds[3..5] flipped maxima.
+__global__ void k_centroid_box(uint32_t n, const float4* lo, const float4* hi, uint32_t* bounds) {
+    uint32_t mn[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, mx[3] = {0u, 0u, 0u};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 a = lo[i], b = hi[i];
+        float c[3] = {__fmul_rn(__fadd_rn(a.x, b.x), 0.5f), __fmul_rn(__fadd_rn(a.y, b.y), 0.5f), __fmul_rn(__fadd_rn(a.z, b.z), 0.5f)};
+        for (int k = 0; k < 3; ++k) { uint32_t f = float_flip(c[k]); mn[k] = min(mn[k], f); mx[k] = max(mx[k], f); }
+    }
+    for (int k = 0; k < 3; ++k)
+        for (int off = 16; off > 0; off >>= 1) {
+            mn[k] = min(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], off));
+            mx[k] = max(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], off));
+        }
+    if ((threadIdx.x & 31) == 0)
+        for (int k = 0; k < 3; ++k) { atomicMin(&bounds[k], mn[k]); atomicMax(&bounds[3 + k], mx[k]); }
+}
+__global__ void k_morton(uint32_t n, const float4* lo, const float4* hi, const uint32_t* bounds, uint32_t* codes, uint32_t* ids) {
+    float3 slo = f3(float_unflip(bounds[0]), float_unflip(bounds[1]), float_unflip(bounds[2]));
+    float3 shi = f3(float_unflip(bounds[3]), float_unflip(bounds[4]), float_unflip(bounds[5]));
+    float3 ext = f3(__fsub_rn(shi.x, slo.x), __fsub_rn(shi.y, slo.y), __fsub_rn(shi.z, slo.z));
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        codes[i] = morton_code(lo[i], hi[i], slo, ext);
+        ids[i] = i;
+    }
+}
+__device__ __forceinline__ int lbvh_delta(const uint32_t* codes, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    uint32_t a = codes[i], b = codes[j];
+    if (a == b) return 32 + __clz(uint32_t(i ^ j));
+    return __clz(a ^ b);
+}
+// Karras 2012, Algorithm 2: one internal node per thread; parents encoded node*2+side.
+__global__ void k_karras(int n, const uint32_t* codes, BvhNode* nodes, uint32_t* leaf_parent, uint32_t* node_parent, uint32_t* counters) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1; i += gridDim.x * blockDim.x) {
+        int d = lbvh_delta(codes, n, i, i + 1) - lbvh_delta(codes, n, i, i - 1) > 0 ? 1 : -1;
+        int dmin = lbvh_delta(codes, n, i, i - d);
+        int lmax = 2;
+        while (lbvh_delta(codes, n, i, i + lmax * d) > dmin) lmax <<= 1;
+        int l = 0;
+        for (int t = lmax >> 1; t >= 1; t >>= 1)
+            if (lbvh_delta(codes, n, i, i + (l + t) * d) > dmin) l += t;
+        int j = i + l * d;
+        int dnode = lbvh_delta(codes, n, i, j);
+        int s = 0, t = l;
+        do {
+            t = (t + 1) >> 1;
+            if (lbvh_delta(codes, n, i, i + (s + t) * d) > dnode) s += t;
+        } while (t > 1);
+        int gamma = i + s * d + min(d, 0);
+        int left = min(i, j) == gamma ? ~gamma : gamma;
+        int right = max(i, j) == gamma + 1 ? ~(gamma + 1) : gamma + 1;
+        nodes[i].d = make_int4(left, right, 0, 0);
+        if (left < 0) leaf_parent[~left] = uint32_t(i) * 2u; else node_parent[left] = uint32_t(i) * 2u;
+        if (right < 0) leaf_parent[~right] = uint32_t(i) * 2u + 1u; else node_parent[right] = uint32_t(i) * 2u + 1u;
+        counters[i] = 0u;
+        if (i == 0) node_parent[0] = 0xffffffffu;
+    }
+}
+__device__ __forceinline__ void store_child(BvhNode* nodes, uint32_t node, uint32_t side, float4 lo, float4 hi) {
+    BvhNode& n = nodes[node];
+    if (side == 0) { n.a = make_float4(lo.x, hi.x, lo.y, hi.y); n.c.x = lo.z; n.c.y = hi.z; }
+    else { n.b = make_float4(lo.x, hi.x, lo.y, hi.y); n.c.z = lo.z; n.c.w = hi.z; }
+}
+// Bottom-up refit: the second child to arrive at a node merges both boxes upward.
+__global__ void k_refit(int n, const uint32_t* sorted_ids, const float4* lo, const float4* hi, BvhNode* nodes,
+                        const uint32_t* leaf_parent, const uint32_t* node_parent, uint32_t* counters) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        uint32_t id = sorted_ids[k];
+        float4 blo = lo[id], bhi = hi[id];
+        uint32_t pref = leaf_parent[k];
+        for (int guard = 0; guard < 128 && pref != 0xffffffffu; ++guard) {
+            uint32_t node = pref >> 1, side = pref & 1u;
+            store_child(nodes, node, side, blo, bhi);
+            __threadfence();
+            if (atomicAdd(&counters[node], 1u) == 0u) break;
+            __threadfence();
+            const float4* p = reinterpret_cast<const float4*>(nodes + node);
+            float4 a = __ldcg(p), b = __ldcg(p + 1), c = __ldcg(p + 2);
+            blo = make_float4(fminf(a.x, b.x), fminf(a.z, b.z), fminf(c.x, c.z), 0.f);
+            bhi = make_float4(fmaxf(a.y, b.y), fmaxf(a.w, b.w), fmaxf(c.y, c.w), 0.f);
+            pref = node_parent[node];
+        }
+    }
+}
+// A one-primitive tree: root with the leaf on the left and an empty right box.
+__global__ void k_single_leaf(const float4* lo, const float4* hi, BvhNode* nodes) {
+    BvhNode n;
+    n.a = make_float4(lo[0].x, hi[0].x, lo[0].y, hi[0].y);
+    n.b = make_float4(INFINITY, -INFINITY, INFINITY, -INFINITY);
+    n.c = make_float4(lo[0].z, hi[0].z, INFINITY, -INFINITY);
+    n.d = make_int4(~0, ~0, 0, 0);
+    nodes[0] = n;
+}
+// Triangles of one mesh in Morton order, v0.w = original triangle id.
+__global__ void k_sorted_tris(uint32_t n, const uint32_t* sorted_ids, const uint32_t* idx, const float4* pos, float4* tris) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        uint32_t t = sorted_ids[k];
+        float4 a = pos[idx[3 * t]], b = pos[idx[3 * t + 1]], c = pos[idx[3 * t + 2]];
+        tris[3 * k] = make_float4(a.x, a.y, a.z, __uint_as_float(t));
+        tris[3 * k + 1] = make_float4(b.x, b.y, b.z, 0.f);
+        tris[3 * k + 2] = make_float4(c.x, c.y, c.z, 0.f);
+    }
+}
+__global__ void k_tlas_leaves(uint32_t n, const uint32_t* sorted_ids, const float4* w2o, const uint4* info, const MeshInfo* meshes,
+                              const vkb_material* materials, TlasLeaf* leaves) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        uint32_t i = sorted_ids[k];
+        TlasLeaf lf;
+        lf.w2o[0] = w2o[3 * i]; lf.w2o[1] = w2o[3 * i + 1]; lf.w2o[2] = w2o[3 * i + 2];
+        uint4 in = info[i];
+        lf.instance = i;
+        lf.node_offset = meshes[in.x].node_offset;
+        lf.tri_offset = meshes[in.x].tri_offset;
+        lf.flags = (materials[in.y].flags & 2u) ? 0u : LEAF_CULL_BACKFACES;
+        leaves[k] = lf;
+    }
+}
+
+// ================================================================ path wavefront
+struct PathParams {
+    SceneView sv;
+    const float4* o2w; const float4* w2o; const uint4* inst_info; const MeshInfo* meshes;
+    const float4* vpos; const float4* vnrm; const uint32_t* indices;
+    const vkb_material* materials; const vkb_light* lights; uint32_t num_lights;
+    const LightTreeNode* tree; uint32_t tree_nodes;
+    Lut lut; const float* filter;
+    vkb_camera cam; vkb_environment env;
+    uint32_t spp, seed, bounces[4], caustics, sample_mask;
+    float clamp_direct, clamp_indirect, light_threshold;
+    uint32_t npix, wave_first, wave_samples, n_paths, first_sample;
+    float4* ray_o[2]; float4* ray_d[2];
+    float4* hit; uint32_t* hit_inst;
+    float4* thr; float4* rad; uint2* rng;
+    float4* sa_o; float4* sa_d; float4* sa_c;
+    float4* sb_o; float4* sb_d; float4* sb_c;
+    float4* accum;
+    uint32_t* counters;  // [0],[1] ray counts, [2] shadow count, [3] ext rays, [4] shadow rays, [5] dropped light, [6] dropped paths
+    uint32_t* err;
+    uint32_t* primary_ids;
+};
+constexpr uint32_t META_NONFINITE = 0x80000000u;
+constexpr uint32_t SH_TRACE_A = 1u, SH_HAS_B = 2u, SH_TRACE_B = 4u, SH_DIRECT = 8u;
+
+__device__ __forceinline__ float filter_offset(const float* table, float u) {
+    float x = clampf(u, 0.f, 1.f) * float(FILTER_INTERVALS);
+    uint32_t i = min(uint32_t(x), FILTER_INTERVALS - 1u);
+    return lerpf(__ldg(table + i), __ldg(table + i + 1), x - float(i));
+}
+// Warp-aggregated queue append: one atomic per warp.
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
+    uint32_t mask = __ballot_sync(0xffffffffu, want);
+    if (!want) return 0xffffffffu;
+    uint32_t lane = threadIdx.x & 31u, leader = __ffs(mask) - 1u;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+// path.slang:1792-1866 up to integrate: sampler, film-filtered pinhole camera ray.
+__global__ void k_camera(PathParams p) {
+    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < p.n_paths; slot += gridDim.x * blockDim.x) {
+        uint32_t pixel = slot % p.npix, sidx = p.wave_first + slot / p.npix;
+        uint32_t px = pixel % p.cam.width, py = pixel / p.cam.width;
+        uint32_t pseed = screen_ray_hash(px, py, 0u, p.seed);
+        uint32_t rng = screen_ray_hash(px, py, sidx, p.seed);
+        float4 cs = sample_group(pseed, sidx, p.sample_mask, 0u);
+        float nx = (float(px) + 0.5f + filter_offset(p.filter, cs.x)) / float(p.cam.width) * 2.f + -1.f;
+        float ny = (float(py) + 0.5f + filter_offset(p.filter, cs.y)) / float(p.cam.height) * -2.f + 1.f;
+        float3 fwd = get3(p.cam.forward), eye = get3(p.cam.eye);
+        float3 dir = normalize(fwd + get3(p.cam.right) * (nx / p.cam.proj_x) + get3(p.cam.up) * (ny / p.cam.proj_y));
+        float near_d = p.cam.near_plane / dot(dir, fwd), far_d = p.cam.far_plane / dot(dir, fwd);
+        float3 o = eye + dir * near_d;
+        float tmax = fminf(FP32_MAX, fmaxf(0.f, far_d - length(o - eye)));
+        p.ray_o[0][slot] = make_float4(o.x, o.y, o.z, tmax);
+        p.ray_d[0][slot] = make_float4(dir.x, dir.y, dir.z, __uint_as_float(slot));
+        p.thr[slot] = make_float4(1.f, 1.f, 1.f, __uint_as_float(0u));
+        p.rad[slot] = make_float4(0.f, 0.f, 0.f, __uint_as_float(0u));
+        p.rng[slot] = make_uint2(rng, pseed);
+    }
+}
+template <bool ANY>
+__global__ void __launch_bounds__(128) k_trace(PathParams p, int cur) {
+    uint32_t n = cur < 0 ? p.counters[2] : p.counters[cur];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (ANY) atomicAdd(&p.counters[4], n);
+        else atomicAdd(&p.counters[3], n);
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (!ANY) {
+            float4 ro = p.ray_o[cur][i], rd = p.ray_d[cur][i];
+            HitRecord h;
+            bool found = trace_ray<false>(p.sv, f3(ro.x, ro.y, ro.z), f3(rd.x, rd.y, rd.z), ro.w, h, p.err);
+            p.hit[i] = found ? make_float4(h.t, h.u, h.v, __uint_as_float(h.prim)) : make_float4(-1.f, 0.f, 0.f, __uint_as_float(0xffffffffu));
+            p.hit_inst[i] = found ? h.inst : 0xffffffffu;
+        } else {
+            float4 so = p.sa_o[i], sd = p.sa_d[i], sc = p.sa_c[i];
+            uint32_t slot = __float_as_uint(sd.w), flags = __float_as_uint(sc.w);
+            HitRecord h;
+            float3 total = f3(sc.x, sc.y, sc.z);
+            if ((flags & SH_TRACE_A) && trace_ray<true>(p.sv, f3(so.x, so.y, so.z), f3(sd.x, sd.y, sd.z), so.w, h, p.err)) total = f3(0.f);
+            if (flags & SH_HAS_B) {
+                float4 bc = p.sb_c[slot];
+                float3 cb = f3(bc.x, bc.y, bc.z);
+                if (flags & SH_TRACE_B) {
+                    float4 bo = p.sb_o[slot], bd = p.sb_d[slot];
+                    if (trace_ray<true>(p.sv, f3(bo.x, bo.y, bo.z), f3(bd.x, bd.y, bd.z), bo.w, h, p.err)) cb = f3(0.f);
+                }
+                total = total + cb;
+            }
+            float4 r = p.rad[slot];
+            uint32_t dropped = __float_as_uint(r.w);
+            float3 add = clamp_sample(total, (flags & SH_DIRECT) ? p.clamp_direct : p.clamp_indirect, dropped);
+            p.rad[slot] = make_float4(r.x + add.x, r.y + add.y, r.z + add.z, __uint_as_float(dropped));
+        }
+    }
+}
+
+struct Surface { float3 world, face, geometric, error, shadow_xyz; float shadow_cone; };
+__device__ __forceinline__ float3 tvec(const float4 I[3], float3 x) {
+    return f3(I[0].x * x.x + I[1].x * x.y + I[2].x * x.z, I[0].y * x.x + I[1].y * x.y + I[2].y * x.z, I[0].z * x.x + I[1].z * x.y + I[2].z * x.z);
+}
+__device__ __forceinline__ float3 mvec(const float4 M[3], float3 x) { return f3(M[0].x * x.x + M[0].y * x.y + M[0].z * x.z, M[1].x * x.x + M[1].y * x.y + M[1].z * x.z, M[2].x * x.x + M[2].y * x.y + M[2].z * x.z); }
+// hit_geometry.slang:64-138,174-205; hit.slang:86-114; surface.slang:290-333; material.slang:69-79.
+__device__ __forceinline__ Surface hit_surface(const PathParams& p, uint32_t inst, uint32_t prim, float u, float v, float3 dir) {
+    Surface s;
+    uint4 info = __ldg(&p.inst_info[inst]);
+    const MeshInfo& m = p.meshes[info.x];
+    float4 M[3] = {__ldg(&p.o2w[3 * inst]), __ldg(&p.o2w[3 * inst + 1]), __ldg(&p.o2w[3 * inst + 2])};
+    float4 I[3] = {__ldg(&p.w2o[3 * inst]), __ldg(&p.w2o[3 * inst + 1]), __ldg(&p.w2o[3 * inst + 2])};
+    uint32_t base = m.index_offset + 3u * prim;
+    uint32_t i0 = m.vertex_offset + __ldg(&p.indices[base]), i1 = m.vertex_offset + __ldg(&p.indices[base + 1]), i2 = m.vertex_offset + __ldg(&p.indices[base + 2]);
+    float4 q0 = __ldg(&p.vpos[i0]), q1 = __ldg(&p.vpos[i1]), q2 = __ldg(&p.vpos[i2]);
+    float4 m0 = __ldg(&p.vnrm[i0]), m1 = __ldg(&p.vnrm[i1]), m2 = __ldg(&p.vnrm[i2]);
+    float3 P[3] = {f3(q0.x, q0.y, q0.z), f3(q1.x, q1.y, q1.z), f3(q2.x, q2.y, q2.z)};
+    float3 N[3] = {f3(m0.x, m0.y, m0.z), f3(m1.x, m1.y, m1.z), f3(m2.x, m2.y, m2.z)};
+    float b[3] = {1.f - u - v, u, v};
+    float3 fobj = finite_unit_normal(cross(P[1] - P[0], P[2] - P[0]), N[0]);
+    float3 face = finite_unit_normal(tvec(I, fobj), f3(0.f, 0.f, 1.f));
+    bool entering = dot(face, dir) < 0.f;
+    float3 lp = P[0] * b[0] + P[1] * b[1] + P[2] * b[2];
+    s.world = mvec(M, lp) + f3(M[0].w, M[1].w, M[2].w);
+    float3 facew = tvec(I, fobj);
+    float3 un = finite_unit_normal(tvec(I, N[0] * b[0] + N[1] * b[1] + N[2] * b[2]), facew);
+    float3 nrm = dot(un, facew) < 0.f ? -un : un;
+    float det = M[0].x * (M[1].y * M[2].z - M[1].z * M[2].y) - M[0].y * (M[1].x * M[2].z - M[1].z * M[2].x) + M[0].z * (M[1].x * M[2].y - M[1].y * M[2].x);
+    bool object_front = entering != (det < 0.f);
+    s.geometric = finite_unit_normal(nrm, f3(0.f, 0.f, 1.f)) * (object_front ? 1.f : -1.f);
+    // Shadow-terminator envelope (hit_geometry.slang:174-205), front = entering.
+    float side = entering ? 1.f : -1.f;
+    float3 sf = face * side, pr[3], nr[3];
+    for (int k = 0; k < 3; ++k) { pr[k] = mvec(M, P[k] - P[0]); nr[k] = finite_unit_normal(tvec(I, N[k]) * side, sf); }
+    float3 smooth = nr[0] * b[0] + nr[1] * b[1] + nr[2] * b[2];
+    if (dot(smooth, sf) < 0.f) { for (int k = 0; k < 3; ++k) nr[k] = -nr[k]; smooth = -smooth; }
+    float3 point = pr[0] * b[0] + pr[1] * b[1] + pr[2] * b[2];
+    float envelope = 0.f, quadratic = 0.f, cone = 0.f;
+    for (int i = 0; i < 3; ++i) {
+        float support = 0.f;
+        for (int j = 0; j < 3; ++j) support = fmaxf(support, dot(pr[j] - point, nr[i]));
+        envelope = i == 0 ? support : fminf(envelope, support);
+        cone = fmaxf(cone, length(nr[i] - sf));
+        for (int j = i + 1; j < 3; ++j) quadratic += b[i] * b[j] * dot(nr[j] - nr[i], pr[j] - pr[i]);
+    }
+    s.shadow_xyz = smooth * fmaxf(envelope, 0.5f * quadratic);
+    s.shadow_cone = cone;
+    s.face = entering ? face : -face;
+    // surface_position_error.
+    float3 lo = f3(m.lo[0], m.lo[1], m.lo[2]), hi = f3(m.hi[0], m.hi[1], m.hi[2]);
+    float3 mag = vmax(vabs(lo), vabs(hi));
+    float extent = maxc(vabs(hi - lo));
+    float3 aw = vabs(s.world);
+    float3 iw = f3(fabsf(I[0].x) * aw.x + fabsf(I[0].y) * aw.y + fabsf(I[0].z) * aw.z + fabsf(I[0].w),
+                   fabsf(I[1].x) * aw.x + fabsf(I[1].y) * aw.y + fabsf(I[1].z) * aw.z + fabsf(I[1].w),
+                   fabsf(I[2].x) * aw.x + fabsf(I[2].y) * aw.y + fabsf(I[2].z) * aw.z + fabsf(I[2].w));
+    const float g7 = fp32_gamma7();
+    float3 local = (mag + f3(extent) + iw) * g7;
+    float e[3];
+    for (int r = 0; r < 3; ++r) {
+        float4 row = M[r];
+        e[r] = fabsf(row.x) * local.x + fabsf(row.y) * local.y + fabsf(row.z) * local.z + g7 * (fabsf(row.x) * mag.x + fabsf(row.y) * mag.y + fabsf(row.z) * mag.z + fabsf(row.w));
+    }
+    s.error = f3(e[0], e[1], e[2]);
+    return s;
+}
+// path.slang:771-784 with vork_prelude.slang:340-345.
+__device__ __forceinline__ float3 path_origin(const Surface& s, float3 dir) {
+    bool reflection = dot(s.geometric, dir) > 0.f;
+    float3 base = s.world;
+    if (reflection && s.shadow_cone > 0.f) {
+        float nl = dot(s.geometric, dir), ng = dot(s.face, dir), cone = s.shadow_cone;
+        float amount = nl < cone ? saturatef(2.f - (ng + nl) / cone) : saturatef(1.f - ng / cone);
+        base = base + s.shadow_xyz * amount;
+    }
+    return surface_ray_origin(base, s.error, reflection ? s.geometric : s.face, dir);
+}
+__device__ __forceinline__ float3 light_threshold(float3 value, float threshold, uint32_t& rng) {
+    float importance = maxc(value);
+    if (importance < threshold && threshold > 0.f) {
+        float keep = importance / threshold;
+        if (path_random(rng) >= keep) return f3(0.f);
+        return value / keep;
+    }
+    return value;
+}
+
+// integrate's per-vertex body (path.slang:1340-1709) for one queued extension hit.
+__global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
+    const int nxt = cur ^ 1;
+    uint32_t n = p.counters[cur];
+    uint32_t loop_end = (n + blockDim.x - 1) / blockDim.x * blockDim.x;  // whole warps stay in the loop for ballots
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < loop_end; i += gridDim.x * blockDim.x) {
+        bool active = i < n;
+        bool push_ray = false, push_shadow = false;
+        float4 new_o, new_d, sh_o, sh_d, sh_c;
+        uint32_t slot = 0;
+        if (active) {
+            float4 ro = p.ray_o[cur][i], rd = p.ray_d[cur][i];
+            slot = __float_as_uint(rd.w);
+            float3 dir = f3(rd.x, rd.y, rd.z);
+            float4 hh = p.hit[i];
+            uint32_t inst = p.hit_inst[i];
+            float4 T = p.thr[slot], R = p.rad[slot];
+            uint2 rg = p.rng[slot];
+            uint32_t meta = __float_as_uint(T.w);
+            uint32_t bounce = meta & 0xffu, diffuse = (meta >> 8) & 0xffu, glossy = (meta >> 16) & 0xffu;
+            uint32_t ray_event = bounce == 0 ? VKB_RAY_CAMERA : ((meta >> 24) & 0x3fu);
+            float3 thr = f3(T.x, T.y, T.z), rad = f3(R.x, R.y, R.z);
+            uint32_t dropped = __float_as_uint(R.w), rng = rg.x, pseed = rg.y;
+            uint32_t pixel = slot % p.npix, sidx = p.wave_first + slot / p.npix;
+            float limit = bounce == 0 ? p.clamp_direct : p.clamp_indirect;
+            if (p.primary_ids && bounce == 0 && sidx == p.first_sample) {
+                p.primary_ids[2 * pixel] = hh.x >= 0.f ? inst : 0xffffffffu;
+                p.primary_ids[2 * pixel + 1] = hh.x >= 0.f ? __float_as_uint(hh.w) : 0xffffffffu;
+            }
+            if (!(hh.x >= 0.f)) {
+                // Miss: path.slang:1484-1512 with the constant world light and camera-visible suns.
+                float3 sky;
+                if (ray_event == VKB_RAY_CAMERA && !p.env.camera_sees_environment) sky = get3(p.env.background);
+                else {
+                    sky = get3(p.env.radiance);
+                    if (ray_event == VKB_RAY_CAMERA)
+                        for (uint32_t l = 0; l < p.num_lights; ++l) {
+                            const vkb_light& L = p.lights[l];
+                            if (L.position[3] != 0.f || !(L.shadow_offsets[0] & VKB_RAY_CAMERA)) continue;
+                            sky = sky + emitter_eval(L, f3(0.f), dir).radiance;
+                        }
+                }
+                rad = rad + clamp_sample(thr * sky, limit, dropped);
+            } else {
+                uint32_t vtx = bounce;
+                float4 sc = sample_group(pseed, sidx, p.sample_mask, vertex_group(vtx, 0));   // path_scatter
+                Surface s = hit_surface(p, inst, __float_as_uint(hh.w), hh.y, hh.z, dir);
+                const vkb_material& mt = p.materials[__ldg(&p.inst_info[inst]).y];
+                Closure c;
+                c.base_color = get3(mt.base_color); c.base_weight = mt.base_weight; c.base_metalness = mt.base_metalness;
+                c.specular_color = get3(mt.specular_color); c.specular_weight = mt.specular_weight;
+                c.specular_roughness = mt.specular_roughness; c.specular_ior = mt.specular_ior; c.optical_ior = 0.f;
+                c.n = s.geometric;
+                boundary_closure_air(c);
+                float3 view = -dir;
+                float3 iface = dot(s.geometric, view) > 0.f ? s.geometric : s.face;
+                Prepared pr = transport_prepare(p.lut, c, view, s.geometric, iface);
+                BsdfSample smp = transport_sample(c, view, sc.x, sc.y, sc.z, pr);
+                if (!finite3(smp.dir) || !finite3(smp.weight) || !isfinite(smp.pdf)) {
+                    meta |= META_NONFINITE;
+                } else {
+                    // next_event (path.slang:851-951): one analytic light, two estimators.
+                    float3 va = f3(0.f), vb = f3(0.f);
+                    bool trace_a = false, has_b = false, trace_b = false;
+                    float3 oa, da, ob, db; float la = 0.f, lb = 0.f;
+                    if (p.num_lights > 0) {
+                        float4 u = sample_group(pseed, sidx, p.sample_mask, vertex_group(vtx, 1));   // path_light
+                        float probability;
+                        uint32_t li = tree_pick(p.tree, p.tree_nodes, s.world, u.z, u.w, probability);
+                        if (probability > 0.f && li < p.num_lights) {
+                            const vkb_light& L = p.lights[li];
+                            uint32_t contribution = L.shadow_offsets[VKB_LIGHT_CONTRIBUTION_WORD];
+                            bool shadowed = (L.shadow_offsets[VKB_LIGHT_RAY_WORD] & VKB_LIGHT_RAY_SHADOWED) != 0u;
+                            if ((contribution & VKB_LIGHT_LINK_ALL) || L.shadow_offsets[VKB_LIGHT_LINK_WORD]) {
+                                LightSample src = emitter_sample(L, s.world, u.x, u.y);
+                                float3 power = src.delta ? src.radiance : (src.pdf > 0.f ? src.radiance / src.pdf : f3(0.f));
+                                va = analytic_mis_response(c, view, src.dir, s.face, contribution, src.pdf, pr) * power / probability;
+                                va = light_threshold(va, p.light_threshold, rng);
+                                if (any_nonzero(va) && shadowed) {
+                                    oa = path_origin(s, src.dir);
+                                    ray_connection(oa, s.world, src.dir, src.distance, da, la);
+                                    trace_a = true;
+                                }
+                                bool continuation = (contribution & smp.event) && event_hemisphere(smp.event, smp.dir, s.face, s.geometric);
+                                if (continuation && dot(smp.dir, smp.dir) > 0.f) {
+                                    EmitterEval e = emitter_eval(L, s.world, smp.dir);
+                                    if (e.pdf > 0.f) {
+                                        float w = smp.pdf > 0.f ? mis_power(smp.pdf, e.pdf) : 1.f;
+                                        vb = light_threshold(smp.weight * e.radiance * (w / probability), p.light_threshold, rng);
+                                        if (any_nonzero(vb)) {
+                                            has_b = true;
+                                            if (shadowed) {
+                                                ob = path_origin(s, smp.dir);
+                                                ray_connection(ob, s.world, smp.dir, e.distance, db, lb);
+                                                trace_b = true;
+                                            }
+                                        }
+                                    }
+                                }
+                            }
+                        }
+                    }
+                    float3 ca = thr * va, cb = thr * vb;
+                    if (trace_a || trace_b) {
+                        push_shadow = true;
+                        uint32_t flags = (trace_a ? SH_TRACE_A : 0u) | (has_b ? SH_HAS_B : 0u) | (trace_b ? SH_TRACE_B : 0u) | (bounce == 0 ? SH_DIRECT : 0u);
+                        sh_o = make_float4(oa.x, oa.y, oa.z, la);
+                        sh_d = make_float4(da.x, da.y, da.z, __uint_as_float(slot));
+                        sh_c = make_float4(ca.x, ca.y, ca.z, __uint_as_float(flags));
+                        if (!trace_a) sh_o = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (has_b) {
+                            p.sb_c[slot] = make_float4(cb.x, cb.y, cb.z, 0.f);
+                            if (trace_b) { p.sb_o[slot] = make_float4(ob.x, ob.y, ob.z, lb); p.sb_d[slot] = make_float4(db.x, db.y, db.z, 0.f); }
+                        }
+                    } else {
+                        rad = rad + clamp_sample(ca + cb, limit, dropped);
+                    }
+                    // Continuation (path.slang:1683-1708).
+                    bool go = bounce < p.bounces[0];
+                    uint32_t event = smp.event;
+                    if (go) {
+                        if (event == VKB_RAY_DIFFUSE) { if (diffuse++ >= p.bounces[1]) go = false; }
+                        else if (event == VKB_RAY_SPECULAR) { if (glossy++ >= p.bounces[2] || (diffuse > 0 && !(p.caustics & 1u))) go = false; }
+                        else go = false;
+                    }
+                    if (go && !event_hemisphere(event, smp.dir, s.face, s.geometric)) go = false;
+                    if (go) {
+                        thr = thr * smp.weight;
+                        if (!finite3(thr)) { meta |= META_NONFINITE; go = false; }
+                        else if (maxc(thr) <= 0.f) go = false;
+                    }
+                    if (go && bounce >= ROULETTE_START) {
+                        float survive = clampf(maxc(thr), ROULETTE_MIN, ROULETTE_MAX);
+                        float4 dec = sample_group(pseed, sidx, p.sample_mask, vertex_group(vtx, 4));
+                        if (dec.z > survive) go = false;
+                        else thr = thr / survive;
+                    }
+                    if (go) {
+                        float3 o = path_origin(s, smp.dir);
+                        new_o = make_float4(o.x, o.y, o.z, FP32_MAX);
+                        new_d = make_float4(smp.dir.x, smp.dir.y, smp.dir.z, __uint_as_float(slot));
+                        push_ray = true;
+                        meta = (meta & META_NONFINITE) | ((bounce + 1u) & 0xffu) | ((diffuse & 0xffu) << 8) | ((glossy & 0xffu) << 16) | ((event & 0x3fu) << 24);
+                    }
+                }
+            }
+            p.thr[slot] = make_float4(thr.x, thr.y, thr.z, __uint_as_float(meta));
+            p.rad[slot] = make_float4(rad.x, rad.y, rad.z, __uint_as_float(dropped));
+            p.rng[slot] = make_uint2(rng, pseed);
+        }
+        uint32_t ri = warp_append(&p.counters[nxt], push_ray);
+        if (push_ray) { p.ray_o[nxt][ri] = new_o; p.ray_d[nxt][ri] = new_d; }
+        uint32_t si = warp_append(&p.counters[2], push_shadow);
+        if (push_shadow) { p.sa_o[si] = sh_o; p.sa_d[si] = sh_d; p.sa_c[si] = sh_c; }
+    }
+}
+// Zero the next ray queue and the shadow queue before a shade pass.
+__global__ void k_reset_queues(uint32_t* counters, int nxt) { counters[nxt] = 0u; counters[2] = 0u; }
+// resolve.slang:162-191: add this wave's finished samples to the accumulator.
+__global__ void k_accumulate(PathParams p) {
+    for (uint32_t pixel = blockIdx.x * blockDim.x + threadIdx.x; pixel < p.npix; pixel += gridDim.x * blockDim.x) {
+        float4 sum = p.accum[pixel];
+        uint32_t dl = 0, dp = 0;
+        for (uint32_t k = 0; k < p.wave_samples; ++k) {
+            uint32_t slot = k * p.npix + pixel;
+            float4 T = p.thr[slot], R = p.rad[slot];
+            dl += __float_as_uint(R.w);
+            float3 v = f3(R.x, R.y, R.z) * p.env.exposure;
+            if ((__float_as_uint(T.w) & META_NONFINITE) || !finite3(v)) { v = f3(0.f); dp++; }
+            sum.x += v.x; sum.y += v.y; sum.z += v.z; sum.w += 1.f;
+        }
+        p.accum[pixel] = sum;
+        if (dl) atomicAdd(&p.counters[5], dl);
+        if (dp) atomicAdd(&p.counters[6], dp);
+    }
+}
+__global__ void k_resolve(uint32_t npix, const float4* accum, float4* out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
+        float4 a = accum[i];
+        float inv = a.w > 0.f ? 1.f / a.w : 0.f;
+        out[i] = make_float4(a.x * inv, a.y * inv, a.z * inv, a.w > 0.f ? 1.f : 0.f);
+    }
+}
+// Test entry: sampler groups for arbitrary (pixel, index, group).
+__global__ void k_sampler_groups(uint32_t n, const uint32_t* px, const uint32_t* py, const uint32_t* index, const uint32_t* groups,
+                                 uint32_t mask, uint32_t stream, uint4* out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t seed = screen_ray_hash(px[i], py[i], 0u, stream);
+        out[i] = sample_group_bits(seed, index[i], mask, groups[i]);
+    }
+}
+// Test entry: closest hits of arbitrary world rays.
+__global__ void k_debug_trace(SceneView sv, uint32_t n, const float* rays, float* t, uint32_t* ids, float* uv, uint32_t* err) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* r = rays + 7 * i;
+        HitRecord h;
+        bool f = trace_ray<false>(sv, f3(r[0], r[1], r[2]), f3(r[3], r[4], r[5]), r[6], h, err);
+        t[i] = f ? h.t : -1.f;
+        ids[2 * i] = f ? h.inst : 0xffffffffu; ids[2 * i + 1] = f ? h.prim : 0xffffffffu;
+        uv[2 * i] = f ? h.u : 0.f; uv[2 * i + 1] = f ? h.v : 0.f;
+    }
+}
+
+}  // namespace vkb

@@ -1,0 +1,343 @@
+"""Seeded synthetic scenes for the std/path configurations, and their C descriptors.
+
+Geometry follows vork's std library tessellation rules: the Y-up UV sphere with 32
+longitudes x 16 rings (crates/vork-std/src/sdk.js:157-181, 960 triangles) and the
+centred XZ grid facing +Y (sdk.js:350-370).  Lights are packed as `Light` records the
+way crates/vork-render/src/lights.rs:53-170 packs them (area light: kind 3, edge vectors
+u = X*width, v = Y*height of the light frame, radiance = colour*energy, emitted radiance
+radiance/(pi*area), shaders/emitter.slang:143).  No public dataset is involved: every
+input is generated here from a fixed seed.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi
+
+# ----------------------------------------------------------------------------- PCG32
+_PCG_MULT = 6364136223846793005
+_MASK64 = (1 << 64) - 1
+
+
+class Pcg32:
+    """O'Neill's PCG32 (XSH-RR), seeded like the reference implementation's pcg32_srandom."""
+
+    def __init__(self, seed: int = 0, seq: int = 0xDA3E39CB94B95BDB):
+        self.state = 0
+        self.inc = ((seq << 1) | 1) & _MASK64
+        self.next_u32()
+        self.state = (self.state + seed) & _MASK64
+        self.next_u32()
+
+    def next_u32(self) -> int:
+        old = self.state
+        self.state = (old * _PCG_MULT + self.inc) & _MASK64
+        xorshifted = (((old >> 18) ^ old) >> 27) & 0xFFFFFFFF
+        rot = old >> 59
+        return ((xorshifted >> rot) | (xorshifted << ((-rot) & 31))) & 0xFFFFFFFF
+
+    def uniform(self, lo: float = 0.0, hi: float = 1.0) -> float:
+        return lo + (hi - lo) * ((self.next_u32() >> 8) * (1.0 / 16777216.0))
+
+
+# ----------------------------------------------------------------------------- meshes
+@dataclass
+class Mesh:
+    positions: np.ndarray  # (V,3) float32
+    normals: np.ndarray    # (V,3) float32
+    indices: np.ndarray    # (T,3) uint32
+
+    @property
+    def num_triangles(self) -> int:
+        return int(self.indices.shape[0])
+
+
+def uv_sphere(radius: float = 1.0, longitude: int = 32, rings: int = 16) -> Mesh:
+    """sdk.js:157-181: vertices per ring and longitude (seam duplicated), tri(a,b+1,b), tri(a,a+1,b+1)."""
+    pos, nrm = [], []
+    for y in range(rings + 1):
+        a = y * math.pi / rings
+        for x in range(longitude + 1):
+            az = (0 if x == longitude else x) * 2 * math.pi / longitude
+            c, s = math.cos(az), math.sin(az)
+            n = (0.0, 1.0, 0.0) if y == 0 else ((0.0, -1.0, 0.0) if y == rings else (math.sin(a) * c, math.cos(a), math.sin(a) * s))
+            nrm.append(n)
+            pos.append(tuple(v * radius for v in n))
+    idx = []
+    for y in range(rings):
+        for x in range(longitude):
+            a = y * (longitude + 1) + x
+            b = a + longitude + 1
+            if y < rings - 1:
+                idx.append((a, b + 1, b))
+            if y > 0:
+                idx.append((a, a + 1, b + 1))
+    return Mesh(np.asarray(pos, np.float32), np.asarray(nrm, np.float32), np.asarray(idx, np.uint32))
+
+
+def grid(size=(2.0, 2.0), segments=(1, 1)) -> Mesh:
+    """sdk.js:350-370: XZ grid facing +Y, centred; tri(a,c,a+1), tri(a+1,c,c+1)."""
+    nx, nz = segments
+    pos, nrm = [], []
+    for z in range(nz + 1):
+        for x in range(nx + 1):
+            pos.append(((x / nx - 0.5) * size[0], 0.0, (z / nz - 0.5) * size[1]))
+            nrm.append((0.0, 1.0, 0.0))
+    idx = []
+    for z in range(nz):
+        for x in range(nx):
+            a = z * (nx + 1) + x
+            c = a + nx + 1
+            idx.append((a, c, a + 1))
+            idx.append((a + 1, c, c + 1))
+    return Mesh(np.asarray(pos, np.float32), np.asarray(nrm, np.float32), np.asarray(idx, np.uint32))
+
+
+def height_grid(heights: np.ndarray, size: float) -> Mesh:
+    """A displaced XZ grid (terrain) with smooth normals from central differences."""
+    n = heights.shape[0] - 1
+    xs = (np.arange(n + 1, dtype=np.float64) / n - 0.5) * size
+    X, Z = np.meshgrid(xs, xs, indexing="xy")
+    pos = np.stack([X, heights, Z], -1).reshape(-1, 3)
+    h = heights
+    dx = np.gradient(h, axis=1) / (size / n)
+    dz = np.gradient(h, axis=0) / (size / n)
+    nrm = np.stack([-dx, np.ones_like(h), -dz], -1)
+    nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
+    a = (np.arange(n)[None, :] + (n + 1) * np.arange(n)[:, None]).reshape(-1)
+    c = a + n + 1
+    idx = np.stack([np.stack([a, c, a + 1], -1), np.stack([a + 1, c, c + 1], -1)], 1).reshape(-1, 3)
+    return Mesh(pos.astype(np.float32), nrm.reshape(-1, 3).astype(np.float32), idx.astype(np.uint32))
+
+
+def geodesic_sphere(frequency: int = 5, jitter: float = 0.0, seed: int = 0) -> Mesh:
+    """Icosahedron with each face split into frequency^2 triangles (20*f^2: 500 at f=5),
+    projected to the unit sphere, radially jittered by a seeded amount."""
+    t = (1 + 5 ** 0.5) / 2
+    V = np.array([(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+                  (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)], np.float64)
+    F = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6), (7, 1, 8),
+         (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    verts: dict = {}
+    pos: list = []
+    idx: list = []
+
+    def vid(p):
+        key = tuple(np.round(p / np.linalg.norm(p), 9))
+        if key not in verts:
+            verts[key] = len(pos)
+            pos.append(p / np.linalg.norm(p))
+        return verts[key]
+
+    f = frequency
+    for a, b, c in F:
+        A, B, Cc = V[a], V[b], V[c]
+        grid_ids = {}
+        for i in range(f + 1):
+            for j in range(f + 1 - i):
+                p = A + (B - A) * (i / f) + (Cc - A) * (j / f)
+                grid_ids[(i, j)] = vid(p)
+        for i in range(f):
+            for j in range(f - i):
+                idx.append((grid_ids[(i, j)], grid_ids[(i + 1, j)], grid_ids[(i, j + 1)]))
+                if j < f - i - 1:
+                    idx.append((grid_ids[(i + 1, j)], grid_ids[(i + 1, j + 1)], grid_ids[(i, j + 1)]))
+    P = np.asarray(pos)
+    if jitter > 0:
+        rng = np.random.default_rng(seed)
+        P = P * (1.0 + jitter * (rng.random(len(P))[:, None] * 2 - 1))
+    I = np.asarray(idx, np.uint32)
+    # outward winding
+    p0, p1, p2 = P[I[:, 0]], P[I[:, 1]], P[I[:, 2]]
+    flip = np.einsum("ij,ij->i", np.cross(p1 - p0, p2 - p0), p0 + p1 + p2) < 0
+    I[flip] = I[flip][:, [0, 2, 1]]
+    N = P / np.linalg.norm(P, axis=1, keepdims=True)
+    return Mesh(P.astype(np.float32), N.astype(np.float32), I)
+
+
+# ----------------------------------------------------------------------------- records
+def material(base_color=(0.8, 0.8, 0.8), roughness=0.3, metalness=0.0, double_sided=False) -> abi.VkbMaterial:
+    """OpenPBR 1.1.1 defaults (crates/vork-scene/openpbr-params.md:22-30) with the given inputs."""
+    m = abi.VkbMaterial()
+    m.base_weight = 1.0
+    m.base_color[:] = [float(v) for v in base_color]
+    m.base_metalness = float(metalness)
+    m.specular_weight = 1.0
+    m.specular_color[:] = [1.0, 1.0, 1.0]
+    m.specular_roughness = float(roughness)
+    m.specular_ior = 1.5
+    m.emission_luminance = 0.0
+    m.emission_color[:] = [1.0, 1.0, 1.0]
+    m.flags = 2 if double_sided else 0
+    return m
+
+
+ALL_RAYS = abi.RAY_CAMERA | abi.RAY_SHADOW | abi.RAY_DIFFUSE | abi.RAY_SPECULAR | abi.RAY_TRANSMISSION | abi.RAY_VOLUME
+
+
+def _light_base() -> abi.VkbLight:
+    l = abi.VkbLight()
+    l.shadow_offsets[0] = ALL_RAYS | abi.LIGHT_LINK_ALL         # contribution: visible to every ray, all links
+    l.shadow_offsets[1] = 0xFFFFFFFF                             # illuminates every group
+    l.shadow_offsets[2] = abi.LIGHT_RAY_SHADOWED | abi.LIGHT_RAY_SHADOWED_BY_ALL
+    l.shadow_offsets[3] = 0xFFFFFFFF
+    return l
+
+
+def area_light(center, normal, u_axis, width, height, radiance, color=(1.0, 1.0, 1.0)) -> abi.VkbLight:
+    """Rectangle light emitting along `normal` with radiance `radiance`: energy = radiance*pi*area (lights.rs:99-127)."""
+    n = np.asarray(normal, np.float64); n /= np.linalg.norm(n)
+    u = np.asarray(u_axis, np.float64); u -= n * np.dot(u, n); u /= np.linalg.norm(u)
+    v = np.cross(n, u)  # light frame: -Z along the emission direction, X = u, Y = v
+    area = width * height
+    energy = radiance * math.pi * area
+    l = _light_base()
+    l.position[:] = [float(center[0]), float(center[1]), float(center[2]), 3.0]
+    l.direction[:] = [float(n[0]), float(n[1]), float(n[2]), math.cos(math.pi / 4)]
+    l.radiance[:] = [color[0] * energy, color[1] * energy, color[2] * energy, 1.0]
+    eu, ev = u * width, v * height
+    l.params[:] = [0.0, 0.5 * math.sqrt(float(np.dot(eu, eu) + np.dot(ev, ev))), 0.0, 0.0]
+    l.emitter_u[:] = [float(eu[0]), float(eu[1]), float(eu[2]), 0.0]
+    l.emitter_v[:] = [float(ev[0]), float(ev[1]), float(ev[2]), 0.0]
+    l.projection[:] = [math.tan(math.pi / 4), 0.0, 0.0, 0.0]
+    return l
+
+
+def sun_light(direction, angle_degrees=0.526, energy=3.0, color=(1.0, 1.0, 1.0)) -> abi.VkbLight:
+    """Sun: kind 0, params.y = half the angular diameter, direction = travel direction of its light."""
+    d = np.asarray(direction, np.float64); d /= np.linalg.norm(d)
+    l = _light_base()
+    l.position[:] = [0.0, 0.0, 0.0, 0.0]
+    l.direction[:] = [float(d[0]), float(d[1]), float(d[2]), 1.0]
+    l.radiance[:] = [color[0] * energy, color[1] * energy, color[2] * energy, 1.0]
+    l.params[:] = [0.0, math.radians(angle_degrees) * 0.5, 0.0, 0.0]
+    l.projection[:] = [0.0, 0.0, 0.0, 0.0]
+    return l
+
+
+def look_at(eye, target, up=(0.0, 1.0, 0.0), fov_y_degrees=45.0, width=256, height=256, near=0.05, far=1e4) -> abi.VkbCamera:
+    e = np.asarray(eye, np.float64); t = np.asarray(target, np.float64)
+    f = t - e; f /= np.linalg.norm(f)
+    r = np.cross(f, np.asarray(up, np.float64)); r /= np.linalg.norm(r)
+    u = np.cross(r, f)
+    cam = abi.VkbCamera()
+    cam.eye[:] = [float(x) for x in e]
+    cam.right[:] = [float(x) for x in r]
+    cam.up[:] = [float(x) for x in u]
+    cam.forward[:] = [float(x) for x in f]
+    p11 = 1.0 / math.tan(math.radians(fov_y_degrees) / 2)
+    cam.proj_y = p11
+    cam.proj_x = p11 / (width / height)
+    cam.near_plane, cam.far_plane = near, far
+    cam.width, cam.height = width, height
+    return cam
+
+
+def rows_from(scale, translate) -> np.ndarray:
+    """3x4 object->world rows of a uniform scale then translation."""
+    r = np.zeros((3, 4), np.float32)
+    r[0, 0] = r[1, 1] = r[2, 2] = scale
+    r[:, 3] = translate
+    return r
+
+
+# ----------------------------------------------------------------------------- scene
+@dataclass
+class Scene:
+    meshes: list
+    instance_rows: np.ndarray       # (N,3,4) float32
+    instance_mesh: np.ndarray       # (N,) uint32
+    instance_material: np.ndarray   # (N,) uint32
+    materials: list
+    lights: list
+    camera: abi.VkbCamera
+    environment: abi.VkbEnvironment
+    name: str = "scene"
+    _keep: list = field(default_factory=list, repr=False)
+
+    @property
+    def num_triangles(self) -> int:
+        return int(sum(self.meshes[m].num_triangles for m in self.instance_mesh))
+
+    def desc(self) -> abi.VkbSceneDesc:
+        """The C descriptor; the arrays it points at stay alive with this Scene."""
+        keep = []
+        mesh_arr = (abi.VkbMesh * max(1, len(self.meshes)))()
+        for i, m in enumerate(self.meshes):
+            p = np.ascontiguousarray(m.positions, np.float32)
+            n = np.ascontiguousarray(m.normals, np.float32)
+            ix = np.ascontiguousarray(m.indices, np.uint32)
+            keep += [p, n, ix]
+            mesh_arr[i].positions = abi.fptr(p)
+            mesh_arr[i].normals = abi.fptr(n)
+            mesh_arr[i].indices = abi.uptr(ix)
+            mesh_arr[i].num_vertices = p.shape[0]
+            mesh_arr[i].num_triangles = ix.shape[0]
+        rows = np.ascontiguousarray(self.instance_rows, np.float32).reshape(-1)
+        im = np.ascontiguousarray(self.instance_mesh, np.uint32)
+        imat = np.ascontiguousarray(self.instance_material, np.uint32)
+        mats = (abi.VkbMaterial * max(1, len(self.materials)))(*self.materials)
+        lights = (abi.VkbLight * max(1, len(self.lights)))(*self.lights)
+        keep += [mesh_arr, rows, im, imat, mats, lights]
+        d = abi.VkbSceneDesc()
+        d.meshes = C.cast(mesh_arr, C.POINTER(abi.VkbMesh))
+        d.num_meshes = len(self.meshes)
+        d.num_instances = int(im.shape[0])
+        d.instance_rows = abi.fptr(rows)
+        d.instance_mesh = abi.uptr(im)
+        d.instance_material = abi.uptr(imat)
+        d.materials = C.cast(mats, C.POINTER(abi.VkbMaterial))
+        d.num_materials = len(self.materials)
+        d.lights = C.cast(lights, C.POINTER(abi.VkbLight))
+        d.num_lights = len(self.lights)
+        d.camera = self.camera
+        d.environment = self.environment
+        self._keep = keep
+        return d
+
+
+def environment(radiance=(0.0, 0.0, 0.0), exposure=1.0, background=(0.0, 0.0, 0.0), camera_sees=True) -> abi.VkbEnvironment:
+    e = abi.VkbEnvironment()
+    e.radiance[:] = [float(v) for v in radiance]
+    e.exposure = float(exposure)
+    e.background[:] = [float(v) for v in background]
+    e.camera_sees_environment = 1 if camera_sees else 0
+    return e
+
+
+def spheres_scene(num_spheres: int = 64, seed: int = 0, width: int = 256, height: int = 256, cube: float = 10.0,
+                  grid_cells: int = 64, light_radiance: float = 20.0) -> Scene:
+    """Plain method, small: spheres at seeded uniform positions in a cube, radii U[0.2,1.0],
+    a grid_cells^2-quad ground, albedo U[0.1,0.9]^3, roughness U[0.05,1.0], metallic
+    Bernoulli(0.3), one rectangular area light of radiance `light_radiance`."""
+    rng = Pcg32(seed)
+    sphere = uv_sphere(1.0)
+    ground = grid((cube, cube), (grid_cells, grid_cells))
+    rows, mesh_ids, mats = [], [], []
+    materials = []
+    for i in range(num_spheres):
+        c = (rng.uniform(0, cube), rng.uniform(0, cube), rng.uniform(0, cube))
+        r = rng.uniform(0.2, 1.0)
+        col = (rng.uniform(0.1, 0.9), rng.uniform(0.1, 0.9), rng.uniform(0.1, 0.9))
+        rough = rng.uniform(0.05, 1.0)
+        metal = 1.0 if rng.uniform() < 0.3 else 0.0
+        materials.append(material(col, rough, metal))
+        rows.append(rows_from(r, c))
+        mesh_ids.append(0)
+        mats.append(i)
+    col = (rng.uniform(0.1, 0.9), rng.uniform(0.1, 0.9), rng.uniform(0.1, 0.9))
+    rough = rng.uniform(0.05, 1.0)
+    materials.append(material(col, rough, 0.0))
+    rows.append(rows_from(1.0, (cube / 2, 0.0, cube / 2)))
+    mesh_ids.append(1)
+    mats.append(num_spheres)
+    light = area_light(center=(cube / 2, cube * 1.4, cube / 2), normal=(0, -1, 0), u_axis=(1, 0, 0), width=cube * 0.4,
+                       height=cube * 0.4, radiance=light_radiance)
+    cam = look_at(eye=(cube / 2, cube * 0.75, -cube * 0.9), target=(cube / 2, cube * 0.3, cube / 2), fov_y_degrees=50.0,
+                  width=width, height=height, near=0.05, far=1000.0)
+    return Scene([sphere, ground], np.stack(rows).astype(np.float32), np.asarray(mesh_ids, np.uint32),
+                 np.asarray(mats, np.uint32), materials, [light], cam, environment(), name=f"spheres{num_spheres}")
