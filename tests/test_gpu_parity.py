@@ -1,0 +1,174 @@
+"""CUDA path against the oracle and the reference's known answers, through the C ABI."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from vork_b200 import Profile, abi, scene as S
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+pytestmark = pytest.mark.gpu
+
+
+def test_sampler_bits_match_golden_and_oracle(renderer, oracle):
+    g = np.load(GOLDEN / "sampler_harness.npz")
+    for name, slot in [("camera", None), ("scatter", 0), ("light", 1), ("mesh", 2), ("environment", 3), ("decisions", 4)]:
+        groups = np.zeros_like(g["px"]) if slot is None else 1 + g["vertex"] * 5 + slot
+        bits = renderer.sampler_groups(g["px"], g["py"], g["index"], groups, 300, 0x5EED)
+        assert np.array_equal(bits, g[name]), name
+    rng = np.random.default_rng(7)
+    n = 1 << 16
+    px, py = rng.integers(0, 1 << 20, n), rng.integers(0, 1 << 20, n)
+    for count in (1, 16, 64, 1000, 1 << 20):
+        idx, grp = rng.integers(0, count, n), rng.integers(0, 5000, n)
+        a = renderer.sampler_groups(px, py, idx, grp, count, 12345)
+        b = oracle.sampler_bits(px, py, idx, grp, count, 12345, 1)
+        assert np.array_equal(a, b), count
+
+
+def test_brdf_atlas_matches_known_texels_and_oracle(renderer, oracle):
+    lut = renderer.brdf_lut()
+    k = json.loads((GOLDEN / "reference_kats.json").read_text())
+    for x, y, e in k["brdf_texels"]:
+        assert abs(lut[y, x, 0] - e) < k["brdf_tolerance"], (x, y, lut[y, x], e)
+    ref = oracle.brdf_lut(False)
+    # fp16 storage: agree to a couple of half ulps (2^-10 relative) plus an absolute floor.
+    assert np.all(np.abs(lut - ref) <= 2e-3 * np.abs(ref) + 2e-4), float(np.abs(lut - ref).max())
+
+
+def test_morton_codes_bit_exact(renderer, oracle, c0_scene):
+    o = oracle.OracleScene(c0_scene)
+    with renderer.install(c0_scene) as s:
+        assert np.array_equal(s.tlas_morton(), o.tlas_morton())
+        for m in range(len(c0_scene.meshes)):
+            assert np.array_equal(s.blas_morton(m), o.blas_morton(m)), m
+
+
+def test_primary_ids_match_oracle(renderer, oracle, c0_scene):
+    o = oracle.OracleScene(c0_scene)
+    prof = Profile.reference_transport(4, 16)
+    rays = o.camera_rays(prof.c(), index=0)
+    t_ref, ids_ref, _ = o.trace(rays, fp64=True)
+    with renderer.install(c0_scene) as s:
+        t, ids, _ = s.trace(rays)
+        mismatch = np.any(ids != ids_ref, axis=1)
+        assert mismatch.mean() <= 1e-4, int(mismatch.sum())
+        hit = ids_ref[:, 0] != 0xFFFFFFFF
+        assert np.allclose(t[hit & ~mismatch], t_ref[hit & ~mismatch], rtol=1e-4, atol=1e-5)
+        # The render's own first-sample IDs (camera rays built on the device).
+        res = s.render(Profile.reference_transport(4, 16, sample_count=1), ids=True)
+        pid = res.primary_ids.reshape(-1, 2)
+        assert np.mean(np.any(pid != ids_ref, axis=1)) <= 1e-3
+        assert res.stats["traversal_overflows"] == 0
+
+
+def test_random_rays_closest_and_any_hits(renderer, oracle, c0_scene):
+    o = oracle.OracleScene(c0_scene)
+    rng = np.random.default_rng(11)
+    n = 20000
+    org = rng.uniform(-2, 12, (n, 3))
+    d = rng.normal(size=(n, 3)); d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.concatenate([org, d, np.full((n, 1), 1e30)], 1).astype(np.float32)
+    t_ref, ids_ref, _ = o.trace(rays, fp64=True)
+    with renderer.install(c0_scene) as s:
+        t, ids, _ = s.trace(rays)
+    mismatch = np.any(ids != ids_ref, axis=1)
+    assert mismatch.mean() <= 2e-3, int(mismatch.sum())
+
+
+def _c0_profile(spp=16, **kw):
+    return Profile.reference_transport(4, spp, **kw)
+
+
+def test_render_matches_fp64_oracle(renderer, oracle, c0_scene):
+    # Same sampler bits per sample: per-pixel agreement on most pixels, and the image
+    # mean within 1% (BASELINE tolerance) of the FP64 restatement.
+    o = oracle.OracleScene(c0_scene)
+    prof = _c0_profile(16)
+    x0, y0, w, h = 96, 96, 64, 64
+    ref, st_ref = o.render(prof.c(), x0, y0, w, h, fp64=True)
+    with renderer.install(c0_scene) as s:
+        res = s.render(prof)
+    img = res.image[y0:y0 + h, x0:x0 + w]
+    assert np.isfinite(res.image).all() and res.stats["dropped_path_samples"] == 0
+    m_gpu, m_ref = img[..., :3].mean((0, 1)), ref[..., :3].mean((0, 1))
+    assert np.all(np.abs(m_gpu / m_ref - 1) < 0.01), (m_gpu, m_ref)
+    rel = np.abs(img[..., :3] - ref[..., :3]).sum(-1) / (ref[..., :3].sum(-1) + 1e-3)
+    assert np.mean(rel < 1e-3) > 0.8, float(np.mean(rel < 1e-3))
+    assert res.stats["traversal_overflows"] == 0
+
+
+def test_full_image_matches_fp32_oracle_at_low_spp(renderer, oracle, c0_scene):
+    o = oracle.OracleScene(c0_scene)
+    prof = _c0_profile(16, sample_count=2)
+    ref, _ = o.render(prof.c(), fp64=False)
+    with renderer.install(c0_scene) as s:
+        img = s.render(prof).image
+    m_gpu, m_ref = img[..., :3].mean((0, 1)), ref[..., :3].mean((0, 1))
+    assert np.all(np.abs(m_gpu / m_ref - 1) < 0.01), (m_gpu, m_ref)
+    rel = np.abs(img[..., :3] - ref[..., :3]).sum(-1) / (ref[..., :3].sum(-1) + 1e-3)
+    assert np.mean(rel < 1e-3) > 0.8
+
+
+def test_white_diffuse_under_coloured_environment(renderer):
+    # environment_tests.rs:117-160: a white Lambert surface under a constant
+    # environment of (1, 0.75, 0.5) returns it, within 3% (here exactly).
+    g = S.grid((200.0, 200.0), (2, 2))
+    m = S.material((1, 1, 1), 0.5, 0.0)
+    m.specular_weight = 0.0
+    rows = S.rows_from(1.0, (0, 0, 0))[None]
+    cam = S.look_at((0, 5, 0.001), (0, 0, 0), width=32, height=32, fov_y_degrees=30)
+    sc = S.Scene([g], rows, np.zeros(1, np.uint32), np.zeros(1, np.uint32), [m], [], cam,
+                 S.environment((1.0, 0.75, 0.5)))
+    with renderer.install(sc) as s:
+        img = s.render(Profile.reference_transport(64, 16)).image
+    mean = img[..., :3].reshape(-1, 3).mean(0)
+    assert np.allclose(mean, [1.0, 0.75, 0.5], rtol=1e-5), mean
+
+
+def test_deterministic_across_waves_and_runs(renderer, c0_scene):
+    with renderer.install(c0_scene) as s:
+        a = s.render(_c0_profile(8)).image
+        b = s.render(_c0_profile(8)).image
+        c = s.render(_c0_profile(8, wave_samples=1)).image
+        d = s.render(_c0_profile(8, wave_samples=3)).image
+        assert np.array_equal(a, b) and np.array_equal(a, c) and np.array_equal(a, d)
+        # Resume: samples [0,4) + [4,8) equal [0,8).
+        h0 = s.render(_c0_profile(8, first_sample=0, sample_count=4)).image
+        h1 = s.render(_c0_profile(8, first_sample=4, sample_count=4)).image
+        assert np.allclose((h0 + h1) / 2, a, rtol=1e-5, atol=1e-6)
+
+
+def test_update_instances_equals_fresh_install(renderer, c0_scene):
+    moved = S.spheres_scene()
+    moved.instance_rows = c0_scene.instance_rows.copy()
+    moved.instance_rows[:64, 1, 3] += 0.5
+    with renderer.install(c0_scene) as s:
+        s.update_instances(moved.instance_rows)
+        a = s.render(_c0_profile(4)).image
+    with renderer.install(moved) as s2:
+        b = s2.render(_c0_profile(4)).image
+    assert np.array_equal(a, b)
+
+
+def test_tiny_scenes_and_errors(renderer):
+    tri = S.Mesh(np.array([[0, 0, 0], [1, 0, 0], [0, 0, -1]], np.float32), np.array([[0, 1, 0]] * 3, np.float32),
+                 np.array([[0, 1, 2]], np.uint32))
+    cam = S.look_at((0.3, 2, -0.3), (0.3, 0, -0.3), width=16, height=16, fov_y_degrees=20)
+    light = S.area_light((0.3, 3, -0.3), (0, -1, 0), (1, 0, 0), 1, 1, 10.0)
+    sc = S.Scene([tri], S.rows_from(1.0, (0, 0, 0))[None], np.zeros(1, np.uint32), np.zeros(1, np.uint32), [S.material()],
+                 [light], cam, S.environment())
+    with renderer.install(sc) as s:
+        img = s.render(Profile.reference_transport(4, 4)).image
+        assert np.isfinite(img).all() and img[..., :3].max() > 0
+        with pytest.raises(abi.VkbError) as e:
+            s.render(Profile(samples=4, adaptive=True))
+        assert e.value.status == abi.VKB_UNSUPPORTED
+        with pytest.raises(abi.VkbError):
+            s.render(Profile(samples=4, first_sample=9))
+    bad = S.Scene([tri], S.rows_from(1.0, (0, 0, 0))[None], np.array([3], np.uint32), np.zeros(1, np.uint32), [S.material()],
+                  [], cam, S.environment())
+    with pytest.raises(abi.VkbError) as e:
+        renderer.install(bad)
+    assert e.value.status == abi.VKB_INVALID_ARG

@@ -30,7 +30,7 @@ struct MeshInfo {
 };
 
 constexpr int TRACE_STACK = 64;
-constexpr uint32_t TRACE_STEP_LIMIT = 1u << 22;
+constexpr uint32_t TRACE_STEP_LIMIT = 1u << 16;
 constexpr int SENTINEL = 0x7fffffff;
 
 // ---------------------------------------------------------------- Morton codes (bit-exact with the CPU restatement)

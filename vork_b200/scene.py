@@ -222,7 +222,10 @@ def sun_light(direction, angle_degrees=0.526, energy=3.0, color=(1.0, 1.0, 1.0))
 def look_at(eye, target, up=(0.0, 1.0, 0.0), fov_y_degrees=45.0, width=256, height=256, near=0.05, far=1e4) -> abi.VkbCamera:
     e = np.asarray(eye, np.float64); t = np.asarray(target, np.float64)
     f = t - e; f /= np.linalg.norm(f)
-    r = np.cross(f, np.asarray(up, np.float64)); r /= np.linalg.norm(r)
+    r = np.cross(f, np.asarray(up, np.float64))
+    if np.linalg.norm(r) < 1e-6:  # looking along `up`: take any perpendicular
+        r = np.cross(f, (0.0, 0.0, 1.0) if abs(f[2]) < 0.9 else (1.0, 0.0, 0.0))
+    r /= np.linalg.norm(r)
     u = np.cross(r, f)
     cam = abi.VkbCamera()
     cam.eye[:] = [float(x) for x in e]
