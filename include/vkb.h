@@ -140,7 +140,12 @@ typedef struct vkb_profile {
     float light_threshold;     /* adaptive.z: stochastic light-sample kill */
     uint32_t adaptive;         /* must be 0: adaptive stopping is outside the built subset */
     uint32_t wave_samples;     /* samples per wavefront wave (0 = automatic) */
+    uint32_t flags;            /* VKB_PROFILE_* measurement switches (0 for production renders) */
 } vkb_profile;
+
+/* Measurement switches of vkb_profile.flags (no reference counterpart: timing hooks). */
+#define VKB_PROFILE_TIME_KERNELS 1u        /* CUDA events around every closest-hit trace launch */
+#define VKB_PROFILE_COUNT_TRAVERSAL 2u     /* instrumented traversal: node and triangle visits */
 
 /* Render output: linear RGBA32F mean image (resolve.slang:162-191). */
 typedef struct vkb_output {
@@ -158,6 +163,14 @@ typedef struct vkb_stats {
     uint64_t traversal_overflows;   /* bounded-stack or iteration-cap exits (error, never a trap) */
     float render_ms;           /* device time of the wavefront, CUDA events */
     float build_ms;            /* device time of the last acceleration-structure build */
+    float trace_ms;            /* VKB_PROFILE_TIME_KERNELS: summed closest-hit trace kernel time */
+    uint32_t trace_launches;   /* closest-hit trace launches in this render */
+    uint32_t kernel_launches;  /* every kernel this library launched for this render */
+    uint64_t nodes_visited;    /* VKB_PROFILE_COUNT_TRAVERSAL: closest-hit BVH node visits */
+    uint64_t triangles_tested; /* closest-hit triangle tests */
+    uint64_t instances_entered;/* closest-hit TLAS leaf (instance) entries */
+    uint64_t shadow_nodes_visited;
+    uint64_t shadow_triangles_tested;
 } vkb_stats;
 
 typedef struct vkb_ctx vkb_ctx;
@@ -181,11 +194,19 @@ vkb_status vkb_scene_destroy(vkb_scene* scene);
  * instance (host pointer, num_instances*12 floats). policy 0: refit-vs-rebuild by the
  * reference's quarter-of-the-bytes rule, 1: always rebuild, 2: always refit. */
 vkb_status vkb_scene_update_instances(vkb_scene* scene, const float* rows, uint32_t num_instances, int policy);
+/* The same with rows already in device memory of the context's GPU (no host copy). */
+vkb_status vkb_scene_update_instances_device(vkb_scene* scene, const float* device_rows, uint32_t num_instances, int policy);
 
 /* passes::path::record + resolve (passes/path.rs:539-724; resolve.slang:162-191): renders
  * samples [first_sample, first_sample+sample_count) of `profile` and writes the mean
  * over them. stats may be NULL. */
 vkb_status vkb_render(vkb_scene* scene, const vkb_profile* profile, vkb_output* out, vkb_stats* stats);
+
+/* The CUDA stream (cudaStream_t) every kernel of this context is launched on, so a
+ * caller can record its own events on it. */
+void* vkb_ctx_stream(vkb_ctx* ctx);
+/* Kernel launches issued so far for this scene (renders and acceleration-structure builds). */
+uint64_t vkb_scene_launch_count(vkb_scene* scene);
 
 /* --- Test and measurement entry points (no reference counterpart beyond the cited tests) --- */
 

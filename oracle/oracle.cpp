@@ -1084,25 +1084,28 @@ template <class R> Hit trace(const Scene<R>& s, V3<R> o, V3<R> d, R tmax, bool a
     R best = tmax;
     V3<R> inv(R(1) / d.x, R(1) / d.y, R(1) / d.z);
     if (s.tlas.nodes.empty()) return h;
-    std::vector<uint32_t> st; st.reserve(64); st.push_back(0);
-    while (!st.empty()) {
-        const BvhNode<R>& nd = s.tlas.nodes[st.back()]; st.pop_back();
+    uint32_t st[256];
+    int sp = 0;
+    st[sp++] = 0;
+    while (sp > 0) {
+        const BvhNode<R>& nd = s.tlas.nodes[st[--sp]];
         if (!box_hit(nd.box, o, inv, best)) continue;
-        if (nd.count == 0) { st.push_back(nd.left); st.push_back(nd.right); continue; }
+        if (nd.count == 0) { if (sp + 2 <= 256) { st[sp++] = nd.left; st[sp++] = nd.right; } continue; }
         for (uint32_t k = nd.first; k < nd.first + nd.count; ++k) {
             uint32_t inst = s.tlas.prims[k];
             const MeshData<R>& m = s.meshes[s.inst_mesh[inst]];
+            if (m.bvh.nodes.empty()) continue;
+            // Facing is decided in object space (hardware facing of the instance's own winding).
             bool cull = !any && !(s.mats[s.inst_mat[inst]].flags & 2u);
-            if (s.model[inst].det() < 0) cull = cull;  // facing is defined in object space (see header note)
             V3<R> oo = s.inv[inst].point(o), od = s.inv[inst].vec(d);
             V3<R> oinv(R(1) / od.x, R(1) / od.y, R(1) / od.z);
-            std::vector<uint32_t> bs; bs.reserve(64);
-            if (m.bvh.nodes.empty()) continue;
-            bs.push_back(0);
-            while (!bs.empty()) {
-                const BvhNode<R>& bn = m.bvh.nodes[bs.back()]; bs.pop_back();
+            uint32_t bs[256];
+            int bp = 0;
+            bs[bp++] = 0;
+            while (bp > 0) {
+                const BvhNode<R>& bn = m.bvh.nodes[bs[--bp]];
                 if (!box_hit(bn.box, oo, oinv, best)) continue;
-                if (bn.count == 0) { bs.push_back(bn.left); bs.push_back(bn.right); continue; }
+                if (bn.count == 0) { if (bp + 2 <= 256) { bs[bp++] = bn.left; bs[bp++] = bn.right; } continue; }
                 for (uint32_t q = bn.first; q < bn.first + bn.count; ++q) {
                     uint32_t tri = m.bvh.prims[q];
                     R t, u, v;
@@ -1543,10 +1546,11 @@ void oracle_bsdf(const vkb_material* m, const double* view, const double* u3, do
     *out_pdf = s.pdf; *out_event = s.event;
 }
 
-void* oracle_scene_create(const vkb_scene_desc* d) {
+// precisions: bit 0 builds the FP32 restatement, bit 1 the FP64 one.
+void* oracle_scene_create(const vkb_scene_desc* d, int precisions) {
     OracleScene* o = new OracleScene();
-    o->s32 = make_scene<float>(d);
-    o->s64 = make_scene<double>(d);
+    if (precisions & 1) o->s32 = make_scene<float>(d);
+    if (precisions & 2) o->s64 = make_scene<double>(d);
     return o;
 }
 void oracle_scene_destroy(void* h) {

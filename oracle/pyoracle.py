@@ -45,7 +45,7 @@ def lib():
         l.oracle_emitter_sample.argtypes = [P, f64p, f64p, f64p, f64p, f64p, f64p]
         l.oracle_emitter_eval.argtypes = [P, f64p, f64p, f64p, f64p, f64p]
         l.oracle_bsdf.argtypes = [P, f64p, f64p, f64p, f64p, f64p, u32p]
-        l.oracle_scene_create.argtypes = [P]
+        l.oracle_scene_create.argtypes = [P, C.c_int]
         l.oracle_scene_create.restype = P
         l.oracle_scene_destroy.argtypes = [P]
         l.oracle_trace.argtypes = [P, C.c_int, C.c_uint32, f32p, C.c_int, f32p, u32p, f32p]
@@ -124,10 +124,10 @@ def bsdf_sample(material, view, u3):
 class OracleScene:
     """The oracle's copy of a scene (FP32 and FP64 restatements)."""
 
-    def __init__(self, scene):
+    def __init__(self, scene, fp32=True, fp64=True):
         self.scene = scene
         self.desc = scene.desc()
-        self.h = lib().oracle_scene_create(C.byref(self.desc))
+        self.h = lib().oracle_scene_create(C.byref(self.desc), (1 if fp32 else 0) | (2 if fp64 else 0))
 
     def close(self):
         if self.h:

@@ -38,6 +38,7 @@ class Profile:
     first_sample: int = 0
     sample_count: int = 0
     wave_samples: int = 0
+    flags: int = 0
 
     @classmethod
     def reference_transport(cls, depth: int, samples: int, seed: int = 0, **kw) -> "Profile":
@@ -52,6 +53,7 @@ class Profile:
         p.clamp_direct, p.clamp_indirect, p.light_threshold = self.clamp_direct, self.clamp_indirect, self.light_threshold
         p.adaptive = 1 if self.adaptive else 0
         p.wave_samples = self.wave_samples
+        p.flags = self.flags
         return p
 
 
@@ -85,6 +87,11 @@ class Renderer:
         abi.check(self.lib.vkb_debug_sampler_groups(self.h, px.size, abi.uptr(px), abi.uptr(py), abi.uptr(index), abi.uptr(groups),
                                                     count, stream, abi.uptr(out)))
         return out
+
+    @property
+    def stream(self) -> int:
+        """The cudaStream_t (as an integer) this device's kernels run on."""
+        return int(self.lib.vkb_ctx_stream(self.h) or 0)
 
     def brdf_lut(self):
         out = np.zeros((2240, 128, 4), np.float32)
@@ -124,6 +131,13 @@ class InstalledScene:
     def update_instances(self, rows: np.ndarray, policy: int = 0):
         rows = np.ascontiguousarray(rows, np.float32).reshape(-1)
         abi.check(self.r.lib.vkb_scene_update_instances(self.h, abi.fptr(rows), rows.size // 12, policy))
+
+    def update_instances_device(self, device_ptr: int, count: int, policy: int = 0):
+        abi.check(self.r.lib.vkb_scene_update_instances_device(self.h, C.c_void_p(device_ptr), count, policy))
+
+    @property
+    def launch_count(self) -> int:
+        return int(self.r.lib.vkb_scene_launch_count(self.h))
 
     def render(self, profile: Profile, ids: bool = False, out: np.ndarray | None = None, device_ptr: int | None = None) -> RenderResult:
         cam = self.scene.camera

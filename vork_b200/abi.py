@@ -63,7 +63,10 @@ class VkbProfile(C.Structure):
     _fields_ = [("samples", C.c_uint32), ("first_sample", C.c_uint32), ("sample_count", C.c_uint32), ("seed", C.c_uint32),
                 ("bounces", C.c_uint32 * 4), ("transparent", C.c_uint32), ("caustics", C.c_uint32),
                 ("clamp_direct", C.c_float), ("clamp_indirect", C.c_float), ("light_threshold", C.c_float),
-                ("adaptive", C.c_uint32), ("wave_samples", C.c_uint32)]
+                ("adaptive", C.c_uint32), ("wave_samples", C.c_uint32), ("flags", C.c_uint32)]
+
+
+PROFILE_TIME_KERNELS, PROFILE_COUNT_TRAVERSAL = 1, 2
 
 
 class VkbOutput(C.Structure):
@@ -73,7 +76,10 @@ class VkbOutput(C.Structure):
 class VkbStats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("dropped_path_samples", C.c_uint64), ("dropped_light_samples", C.c_uint64),
-                ("traversal_overflows", C.c_uint64), ("render_ms", C.c_float), ("build_ms", C.c_float)]
+                ("traversal_overflows", C.c_uint64), ("render_ms", C.c_float), ("build_ms", C.c_float),
+                ("trace_ms", C.c_float), ("trace_launches", C.c_uint32), ("kernel_launches", C.c_uint32),
+                ("nodes_visited", C.c_uint64), ("triangles_tested", C.c_uint64), ("instances_entered", C.c_uint64),
+                ("shadow_nodes_visited", C.c_uint64), ("shadow_triangles_tested", C.c_uint64)]
 
 
 # Every symbol include/vkb.h declares, with its ctypes signature.
@@ -86,7 +92,10 @@ SIGNATURES = {
     "vkb_scene_create": (C.c_int, [_P, C.POINTER(VkbSceneDesc), C.POINTER(_P)]),
     "vkb_scene_destroy": (C.c_int, [_P]),
     "vkb_scene_update_instances": (C.c_int, [_P, C.POINTER(C.c_float), C.c_uint32, C.c_int]),
+    "vkb_scene_update_instances_device": (C.c_int, [_P, C.c_void_p, C.c_uint32, C.c_int]),
     "vkb_render": (C.c_int, [_P, C.POINTER(VkbProfile), C.POINTER(VkbOutput), C.POINTER(VkbStats)]),
+    "vkb_ctx_stream": (C.c_void_p, [_P]),
+    "vkb_scene_launch_count": (C.c_uint64, [_P]),
     "vkb_debug_sampler_groups": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                            C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_uint32, C.c_uint32,
                                            C.POINTER(C.c_uint32)]),

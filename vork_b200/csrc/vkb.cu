@@ -161,8 +161,9 @@ struct LbvhScratch {
 
 // Build one LBVH over n boxes into nodes (n-1 internal nodes, or 1 for n == 1).
 // On return scratch.ids_sorted holds the leaf order and scratch.codes the codes in input order.
-void build_lbvh(uint32_t n, const float4* lo, const float4* hi, BvhNode* nodes, LbvhScratch& sc, cudaStream_t s, int sms) {
+void build_lbvh(uint32_t n, const float4* lo, const float4* hi, BvhNode* nodes, LbvhScratch& sc, cudaStream_t s, int sms, uint64_t& launches) {
     if (n == 0) return;
+    launches += n == 1 ? 3 : 4;
     sc.reserve(n, s);
     VKB_CUDA(cudaMemsetAsync(sc.bounds.p, 0xff, 3 * sizeof(uint32_t), s));
     VKB_CUDA(cudaMemsetAsync(sc.bounds.p + 3, 0x00, 3 * sizeof(uint32_t), s));
@@ -215,9 +216,12 @@ struct vkb_scene {
     // wavefront
     DBuf<float4> ray_o0, ray_d0, ray_o1, ray_d1, hit, thr, rad, sa_o, sa_d, sa_c, sb_o, sb_d, sb_c, accum, out_rgba;
     DBuf<uint32_t> hit_inst, counters, err, ids;
+    DBuf<unsigned long long> work;
     DBuf<uint2> rng;
     float build_ms = 0.f;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> kernel_events;  // pairs around timed trace launches
+    uint64_t launches = 0;                    // kernels launched for this scene so far
 };
 
 namespace {
@@ -254,7 +258,8 @@ void build_tlas(vkb_scene* s) {
     if (n == 0) return;
     VKB_CUDA(cudaEventRecord(s->ev0, st));
     k_instances<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->o2w.p, s->inst_info.p, s->meshes.p, s->w2o.p, s->inst_lo.p, s->inst_hi.p);
-    build_lbvh(n, s->inst_lo.p, s->inst_hi.p, s->tlas_nodes.p, s->scratch, st, sms);
+    build_lbvh(n, s->inst_lo.p, s->inst_hi.p, s->tlas_nodes.p, s->scratch, st, sms, s->launches);
+    s->launches += 2;
     k_tlas_leaves<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->scratch.ids_sorted.p, s->w2o.p, s->inst_info.p, s->meshes.p, s->d_materials.p, s->tlas_leaves.p);
     VKB_CUDA(cudaMemcpyAsync(s->tlas_codes.p, s->scratch.codes.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     VKB_CUDA(cudaEventRecord(s->ev1, st));
@@ -382,7 +387,8 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
             const uint32_t* mid = s->indices.p + mi.index_offset;
             const float4* mpos = s->vpos.p + mi.vertex_offset;
             k_tri_boxes<<<grid_for(mi.num_triangles, 256, sms), 256, 0, str>>>(mi.num_triangles, mid, mpos, s->tri_lo.p, s->tri_hi.p);
-            build_lbvh(mi.num_triangles, s->tri_lo.p, s->tri_hi.p, s->blas_nodes.p + mi.node_offset, s->scratch, str, sms);
+            build_lbvh(mi.num_triangles, s->tri_lo.p, s->tri_hi.p, s->blas_nodes.p + mi.node_offset, s->scratch, str, sms, s->launches);
+            s->launches += 2;
             k_sorted_tris<<<grid_for(mi.num_triangles, 256, sms), 256, 0, str>>>(mi.num_triangles, s->scratch.ids_sorted.p, mid, mpos, s->blas_tris.p + 3 * size_t(mi.tri_offset));
         }
         VKB_CUDA(cudaEventRecord(s->ev1, str));
@@ -431,7 +437,8 @@ vkb_status vkb_scene_destroy(vkb_scene* s) {
     for (auto* b : f4) b->release();
     s->indices.release(); s->tlas_codes.release(); s->inst_info.release(); s->meshes.release();
     s->blas_nodes.release(); s->tlas_nodes.release(); s->tlas_leaves.release(); s->d_materials.release(); s->d_lights.release();
-    s->tree.release(); s->hit_inst.release(); s->counters.release(); s->err.release(); s->ids.release(); s->rng.release();
+    s->tree.release(); s->hit_inst.release(); s->counters.release(); s->err.release(); s->ids.release(); s->rng.release(); s->work.release();
+    for (cudaEvent_t e : s->kernel_events) cudaEventDestroy(e);
     s->scratch.codes.release(); s->scratch.codes_sorted.release(); s->scratch.ids.release(); s->scratch.ids_sorted.release();
     s->scratch.leaf_parent.release(); s->scratch.node_parent.release(); s->scratch.counters.release(); s->scratch.bounds.release(); s->scratch.cub_temp.release();
     if (s->ev0) cudaEventDestroy(s->ev0);
@@ -456,6 +463,17 @@ vkb_status vkb_scene_update_instances(vkb_scene* s, const float* rows, uint32_t 
     });
 }
 
+vkb_status vkb_scene_update_instances_device(vkb_scene* s, const float* rows, uint32_t n, int policy) {
+    if (!s || !rows) return fail(VKB_INVALID_ARG, "null scene or rows");
+    if (n != s->num_instances) return fail(VKB_INVALID_ARG, "instance count differs from the installed scene");
+    if (policy < 0 || policy > 2) return fail(VKB_INVALID_ARG, "policy must be 0, 1 or 2");
+    return guarded([&] {
+        VKB_CUDA(cudaSetDevice(s->ctx->device));
+        VKB_CUDA(cudaMemcpyAsync(s->o2w.p, rows, size_t(n) * 3 * sizeof(float4), cudaMemcpyDeviceToDevice, s->ctx->stream));
+        build_tlas(s);
+    });
+}
+
 vkb_status vkb_render(vkb_scene* s, const vkb_profile* pf, vkb_output* out, vkb_stats* stats) {
     if (!s || !pf || !out || !out->rgba) return fail(VKB_INVALID_ARG, "null scene, profile or output");
     return guarded([&] {
@@ -477,7 +495,10 @@ vkb_status vkb_render(vkb_scene* s, const vkb_profile* pf, vkb_output* out, vkb_
         s->ray_o0.alloc(slots); s->ray_d0.alloc(slots); s->ray_o1.alloc(slots); s->ray_d1.alloc(slots);
         s->hit.alloc(slots); s->hit_inst.alloc(slots); s->thr.alloc(slots); s->rad.alloc(slots); s->rng.alloc(slots);
         s->sa_o.alloc(slots); s->sa_d.alloc(slots); s->sa_c.alloc(slots); s->sb_o.alloc(slots); s->sb_d.alloc(slots); s->sb_c.alloc(slots);
-        s->accum.alloc(npix); s->counters.alloc(16); s->err.alloc(1);
+        s->accum.alloc(npix); s->counters.alloc(16); s->err.alloc(1); s->work.alloc(8);
+        const bool timed = (pf->flags & VKB_PROFILE_TIME_KERNELS) != 0, counted = (pf->flags & VKB_PROFILE_COUNT_TRAVERSAL) != 0;
+        uint32_t launches = 0, trace_launches = 0;
+        VKB_CUDA(cudaMemsetAsync(s->work.p, 0, 8 * sizeof(unsigned long long), st));
         if (out->primary_ids) s->ids.alloc(size_t(npix) * 2);
         VKB_CUDA(cudaMemsetAsync(s->accum.p, 0, npix * sizeof(float4), st));
         VKB_CUDA(cudaMemsetAsync(s->counters.p, 0, 16 * sizeof(uint32_t), st));
@@ -499,7 +520,7 @@ vkb_status vkb_render(vkb_scene* s, const vkb_profile* pf, vkb_output* out, vkb_
         p.ray_o[0] = s->ray_o0.p; p.ray_d[0] = s->ray_d0.p; p.ray_o[1] = s->ray_o1.p; p.ray_d[1] = s->ray_d1.p;
         p.hit = s->hit.p; p.hit_inst = s->hit_inst.p; p.thr = s->thr.p; p.rad = s->rad.p; p.rng = s->rng.p;
         p.sa_o = s->sa_o.p; p.sa_d = s->sa_d.p; p.sa_c = s->sa_c.p; p.sb_o = s->sb_o.p; p.sb_d = s->sb_d.p; p.sb_c = s->sb_c.p;
-        p.accum = s->accum.p; p.counters = s->counters.p; p.err = s->err.p;
+        p.accum = s->accum.p; p.counters = s->counters.p; p.err = s->err.p; p.work = s->work.p;
         p.primary_ids = out->primary_ids ? s->ids.p : nullptr;
         VKB_CUDA(cudaEventRecord(s->ev0, st));
         for (uint32_t done = 0; done < count; done += wave) {
@@ -512,12 +533,26 @@ vkb_status vkb_render(vkb_scene* s, const vkb_profile* pf, vkb_output* out, vkb_
             const int tgrid = sms * 16, sgrid = sms * 16;
             for (uint32_t b = 0; b <= pf->bounces[0]; ++b) {
                 int cur = int(b & 1u);
-                k_trace<false><<<tgrid, 128, 0, st>>>(p, cur);
+                if (timed) {
+                    while (s->kernel_events.size() < 2 * (trace_launches + 1)) {
+                        cudaEvent_t e;
+                        VKB_CUDA(cudaEventCreate(&e));
+                        s->kernel_events.push_back(e);
+                    }
+                    VKB_CUDA(cudaEventRecord(s->kernel_events[2 * trace_launches], st));
+                }
+                if (counted) k_trace<false, true><<<tgrid, 128, 0, st>>>(p, cur);
+                else k_trace<false, false><<<tgrid, 128, 0, st>>>(p, cur);
+                if (timed) VKB_CUDA(cudaEventRecord(s->kernel_events[2 * trace_launches + 1], st));
+                trace_launches++;
                 k_reset_queues<<<1, 1, 0, st>>>(s->counters.p, cur ^ 1);
                 k_shade<<<sgrid, 128, 0, st>>>(p, cur);
-                k_trace<true><<<tgrid, 128, 0, st>>>(p, -1);
+                if (counted) k_trace<true, true><<<tgrid, 128, 0, st>>>(p, -1);
+                else k_trace<true, false><<<tgrid, 128, 0, st>>>(p, -1);
+                launches += 4;
             }
             k_accumulate<<<grid_for(npix, 256, sms), 256, 0, st>>>(p);
+            launches += 2;
             VKB_CUDA(cudaGetLastError());
         }
         VKB_CUDA(cudaEventRecord(s->ev1, st));
@@ -525,6 +560,10 @@ vkb_status vkb_render(vkb_scene* s, const vkb_profile* pf, vkb_output* out, vkb_
         if (out->on_device) dst = reinterpret_cast<float4*>(out->rgba);
         else { s->out_rgba.alloc(npix); dst = s->out_rgba.p; }
         k_resolve<<<grid_for(npix, 256, sms), 256, 0, st>>>(npix, s->accum.p, dst);
+        launches += 1;
+        s->launches += launches;
+        unsigned long long work[8] = {};
+        VKB_CUDA(cudaMemcpyAsync(work, s->work.p, sizeof(work), cudaMemcpyDeviceToHost, st));
         if (!out->on_device) VKB_CUDA(cudaMemcpyAsync(out->rgba, dst, npix * sizeof(float4), cudaMemcpyDeviceToHost, st));
         if (out->primary_ids) VKB_CUDA(cudaMemcpyAsync(out->primary_ids, s->ids.p, size_t(npix) * 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         uint32_t ctr[16], err = 0;
@@ -542,9 +581,26 @@ vkb_status vkb_render(vkb_scene* s, const vkb_profile* pf, vkb_output* out, vkb_
             stats->traversal_overflows = err;
             stats->render_ms = ms;
             stats->build_ms = s->build_ms;
+            stats->trace_ms = 0.f;
+            if (timed)
+                for (uint32_t k = 0; k < trace_launches; ++k) {
+                    float e = 0.f;
+                    VKB_CUDA(cudaEventElapsedTime(&e, s->kernel_events[2 * k], s->kernel_events[2 * k + 1]));
+                    stats->trace_ms += e;
+                }
+            stats->trace_launches = trace_launches;
+            stats->kernel_launches = launches;
+            stats->nodes_visited = work[0];
+            stats->triangles_tested = work[1];
+            stats->instances_entered = work[2];
+            stats->shadow_nodes_visited = work[3];
+            stats->shadow_triangles_tested = work[4];
         }
     });
 }
+
+void* vkb_ctx_stream(vkb_ctx* c) { return c ? reinterpret_cast<void*>(c->stream) : nullptr; }
+uint64_t vkb_scene_launch_count(vkb_scene* s) { return s ? s->launches : 0; }
 
 vkb_status vkb_debug_sampler_groups(vkb_ctx* c, uint32_t n, const uint32_t* px, const uint32_t* py, const uint32_t* index,
                                     const uint32_t* groups, uint32_t count, uint32_t stream, uint32_t* out_bits) {

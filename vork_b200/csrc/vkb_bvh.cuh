@@ -134,10 +134,14 @@ struct SceneView {
     uint32_t num_instances;
 };
 
+// Traversal work of one ray (instrumented builds only): node visits, triangle tests, instance entries.
+struct TraceCount { uint32_t nodes = 0, tris = 0, instances = 0; };
+
 // Closest hit (any == false) or first hit (any == true) of a world ray over the
 // two-level BVH.  Error: overflow/step-limit exits set *err and return the best so far.
-template <bool ANY>
-__device__ __forceinline__ bool trace_ray(const SceneView& s, float3 o, float3 d, float tmax, HitRecord& hit, uint32_t* err) {
+template <bool ANY, bool COUNT = false>
+__device__ __forceinline__ bool trace_ray(const SceneView& s, float3 o, float3 d, float tmax, HitRecord& hit, uint32_t* err,
+                                          TraceCount* count = nullptr) {
     RaySpace ws, rs;
     make_space(ws, o, d);
     rs = ws;
@@ -154,6 +158,7 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, float3 o, float3 d
     for (uint32_t steps = 0;; ++steps) {
         if (steps >= TRACE_STEP_LIMIT) { atomicOr(err, 2u); break; }
         if (node >= 0) {
+            if (COUNT) count->nodes++;
             BvhNode n;
             const float4* p = reinterpret_cast<const float4*>(nodes + node);
             n.a = __ldg(p); n.b = __ldg(p + 1); n.c = __ldg(p + 2);
@@ -171,6 +176,7 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, float3 o, float3 d
             if (hl) { node = n.d.x; continue; }
             if (hr) { node = n.d.y; continue; }
         } else if (!in_blas) {
+            if (COUNT) count->instances++;
             const TlasLeaf* lf = s.tlas_leaves + (~node);
             float4 r0 = __ldg(&lf->w2o[0]), r1 = __ldg(&lf->w2o[1]), r2 = __ldg(&lf->w2o[2]);
             uint4 info = __ldg(reinterpret_cast<const uint4*>(&lf->instance));
@@ -187,6 +193,7 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, float3 o, float3 d
             node = 0;
             continue;
         } else {
+            if (COUNT) count->tris++;
             const float4* tp = tris + 3u * (tri_base + uint32_t(~node));
             float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
             float t, b1, b2;

@@ -242,6 +242,7 @@ struct PathParams {
     float4* sb_o; float4* sb_d; float4* sb_c;
     float4* accum;
     uint32_t* counters;  // [0],[1] ray counts, [2] shadow count, [3] ext rays, [4] shadow rays, [5] dropped light, [6] dropped paths
+    unsigned long long* work;  // instrumented traversal: closest nodes, tris, instances; shadow nodes, tris
     uint32_t* err;
     uint32_t* primary_ids;
 };
@@ -286,18 +287,26 @@ __global__ void k_camera(PathParams p) {
         p.rng[slot] = make_uint2(rng, pseed);
     }
 }
-template <bool ANY>
+__device__ __forceinline__ void flush_count(unsigned long long* dst, uint32_t v) {
+    unsigned long long x = v;
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+    if ((threadIdx.x & 31u) == 0u && x) atomicAdd(dst, x);
+}
+template <bool ANY, bool COUNT>
 __global__ void __launch_bounds__(128) k_trace(PathParams p, int cur) {
     uint32_t n = cur < 0 ? p.counters[2] : p.counters[cur];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (ANY) atomicAdd(&p.counters[4], n);
         else atomicAdd(&p.counters[3], n);
     }
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    TraceCount tc;
+    uint32_t loop_end = COUNT ? (n + 31u) / 32u * 32u : n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < loop_end; i += gridDim.x * blockDim.x) {
+        if (COUNT && i >= n) continue;
         if (!ANY) {
             float4 ro = p.ray_o[cur][i], rd = p.ray_d[cur][i];
             HitRecord h;
-            bool found = trace_ray<false>(p.sv, f3(ro.x, ro.y, ro.z), f3(rd.x, rd.y, rd.z), ro.w, h, p.err);
+            bool found = trace_ray<false, COUNT>(p.sv, f3(ro.x, ro.y, ro.z), f3(rd.x, rd.y, rd.z), ro.w, h, p.err, &tc);
             p.hit[i] = found ? make_float4(h.t, h.u, h.v, __uint_as_float(h.prim)) : make_float4(-1.f, 0.f, 0.f, __uint_as_float(0xffffffffu));
             p.hit_inst[i] = found ? h.inst : 0xffffffffu;
         } else {
@@ -305,13 +314,13 @@ __global__ void __launch_bounds__(128) k_trace(PathParams p, int cur) {
             uint32_t slot = __float_as_uint(sd.w), flags = __float_as_uint(sc.w);
             HitRecord h;
             float3 total = f3(sc.x, sc.y, sc.z);
-            if ((flags & SH_TRACE_A) && trace_ray<true>(p.sv, f3(so.x, so.y, so.z), f3(sd.x, sd.y, sd.z), so.w, h, p.err)) total = f3(0.f);
+            if ((flags & SH_TRACE_A) && trace_ray<true, COUNT>(p.sv, f3(so.x, so.y, so.z), f3(sd.x, sd.y, sd.z), so.w, h, p.err, &tc)) total = f3(0.f);
             if (flags & SH_HAS_B) {
                 float4 bc = p.sb_c[slot];
                 float3 cb = f3(bc.x, bc.y, bc.z);
                 if (flags & SH_TRACE_B) {
                     float4 bo = p.sb_o[slot], bd = p.sb_d[slot];
-                    if (trace_ray<true>(p.sv, f3(bo.x, bo.y, bo.z), f3(bd.x, bd.y, bd.z), bo.w, h, p.err)) cb = f3(0.f);
+                    if (trace_ray<true, COUNT>(p.sv, f3(bo.x, bo.y, bo.z), f3(bd.x, bd.y, bd.z), bo.w, h, p.err, &tc)) cb = f3(0.f);
                 }
                 total = total + cb;
             }
@@ -320,6 +329,12 @@ __global__ void __launch_bounds__(128) k_trace(PathParams p, int cur) {
             float3 add = clamp_sample(total, (flags & SH_DIRECT) ? p.clamp_direct : p.clamp_indirect, dropped);
             p.rad[slot] = make_float4(r.x + add.x, r.y + add.y, r.z + add.z, __uint_as_float(dropped));
         }
+    }
+    if (COUNT) {
+        // Every lane of a warp reaches here (the loop runs whole warps).
+        flush_count(&p.work[ANY ? 3 : 0], tc.nodes);
+        flush_count(&p.work[ANY ? 4 : 1], tc.tris);
+        if (!ANY) flush_count(&p.work[2], tc.instances);
     }
 }
 

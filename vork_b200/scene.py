@@ -344,3 +344,102 @@ def spheres_scene(num_spheres: int = 64, seed: int = 0, width: int = 256, height
                   width=width, height=height, near=0.05, far=1000.0)
     return Scene([sphere, ground], np.stack(rows).astype(np.float32), np.asarray(mesh_ids, np.uint32),
                  np.asarray(mats, np.uint32), materials, [light], cam, environment(), name=f"spheres{num_spheres}")
+
+
+# ----------------------------------------------------------------------------- plain method, large
+def value_noise_heights(cells: int, size: float, seed: int = 0, amplitude: float = 30.0, octaves: int = 6) -> np.ndarray:
+    """(cells+1)^2 heights of seeded fBm value noise (smoothstep-interpolated lattice values)."""
+    rng = np.random.default_rng(seed)
+    xs = np.linspace(0.0, 1.0, cells + 1)
+    h = np.zeros((cells + 1, cells + 1))
+    freq, amp = 4, amplitude
+    for _ in range(octaves):
+        lattice = rng.uniform(-1, 1, (freq + 2, freq + 2))
+        u = xs * freq
+        i = np.minimum(u.astype(np.int64), freq)
+        f = u - i
+        f = f * f * (3 - 2 * f)
+        a = lattice[i][:, i]; b = lattice[i + 1][:, i]; c = lattice[i][:, i + 1]; d = lattice[i + 1][:, i + 1]
+        fz, fx = f[:, None], f[None, :]
+        h += amp * ((a * (1 - fz) + b * fz) * (1 - fx) + (c * (1 - fz) + d * fz) * fx)
+        freq *= 2
+        amp *= 0.5
+    return h
+
+
+class Flock:
+    """Seeded boid flock (cohesion, alignment, separation) over a uniform grid of cells.
+
+    Each boid steers toward its cell's mean position and velocity and away from the
+    cell mean when crowded, plus a weak pull toward the flock centre.  Cell sums use
+    one sort per frame, O(N log N)."""
+
+    def __init__(self, n: int, seed: int = 0, center=(0.0, 60.0, 0.0), extent=(240.0, 60.0, 240.0), cell: float = 4.0):
+        rng = np.random.default_rng(seed)
+        self.center = np.asarray(center, np.float64)
+        self.extent = np.asarray(extent, np.float64)
+        self.pos = self.center + (rng.random((n, 3)) - 0.5) * self.extent
+        ang = rng.uniform(0, 2 * np.pi, n)
+        self.vel = np.stack([np.cos(ang), rng.uniform(-0.2, 0.2, n), np.sin(ang)], 1) * 8.0
+        self.cell = cell
+
+    def step(self, dt: float = 1.0 / 24.0):
+        key = np.floor(self.pos / self.cell).astype(np.int64)
+        k = (key[:, 0] * 73856093) ^ (key[:, 1] * 19349663) ^ (key[:, 2] * 83492791)
+        _, inv, counts = np.unique(k, return_inverse=True, return_counts=True)
+        cnt = counts[inv][:, None].astype(np.float64)
+        mean_p = np.stack([np.bincount(inv, self.pos[:, a]) for a in range(3)], 1)[inv] / cnt
+        mean_v = np.stack([np.bincount(inv, self.vel[:, a]) for a in range(3)], 1)[inv] / cnt
+        cohesion = (mean_p - self.pos) * 0.5
+        alignment = (mean_v - self.vel) * 0.8
+        separation = (self.pos - mean_p) * np.minimum(cnt, 8.0) * 0.6
+        centre = (self.center - self.pos) / self.extent * 4.0
+        self.vel += (cohesion + alignment + separation + centre) * dt
+        speed = np.linalg.norm(self.vel, axis=1, keepdims=True)
+        self.vel *= np.clip(speed, 4.0, 14.0) / np.maximum(speed, 1e-6)
+        self.pos += self.vel * dt
+
+    def rows(self, length: float = 0.35, width: float = 0.14) -> np.ndarray:
+        """(N,3,4) object->world rows: the bird's long axis along its velocity."""
+        f = self.vel / np.linalg.norm(self.vel, axis=1, keepdims=True)
+        up = np.array([0.0, 1.0, 0.0])
+        r = np.cross(up, f)
+        r /= np.maximum(np.linalg.norm(r, axis=1, keepdims=True), 1e-9)
+        u = np.cross(f, r)
+        out = np.empty((len(f), 3, 4), np.float32)
+        out[:, :, 0] = r * width
+        out[:, :, 1] = u * width
+        out[:, :, 2] = f * length
+        out[:, :, 3] = self.pos
+        return out
+
+
+def flock_scene(num_birds: int = 1_000_000, seed: int = 0, width: int = 1920, height: int = 1080,
+                terrain_cells: int = 1000, terrain_size: float = 1000.0, num_materials: int = 16):
+    """Plain method, large: `num_birds` instances of a seeded 500-triangle geodesic
+    (icosphere-derived) mesh placed by a boid flock, a 2*terrain_cells^2-triangle
+    noise-displaced terrain, materials drawn as in the small configuration, a sun and a
+    constant environment light.  Returns (Scene, Flock); Flock.step()/rows() give the
+    following animation frames."""
+    rng = Pcg32(seed)
+    bird = geodesic_sphere(5, jitter=0.12, seed=seed)
+    terrain = height_grid(value_noise_heights(terrain_cells, terrain_size, seed=seed + 1), terrain_size)
+    materials = []
+    for _ in range(num_materials):
+        col = (rng.uniform(0.1, 0.9), rng.uniform(0.1, 0.9), rng.uniform(0.1, 0.9))
+        rough = rng.uniform(0.05, 1.0)
+        metal = 1.0 if rng.uniform() < 0.3 else 0.0
+        materials.append(material(col, rough, metal))
+    materials.append(material((0.32, 0.28, 0.22), 0.85, 0.0))
+    flock = Flock(num_birds, seed=seed + 2)
+    rows = np.concatenate([flock.rows(), rows_from(1.0, (0.0, 0.0, 0.0))[None]], 0)
+    mesh_ids = np.zeros(num_birds + 1, np.uint32)
+    mesh_ids[-1] = 1
+    mat_ids = (np.arange(num_birds + 1, dtype=np.uint64) * 2654435761 % num_materials).astype(np.uint32)
+    mat_ids[-1] = num_materials
+    sun = sun_light(direction=(-0.35, -0.8, 0.45), angle_degrees=0.526, energy=3.0, color=(1.0, 0.95, 0.88))
+    cam = look_at(eye=(0.0, 75.0, -330.0), target=(0.0, 48.0, 0.0), fov_y_degrees=40.0, width=width, height=height,
+                  near=0.1, far=1e5)
+    env = environment(radiance=(0.18, 0.26, 0.42))
+    sc = Scene([bird, terrain], rows, mesh_ids, mat_ids, materials, [sun], cam, env, name="flock")
+    return sc, flock
