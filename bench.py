@@ -44,6 +44,12 @@ def workload(config: str, seed: int = 0):
         sc = scene.spheres_scene(seed=seed)
         prof = Profile.reference_transport(4, 16)
         return sc, None, prof, {"workload": "plain-small: 256x256, 16 spp, depth 4, 64 UV spheres + 8192-tri grid, 1 area light"}
+    if config == "profile":
+        # The large scene (BVH data far larger than L2) at 480x270 and 4 spp: a case small
+        # enough for a full ncu capture of one launch.
+        sc, flock = scene.flock_scene(seed=seed, width=480, height=270)
+        prof = Profile.reference_transport(8, 4)
+        return sc, flock, prof, {"workload": "plain-large scene at 480x270, 4 spp, depth 8 (profiling case)"}
     sc, flock = scene.flock_scene(seed=seed)
     prof = Profile.reference_transport(8, 64)
     return sc, flock, prof, {"workload": "plain-large: 1920x1080, 64 spp, depth 8, 1,000,000 boid-placed instances of a 500-tri "
@@ -192,7 +198,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="vkb", choices=["vkb", "reference"])
-    ap.add_argument("--config", default="large", choices=["large", "small"])
+    ap.add_argument("--config", default="large", choices=["large", "small", "profile"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 
