@@ -295,12 +295,14 @@ def main():
         pk = peaks()
         alg_bytes = roofline_bytes(counted)
         achieved_gbs = alg_bytes / (trace_ms / args.steps / 1000.0) / 1e9 if trace_ms > 0 else None
+        launches_per_frame = trace_launches / args.steps
         traffic = None
         prof_note = ROOT / "profiles" / "trace_closest_traffic.json"
-        if prof_note.exists():
+        if prof_note.exists() and args.config in ("large", "profile"):
+            # ncu capture of a smaller case of the same scene, scaled by rays per launch.
             tr = json.loads(prof_note.read_text())
-            if tr.get("config") == args.config:
-                traffic = tr.get("traffic_bytes_per_launch")
+            rays_per_launch = counted["extension_rays"] / max(1, counted["trace_launches"])
+            traffic = tr["traffic_bytes_per_ray"] * rays_per_launch
         line = {
             "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -311,6 +313,7 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "k_trace<closest>", "achieved": achieved_gbs, "peak": pk["hbm_gbs"],
                          "peak_source": pk["source"], "unit": "GB/s",
                          "frac": (achieved_gbs / pk["hbm_gbs"]) if achieved_gbs else None, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": alg_bytes / max(1.0, launches_per_frame),
                          "algorithmic_bytes_per_frame": alg_bytes, "trace_ms_per_frame": trace_ms / args.steps,
                          "trace_launches_per_frame": trace_launches / args.steps,
                          "share_of_step": trace_ms / elapsed_ms if elapsed_ms else None},
