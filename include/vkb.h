@@ -208,6 +208,22 @@ void* vkb_ctx_stream(vkb_ctx* ctx);
 /* Kernel launches issued so far for this scene (renders and acceleration-structure builds). */
 uint64_t vkb_scene_launch_count(vkb_scene* scene);
 
+/* Render without allocating (no counterpart in the reference: it exists for callers
+ * that cannot allocate device memory while they render, e.g. a host renderer whose
+ * own memory manager owns every device allocation, or a serving loop with a fixed
+ * footprint).  Same semantics and results as vkb_render, but every wavefront queue,
+ * accumulator and counter lives in one fixed device array of VKB_NOALLOC_SCRATCH_MIB
+ * MiB that each GPU loading the library holds until process exit; no cudaMalloc or
+ * cudaFree is called.  An image needs about 236 bytes per pixel for one sample per
+ * wave (16 accumulator + 220 queue bytes, +16 with host output, +8 with primary_ids);
+ * larger images are rejected with VKB_INVALID_ARG.  The first call on a device looks
+ * up the array's device address with that device current: make that first call
+ * before any stream capture.  All calls share the array and it keeps the previous
+ * call's contents: calls that overlap on the GPU (another stream, another thread)
+ * race, so serialise them.  VKB_PROFILE_TIME_KERNELS is ignored (no events). */
+#define VKB_NOALLOC_SCRATCH_MIB 32u
+vkb_status vkb_render_noalloc(vkb_scene* scene, const vkb_profile* profile, vkb_output* out, vkb_stats* stats);
+
 /* --- Test and measurement entry points (no reference counterpart beyond the cited tests) --- */
 
 /* Sampler groups, bit-exact with path_sampler.slang:53-95 (the harness of

@@ -67,6 +67,7 @@ class VkbProfile(C.Structure):
 
 
 PROFILE_TIME_KERNELS, PROFILE_COUNT_TRAVERSAL = 1, 2
+NOALLOC_SCRATCH_MIB = 32
 
 
 class VkbOutput(C.Structure):
@@ -94,6 +95,7 @@ SIGNATURES = {
     "vkb_scene_update_instances": (C.c_int, [_P, C.POINTER(C.c_float), C.c_uint32, C.c_int]),
     "vkb_scene_update_instances_device": (C.c_int, [_P, C.c_void_p, C.c_uint32, C.c_int]),
     "vkb_render": (C.c_int, [_P, C.POINTER(VkbProfile), C.POINTER(VkbOutput), C.POINTER(VkbStats)]),
+    "vkb_render_noalloc": (C.c_int, [_P, C.POINTER(VkbProfile), C.POINTER(VkbOutput), C.POINTER(VkbStats)]),
     "vkb_ctx_stream": (C.c_void_p, [_P]),
     "vkb_scene_launch_count": (C.c_uint64, [_P]),
     "vkb_debug_sampler_groups": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),

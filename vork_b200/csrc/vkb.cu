@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -686,3 +687,164 @@ vkb_status vkb_debug_trace(vkb_scene* s, uint32_t n, const float* rays7, float* 
 }
 
 }  // extern "C"
+
+// ================================================================ render without allocation
+//
+// Some callers cannot allocate device memory while they render: a host renderer
+// that owns every device allocation through its own memory manager and residency
+// budget (vork's gpu_memory / residency model), a serving loop that must not change
+// its footprint after admission, or code running while the device allocator is
+// locked.  vkb_render_noalloc serves them: it renders an installed scene with every
+// wavefront queue, accumulator and counter carved from one fixed device array that
+// the library holds for the life of the process, and calls no cudaMalloc/cudaFree.
+namespace {
+
+constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(VKB_NOALLOC_SCRATCH_MIB) << 20;
+// Every GPU that loads this library holds this array until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+// Device address of g_noalloc_scratch per device ordinal, looked up once with that
+// device current (the host-side symbol is only a stand-in, never a device address).
+constexpr int NOALLOC_MAX_DEVICES = 64;
+unsigned char* g_noalloc_base[NOALLOC_MAX_DEVICES] = {};
+std::mutex g_noalloc_mutex;
+
+unsigned char* noalloc_scratch(int device) {
+    if (device < 0 || device >= NOALLOC_MAX_DEVICES) throw ArgError{"device ordinal beyond the no-alloc table"};
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_base[device]) {
+        void* p = nullptr;
+        VKB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_base[device] = static_cast<unsigned char*>(p);
+    }
+    return g_noalloc_base[device];
+}
+
+struct Carver {
+    unsigned char* base;
+    size_t used = 0, cap;
+    template <class T> T* take(size_t count) {
+        size_t off = (used + 255) & ~size_t(255);
+        size_t bytes = count * sizeof(T);
+        if (off + bytes > cap) return nullptr;
+        used = off + bytes;
+        return reinterpret_cast<T*>(base + off);
+    }
+};
+
+}  // namespace
+
+extern "C" vkb_status vkb_render_noalloc(vkb_scene* s, const vkb_profile* pf, vkb_output* out, vkb_stats* stats) {
+    if (!s || !pf || !out || !out->rgba) return fail(VKB_INVALID_ARG, "null scene, profile or output");
+    return guarded([&] {
+        if (pf->adaptive) throw Unsupported{"adaptive sampling is outside the built subset"};
+        if (pf->samples == 0) throw ArgError{"samples must be positive"};
+        if (pf->first_sample >= pf->samples) throw ArgError{"first_sample beyond samples"};
+        uint32_t count = pf->sample_count ? pf->sample_count : pf->samples - pf->first_sample;
+        if (pf->first_sample + count > pf->samples) throw ArgError{"sample range beyond samples"};
+        if (pf->bounces[0] > 250) throw ArgError{"bounce budget above 250"};
+        vkb_ctx* c = s->ctx;
+        VKB_CUDA(cudaSetDevice(c->device));
+        unsigned char* base = noalloc_scratch(c->device);
+        cudaStream_t st = c->stream;
+        int sms = c->sms;
+        const uint32_t W = s->camera.width, H = s->camera.height, npix = W * H;
+        // Fixed part: counters, error word, traversal counters, accumulator, optional ids and host staging.
+        Carver cv{base, 0, NOALLOC_SCRATCH_BYTES};
+        uint32_t* counters = cv.take<uint32_t>(16);
+        uint32_t* err = cv.take<uint32_t>(1);
+        unsigned long long* work = cv.take<unsigned long long>(8);
+        float4* accum = cv.take<float4>(npix);
+        uint32_t* ids = out->primary_ids ? cv.take<uint32_t>(size_t(npix) * 2) : nullptr;
+        float4* staging = out->on_device ? reinterpret_cast<float4*>(out->rgba) : cv.take<float4>(npix);
+        // Per-slot part: 13 float4 queues/state + hit instance + rng = 220 bytes per path slot.
+        const size_t per_slot = 13 * sizeof(float4) + sizeof(uint32_t) + sizeof(uint2);
+        const size_t fixed = (cv.used + 255) & ~size_t(255);
+        size_t free_bytes = fixed < NOALLOC_SCRATCH_BYTES ? NOALLOC_SCRATCH_BYTES - fixed : 0;
+        // 15 regions, each rounded up to 256 bytes.
+        size_t slots_fit = free_bytes > 15 * 256 ? (free_bytes - 15 * 256) / per_slot : 0;
+        if (!counters || !err || !work || !accum || (out->primary_ids && !ids) || !staging || slots_fit < npix)
+            throw ArgError{"vkb_render_noalloc: a " + std::to_string(W) + "x" + std::to_string(H) + " image needs " +
+                           std::to_string((fixed + size_t(npix) * per_slot + 15 * 256) >> 10) + " KiB of scratch for one sample per wave; the fixed array holds " +
+                           std::to_string(NOALLOC_SCRATCH_BYTES >> 10) + " KiB (use vkb_render)"};
+        uint32_t wave = uint32_t(std::min<size_t>(slots_fit / npix, count));
+        if (pf->wave_samples) wave = std::min(wave, pf->wave_samples);
+        wave = std::max(1u, wave);
+        size_t slots = size_t(npix) * wave;
+        PathParams p{};
+        p.ray_o[0] = cv.take<float4>(slots); p.ray_d[0] = cv.take<float4>(slots);
+        p.ray_o[1] = cv.take<float4>(slots); p.ray_d[1] = cv.take<float4>(slots);
+        p.hit = cv.take<float4>(slots); p.hit_inst = cv.take<uint32_t>(slots);
+        p.thr = cv.take<float4>(slots); p.rad = cv.take<float4>(slots); p.rng = cv.take<uint2>(slots);
+        p.sa_o = cv.take<float4>(slots); p.sa_d = cv.take<float4>(slots); p.sa_c = cv.take<float4>(slots);
+        p.sb_o = cv.take<float4>(slots); p.sb_d = cv.take<float4>(slots); p.sb_c = cv.take<float4>(slots);
+        if (!p.sb_c) throw ArgError{"vkb_render_noalloc: scratch layout overflow"};
+        // The array keeps the previous call's contents: clear what must start at zero.
+        VKB_CUDA(cudaMemsetAsync(accum, 0, npix * sizeof(float4), st));
+        VKB_CUDA(cudaMemsetAsync(counters, 0, 16 * sizeof(uint32_t), st));
+        VKB_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), st));
+        VKB_CUDA(cudaMemsetAsync(work, 0, 8 * sizeof(unsigned long long), st));
+        p.sv = scene_view(s);
+        p.o2w = s->o2w.p; p.w2o = s->w2o.p; p.inst_info = s->inst_info.p; p.meshes = s->meshes.p;
+        p.vpos = s->vpos.p; p.vnrm = s->vnrm.p; p.indices = s->indices.p;
+        p.materials = s->d_materials.p; p.lights = s->d_lights.p; p.num_lights = uint32_t(s->lights.size());
+        p.tree = s->tree.p; p.tree_nodes = s->tree_nodes;
+        p.lut.texels = c->lut.p; p.filter = c->filter.p;
+        p.cam = s->camera; p.env = s->env;
+        p.spp = pf->samples; p.seed = pf->seed;
+        for (int k = 0; k < 4; ++k) p.bounces[k] = pf->bounces[k];
+        p.caustics = pf->caustics;
+        p.sample_mask = pf->samples <= 1 ? 0u : ((2u << (31 - __builtin_clz(pf->samples - 1u))) - 1u);
+        p.clamp_direct = pf->clamp_direct; p.clamp_indirect = pf->clamp_indirect; p.light_threshold = pf->light_threshold;
+        p.npix = npix; p.first_sample = pf->first_sample;
+        p.accum = accum; p.counters = counters; p.err = err; p.work = work;
+        p.primary_ids = ids;
+        uint32_t launches = 0;
+        const bool counted = (pf->flags & VKB_PROFILE_COUNT_TRAVERSAL) != 0;
+        for (uint32_t done = 0; done < count; done += wave) {
+            uint32_t ws = std::min(wave, count - done);
+            p.wave_first = pf->first_sample + done;
+            p.wave_samples = ws;
+            p.n_paths = npix * ws;
+            k_set_count<<<1, 1, 0, st>>>(counters, p.n_paths);
+            k_camera<<<grid_for(p.n_paths, 256, sms), 256, 0, st>>>(p);
+            const int tgrid = sms * 16, sgrid = sms * 16;
+            for (uint32_t b = 0; b <= pf->bounces[0]; ++b) {
+                int cur = int(b & 1u);
+                if (counted) k_trace<false, true><<<tgrid, 128, 0, st>>>(p, cur);
+                else k_trace<false, false><<<tgrid, 128, 0, st>>>(p, cur);
+                k_reset_queues<<<1, 1, 0, st>>>(counters, cur ^ 1);
+                k_shade<<<sgrid, 128, 0, st>>>(p, cur);
+                if (counted) k_trace<true, true><<<tgrid, 128, 0, st>>>(p, -1);
+                else k_trace<true, false><<<tgrid, 128, 0, st>>>(p, -1);
+                launches += 4;
+            }
+            k_accumulate<<<grid_for(npix, 256, sms), 256, 0, st>>>(p);
+            launches += 3;
+            VKB_CUDA(cudaGetLastError());
+        }
+        k_resolve<<<grid_for(npix, 256, sms), 256, 0, st>>>(npix, accum, staging);
+        launches += 1;
+        s->launches += launches;
+        if (!out->on_device) VKB_CUDA(cudaMemcpyAsync(out->rgba, staging, npix * sizeof(float4), cudaMemcpyDeviceToHost, st));
+        if (out->primary_ids) VKB_CUDA(cudaMemcpyAsync(out->primary_ids, ids, size_t(npix) * 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        uint32_t ctr[16], e = 0;
+        unsigned long long wk[8];
+        VKB_CUDA(cudaMemcpyAsync(ctr, counters, sizeof(ctr), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaMemcpyAsync(&e, err, sizeof(e), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaMemcpyAsync(wk, work, sizeof(wk), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaStreamSynchronize(st));
+        if (stats) {
+            std::memset(stats, 0, sizeof(*stats));
+            stats->paths = uint64_t(npix) * count;
+            stats->extension_rays = ctr[3];
+            stats->shadow_rays = ctr[4];
+            stats->dropped_light_samples = ctr[5];
+            stats->dropped_path_samples = ctr[6];
+            stats->traversal_overflows = e;
+            stats->kernel_launches = launches;
+            stats->nodes_visited = wk[0]; stats->triangles_tested = wk[1]; stats->instances_entered = wk[2];
+            stats->shadow_nodes_visited = wk[3]; stats->shadow_triangles_tested = wk[4];
+        }
+    });
+}

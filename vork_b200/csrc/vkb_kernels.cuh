@@ -581,6 +581,8 @@ __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
         if (push_shadow) { p.sa_o[si] = sh_o; p.sa_d[si] = sh_d; p.sa_c[si] = sh_c; }
     }
 }
+// Seed the first ray queue's count (the no-alloc render, whose counters live in device scratch).
+__global__ void k_set_count(uint32_t* counters, uint32_t n) { counters[0] = n; }
 // Zero the next ray queue and the shadow queue before a shade pass.
 __global__ void k_reset_queues(uint32_t* counters, int nxt) { counters[nxt] = 0u; counters[2] = 0u; }
 // resolve.slang:162-191: add this wave's finished samples to the accumulator.
