@@ -322,7 +322,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
             "work": {k: counted[k] for k in ("extension_rays", "shadow_rays", "nodes_visited", "triangles_tested",
-                                             "instances_entered", "shadow_nodes_visited", "shadow_triangles_tested",
+                                             "instances_entered", "blas_nodes_visited", "shadow_nodes_visited", "shadow_triangles_tested",
                                              "traversal_overflows", "dropped_path_samples")},
         }
         if not args.no_cpu_baseline:

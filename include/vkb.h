@@ -171,6 +171,7 @@ typedef struct vkb_stats {
     uint64_t instances_entered;/* closest-hit TLAS leaf (instance) entries */
     uint64_t shadow_nodes_visited;
     uint64_t shadow_triangles_tested;
+    uint64_t blas_nodes_visited;   /* closest-hit node visits inside instance BLASes (the rest are TLAS) */
 } vkb_stats;
 
 typedef struct vkb_ctx vkb_ctx;

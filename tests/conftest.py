@@ -33,6 +33,6 @@ def renderer():
 
 
 @pytest.fixture(scope="session")
-def c0_scene():
+def small_scene():
     from vork_b200 import scene
     return scene.spheres_scene()

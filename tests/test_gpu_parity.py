@@ -37,20 +37,20 @@ def test_brdf_atlas_matches_known_texels_and_oracle(renderer, oracle):
     assert np.all(np.abs(lut - ref) <= 2e-3 * np.abs(ref) + 2e-4), float(np.abs(lut - ref).max())
 
 
-def test_morton_codes_bit_exact(renderer, oracle, c0_scene):
-    o = oracle.OracleScene(c0_scene)
-    with renderer.install(c0_scene) as s:
+def test_morton_codes_bit_exact(renderer, oracle, small_scene):
+    o = oracle.OracleScene(small_scene)
+    with renderer.install(small_scene) as s:
         assert np.array_equal(s.tlas_morton(), o.tlas_morton())
-        for m in range(len(c0_scene.meshes)):
+        for m in range(len(small_scene.meshes)):
             assert np.array_equal(s.blas_morton(m), o.blas_morton(m)), m
 
 
-def test_primary_ids_match_oracle(renderer, oracle, c0_scene):
-    o = oracle.OracleScene(c0_scene)
+def test_primary_ids_match_oracle(renderer, oracle, small_scene):
+    o = oracle.OracleScene(small_scene)
     prof = Profile.reference_transport(4, 16)
     rays = o.camera_rays(prof.c(), index=0)
     t_ref, ids_ref, _ = o.trace(rays, fp64=True)
-    with renderer.install(c0_scene) as s:
+    with renderer.install(small_scene) as s:
         t, ids, _ = s.trace(rays)
         mismatch = np.any(ids != ids_ref, axis=1)
         assert mismatch.mean() <= 1e-4, int(mismatch.sum())
@@ -63,32 +63,32 @@ def test_primary_ids_match_oracle(renderer, oracle, c0_scene):
         assert res.stats["traversal_overflows"] == 0
 
 
-def test_random_rays_closest_and_any_hits(renderer, oracle, c0_scene):
-    o = oracle.OracleScene(c0_scene)
+def test_random_rays_closest_and_any_hits(renderer, oracle, small_scene):
+    o = oracle.OracleScene(small_scene)
     rng = np.random.default_rng(11)
     n = 20000
     org = rng.uniform(-2, 12, (n, 3))
     d = rng.normal(size=(n, 3)); d /= np.linalg.norm(d, axis=1, keepdims=True)
     rays = np.concatenate([org, d, np.full((n, 1), 1e30)], 1).astype(np.float32)
     t_ref, ids_ref, _ = o.trace(rays, fp64=True)
-    with renderer.install(c0_scene) as s:
+    with renderer.install(small_scene) as s:
         t, ids, _ = s.trace(rays)
     mismatch = np.any(ids != ids_ref, axis=1)
     assert mismatch.mean() <= 2e-3, int(mismatch.sum())
 
 
-def _c0_profile(spp=16, **kw):
+def _small_profile(spp=16, **kw):
     return Profile.reference_transport(4, spp, **kw)
 
 
-def test_render_matches_fp64_oracle(renderer, oracle, c0_scene):
+def test_render_matches_fp64_oracle(renderer, oracle, small_scene):
     # Same sampler bits per sample: per-pixel agreement on most pixels, and the image
     # mean within 1% (BASELINE tolerance) of the FP64 restatement.
-    o = oracle.OracleScene(c0_scene)
-    prof = _c0_profile(16)
+    o = oracle.OracleScene(small_scene)
+    prof = _small_profile(16)
     x0, y0, w, h = 96, 96, 64, 64
     ref, st_ref = o.render(prof.c(), x0, y0, w, h, fp64=True)
-    with renderer.install(c0_scene) as s:
+    with renderer.install(small_scene) as s:
         res = s.render(prof)
     img = res.image[y0:y0 + h, x0:x0 + w]
     assert np.isfinite(res.image).all() and res.stats["dropped_path_samples"] == 0
@@ -99,11 +99,11 @@ def test_render_matches_fp64_oracle(renderer, oracle, c0_scene):
     assert res.stats["traversal_overflows"] == 0
 
 
-def test_full_image_matches_fp32_oracle_at_low_spp(renderer, oracle, c0_scene):
-    o = oracle.OracleScene(c0_scene)
-    prof = _c0_profile(16, sample_count=2)
+def test_full_image_matches_fp32_oracle_at_low_spp(renderer, oracle, small_scene):
+    o = oracle.OracleScene(small_scene)
+    prof = _small_profile(16, sample_count=2)
     ref, _ = o.render(prof.c(), fp64=False)
-    with renderer.install(c0_scene) as s:
+    with renderer.install(small_scene) as s:
         img = s.render(prof).image
     m_gpu, m_ref = img[..., :3].mean((0, 1)), ref[..., :3].mean((0, 1))
     assert np.all(np.abs(m_gpu / m_ref - 1) < 0.01), (m_gpu, m_ref)
@@ -127,28 +127,28 @@ def test_white_diffuse_under_coloured_environment(renderer):
     assert np.allclose(mean, [1.0, 0.75, 0.5], rtol=1e-5), mean
 
 
-def test_deterministic_across_waves_and_runs(renderer, c0_scene):
-    with renderer.install(c0_scene) as s:
-        a = s.render(_c0_profile(8)).image
-        b = s.render(_c0_profile(8)).image
-        c = s.render(_c0_profile(8, wave_samples=1)).image
-        d = s.render(_c0_profile(8, wave_samples=3)).image
+def test_deterministic_across_waves_and_runs(renderer, small_scene):
+    with renderer.install(small_scene) as s:
+        a = s.render(_small_profile(8)).image
+        b = s.render(_small_profile(8)).image
+        c = s.render(_small_profile(8, wave_samples=1)).image
+        d = s.render(_small_profile(8, wave_samples=3)).image
         assert np.array_equal(a, b) and np.array_equal(a, c) and np.array_equal(a, d)
         # Resume: samples [0,4) + [4,8) equal [0,8).
-        h0 = s.render(_c0_profile(8, first_sample=0, sample_count=4)).image
-        h1 = s.render(_c0_profile(8, first_sample=4, sample_count=4)).image
+        h0 = s.render(_small_profile(8, first_sample=0, sample_count=4)).image
+        h1 = s.render(_small_profile(8, first_sample=4, sample_count=4)).image
         assert np.allclose((h0 + h1) / 2, a, rtol=1e-5, atol=1e-6)
 
 
-def test_update_instances_equals_fresh_install(renderer, c0_scene):
+def test_update_instances_equals_fresh_install(renderer, small_scene):
     moved = S.spheres_scene()
-    moved.instance_rows = c0_scene.instance_rows.copy()
+    moved.instance_rows = small_scene.instance_rows.copy()
     moved.instance_rows[:64, 1, 3] += 0.5
-    with renderer.install(c0_scene) as s:
+    with renderer.install(small_scene) as s:
         s.update_instances(moved.instance_rows)
-        a = s.render(_c0_profile(4)).image
+        a = s.render(_small_profile(4)).image
     with renderer.install(moved) as s2:
-        b = s2.render(_c0_profile(4)).image
+        b = s2.render(_small_profile(4)).image
     assert np.array_equal(a, b)
 
 

@@ -80,7 +80,8 @@ class VkbStats(C.Structure):
                 ("traversal_overflows", C.c_uint64), ("render_ms", C.c_float), ("build_ms", C.c_float),
                 ("trace_ms", C.c_float), ("trace_launches", C.c_uint32), ("kernel_launches", C.c_uint32),
                 ("nodes_visited", C.c_uint64), ("triangles_tested", C.c_uint64), ("instances_entered", C.c_uint64),
-                ("shadow_nodes_visited", C.c_uint64), ("shadow_triangles_tested", C.c_uint64)]
+                ("shadow_nodes_visited", C.c_uint64), ("shadow_triangles_tested", C.c_uint64),
+                ("blas_nodes_visited", C.c_uint64)]
 
 
 # Every symbol include/vkb.h declares, with its ctypes signature.

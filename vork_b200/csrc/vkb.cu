@@ -209,6 +209,9 @@ struct vkb_scene {
     DBuf<uint4> inst_info;
     DBuf<MeshInfo> meshes;
     DBuf<BvhNode> blas_nodes, tlas_nodes;
+    DBuf<WideNode> blas_wide, tlas_wide;
+    DBuf<uint2> collapse_work;
+    DBuf<uint32_t> collapse_counts;
     DBuf<TlasLeaf> tlas_leaves;
     DBuf<vkb_material> d_materials;
     DBuf<vkb_light> d_lights;
@@ -248,7 +251,26 @@ SceneView scene_view(const vkb_scene* s) {
     v.tlas_nodes = s->tlas_nodes.p; v.tlas_leaves = s->tlas_leaves.p;
     v.blas_nodes = s->blas_nodes.p; v.blas_tris = s->blas_tris.p;
     v.num_instances = s->num_instances;
+    v.tlas_wide = s->tlas_wide.p; v.blas_wide = s->blas_wide.p;
     return v;
+}
+
+// Collapse a binary LBVH of n primitives into the 8-wide BVH at `wide` (root at 0):
+// 64 levels back to back, each reading the previous level's work list on the device.
+void collapse(vkb_scene* s, const BvhNode* bin, uint32_t n, WideNode* wide) {
+    if (n == 0) return;
+    cudaStream_t st = s->ctx->stream;
+    s->collapse_work.alloc(3 * size_t(std::max(1u, n)));
+    s->collapse_counts.alloc(4);
+    uint2* w[3] = {s->collapse_work.p, s->collapse_work.p + n, s->collapse_work.p + 2 * size_t(n)};
+    uint32_t* c = s->collapse_counts.p;
+    VKB_CUDA(cudaMemsetAsync(c, 0, 4 * sizeof(uint32_t), st));
+    k_collapse_seed<<<1, 1, 0, st>>>(w[0], &c[0], &c[3]);
+    int grid = std::max(1, std::min(s->ctx->sms * 4, int((n + 127) / 128)));
+    for (int level = 0; level < 64; ++level)
+        k_collapse<<<grid, 128, 0, st>>>(bin, wide, w[level % 3], &c[level % 3], w[(level + 1) % 3], &c[(level + 1) % 3], &c[3], &c[(level + 2) % 3]);
+    s->launches += 65;
+    VKB_CUDA(cudaGetLastError());
 }
 
 // Instance rows -> w2o, world boxes, TLAS (LBVH) and its leaf records.
@@ -260,6 +282,7 @@ void build_tlas(vkb_scene* s) {
     VKB_CUDA(cudaEventRecord(s->ev0, st));
     k_instances<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->o2w.p, s->inst_info.p, s->meshes.p, s->w2o.p, s->inst_lo.p, s->inst_hi.p);
     build_lbvh(n, s->inst_lo.p, s->inst_hi.p, s->tlas_nodes.p, s->scratch, st, sms, s->launches);
+    if (VKB_WIDE_BVH) collapse(s, s->tlas_nodes.p, n, s->tlas_wide.p);
     s->launches += 2;
     k_tlas_leaves<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->scratch.ids_sorted.p, s->w2o.p, s->inst_info.p, s->meshes.p, s->d_materials.p, s->tlas_leaves.p);
     VKB_CUDA(cudaMemcpyAsync(s->tlas_codes.p, s->scratch.codes.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
@@ -376,6 +399,7 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         uint32_t node_total = 0;
         for (auto& mi : s->mesh_info) { mi.node_offset = node_total; node_total += std::max(1u, mi.num_triangles > 1 ? mi.num_triangles - 1u : 1u); }
         s->blas_nodes.alloc(std::max(1u, node_total));
+        s->blas_wide.alloc(std::max(1u, node_total));
         s->blas_tris.alloc(std::max<size_t>(1, size_t(nt) * 3));
         uint32_t max_tris = 0;
         for (auto& mi : s->mesh_info) max_tris = std::max(max_tris, mi.num_triangles);
@@ -389,6 +413,7 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
             const float4* mpos = s->vpos.p + mi.vertex_offset;
             k_tri_boxes<<<grid_for(mi.num_triangles, 256, sms), 256, 0, str>>>(mi.num_triangles, mid, mpos, s->tri_lo.p, s->tri_hi.p);
             build_lbvh(mi.num_triangles, s->tri_lo.p, s->tri_hi.p, s->blas_nodes.p + mi.node_offset, s->scratch, str, sms, s->launches);
+            if (VKB_WIDE_BVH) collapse(s, s->blas_nodes.p + mi.node_offset, mi.num_triangles, s->blas_wide.p + mi.node_offset);
             s->launches += 2;
             k_sorted_tris<<<grid_for(mi.num_triangles, 256, sms), 256, 0, str>>>(mi.num_triangles, s->scratch.ids_sorted.p, mid, mpos, s->blas_tris.p + 3 * size_t(mi.tri_offset));
         }
@@ -415,6 +440,7 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         s->w2o.alloc(size_t(n) * 3);
         s->inst_lo.alloc(n); s->inst_hi.alloc(n);
         s->tlas_nodes.alloc(std::max(1u, n > 1 ? n - 1 : 1u));
+        s->tlas_wide.alloc(std::max(1u, n > 1 ? n - 1 : 1u));
         s->tlas_leaves.alloc(std::max(1u, n));
         s->tlas_codes.alloc(std::max(1u, n));
         VKB_CUDA(cudaStreamSynchronize(str));
@@ -437,7 +463,8 @@ vkb_status vkb_scene_destroy(vkb_scene* s) {
                           &s->sb_o, &s->sb_d, &s->sb_c, &s->accum, &s->out_rgba};
     for (auto* b : f4) b->release();
     s->indices.release(); s->tlas_codes.release(); s->inst_info.release(); s->meshes.release();
-    s->blas_nodes.release(); s->tlas_nodes.release(); s->tlas_leaves.release(); s->d_materials.release(); s->d_lights.release();
+    s->blas_nodes.release(); s->tlas_nodes.release(); s->blas_wide.release(); s->tlas_wide.release();
+    s->collapse_work.release(); s->collapse_counts.release(); s->tlas_leaves.release(); s->d_materials.release(); s->d_lights.release();
     s->tree.release(); s->hit_inst.release(); s->counters.release(); s->err.release(); s->ids.release(); s->rng.release(); s->work.release();
     for (cudaEvent_t e : s->kernel_events) cudaEventDestroy(e);
     s->scratch.codes.release(); s->scratch.codes_sorted.release(); s->scratch.ids.release(); s->scratch.ids_sorted.release();
@@ -596,6 +623,7 @@ vkb_status vkb_render(vkb_scene* s, const vkb_profile* pf, vkb_output* out, vkb_
             stats->instances_entered = work[2];
             stats->shadow_nodes_visited = work[3];
             stats->shadow_triangles_tested = work[4];
+            stats->blas_nodes_visited = work[5];
         }
     });
 }

@@ -30,6 +30,17 @@ struct MeshInfo {
 };
 
 constexpr int TRACE_STACK = 64;
+#ifndef VKB_SMEM_STACK
+#define VKB_SMEM_STACK 48
+#endif
+#ifndef VKB_POP_CULL
+#define VKB_POP_CULL 0
+#endif
+// Traversal stacks live in shared memory as [entry][thread]: lane l of a 128-thread
+// block always touches bank l, whatever depth each lane is at (no bank conflicts).
+constexpr int SMEM_STACK = VKB_SMEM_STACK;
+constexpr int TRACE_BLOCK = 128;
+struct TraceStack { int* r; float* t; };
 constexpr uint32_t TRACE_STEP_LIMIT = 1u << 16;
 constexpr int SENTINEL = 0x7fffffff;
 
@@ -126,39 +137,39 @@ __device__ __forceinline__ bool tri_test(const RaySpace& r, float3 v0, float3 v1
 
 struct HitRecord { float t, u, v; uint32_t prim, inst; };
 
+struct WideNode;
 struct SceneView {
     const BvhNode* tlas_nodes;
     const TlasLeaf* tlas_leaves;
     const BvhNode* blas_nodes;
     const float4* blas_tris;     // 3 per triangle (Morton order within a mesh); v0.w = original triangle id
     uint32_t num_instances;
+    const WideNode* tlas_wide;   // 8-wide collapse of tlas_nodes (traversed by the renders)
+    const WideNode* blas_wide;   // 8-wide collapse of every BLAS, same per-mesh offsets as blas_nodes
 };
 
 // Traversal work of one ray (instrumented builds only): node visits, triangle tests, instance entries.
-struct TraceCount { uint32_t nodes = 0, tris = 0, instances = 0; };
+struct TraceCount { uint32_t nodes = 0, tris = 0, instances = 0, blas_nodes = 0; };
 
 // Closest hit (any == false) or first hit (any == true) of a world ray over the
 // two-level BVH.  Error: overflow/step-limit exits set *err and return the best so far.
 template <bool ANY, bool COUNT = false>
 __device__ __forceinline__ bool trace_ray(const SceneView& s, float3 o, float3 d, float tmax, HitRecord& hit, uint32_t* err,
-                                          TraceCount* count = nullptr) {
-    RaySpace ws, rs;
-    make_space(ws, o, d);
-    rs = ws;
-    int stack[TRACE_STACK];
+                                          TraceCount* count, TraceStack stk) {
+    RaySpace rs;
+    make_space(rs, o, d);
     int sp = 0;
     float tbest = tmax;
-    bool found = false, in_blas = false;
+    bool found = false, in_blas = false, cull = false;
     const BvhNode* nodes = s.tlas_nodes;
     const float4* tris = s.blas_tris;
     uint32_t tri_base = 0, cur_instance = 0;
-    bool cull = false;
     int node = 0;
     if (s.num_instances == 0) return false;
     for (uint32_t steps = 0;; ++steps) {
         if (steps >= TRACE_STEP_LIMIT) { atomicOr(err, 2u); break; }
         if (node >= 0) {
-            if (COUNT) count->nodes++;
+            if (COUNT) { count->nodes++; if (in_blas) count->blas_nodes++; }
             BvhNode n;
             const float4* p = reinterpret_cast<const float4*>(nodes + node);
             n.a = __ldg(p); n.b = __ldg(p + 1); n.c = __ldg(p + 2);
@@ -167,10 +178,12 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, float3 o, float3 d
             node_boxes(n, rs, tbest, tl, tr);
             bool hl = tl != __int_as_float(0x7f800000), hr = tr != __int_as_float(0x7f800000);
             if (hl && hr) {
-                int nearer = tl <= tr ? n.d.x : n.d.y, farther = tl <= tr ? n.d.y : n.d.x;
-                if (sp >= TRACE_STACK) { atomicOr(err, 1u); break; }
-                stack[sp++] = farther;
-                node = nearer;
+                bool lfirst = tl <= tr;
+                if (sp >= SMEM_STACK) { atomicOr(err, 1u); break; }
+                stk.r[sp * TRACE_BLOCK] = lfirst ? n.d.y : n.d.x;
+                if (VKB_POP_CULL) stk.t[sp * TRACE_BLOCK] = lfirst ? tr : tl;
+                ++sp;
+                node = lfirst ? n.d.x : n.d.y;
                 continue;
             }
             if (hl) { node = n.d.x; continue; }
@@ -187,8 +200,10 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, float3 o, float3 d
             nodes = s.blas_nodes + info.y;
             tri_base = info.z;
             cull = !ANY && (info.w & LEAF_CULL_BACKFACES);
-            if (sp >= TRACE_STACK) { atomicOr(err, 1u); break; }
-            stack[sp++] = SENTINEL;
+            if (sp >= SMEM_STACK) { atomicOr(err, 1u); break; }
+            stk.r[sp * TRACE_BLOCK] = SENTINEL;
+            if (VKB_POP_CULL) stk.t[sp * TRACE_BLOCK] = 0.f;
+            ++sp;
             in_blas = true;
             node = 0;
             continue;
@@ -203,14 +218,18 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, float3 o, float3 d
                 if (ANY) return true;
             }
         }
-        // pop
+        // pop (with VKB_POP_CULL, an entry farther than the closest hit so far is skipped without a fetch)
         for (;;) {
             if (sp == 0) return found;
-            node = stack[--sp];
-            if (node != SENTINEL) break;
-            in_blas = false;
-            rs = ws;
-            nodes = s.tlas_nodes;
+            --sp;
+            node = stk.r[sp * TRACE_BLOCK];
+            if (node == SENTINEL) {
+                in_blas = false;
+                make_space(rs, o, d);
+                nodes = s.tlas_nodes;
+                continue;
+            }
+            if (!VKB_POP_CULL || stk.t[sp * TRACE_BLOCK] <= tbest) break;
         }
     }
     return found;

@@ -4,6 +4,7 @@
 #include <cstdint>
 #include "vkb_device.cuh"
 #include "vkb_bvh.cuh"
+#include "vkb_wide.cuh"
 
 namespace vkb {
 
@@ -292,8 +293,30 @@ __device__ __forceinline__ void flush_count(unsigned long long* dst, uint32_t v)
     for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
     if ((threadIdx.x & 31u) == 0u && x) atomicAdd(dst, x);
 }
+#ifndef VKB_WIDE_BVH
+#define VKB_WIDE_BVH 0
+#endif
+#ifndef VKB_TRACE_MIN_BLOCKS
+#define VKB_TRACE_MIN_BLOCKS 8
+#endif
+// The traversal the renders use: binary (BVH2) or 8-wide.
 template <bool ANY, bool COUNT>
-__global__ void __launch_bounds__(128) k_trace(PathParams p, int cur) {
+__device__ __forceinline__ bool trace_any(const SceneView& sv, float3 o, float3 d, float tmax, HitRecord& h, uint32_t* err, TraceCount* tc,
+                                          TraceStack stk) {
+#if VKB_WIDE_BVH
+    return trace_wide<ANY, COUNT>(sv.tlas_wide, sv.tlas_leaves, sv.blas_wide, sv.blas_tris, sv.num_instances, o, d, tmax, h, err, tc, stk);
+#else
+    return trace_ray<ANY, COUNT>(sv, o, d, tmax, h, err, tc, stk);
+#endif
+}
+// This thread's column of the block's shared-memory traversal stack.
+#define VKB_STACK_DECL                                                                                   \
+    __shared__ int stack_r_[SMEM_STACK * TRACE_BLOCK];                                                  \
+    __shared__ float stack_t_[(VKB_WIDE_BVH || VKB_POP_CULL) ? SMEM_STACK * TRACE_BLOCK : 1];          \
+    TraceStack stk{stack_r_ + threadIdx.x, stack_t_ + ((VKB_WIDE_BVH || VKB_POP_CULL) ? threadIdx.x : 0)};
+template <bool ANY, bool COUNT>
+__global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace(PathParams p, int cur) {
+    VKB_STACK_DECL
     uint32_t n = cur < 0 ? p.counters[2] : p.counters[cur];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (ANY) atomicAdd(&p.counters[4], n);
@@ -306,7 +329,7 @@ __global__ void __launch_bounds__(128) k_trace(PathParams p, int cur) {
         if (!ANY) {
             float4 ro = p.ray_o[cur][i], rd = p.ray_d[cur][i];
             HitRecord h;
-            bool found = trace_ray<false, COUNT>(p.sv, f3(ro.x, ro.y, ro.z), f3(rd.x, rd.y, rd.z), ro.w, h, p.err, &tc);
+            bool found = trace_any<false, COUNT>(p.sv, f3(ro.x, ro.y, ro.z), f3(rd.x, rd.y, rd.z), ro.w, h, p.err, &tc, stk);
             p.hit[i] = found ? make_float4(h.t, h.u, h.v, __uint_as_float(h.prim)) : make_float4(-1.f, 0.f, 0.f, __uint_as_float(0xffffffffu));
             p.hit_inst[i] = found ? h.inst : 0xffffffffu;
         } else {
@@ -314,13 +337,13 @@ __global__ void __launch_bounds__(128) k_trace(PathParams p, int cur) {
             uint32_t slot = __float_as_uint(sd.w), flags = __float_as_uint(sc.w);
             HitRecord h;
             float3 total = f3(sc.x, sc.y, sc.z);
-            if ((flags & SH_TRACE_A) && trace_ray<true, COUNT>(p.sv, f3(so.x, so.y, so.z), f3(sd.x, sd.y, sd.z), so.w, h, p.err, &tc)) total = f3(0.f);
+            if ((flags & SH_TRACE_A) && trace_any<true, COUNT>(p.sv, f3(so.x, so.y, so.z), f3(sd.x, sd.y, sd.z), so.w, h, p.err, &tc, stk)) total = f3(0.f);
             if (flags & SH_HAS_B) {
                 float4 bc = p.sb_c[slot];
                 float3 cb = f3(bc.x, bc.y, bc.z);
                 if (flags & SH_TRACE_B) {
                     float4 bo = p.sb_o[slot], bd = p.sb_d[slot];
-                    if (trace_ray<true, COUNT>(p.sv, f3(bo.x, bo.y, bo.z), f3(bd.x, bd.y, bd.z), bo.w, h, p.err, &tc)) cb = f3(0.f);
+                    if (trace_any<true, COUNT>(p.sv, f3(bo.x, bo.y, bo.z), f3(bd.x, bd.y, bd.z), bo.w, h, p.err, &tc, stk)) cb = f3(0.f);
                 }
                 total = total + cb;
             }
@@ -335,6 +358,7 @@ __global__ void __launch_bounds__(128) k_trace(PathParams p, int cur) {
         flush_count(&p.work[ANY ? 3 : 0], tc.nodes);
         flush_count(&p.work[ANY ? 4 : 1], tc.tris);
         if (!ANY) flush_count(&p.work[2], tc.instances);
+        flush_count(&p.work[ANY ? 6 : 5], tc.blas_nodes);
     }
 }
 
@@ -619,11 +643,12 @@ __global__ void k_sampler_groups(uint32_t n, const uint32_t* px, const uint32_t*
     }
 }
 // Test entry: closest hits of arbitrary world rays.
-__global__ void k_debug_trace(SceneView sv, uint32_t n, const float* rays, float* t, uint32_t* ids, float* uv, uint32_t* err) {
+__global__ void __launch_bounds__(TRACE_BLOCK) k_debug_trace(SceneView sv, uint32_t n, const float* rays, float* t, uint32_t* ids, float* uv, uint32_t* err) {
+    VKB_STACK_DECL
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float* r = rays + 7 * i;
         HitRecord h;
-        bool f = trace_ray<false>(sv, f3(r[0], r[1], r[2]), f3(r[3], r[4], r[5]), r[6], h, err);
+        bool f = trace_any<false, false>(sv, f3(r[0], r[1], r[2]), f3(r[3], r[4], r[5]), r[6], h, err, nullptr, stk);
         t[i] = f ? h.t : -1.f;
         ids[2 * i] = f ? h.inst : 0xffffffffu; ids[2 * i + 1] = f ? h.prim : 0xffffffffu;
         uv[2 * i] = f ? h.u : 0.f; uv[2 * i + 1] = f ? h.v : 0.f;
