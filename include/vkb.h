@@ -192,8 +192,10 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* desc, vkb_scene*
 vkb_status vkb_scene_destroy(vkb_scene* scene);
 
 /* rt::encode / rebuild_tlas (rt.rs:1387-1476): new object->world rows for every
- * instance (host pointer, num_instances*12 floats). policy 0: refit-vs-rebuild by the
- * reference's quarter-of-the-bytes rule, 1: always rebuild, 2: always refit. */
+ * instance (host pointer, num_instances*12 floats). policy 0: refit, or rebuild once
+ * the changed object bytes accumulated since the last rebuild reach a quarter of the
+ * object buffer (the reference's rule); 1: always rebuild; 2: always refit (the
+ * topology of the last rebuild is kept; boxes and matrices are replaced). */
 vkb_status vkb_scene_update_instances(vkb_scene* scene, const float* rows, uint32_t num_instances, int policy);
 /* The same with rows already in device memory of the context's GPU (no host copy). */
 vkb_status vkb_scene_update_instances_device(vkb_scene* scene, const float* device_rows, uint32_t num_instances, int policy);
@@ -202,6 +204,20 @@ vkb_status vkb_scene_update_instances_device(vkb_scene* scene, const float* devi
  * samples [first_sample, first_sample+sample_count) of `profile` and writes the mean
  * over them. stats may be NULL. */
 vkb_status vkb_render(vkb_scene* scene, const vkb_profile* profile, vkb_output* out, vkb_stats* stats);
+
+/* Installed-scene facts: sizes, device bytes of the scene structures, and the TLAS
+ * update history of vkb_scene_update_instances (rebuilds vs refits, rt.rs:1465-1476). */
+typedef struct vkb_scene_info_t {
+    uint64_t num_instances;
+    uint64_t num_triangles;
+    uint64_t scene_bytes;      /* device bytes of meshes, BLAS, TLAS and instance records */
+    uint64_t tlas_rebuilds;
+    uint64_t tlas_refits;
+    uint64_t motion_bytes;     /* changed object bytes accumulated since the last rebuild */
+    float build_ms;            /* device time of the last TLAS build or refit */
+    uint32_t reserved;
+} vkb_scene_info_t;
+vkb_status vkb_scene_info(vkb_scene* scene, vkb_scene_info_t* out);
 
 /* The CUDA stream (cudaStream_t) every kernel of this context is launched on, so a
  * caller can record its own events on it. */

@@ -172,3 +172,30 @@ def test_tiny_scenes_and_errors(renderer):
     with pytest.raises(abi.VkbError) as e:
         renderer.install(bad)
     assert e.value.status == abi.VKB_INVALID_ARG
+
+
+def test_tlas_refit_matches_rebuild_and_follows_the_quarter_rule(renderer, small_scene):
+    # rt.rs:1465-1476: refit until the changed object bytes reach a quarter of the object buffer.
+    rows = small_scene.instance_rows.copy()
+    with renderer.install(small_scene) as s:
+        base = s.info()
+        few = rows.copy(); few[:8, 1, 3] += 0.05                  # 8 of 65 rows: below a quarter -> refit
+        s.update_instances(few, policy=0)
+        i1 = s.info()
+        assert i1["tlas_refits"] == base["tlas_refits"] + 1 and i1["tlas_rebuilds"] == base["tlas_rebuilds"]
+        refit_img = s.render(_small_profile(4)).image
+        s.update_instances(few, policy=1)                         # same rows, forced rebuild
+        rebuilt_img = s.render(_small_profile(4)).image
+        assert np.array_equal(refit_img, rebuilt_img)
+        more = few.copy(); more[8:25, 1, 3] += 0.05               # 17 rows since the forced rebuild: >= 1/4 -> rebuild
+        s.update_instances(more, policy=0)
+        i2 = s.info()
+        assert i2["tlas_rebuilds"] == i1["tlas_rebuilds"] + 2 and i2["motion_bytes"] == 0
+        s.update_instances(more, policy=0)                        # nothing changed: no work
+        assert s.info()["tlas_refits"] == i2["tlas_refits"]
+        big = more.copy(); big[:, 1, 3] += 0.3
+        s.update_instances(big, policy=2)                         # forced refit after large motion
+        a = s.render(_small_profile(4)).image
+        s.update_instances(big, policy=1)
+        b = s.render(_small_profile(4)).image
+        assert np.array_equal(a, b)

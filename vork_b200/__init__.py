@@ -135,6 +135,11 @@ class InstalledScene:
     def update_instances_device(self, device_ptr: int, count: int, policy: int = 0):
         abi.check(self.r.lib.vkb_scene_update_instances_device(self.h, C.c_void_p(device_ptr), count, policy))
 
+    def info(self) -> dict:
+        i = abi.VkbSceneInfo()
+        abi.check(self.r.lib.vkb_scene_info(self.h, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in abi.VkbSceneInfo._fields_ if k != "reserved"}
+
     @property
     def launch_count(self) -> int:
         return int(self.r.lib.vkb_scene_launch_count(self.h))

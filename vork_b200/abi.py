@@ -84,6 +84,12 @@ class VkbStats(C.Structure):
                 ("blas_nodes_visited", C.c_uint64)]
 
 
+class VkbSceneInfo(C.Structure):
+    _fields_ = [("num_instances", C.c_uint64), ("num_triangles", C.c_uint64), ("scene_bytes", C.c_uint64),
+                ("tlas_rebuilds", C.c_uint64), ("tlas_refits", C.c_uint64), ("motion_bytes", C.c_uint64),
+                ("build_ms", C.c_float), ("reserved", C.c_uint32)]
+
+
 # Every symbol include/vkb.h declares, with its ctypes signature.
 _P = C.c_void_p
 SIGNATURES = {
@@ -97,6 +103,7 @@ SIGNATURES = {
     "vkb_scene_update_instances_device": (C.c_int, [_P, C.c_void_p, C.c_uint32, C.c_int]),
     "vkb_render": (C.c_int, [_P, C.POINTER(VkbProfile), C.POINTER(VkbOutput), C.POINTER(VkbStats)]),
     "vkb_render_noalloc": (C.c_int, [_P, C.POINTER(VkbProfile), C.POINTER(VkbOutput), C.POINTER(VkbStats)]),
+    "vkb_scene_info": (C.c_int, [_P, C.POINTER(VkbSceneInfo)]),
     "vkb_ctx_stream": (C.c_void_p, [_P]),
     "vkb_scene_launch_count": (C.c_uint64, [_P]),
     "vkb_debug_sampler_groups": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),

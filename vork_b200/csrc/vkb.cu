@@ -147,6 +147,110 @@ std::vector<LightTreeNode> light_tree(const vkb_light* lights, uint32_t n) {
     return nodes;
 }
 
+// Binned-SAH BLAS over one mesh's triangles (object space), built once at install:
+// BVH2 nodes in the device layout (both child boxes per node), leaves of up to
+// BLAS_LEAF_MAX triangles referenced as ~((first << 2) | (count - 1)), triangles
+// reordered into leaf order.  The per-frame TLAS keeps the GPU LBVH.
+constexpr uint32_t BLAS_LEAF_MAX = 4;
+struct SahBlas {
+    std::vector<BvhNode> nodes;
+    std::vector<uint32_t> order;  // leaf-ordered original triangle ids
+    const float* lo; const float* hi; const float* c;
+    std::vector<uint32_t> ids;
+    struct Box { float lo[3], hi[3]; };
+    static float area(const Box& b) {
+        float x = std::max(b.hi[0] - b.lo[0], 0.f), y = std::max(b.hi[1] - b.lo[1], 0.f), z = std::max(b.hi[2] - b.lo[2], 0.f);
+        return x * y + y * z + z * x;
+    }
+    static void grow(Box& a, const float* l, const float* h) { for (int k = 0; k < 3; ++k) { a.lo[k] = std::min(a.lo[k], l[k]); a.hi[k] = std::max(a.hi[k], h[k]); } }
+    static Box empty() { Box b; for (int k = 0; k < 3; ++k) { b.lo[k] = INFINITY; b.hi[k] = -INFINITY; } return b; }
+    static void set_child(BvhNode& n, int side, const Box& b, int ref) {
+        if (side == 0) { n.a = make_float4(b.lo[0], b.hi[0], b.lo[1], b.hi[1]); n.c.x = b.lo[2]; n.c.y = b.hi[2]; n.d.x = ref; }
+        else { n.b = make_float4(b.lo[0], b.hi[0], b.lo[1], b.hi[1]); n.c.z = b.lo[2]; n.c.w = b.hi[2]; n.d.y = ref; }
+    }
+    // Returns the reference of the subtree over ids[first, first+count) and its box.
+    int build(uint32_t first, uint32_t count, Box& out, int depth) {
+        Box b = empty(), cb = empty();
+        for (uint32_t i = first; i < first + count; ++i) { grow(b, lo + 3 * ids[i], hi + 3 * ids[i]); grow(cb, c + 3 * ids[i], c + 3 * ids[i]); }
+        out = b;
+        const int BINS = 16;
+        float best = INFINITY; int best_axis = -1, best_bin = 0;
+        if (count > 1 && depth < 60) {
+            for (int axis = 0; axis < 3; ++axis) {
+                float l = cb.lo[axis], h = cb.hi[axis];
+                if (!(h > l)) continue;
+                Box bb[BINS]; uint32_t cnt[BINS] = {};
+                for (int k = 0; k < BINS; ++k) bb[k] = empty();
+                float sc = float(BINS) / (h - l);
+                for (uint32_t i = first; i < first + count; ++i) {
+                    int k = std::min(BINS - 1, int((c[3 * ids[i] + axis] - l) * sc));
+                    grow(bb[k], lo + 3 * ids[i], hi + 3 * ids[i]); cnt[k]++;
+                }
+                float la[BINS]; uint32_t lc[BINS];
+                Box acc = empty(); uint32_t ac = 0;
+                for (int k = 0; k < BINS; ++k) { grow(acc, bb[k].lo, bb[k].hi); ac += cnt[k]; la[k] = area(acc); lc[k] = ac; }
+                acc = empty(); ac = 0;
+                for (int k = BINS - 1; k > 0; --k) {
+                    grow(acc, bb[k].lo, bb[k].hi); ac += cnt[k];
+                    if (lc[k - 1] == 0 || ac == 0) continue;
+                    float cost = la[k - 1] * float(lc[k - 1]) + area(acc) * float(ac);
+                    if (cost < best) { best = cost; best_axis = axis; best_bin = k; }
+                }
+            }
+        }
+        float parent = area(b);
+        // SAH with traversal cost 1 and triangle cost 1, relative to the parent's area.
+        bool leaf = count == 1 || (count <= BLAS_LEAF_MAX && (best_axis < 0 || float(count) * parent <= parent + best));
+        if (!leaf && best_axis < 0 && count > BLAS_LEAF_MAX) best_axis = -2;  // degenerate centroids: median split
+        if (leaf) {
+            uint32_t f = uint32_t(order.size());
+            for (uint32_t i = first; i < first + count; ++i) order.push_back(ids[i]);
+            return ~int((f << 2) | (count - 1));
+        }
+        uint32_t mid;
+        if (best_axis >= 0) {
+            float l = cb.lo[best_axis], sc = float(BINS) / (cb.hi[best_axis] - l);
+            auto it = std::partition(ids.begin() + first, ids.begin() + first + count, [&](uint32_t p) {
+                return std::min(BINS - 1, int((c[3 * p + best_axis] - l) * sc)) < best_bin; });
+            mid = uint32_t(it - ids.begin());
+            if (mid == first || mid == first + count) mid = first + count / 2;
+        } else {
+            mid = first + count / 2;
+        }
+        int index = int(nodes.size());
+        nodes.push_back(BvhNode{});
+        Box lb, rb;
+        int lref = build(first, mid - first, lb, depth + 1);
+        int rref = build(mid, first + count - mid, rb, depth + 1);
+        set_child(nodes[index], 0, lb, lref);
+        set_child(nodes[index], 1, rb, rref);
+        nodes[index].d.z = nodes[index].d.w = 0;
+        return index;
+    }
+    void run(uint32_t n, const float* l, const float* h, const float* cent) {
+        lo = l; hi = h; c = cent;
+        ids.resize(n);
+        for (uint32_t i = 0; i < n; ++i) ids[i] = i;
+        nodes.clear(); order.clear();
+        nodes.push_back(BvhNode{});  // root
+        Box b = empty(), cb = empty();
+        for (uint32_t i = 0; i < n; ++i) grow(b, l + 3 * i, h + 3 * i);
+        (void)cb;
+        if (n <= BLAS_LEAF_MAX) {
+            order.assign(ids.begin(), ids.end());
+            set_child(nodes[0], 0, b, ~int(n - 1));
+            set_child(nodes[0], 1, empty(), ~int(n - 1));
+            nodes[0].d.z = nodes[0].d.w = 0;
+            return;
+        }
+        // The root is node 0: build its two halves under it.
+        Box rb;
+        nodes.pop_back();
+        int r = build(0, n, rb, 0);
+        (void)r;  // r == 0: the root node was allocated first
+    }
+};
+
 // Scratch of one LBVH build, reused across builds.
 struct LbvhScratch {
     DBuf<uint32_t> codes, codes_sorted, ids, ids_sorted, leaf_parent, node_parent, counters, bounds;
@@ -202,16 +306,15 @@ struct vkb_scene {
     vkb_camera camera{};
     vkb_environment env{};
     uint32_t tree_nodes = 0;
-    double changed_bytes = 0;
+    std::vector<float> host_rows;  // last rows from the host, for the changed-bytes count
     // device scene
     DBuf<float4> vpos, vnrm, blas_tris, o2w, w2o, inst_lo, inst_hi, tri_lo, tri_hi;
     DBuf<uint32_t> indices, tlas_codes;
+    DBuf<uint32_t> tlas_order, tlas_leaf_parent, tlas_node_parent, tlas_counters;  // TLAS topology kept for refits
+    uint64_t motion_bytes = 0, tlas_rebuilds = 0, tlas_refits = 0;
     DBuf<uint4> inst_info;
     DBuf<MeshInfo> meshes;
     DBuf<BvhNode> blas_nodes, tlas_nodes;
-    DBuf<WideNode> blas_wide, tlas_wide;
-    DBuf<uint2> collapse_work;
-    DBuf<uint32_t> collapse_counts;
     DBuf<TlasLeaf> tlas_leaves;
     DBuf<vkb_material> d_materials;
     DBuf<vkb_light> d_lights;
@@ -251,26 +354,7 @@ SceneView scene_view(const vkb_scene* s) {
     v.tlas_nodes = s->tlas_nodes.p; v.tlas_leaves = s->tlas_leaves.p;
     v.blas_nodes = s->blas_nodes.p; v.blas_tris = s->blas_tris.p;
     v.num_instances = s->num_instances;
-    v.tlas_wide = s->tlas_wide.p; v.blas_wide = s->blas_wide.p;
     return v;
-}
-
-// Collapse a binary LBVH of n primitives into the 8-wide BVH at `wide` (root at 0):
-// 64 levels back to back, each reading the previous level's work list on the device.
-void collapse(vkb_scene* s, const BvhNode* bin, uint32_t n, WideNode* wide) {
-    if (n == 0) return;
-    cudaStream_t st = s->ctx->stream;
-    s->collapse_work.alloc(3 * size_t(std::max(1u, n)));
-    s->collapse_counts.alloc(4);
-    uint2* w[3] = {s->collapse_work.p, s->collapse_work.p + n, s->collapse_work.p + 2 * size_t(n)};
-    uint32_t* c = s->collapse_counts.p;
-    VKB_CUDA(cudaMemsetAsync(c, 0, 4 * sizeof(uint32_t), st));
-    k_collapse_seed<<<1, 1, 0, st>>>(w[0], &c[0], &c[3]);
-    int grid = std::max(1, std::min(s->ctx->sms * 4, int((n + 127) / 128)));
-    for (int level = 0; level < 64; ++level)
-        k_collapse<<<grid, 128, 0, st>>>(bin, wide, w[level % 3], &c[level % 3], w[(level + 1) % 3], &c[(level + 1) % 3], &c[3], &c[(level + 2) % 3]);
-    s->launches += 65;
-    VKB_CUDA(cudaGetLastError());
 }
 
 // Instance rows -> w2o, world boxes, TLAS (LBVH) and its leaf records.
@@ -282,13 +366,55 @@ void build_tlas(vkb_scene* s) {
     VKB_CUDA(cudaEventRecord(s->ev0, st));
     k_instances<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->o2w.p, s->inst_info.p, s->meshes.p, s->w2o.p, s->inst_lo.p, s->inst_hi.p);
     build_lbvh(n, s->inst_lo.p, s->inst_hi.p, s->tlas_nodes.p, s->scratch, st, sms, s->launches);
-    if (VKB_WIDE_BVH) collapse(s, s->tlas_nodes.p, n, s->tlas_wide.p);
     s->launches += 2;
     k_tlas_leaves<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->scratch.ids_sorted.p, s->w2o.p, s->inst_info.p, s->meshes.p, s->d_materials.p, s->tlas_leaves.p);
     VKB_CUDA(cudaMemcpyAsync(s->tlas_codes.p, s->scratch.codes.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    // Keep the topology for later refits (the LBVH scratch is shared with other builds).
+    s->tlas_order.alloc(n); s->tlas_leaf_parent.alloc(n); s->tlas_node_parent.alloc(std::max(1u, n)); s->tlas_counters.alloc(std::max(1u, n));
+    VKB_CUDA(cudaMemcpyAsync(s->tlas_order.p, s->scratch.ids_sorted.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    if (n > 1) {
+        VKB_CUDA(cudaMemcpyAsync(s->tlas_leaf_parent.p, s->scratch.leaf_parent.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+        VKB_CUDA(cudaMemcpyAsync(s->tlas_node_parent.p, s->scratch.node_parent.p, (n - 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    }
+    s->tlas_rebuilds++;
     VKB_CUDA(cudaEventRecord(s->ev1, st));
     VKB_CUDA(cudaEventSynchronize(s->ev1));
     VKB_CUDA(cudaEventElapsedTime(&s->build_ms, s->ev0, s->ev1));
+}
+
+// Refit the TLAS in place: new instance boxes and world->object rows, same topology.
+void refit_tlas(vkb_scene* s) {
+    cudaStream_t st = s->ctx->stream;
+    int sms = s->ctx->sms;
+    uint32_t n = s->num_instances;
+    if (n == 0) return;
+    VKB_CUDA(cudaEventRecord(s->ev0, st));
+    k_instances<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->o2w.p, s->inst_info.p, s->meshes.p, s->w2o.p, s->inst_lo.p, s->inst_hi.p);
+    if (n == 1) {
+        k_single_leaf<<<1, 1, 0, st>>>(s->inst_lo.p, s->inst_hi.p, s->tlas_nodes.p);
+    } else {
+        VKB_CUDA(cudaMemsetAsync(s->tlas_counters.p, 0, (n - 1) * sizeof(uint32_t), st));
+        k_refit<<<grid_for(n, 256, sms), 256, 0, st>>>(int(n), s->tlas_order.p, s->inst_lo.p, s->inst_hi.p, s->tlas_nodes.p, s->tlas_leaf_parent.p,
+                                                       s->tlas_node_parent.p, s->tlas_counters.p);
+    }
+    k_tlas_leaves<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->tlas_order.p, s->w2o.p, s->inst_info.p, s->meshes.p, s->d_materials.p, s->tlas_leaves.p);
+    s->launches += 3;
+    VKB_CUDA(cudaGetLastError());
+    VKB_CUDA(cudaEventRecord(s->ev1, st));
+    VKB_CUDA(cudaEventSynchronize(s->ev1));
+    VKB_CUDA(cudaEventElapsedTime(&s->build_ms, s->ev0, s->ev1));
+    s->tlas_refits++;
+}
+
+// rt.rs:1465-1476: accumulate the changed object bytes; rebuild once they reach a
+// quarter of the object buffer, otherwise refit (policy 0).  1 rebuilds, 2 refits.
+void update_tlas(vkb_scene* s, uint64_t changed_bytes, int policy) {
+    uint64_t total = uint64_t(s->num_instances) * 48u;
+    uint64_t threshold = std::max<uint64_t>(1, (total + 3) / 4);
+    s->motion_bytes += changed_bytes;
+    bool rebuild = policy == 1 || (policy == 0 && s->motion_bytes >= threshold);
+    if (rebuild) { s->motion_bytes = 0; build_tlas(s); }
+    else refit_tlas(s);
 }
 
 void validate_desc(const vkb_scene_desc* d) {
@@ -399,24 +525,45 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         uint32_t node_total = 0;
         for (auto& mi : s->mesh_info) { mi.node_offset = node_total; node_total += std::max(1u, mi.num_triangles > 1 ? mi.num_triangles - 1u : 1u); }
         s->blas_nodes.alloc(std::max(1u, node_total));
-        s->blas_wide.alloc(std::max(1u, node_total));
         s->blas_tris.alloc(std::max<size_t>(1, size_t(nt) * 3));
         uint32_t max_tris = 0;
         for (auto& mi : s->mesh_info) max_tris = std::max(max_tris, mi.num_triangles);
         s->tri_lo.alloc(std::max(1u, max_tris)); s->tri_hi.alloc(std::max(1u, max_tris));
         VKB_CUDA(cudaEventRecord(s->ev0, str));
+        std::vector<BvhNode> all_nodes(std::max(1u, node_total));
+        std::vector<float4> all_tris(std::max<size_t>(1, size_t(nt) * 3));
         for (uint32_t m = 0; m < d->num_meshes; ++m) {
             const MeshInfo& mi = s->mesh_info[m];
-            if (mi.num_triangles == 0) continue;
-            // Relative index buffer -> absolute for the box and sorted-triangle kernels.
-            const uint32_t* mid = s->indices.p + mi.index_offset;
-            const float4* mpos = s->vpos.p + mi.vertex_offset;
-            k_tri_boxes<<<grid_for(mi.num_triangles, 256, sms), 256, 0, str>>>(mi.num_triangles, mid, mpos, s->tri_lo.p, s->tri_hi.p);
-            build_lbvh(mi.num_triangles, s->tri_lo.p, s->tri_hi.p, s->blas_nodes.p + mi.node_offset, s->scratch, str, sms, s->launches);
-            if (VKB_WIDE_BVH) collapse(s, s->blas_nodes.p + mi.node_offset, mi.num_triangles, s->blas_wide.p + mi.node_offset);
-            s->launches += 2;
-            k_sorted_tris<<<grid_for(mi.num_triangles, 256, sms), 256, 0, str>>>(mi.num_triangles, s->scratch.ids_sorted.p, mid, mpos, s->blas_tris.p + 3 * size_t(mi.tri_offset));
+            const vkb_mesh& me = d->meshes[m];
+            uint32_t n = mi.num_triangles;
+            if (n == 0) continue;
+            std::vector<float> lo(3 * size_t(n)), hi(3 * size_t(n)), cen(3 * size_t(n));
+            for (uint32_t t = 0; t < n; ++t)
+                for (int a = 0; a < 3; ++a) {
+                    float v0 = me.positions[3 * me.indices[3 * t] + a], v1 = me.positions[3 * me.indices[3 * t + 1] + a], v2 = me.positions[3 * me.indices[3 * t + 2] + a];
+                    lo[3 * t + a] = std::min(v0, std::min(v1, v2)); hi[3 * t + a] = std::max(v0, std::max(v1, v2));
+                    cen[3 * t + a] = 0.5f * (lo[3 * t + a] + hi[3 * t + a]);
+                }
+            SahBlas sah;
+            sah.run(n, lo.data(), hi.data(), cen.data());
+            if (sah.nodes.size() > std::max(1u, n > 1 ? n - 1 : 1u)) throw ArgError{"BLAS node count above its bound"};
+            std::copy(sah.nodes.begin(), sah.nodes.end(), all_nodes.begin() + mi.node_offset);
+            for (uint32_t k = 0; k < n; ++k) {
+                uint32_t t = sah.order[k];
+                const float* p0 = me.positions + 3 * me.indices[3 * t];
+                const float* p1 = me.positions + 3 * me.indices[3 * t + 1];
+                const float* p2 = me.positions + 3 * me.indices[3 * t + 2];
+                size_t o = 3 * (size_t(mi.tri_offset) + k);
+                float tid;
+                std::memcpy(&tid, &t, sizeof(tid));
+                all_tris[o] = make_float4(p0[0], p0[1], p0[2], tid);
+                all_tris[o + 1] = make_float4(p1[0], p1[1], p1[2], 0.f);
+                all_tris[o + 2] = make_float4(p2[0], p2[1], p2[2], 0.f);
+            }
         }
+        VKB_CUDA(cudaMemcpyAsync(s->blas_nodes.p, all_nodes.data(), all_nodes.size() * sizeof(BvhNode), cudaMemcpyHostToDevice, str));
+        VKB_CUDA(cudaMemcpyAsync(s->blas_tris.p, all_tris.data(), all_tris.size() * sizeof(float4), cudaMemcpyHostToDevice, str));
+        VKB_CUDA(cudaStreamSynchronize(str));
         VKB_CUDA(cudaEventRecord(s->ev1, str));
         s->meshes.upload(s->mesh_info.data(), s->mesh_info.size(), str);
         // Materials, lights, light tree.
@@ -437,10 +584,10 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         for (uint32_t i = 0; i < n; ++i) info[i] = make_uint4(d->instance_mesh[i], d->instance_material[i], 0u, 0u);
         s->inst_info.upload(info.data(), n, str);
         s->o2w.upload(reinterpret_cast<const float4*>(d->instance_rows), size_t(n) * 3, str);
+        s->host_rows.assign(d->instance_rows, d->instance_rows + size_t(n) * 12);
         s->w2o.alloc(size_t(n) * 3);
         s->inst_lo.alloc(n); s->inst_hi.alloc(n);
         s->tlas_nodes.alloc(std::max(1u, n > 1 ? n - 1 : 1u));
-        s->tlas_wide.alloc(std::max(1u, n > 1 ? n - 1 : 1u));
         s->tlas_leaves.alloc(std::max(1u, n));
         s->tlas_codes.alloc(std::max(1u, n));
         VKB_CUDA(cudaStreamSynchronize(str));
@@ -462,9 +609,9 @@ vkb_status vkb_scene_destroy(vkb_scene* s) {
                           &s->ray_o0, &s->ray_d0, &s->ray_o1, &s->ray_d1, &s->hit, &s->thr, &s->rad, &s->sa_o, &s->sa_d, &s->sa_c,
                           &s->sb_o, &s->sb_d, &s->sb_c, &s->accum, &s->out_rgba};
     for (auto* b : f4) b->release();
-    s->indices.release(); s->tlas_codes.release(); s->inst_info.release(); s->meshes.release();
-    s->blas_nodes.release(); s->tlas_nodes.release(); s->blas_wide.release(); s->tlas_wide.release();
-    s->collapse_work.release(); s->collapse_counts.release(); s->tlas_leaves.release(); s->d_materials.release(); s->d_lights.release();
+    s->indices.release(); s->tlas_codes.release();
+    s->tlas_order.release(); s->tlas_leaf_parent.release(); s->tlas_node_parent.release(); s->tlas_counters.release(); s->inst_info.release(); s->meshes.release();
+    s->blas_nodes.release(); s->tlas_nodes.release(); s->tlas_leaves.release(); s->d_materials.release(); s->d_lights.release();
     s->tree.release(); s->hit_inst.release(); s->counters.release(); s->err.release(); s->ids.release(); s->rng.release(); s->work.release();
     for (cudaEvent_t e : s->kernel_events) cudaEventDestroy(e);
     s->scratch.codes.release(); s->scratch.codes_sorted.release(); s->scratch.ids.release(); s->scratch.ids_sorted.release();
@@ -481,13 +628,18 @@ vkb_status vkb_scene_update_instances(vkb_scene* s, const float* rows, uint32_t 
     if (policy < 0 || policy > 2) return fail(VKB_INVALID_ARG, "policy must be 0, 1 or 2");
     return guarded([&] {
         VKB_CUDA(cudaSetDevice(s->ctx->device));
+        // Changed bytes: rows that differ from the installed ones (host copy kept per scene).
+        uint64_t changed = 0;
+        if (s->host_rows.size() == size_t(n) * 12) {
+            for (uint32_t i = 0; i < n; ++i)
+                if (std::memcmp(&s->host_rows[12 * size_t(i)], rows + 12 * size_t(i), 48) != 0) changed += 48;
+        } else {
+            changed = uint64_t(n) * 48u;
+        }
+        s->host_rows.assign(rows, rows + size_t(n) * 12);
+        if (changed == 0 && policy == 0) return;
         s->o2w.upload(reinterpret_cast<const float4*>(rows), size_t(n) * 3, s->ctx->stream);
-        // rt.rs:1465-1476: rebuild once the changed object bytes reach a quarter of
-        // the object buffer; every row changed here, so policy 0 rebuilds.  Refit
-        // (policy 2) keeps the topology and would reuse it; both rebuild for now.
-        s->changed_bytes += double(n) * 48.0;
-        build_tlas(s);
-        s->changed_bytes = 0;
+        update_tlas(s, changed, policy);
     });
 }
 
@@ -498,7 +650,8 @@ vkb_status vkb_scene_update_instances_device(vkb_scene* s, const float* rows, ui
     return guarded([&] {
         VKB_CUDA(cudaSetDevice(s->ctx->device));
         VKB_CUDA(cudaMemcpyAsync(s->o2w.p, rows, size_t(n) * 3 * sizeof(float4), cudaMemcpyDeviceToDevice, s->ctx->stream));
-        build_tlas(s);
+        s->host_rows.clear();  // device rows: every row counts as changed
+        update_tlas(s, uint64_t(n) * 48u, policy);
     });
 }
 
@@ -626,6 +779,22 @@ vkb_status vkb_render(vkb_scene* s, const vkb_profile* pf, vkb_output* out, vkb_
             stats->blas_nodes_visited = work[5];
         }
     });
+}
+
+vkb_status vkb_scene_info(vkb_scene* s, vkb_scene_info_t* out) {
+    if (!s || !out) return fail(VKB_INVALID_ARG, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    out->num_instances = s->num_instances;
+    out->num_triangles = s->total_tris;
+    out->tlas_rebuilds = s->tlas_rebuilds;
+    out->tlas_refits = s->tlas_refits;
+    out->motion_bytes = s->motion_bytes;
+    size_t dev = 0;
+    dev += s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas_nodes.n * sizeof(BvhNode) + s->blas_tris.n * sizeof(float4);
+    dev += s->tlas_nodes.n * sizeof(BvhNode) + s->tlas_leaves.n * sizeof(TlasLeaf) + (s->o2w.n + s->w2o.n) * sizeof(float4);
+    out->scene_bytes = dev;
+    out->build_ms = s->build_ms;
+    return VKB_OK;
 }
 
 void* vkb_ctx_stream(vkb_ctx* c) { return c ? reinterpret_cast<void*>(c->stream) : nullptr; }

@@ -1,6 +1,7 @@
-// Acceleration structures for the B200 backend (B200 has no RT cores): per-mesh BLAS
-// and a per-frame instance TLAS, both linear BVHs (Karras 2012) over 30-bit Morton
-// codes, sorted with cub's radix sort and refitted bottom-up with atomic counters.
+// Acceleration structures for the B200 backend (B200 has no RT cores): a per-frame
+// instance TLAS built as a linear BVH (Karras 2012) over 30-bit Morton codes, sorted
+// with cub's radix sort and refitted bottom-up with atomic counters, and per-mesh BLAS
+// built once at install with a binned SAH (host, vkb.cu) in the same node format.
 // The reference builds these inside the Vulkan driver (crates/vork-render/src/rt.rs:
 // Rays::new :1098-1289 for BLAS batches, FrameRays::new :1339-1385 and encode /
 // rebuild_tlas :1387-1476 for the instance TLAS); its traversal is RayQuery::Proceed
@@ -137,15 +138,12 @@ __device__ __forceinline__ bool tri_test(const RaySpace& r, float3 v0, float3 v1
 
 struct HitRecord { float t, u, v; uint32_t prim, inst; };
 
-struct WideNode;
 struct SceneView {
     const BvhNode* tlas_nodes;
     const TlasLeaf* tlas_leaves;
     const BvhNode* blas_nodes;
     const float4* blas_tris;     // 3 per triangle (Morton order within a mesh); v0.w = original triangle id
     uint32_t num_instances;
-    const WideNode* tlas_wide;   // 8-wide collapse of tlas_nodes (traversed by the renders)
-    const WideNode* blas_wide;   // 8-wide collapse of every BLAS, same per-mesh offsets as blas_nodes
 };
 
 // Traversal work of one ray (instrumented builds only): node visits, triangle tests, instance entries.
@@ -208,14 +206,18 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, float3 o, float3 d
             node = 0;
             continue;
         } else {
-            if (COUNT) count->tris++;
-            const float4* tp = tris + 3u * (tri_base + uint32_t(~node));
-            float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
-            float t, b1, b2;
-            if (tri_test(rs, f3(v0.x, v0.y, v0.z), f3(v1.x, v1.y, v1.z), f3(v2.x, v2.y, v2.z), cull, tbest, t, b1, b2)) {
-                tbest = t; found = true;
-                hit.t = t; hit.u = b1; hit.v = b2; hit.prim = __float_as_uint(v0.w); hit.inst = cur_instance;
-                if (ANY) return true;
+            // BLAS leaf: up to four triangles in leaf order, ~((first << 2) | (count - 1)).
+            uint32_t v = uint32_t(~node), first = v >> 2, cnt = (v & 3u) + 1u;
+            for (uint32_t k = 0; k < cnt; ++k) {
+                if (COUNT) count->tris++;
+                const float4* tp = tris + 3u * (tri_base + first + k);
+                float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
+                float t, b1, b2;
+                if (tri_test(rs, f3(v0.x, v0.y, v0.z), f3(v1.x, v1.y, v1.z), f3(v2.x, v2.y, v2.z), cull, tbest, t, b1, b2)) {
+                    tbest = t; found = true;
+                    hit.t = t; hit.u = b1; hit.v = b2; hit.prim = __float_as_uint(v0.w); hit.inst = cur_instance;
+                    if (ANY) return true;
+                }
             }
         }
         // pop (with VKB_POP_CULL, an entry farther than the closest hit so far is skipped without a fetch)

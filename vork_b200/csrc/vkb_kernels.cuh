@@ -4,7 +4,6 @@
 #include <cstdint>
 #include "vkb_device.cuh"
 #include "vkb_bvh.cuh"
-#include "vkb_wide.cuh"
 
 namespace vkb {
 
@@ -293,27 +292,19 @@ __device__ __forceinline__ void flush_count(unsigned long long* dst, uint32_t v)
     for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
     if ((threadIdx.x & 31u) == 0u && x) atomicAdd(dst, x);
 }
-#ifndef VKB_WIDE_BVH
-#define VKB_WIDE_BVH 0
-#endif
 #ifndef VKB_TRACE_MIN_BLOCKS
 #define VKB_TRACE_MIN_BLOCKS 8
 #endif
-// The traversal the renders use: binary (BVH2) or 8-wide.
 template <bool ANY, bool COUNT>
 __device__ __forceinline__ bool trace_any(const SceneView& sv, float3 o, float3 d, float tmax, HitRecord& h, uint32_t* err, TraceCount* tc,
                                           TraceStack stk) {
-#if VKB_WIDE_BVH
-    return trace_wide<ANY, COUNT>(sv.tlas_wide, sv.tlas_leaves, sv.blas_wide, sv.blas_tris, sv.num_instances, o, d, tmax, h, err, tc, stk);
-#else
     return trace_ray<ANY, COUNT>(sv, o, d, tmax, h, err, tc, stk);
-#endif
 }
 // This thread's column of the block's shared-memory traversal stack.
 #define VKB_STACK_DECL                                                                                   \
     __shared__ int stack_r_[SMEM_STACK * TRACE_BLOCK];                                                  \
-    __shared__ float stack_t_[(VKB_WIDE_BVH || VKB_POP_CULL) ? SMEM_STACK * TRACE_BLOCK : 1];          \
-    TraceStack stk{stack_r_ + threadIdx.x, stack_t_ + ((VKB_WIDE_BVH || VKB_POP_CULL) ? threadIdx.x : 0)};
+    __shared__ float stack_t_[VKB_POP_CULL ? SMEM_STACK * TRACE_BLOCK : 1];                            \
+    TraceStack stk{stack_r_ + threadIdx.x, stack_t_ + (VKB_POP_CULL ? threadIdx.x : 0)};
 template <bool ANY, bool COUNT>
 __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace(PathParams p, int cur) {
     VKB_STACK_DECL
