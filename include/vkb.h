@@ -205,6 +205,59 @@ vkb_status vkb_scene_update_instances_device(vkb_scene* scene, const float* devi
  * over them. stats may be NULL. */
 vkb_status vkb_render(vkb_scene* scene, const vkb_profile* profile, vkb_output* out, vkb_stats* stats);
 
+/* Batched previews: many render jobs (each its own installed scene of this context,
+ * profile and output) share every wavefront wave; each wave's kernel sequence is
+ * replayed from a captured CUDA graph.  No reference counterpart: vork renders one
+ * shot per Renderer at a time (crates/vork-render/src/shot.rs:374).  Per-job results
+ * equal vkb_render's for the same scene and profile.  flags: VKB_PROFILE_* switches. */
+typedef struct vkb_job {
+    vkb_scene* scene;
+    vkb_profile profile;
+    vkb_output out;
+} vkb_job;
+vkb_status vkb_render_batch(vkb_ctx* ctx, vkb_job* jobs, uint32_t njobs, uint32_t flags, vkb_stats* stats);
+
+/* Autotuner of the wavefront: times one sample of `jobs` for every candidate wave
+ * capacity (path slots per wave: 2, 4, 8, 16 Mi) and trace/shade grid (8, 16, 32
+ * blocks per SM) and keeps the fastest for this context's later renders. */
+typedef struct vkb_tune_result {
+    uint32_t tried;
+    uint32_t best_blocks_per_sm;
+    uint64_t best_capacity;
+    float best_ms;
+    uint32_t blocks_per_sm[16];
+    uint64_t capacity[16];
+    float ms[16];
+} vkb_tune_result;
+vkb_status vkb_autotune(vkb_ctx* ctx, vkb_job* jobs, uint32_t njobs, vkb_tune_result* out);
+
+/* Serving with continuous batching (vkb_job_submit/poll of the boundary plan): requests
+ * queue on the host; every vkb_server_step admits queued requests at the wave boundary
+ * (FIFO) while `max_jobs` and the device-memory budget allow (resident scenes + the
+ * shared wavefront + 32 bytes per pixel of every admitted request), runs one wave over
+ * all admitted requests, and copies finished images to their host buffers.  No
+ * reference counterpart beyond vork's one-request-at-a-time session
+ * (crates/vork-cli/src/session.rs:1-60). */
+typedef struct vkb_server vkb_server;
+typedef struct vkb_server_config {
+    uint64_t memory_budget_bytes;  /* 0: unbounded */
+    uint32_t max_jobs;             /* admitted requests at once (job-table entries) */
+    uint32_t flags;                /* VKB_PROFILE_* switches for every wave */
+    uint64_t wave_capacity;        /* path slots per wave (0: the context's autotuned value) */
+} vkb_server_config;
+typedef struct vkb_server_status {
+    uint32_t queued, running, finished;   /* finished: requests completed by this step */
+    uint32_t reserved;
+    uint64_t used_bytes, peak_bytes;      /* device bytes under the budget now / at peak */
+} vkb_server_status;
+vkb_status vkb_server_create(vkb_ctx* ctx, const vkb_server_config* cfg, vkb_server** out);
+/* host_rgba (width*height*4 floats) must stay valid until the request is done. */
+vkb_status vkb_server_submit(vkb_server* server, vkb_scene* scene, const vkb_profile* profile, float* host_rgba, uint64_t* id);
+vkb_status vkb_server_step(vkb_server* server, vkb_server_status* status);
+/* state: 0 queued, 1 running, 2 done (its host_rgba holds the mean image). */
+vkb_status vkb_server_poll(vkb_server* server, uint64_t id, int* state);
+vkb_status vkb_server_destroy(vkb_server* server);
+
 /* Installed-scene facts: sizes, device bytes of the scene structures, and the TLAS
  * update history of vkb_scene_update_instances (rebuilds vs refits, rt.rs:1465-1476). */
 typedef struct vkb_scene_info_t {

@@ -88,6 +88,36 @@ class Renderer:
                                                     count, stream, abi.uptr(out)))
         return out
 
+    def render_batch(self, items, flags: int = 0):
+        """Render [(InstalledScene, Profile), ...] together (vkb_render_batch): one shared
+        wavefront, per-job images identical to InstalledScene.render."""
+        n = len(items)
+        jobs = (abi.VkbJob * max(1, n))()
+        images = []
+        for k, (inst, prof) in enumerate(items):
+            cam = inst.scene.camera
+            img = np.empty((cam.height, cam.width, 4), np.float32)
+            images.append(img)
+            jobs[k].scene = inst.h
+            jobs[k].profile = prof.c()
+            jobs[k].out.rgba = img.ctypes.data_as(C.c_void_p)
+            jobs[k].out.on_device = 0
+        st = abi.VkbStats()
+        abi.check(self.lib.vkb_render_batch(self.h, jobs, n, flags, C.byref(st)))
+        return images, {k: getattr(st, k) for k, _ in abi.VkbStats._fields_}
+
+    def autotune(self, items) -> dict:
+        """Pick the wave capacity and trace grid for these jobs (vkb_autotune)."""
+        n = len(items)
+        jobs = (abi.VkbJob * max(1, n))()
+        for k, (inst, prof) in enumerate(items):
+            jobs[k].scene = inst.h
+            jobs[k].profile = prof.c()
+        r = abi.VkbTuneResult()
+        abi.check(self.lib.vkb_autotune(self.h, jobs, n, C.byref(r)))
+        return {"best_capacity": r.best_capacity, "best_blocks_per_sm": r.best_blocks_per_sm, "best_ms": r.best_ms,
+                "tried": [(r.capacity[i], r.blocks_per_sm[i], r.ms[i]) for i in range(min(r.tried, 16))]}
+
     @property
     def stream(self) -> int:
         """The cudaStream_t (as an integer) this device's kernels run on."""

@@ -84,6 +84,24 @@ class VkbStats(C.Structure):
                 ("blas_nodes_visited", C.c_uint64)]
 
 
+class VkbJob(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("profile", VkbProfile), ("out", VkbOutput)]
+
+
+class VkbTuneResult(C.Structure):
+    _fields_ = [("tried", C.c_uint32), ("best_blocks_per_sm", C.c_uint32), ("best_capacity", C.c_uint64), ("best_ms", C.c_float),
+                ("blocks_per_sm", C.c_uint32 * 16), ("capacity", C.c_uint64 * 16), ("ms", C.c_float * 16)]
+
+
+class VkbServerConfig(C.Structure):
+    _fields_ = [("memory_budget_bytes", C.c_uint64), ("max_jobs", C.c_uint32), ("flags", C.c_uint32), ("wave_capacity", C.c_uint64)]
+
+
+class VkbServerStatus(C.Structure):
+    _fields_ = [("queued", C.c_uint32), ("running", C.c_uint32), ("finished", C.c_uint32), ("reserved", C.c_uint32),
+                ("used_bytes", C.c_uint64), ("peak_bytes", C.c_uint64)]
+
+
 class VkbSceneInfo(C.Structure):
     _fields_ = [("num_instances", C.c_uint64), ("num_triangles", C.c_uint64), ("scene_bytes", C.c_uint64),
                 ("tlas_rebuilds", C.c_uint64), ("tlas_refits", C.c_uint64), ("motion_bytes", C.c_uint64),
@@ -104,6 +122,13 @@ SIGNATURES = {
     "vkb_render": (C.c_int, [_P, C.POINTER(VkbProfile), C.POINTER(VkbOutput), C.POINTER(VkbStats)]),
     "vkb_render_noalloc": (C.c_int, [_P, C.POINTER(VkbProfile), C.POINTER(VkbOutput), C.POINTER(VkbStats)]),
     "vkb_scene_info": (C.c_int, [_P, C.POINTER(VkbSceneInfo)]),
+    "vkb_server_create": (C.c_int, [_P, C.POINTER(VkbServerConfig), C.POINTER(_P)]),
+    "vkb_server_submit": (C.c_int, [_P, _P, C.POINTER(VkbProfile), C.POINTER(C.c_float), C.POINTER(C.c_uint64)]),
+    "vkb_server_step": (C.c_int, [_P, C.POINTER(VkbServerStatus)]),
+    "vkb_server_poll": (C.c_int, [_P, C.c_uint64, C.POINTER(C.c_int)]),
+    "vkb_server_destroy": (C.c_int, [_P]),
+    "vkb_render_batch": (C.c_int, [_P, C.POINTER(VkbJob), C.c_uint32, C.c_uint32, C.POINTER(VkbStats)]),
+    "vkb_autotune": (C.c_int, [_P, C.POINTER(VkbJob), C.c_uint32, C.POINTER(VkbTuneResult)]),
     "vkb_ctx_stream": (C.c_void_p, [_P]),
     "vkb_scene_launch_count": (C.c_uint64, [_P]),
     "vkb_debug_sampler_groups": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),

@@ -10,6 +10,9 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
+#include <deque>
+#include <map>
+#include <memory>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -287,12 +290,66 @@ void build_lbvh(uint32_t n, const float4* lo, const float4* hi, BvhNode* nodes, 
 
 }  // namespace
 
+// Device pointers of one wavefront: queues and path state for `capacity` path slots,
+// the counters, and the job table of `job_capacity` entries.
+struct WaveBuffers {
+    size_t capacity = 0;
+    uint32_t job_capacity = 0;
+    float4 *ray_o0 = nullptr, *ray_d0 = nullptr, *ray_o1 = nullptr, *ray_d1 = nullptr, *hit = nullptr, *thr = nullptr, *rad = nullptr;
+    float4 *sa_o = nullptr, *sa_d = nullptr, *sa_c = nullptr, *sb_o = nullptr, *sb_d = nullptr, *sb_c = nullptr;
+    uint32_t *hit_inst = nullptr, *slot_job = nullptr, *counters = nullptr, *err = nullptr;
+    uint2* rng = nullptr;
+    unsigned long long* work = nullptr;
+    Job* jobs = nullptr;
+};
+// The context's own wavefront storage (grown on demand, reused by every render).
+struct Wavefront {
+    DBuf<float4> ray_o0, ray_d0, ray_o1, ray_d1, hit, thr, rad, sa_o, sa_d, sa_c, sb_o, sb_d, sb_c;
+    DBuf<uint32_t> hit_inst, slot_job, counters, err;
+    DBuf<uint2> rng;
+    DBuf<unsigned long long> work;
+    DBuf<Job> jobs;
+    uint64_t generation = 0;  // bumps when a buffer moves (captured graphs refer to the old ones)
+    WaveBuffers view() const {
+        WaveBuffers w;
+        w.capacity = ray_o0.n; w.job_capacity = uint32_t(jobs.n);
+        w.ray_o0 = ray_o0.p; w.ray_d0 = ray_d0.p; w.ray_o1 = ray_o1.p; w.ray_d1 = ray_d1.p; w.hit = hit.p; w.thr = thr.p; w.rad = rad.p;
+        w.sa_o = sa_o.p; w.sa_d = sa_d.p; w.sa_c = sa_c.p; w.sb_o = sb_o.p; w.sb_d = sb_d.p; w.sb_c = sb_c.p;
+        w.hit_inst = hit_inst.p; w.slot_job = slot_job.p; w.counters = counters.p; w.err = err.p; w.rng = rng.p; w.work = work.p; w.jobs = jobs.p;
+        return w;
+    }
+    void reserve(size_t slots, uint32_t njobs) {
+        if (slots > ray_o0.n) {
+            DBuf<float4>* f4[] = {&ray_o0, &ray_d0, &ray_o1, &ray_d1, &hit, &thr, &rad, &sa_o, &sa_d, &sa_c, &sb_o, &sb_d, &sb_c};
+            for (auto* b : f4) b->alloc(slots);
+            hit_inst.alloc(slots); slot_job.alloc(slots); rng.alloc(slots);
+            generation++;
+        }
+        if (!counters.p) { counters.alloc(16); err.alloc(1); work.alloc(8); generation++; }
+        if (njobs > jobs.n) { jobs.alloc(std::max<size_t>(njobs, 16)); generation++; }
+    }
+    void release() {
+        DBuf<float4>* f4[] = {&ray_o0, &ray_d0, &ray_o1, &ray_d1, &hit, &thr, &rad, &sa_o, &sa_d, &sa_c, &sb_o, &sb_d, &sb_c};
+        for (auto* b : f4) b->release();
+        hit_inst.release(); slot_job.release(); rng.release(); counters.release(); err.release(); work.release(); jobs.release();
+    }
+};
+struct GraphEntry { uint64_t key; cudaGraphExec_t exec; };
+
 struct vkb_ctx {
     int device = 0;
     int sms = 148;
     cudaStream_t stream = nullptr;
     DBuf<ushort4> lut;
     DBuf<float> filter;
+    Wavefront wave;
+    DBuf<float4> accum, staging;        // per-render accumulators and host-output staging (all jobs of a call)
+    DBuf<uint32_t> ids;                 // primary ids of the jobs that asked for them
+    size_t wave_capacity = 8u << 20;    // path slots per wave (autotuned)
+    int trace_blocks_per_sm = 16;       // trace/shade grid = SMs x this (autotuned)
+    uint64_t launches = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> kernel_events;
 };
 
 struct vkb_scene {
@@ -320,14 +377,8 @@ struct vkb_scene {
     DBuf<vkb_light> d_lights;
     DBuf<LightTreeNode> tree;
     LbvhScratch scratch;
-    // wavefront
-    DBuf<float4> ray_o0, ray_d0, ray_o1, ray_d1, hit, thr, rad, sa_o, sa_d, sa_c, sb_o, sb_d, sb_c, accum, out_rgba;
-    DBuf<uint32_t> hit_inst, counters, err, ids;
-    DBuf<unsigned long long> work;
-    DBuf<uint2> rng;
     float build_ms = 0.f;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::vector<cudaEvent_t> kernel_events;  // pairs around timed trace launches
     uint64_t launches = 0;                    // kernels launched for this scene so far
 };
 
@@ -442,6 +493,307 @@ void validate_desc(const vkb_scene_desc* d) {
     if (d->camera.width == 0 || d->camera.height == 0) throw ArgError{"camera resolution is zero"};
 }
 
+
+// ================================================================ wave engine
+// One job of a render call: a scene, its profile, and where its mean image goes.
+struct EngineJob {
+    vkb_scene* s = nullptr;
+    vkb_profile pf{};
+    float4* out_dev = nullptr;      // device destination of the mean image
+    uint32_t* ids_dev = nullptr;    // device primary ids (first sample) or null
+    float4* accum = nullptr;        // device accumulator, npix
+    uint32_t npix = 0, count = 0, done = 0, pixel_base = 0;
+};
+struct WaveTotals {
+    uint32_t launches = 0, trace_launches = 0;
+    float trace_ms = 0.f, render_ms = 0.f;
+    uint32_t counters[16] = {};
+    unsigned long long work[8] = {};
+    uint32_t err = 0;
+};
+
+void validate_profile(const vkb_profile* pf) {
+    if (pf->adaptive) throw Unsupported{"adaptive sampling is outside the built subset"};
+    if (pf->samples == 0) throw ArgError{"samples must be positive"};
+    if (pf->first_sample >= pf->samples) throw ArgError{"first_sample beyond samples"};
+    uint32_t count = pf->sample_count ? pf->sample_count : pf->samples - pf->first_sample;
+    if (pf->first_sample + count > pf->samples) throw ArgError{"sample range beyond samples"};
+    if (pf->bounces[0] > 250) throw ArgError{"bounce budget above 250"};
+}
+uint32_t sample_mask_of(uint32_t samples) { return samples <= 1 ? 0u : ((2u << (31 - __builtin_clz(samples - 1u))) - 1u); }
+
+// The static part of a job's device record (the wave fields are set per wave).
+Job make_job(const EngineJob& e) {
+    const vkb_scene* s = e.s;
+    const vkb_profile& pf = e.pf;
+    Job j{};
+    j.sv = scene_view(s);
+    j.o2w = s->o2w.p; j.w2o = s->w2o.p; j.inst_info = s->inst_info.p; j.meshes = s->meshes.p;
+    j.vpos = s->vpos.p; j.vnrm = s->vnrm.p; j.indices = s->indices.p;
+    j.materials = s->d_materials.p; j.lights = s->d_lights.p; j.num_lights = uint32_t(s->lights.size());
+    j.tree = s->tree.p; j.tree_nodes = s->tree_nodes;
+    j.cam = s->camera; j.env = s->env;
+    j.spp = pf.samples; j.seed = pf.seed;
+    for (int k = 0; k < 4; ++k) j.bounces[k] = pf.bounces[k];
+    j.caustics = pf.caustics;
+    j.sample_mask = sample_mask_of(pf.samples);
+    j.clamp_direct = pf.clamp_direct; j.clamp_indirect = pf.clamp_indirect; j.light_threshold = pf.light_threshold;
+    j.npix = e.npix; j.first_sample = pf.first_sample;
+    j.pixel_base = e.pixel_base;
+    j.accum = e.accum; j.primary_ids = e.ids_dev; j.out = e.out_dev;
+    return j;
+}
+
+PathParams path_params(const vkb_ctx* c, const WaveBuffers& w, uint32_t njobs) {
+    PathParams p{};
+    p.jobs = w.jobs; p.njobs = njobs; p.slot_job = w.slot_job;
+    p.lut.texels = c->lut.p; p.filter = c->filter.p;
+    p.ray_o[0] = w.ray_o0; p.ray_d[0] = w.ray_d0; p.ray_o[1] = w.ray_o1; p.ray_d[1] = w.ray_d1;
+    p.hit = w.hit; p.hit_inst = w.hit_inst; p.thr = w.thr; p.rad = w.rad; p.rng = w.rng;
+    p.sa_o = w.sa_o; p.sa_d = w.sa_d; p.sa_c = w.sa_c; p.sb_o = w.sb_o; p.sb_d = w.sb_d; p.sb_c = w.sb_c;
+    p.counters = w.counters; p.work = w.work; p.err = w.err;
+    return p;
+}
+
+// The kernels of one wave: camera, then per bounce closest-hit trace, shade, shadow trace;
+// then accumulation.  Timed mode records events around every closest-hit trace.
+template <bool BATCH>
+void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counted, bool timed, WaveTotals& tot) {
+    cudaStream_t st = c->stream;
+    const int sms = c->sms, tgrid = sms * c->trace_blocks_per_sm, sgrid = sms * c->trace_blocks_per_sm;
+    k_start_wave<<<1, 1, 0, st>>>(p.counters);
+    k_camera<BATCH><<<sms * 8, 256, 0, st>>>(p);
+    for (uint32_t b = 0; b <= bounces; ++b) {
+        int cur = int(b & 1u);
+        if (timed) {
+            while (c->kernel_events.size() < 2 * (tot.trace_launches + 1)) {
+                cudaEvent_t e;
+                VKB_CUDA(cudaEventCreate(&e));
+                c->kernel_events.push_back(e);
+            }
+            VKB_CUDA(cudaEventRecord(c->kernel_events[2 * tot.trace_launches], st));
+        }
+        if (counted) k_trace<false, true, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p, cur);
+        else k_trace<false, false, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p, cur);
+        if (timed) VKB_CUDA(cudaEventRecord(c->kernel_events[2 * tot.trace_launches + 1], st));
+        tot.trace_launches++;
+        k_reset_queues<<<1, 1, 0, st>>>(p.counters, cur ^ 1);
+        k_shade<BATCH><<<sgrid, 128, 0, st>>>(p, cur);
+        if (counted) k_trace<true, true, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p, -1);
+        else k_trace<true, false, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p, -1);
+    }
+    k_accumulate<BATCH><<<sms * 8, 256, 0, st>>>(p);
+    tot.launches += 3 + 4 * (bounces + 1);
+}
+
+// A wavefront that runs jobs wave by wave.  Each wave gives one sample to every
+// unfinished job that fits (in admission order), then more samples while path slots
+// remain; uploads the job table; and runs the wave, replayed from a captured CUDA
+// graph when several jobs share it.  Jobs may be added between waves (continuous
+// batching) and are resolved into their out_dev when finished.
+struct WaveEngine {
+    vkb_ctx* c;
+    WaveBuffers w;
+    size_t capacity;
+    uint32_t flags;
+    bool graphs;
+    std::vector<EngineJob> jobs;
+    std::vector<Job> table;
+    WaveTotals tot;
+    std::vector<GraphEntry> captured;   // this engine's wave graphs (they point at its buffers)
+    ~WaveEngine() { for (auto& g : captured) cudaGraphExecDestroy(g.exec); }
+    WaveEngine(vkb_ctx* ctx, const WaveBuffers& wb, size_t cap, uint32_t fl, bool use_graphs) : c(ctx), w(wb), capacity(cap), flags(fl), graphs(use_graphs) {
+        cudaStream_t st = c->stream;
+        VKB_CUDA(cudaMemsetAsync(w.counters, 0, 16 * sizeof(uint32_t), st));
+        VKB_CUDA(cudaMemsetAsync(w.err, 0, sizeof(uint32_t), st));
+        VKB_CUDA(cudaMemsetAsync(w.work, 0, 8 * sizeof(unsigned long long), st));
+    }
+    void add(EngineJob e) {
+        VKB_CUDA(cudaMemsetAsync(e.accum, 0, size_t(e.npix) * sizeof(float4), c->stream));
+        jobs.push_back(e);
+        table.push_back(make_job(jobs.back()));
+    }
+    bool finished(size_t k) const { return jobs[k].done >= jobs[k].count; }
+    // Drop finished jobs (after resolve) from the front of the table.
+    void compact() {
+        size_t o = 0;
+        for (size_t k = 0; k < jobs.size(); ++k)
+            if (!finished(k)) { jobs[o] = jobs[k]; table[o] = table[k]; ++o; }
+        jobs.resize(o); table.resize(o);
+    }
+    // One wave; false when no job has work left.
+    bool step() {
+        cudaStream_t st = c->stream;
+        const uint32_t njobs = uint32_t(jobs.size());
+        if (njobs == 0) return false;
+        if (njobs > w.job_capacity) throw ArgError{"more active jobs than the job table holds"};
+        const bool batch = njobs > 1;
+        const bool timed = (flags & VKB_PROFILE_TIME_KERNELS) != 0, counted = (flags & VKB_PROFILE_COUNT_TRAVERSAL) != 0;
+        const bool use_graph = graphs && batch && !timed;
+        std::vector<uint32_t> take(njobs, 0u);
+        size_t left = capacity;
+        bool any = false;
+        for (uint32_t k = 0; k < njobs; ++k) {
+            EngineJob& e = jobs[k];
+            if (finished(k)) continue;
+            if (size_t(e.npix) <= left || !any) { take[k] = 1; left = size_t(e.npix) <= left ? left - e.npix : 0; any = true; }
+        }
+        if (!any) return false;
+        for (uint32_t k = 0; k < njobs; ++k) {
+            if (!take[k]) continue;
+            EngineJob& e = jobs[k];
+            uint32_t more = uint32_t(std::min<size_t>(e.count - e.done - 1, left / e.npix));
+            take[k] += more;
+            left -= size_t(more) * e.npix;
+        }
+        uint32_t n_paths = 0, bounces = 0, total_pixels = 0;
+        for (uint32_t k = 0; k < njobs; ++k) {
+            EngineJob& e = jobs[k];
+            Job& j = table[k];
+            e.pixel_base = total_pixels; j.pixel_base = total_pixels; total_pixels += e.npix;
+            j.wave_first = e.pf.first_sample + e.done;
+            j.wave_samples = take[k];
+            j.slot_base = n_paths;
+            n_paths += take[k] * e.npix;
+            e.done += take[k];
+            if (take[k]) bounces = std::max(bounces, e.pf.bounces[0]);
+        }
+        uint32_t wave_counts[2] = {n_paths, total_pixels};
+        VKB_CUDA(cudaMemcpyAsync(w.jobs, table.data(), njobs * sizeof(Job), cudaMemcpyHostToDevice, st));
+        VKB_CUDA(cudaMemcpyAsync(w.counters + 7, wave_counts, sizeof(wave_counts), cudaMemcpyHostToDevice, st));
+        PathParams p = path_params(c, w, njobs);
+        p.job0 = table[0];
+        if (use_graph) {
+            uint64_t key = (uint64_t(bounces) << 1) | 1u;
+            key = key * 1315423911ull + (counted ? 7u : 3u);
+            key = key * 40503ull + njobs;
+            key = key * 97ull + uint64_t(c->trace_blocks_per_sm);
+            cudaGraphExec_t exec = nullptr;
+            for (auto& g : captured) if (g.key == key) exec = g.exec;
+            if (!exec) {
+                cudaGraph_t g;
+                VKB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                WaveTotals scratch;
+                wave_kernels<true>(c, p, bounces, counted, false, scratch);
+                VKB_CUDA(cudaStreamEndCapture(st, &g));
+                VKB_CUDA(cudaGraphInstantiate(&exec, g, 0));
+                VKB_CUDA(cudaGraphDestroy(g));
+                captured.push_back({key, exec});
+            }
+            VKB_CUDA(cudaGraphLaunch(exec, st));
+            tot.launches += 3 + 4 * (bounces + 1);
+            tot.trace_launches += bounces + 1;
+        } else if (batch) {
+            wave_kernels<true>(c, p, bounces, counted, timed, tot);
+        } else {
+            wave_kernels<false>(c, p, bounces, counted, timed, tot);
+        }
+        VKB_CUDA(cudaGetLastError());
+        return true;
+    }
+    // Mean image of job k into its out_dev.
+    void resolve(size_t k) {
+        PathParams p = path_params(c, w, 1);
+        p.job0 = table[k];
+        p.job0.pixel_base = 0;
+        k_resolve<false><<<grid_for(jobs[k].npix, 256, c->sms), 256, 0, c->stream>>>(p, jobs[k].npix);
+        tot.launches += 1;
+    }
+    // Counters, traversal work and device time of everything run so far (synchronises).
+    void collect(float ms_since_ev0) {
+        cudaStream_t st = c->stream;
+        VKB_CUDA(cudaMemcpyAsync(tot.counters, w.counters, sizeof(tot.counters), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaMemcpyAsync(tot.work, w.work, sizeof(tot.work), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaMemcpyAsync(&tot.err, w.err, sizeof(tot.err), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaStreamSynchronize(st));
+        tot.render_ms = ms_since_ev0;
+        if (flags & VKB_PROFILE_TIME_KERNELS)
+            for (uint32_t k = 0; k < tot.trace_launches; ++k) {
+                float e = 0.f;
+                VKB_CUDA(cudaEventElapsedTime(&e, c->kernel_events[2 * k], c->kernel_events[2 * k + 1]));
+                tot.trace_ms += e;
+            }
+    }
+};
+
+// Run `jobs` to completion on the wavefront `w` and resolve each into its out_dev.
+void run_engine(vkb_ctx* c, std::vector<EngineJob>& jobs, const WaveBuffers& w, size_t capacity, uint32_t flags, bool graphs, WaveTotals& tot) {
+    WaveEngine eng(c, w, capacity, flags, graphs);
+    for (auto& e : jobs) eng.add(e);
+    VKB_CUDA(cudaEventRecord(c->ev0, c->stream));
+    while (eng.step()) {}
+    VKB_CUDA(cudaEventRecord(c->ev1, c->stream));
+    for (size_t k = 0; k < eng.jobs.size(); ++k) eng.resolve(k);
+    VKB_CUDA(cudaEventSynchronize(c->ev1));
+    float ms = 0.f;
+    VKB_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    eng.collect(ms);
+    tot = eng.tot;
+    for (size_t k = 0; k < jobs.size(); ++k) jobs[k] = eng.jobs[k];
+}
+
+void fill_stats(vkb_stats* stats, const WaveTotals& t, uint64_t paths, float build_ms) {
+    if (!stats) return;
+    std::memset(stats, 0, sizeof(*stats));
+    stats->paths = paths;
+    stats->extension_rays = t.counters[3];
+    stats->shadow_rays = t.counters[4];
+    stats->dropped_light_samples = t.counters[5];
+    stats->dropped_path_samples = t.counters[6];
+    stats->traversal_overflows = t.err;
+    stats->render_ms = t.render_ms;
+    stats->build_ms = build_ms;
+    stats->trace_ms = t.trace_ms;
+    stats->trace_launches = t.trace_launches;
+    stats->kernel_launches = t.launches;
+    stats->nodes_visited = t.work[0];
+    stats->triangles_tested = t.work[1];
+    stats->instances_entered = t.work[2];
+    stats->shadow_nodes_visited = t.work[3];
+    stats->shadow_triangles_tested = t.work[4];
+    stats->blas_nodes_visited = t.work[5];
+}
+
+// Render jobs with the context's own buffers (grown on demand).
+void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile>>& in, std::vector<vkb_output*>& outs, uint32_t flags,
+                 uint32_t wave_samples_hint, WaveTotals& tot, uint64_t& paths) {
+    cudaStream_t st = c->stream;
+    size_t total_pixels = 0, max_pix = 0, ids_words = 0, staged = 0;
+    for (size_t k = 0; k < in.size(); ++k) {
+        const vkb_camera& cam = in[k].first->camera;
+        size_t npix = size_t(cam.width) * cam.height;
+        total_pixels += npix; max_pix = std::max(max_pix, npix);
+        if (outs[k]->primary_ids) ids_words += 2 * npix;
+        if (!outs[k]->on_device) staged += npix;
+    }
+    size_t capacity = c->wave_capacity;
+    if (in.size() == 1 && wave_samples_hint) capacity = max_pix * wave_samples_hint;
+    capacity = std::max(capacity, max_pix);
+    c->wave.reserve(capacity, uint32_t(in.size()));
+    c->accum.alloc(std::max<size_t>(1, total_pixels));
+    if (staged) c->staging.alloc(staged);
+    if (ids_words) c->ids.alloc(ids_words);
+    std::vector<EngineJob> jobs(in.size());
+    size_t acc = 0, stg = 0, idw = 0;
+    for (size_t k = 0; k < in.size(); ++k) {
+        EngineJob& e = jobs[k];
+        e.s = in[k].first; e.pf = in[k].second;
+        e.npix = e.s->camera.width * e.s->camera.height;
+        e.count = e.pf.sample_count ? e.pf.sample_count : e.pf.samples - e.pf.first_sample;
+        e.accum = c->accum.p + acc; acc += e.npix;
+        if (outs[k]->on_device) e.out_dev = reinterpret_cast<float4*>(outs[k]->rgba);
+        else { e.out_dev = c->staging.p + stg; stg += e.npix; }
+        if (outs[k]->primary_ids) { e.ids_dev = c->ids.p + idw; idw += 2 * size_t(e.npix); }
+        paths += uint64_t(e.npix) * e.count;
+    }
+    run_engine(c, jobs, c->wave.view(), capacity, flags, true, tot);
+    for (size_t k = 0; k < in.size(); ++k) {
+        if (!outs[k]->on_device) VKB_CUDA(cudaMemcpyAsync(outs[k]->rgba, jobs[k].out_dev, size_t(jobs[k].npix) * sizeof(float4), cudaMemcpyDeviceToHost, st));
+        if (outs[k]->primary_ids) VKB_CUDA(cudaMemcpyAsync(outs[k]->primary_ids, jobs[k].ids_dev, size_t(jobs[k].npix) * 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    }
+    VKB_CUDA(cudaStreamSynchronize(st));
+    c->launches += tot.launches;
+}
 }  // namespace
 
 extern "C" {
@@ -458,6 +810,8 @@ vkb_status vkb_open(int device, vkb_ctx** out) {
         VKB_CUDA(cudaSetDevice(device));
         VKB_CUDA(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
         VKB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        VKB_CUDA(cudaEventCreate(&c->ev0));
+        VKB_CUDA(cudaEventCreate(&c->ev1));
         c->lut.alloc(size_t(BRDF_SIZE) * BRDF_HEIGHT);
         k_bake_lut<<<dim3(1, BRDF_HEIGHT), BRDF_SIZE, 0, c->stream>>>(c->lut.p);
         VKB_CUDA(cudaGetLastError());
@@ -473,6 +827,12 @@ vkb_status vkb_open(int device, vkb_ctx** out) {
 vkb_status vkb_close(vkb_ctx* c) {
     if (!c) return VKB_OK;
     cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (cudaEvent_t e : c->kernel_events) cudaEventDestroy(e);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    c->wave.release();
+    c->accum.release(); c->staging.release(); c->ids.release();
     c->lut.release(); c->filter.release();
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -605,15 +965,12 @@ vkb_status vkb_scene_destroy(vkb_scene* s) {
     if (!s) return VKB_OK;
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->ctx->stream);
-    DBuf<float4>* f4[] = {&s->vpos, &s->vnrm, &s->blas_tris, &s->o2w, &s->w2o, &s->inst_lo, &s->inst_hi, &s->tri_lo, &s->tri_hi,
-                          &s->ray_o0, &s->ray_d0, &s->ray_o1, &s->ray_d1, &s->hit, &s->thr, &s->rad, &s->sa_o, &s->sa_d, &s->sa_c,
-                          &s->sb_o, &s->sb_d, &s->sb_c, &s->accum, &s->out_rgba};
+    DBuf<float4>* f4[] = {&s->vpos, &s->vnrm, &s->blas_tris, &s->o2w, &s->w2o, &s->inst_lo, &s->inst_hi, &s->tri_lo, &s->tri_hi};
     for (auto* b : f4) b->release();
     s->indices.release(); s->tlas_codes.release();
     s->tlas_order.release(); s->tlas_leaf_parent.release(); s->tlas_node_parent.release(); s->tlas_counters.release(); s->inst_info.release(); s->meshes.release();
     s->blas_nodes.release(); s->tlas_nodes.release(); s->tlas_leaves.release(); s->d_materials.release(); s->d_lights.release();
-    s->tree.release(); s->hit_inst.release(); s->counters.release(); s->err.release(); s->ids.release(); s->rng.release(); s->work.release();
-    for (cudaEvent_t e : s->kernel_events) cudaEventDestroy(e);
+    s->tree.release();
     s->scratch.codes.release(); s->scratch.codes_sorted.release(); s->scratch.ids.release(); s->scratch.ids_sorted.release();
     s->scratch.leaf_parent.release(); s->scratch.node_parent.release(); s->scratch.counters.release(); s->scratch.bounds.release(); s->scratch.cub_temp.release();
     if (s->ev0) cudaEventDestroy(s->ev0);
@@ -658,125 +1015,105 @@ vkb_status vkb_scene_update_instances_device(vkb_scene* s, const float* rows, ui
 vkb_status vkb_render(vkb_scene* s, const vkb_profile* pf, vkb_output* out, vkb_stats* stats) {
     if (!s || !pf || !out || !out->rgba) return fail(VKB_INVALID_ARG, "null scene, profile or output");
     return guarded([&] {
-        if (pf->adaptive) throw Unsupported{"adaptive sampling is outside the built subset"};
-        if (pf->samples == 0) throw ArgError{"samples must be positive"};
-        if (pf->first_sample >= pf->samples) throw ArgError{"first_sample beyond samples"};
-        uint32_t count = pf->sample_count ? pf->sample_count : pf->samples - pf->first_sample;
-        if (pf->first_sample + count > pf->samples) throw ArgError{"sample range beyond samples"};
-        if (pf->bounces[0] > 250) throw ArgError{"bounce budget above 250"};
+        validate_profile(pf);
         vkb_ctx* c = s->ctx;
         VKB_CUDA(cudaSetDevice(c->device));
-        cudaStream_t st = c->stream;
-        int sms = c->sms;
-        const uint32_t W = s->camera.width, H = s->camera.height, npix = W * H;
-        uint32_t wave = pf->wave_samples;
-        if (wave == 0) wave = std::max(1u, std::min(count, (8u << 20) / std::max(1u, npix)));
-        wave = std::min(wave, count);
-        size_t slots = size_t(npix) * wave;
-        s->ray_o0.alloc(slots); s->ray_d0.alloc(slots); s->ray_o1.alloc(slots); s->ray_d1.alloc(slots);
-        s->hit.alloc(slots); s->hit_inst.alloc(slots); s->thr.alloc(slots); s->rad.alloc(slots); s->rng.alloc(slots);
-        s->sa_o.alloc(slots); s->sa_d.alloc(slots); s->sa_c.alloc(slots); s->sb_o.alloc(slots); s->sb_d.alloc(slots); s->sb_c.alloc(slots);
-        s->accum.alloc(npix); s->counters.alloc(16); s->err.alloc(1); s->work.alloc(8);
-        const bool timed = (pf->flags & VKB_PROFILE_TIME_KERNELS) != 0, counted = (pf->flags & VKB_PROFILE_COUNT_TRAVERSAL) != 0;
-        uint32_t launches = 0, trace_launches = 0;
-        VKB_CUDA(cudaMemsetAsync(s->work.p, 0, 8 * sizeof(unsigned long long), st));
-        if (out->primary_ids) s->ids.alloc(size_t(npix) * 2);
-        VKB_CUDA(cudaMemsetAsync(s->accum.p, 0, npix * sizeof(float4), st));
-        VKB_CUDA(cudaMemsetAsync(s->counters.p, 0, 16 * sizeof(uint32_t), st));
-        VKB_CUDA(cudaMemsetAsync(s->err.p, 0, sizeof(uint32_t), st));
-        PathParams p{};
-        p.sv = scene_view(s);
-        p.o2w = s->o2w.p; p.w2o = s->w2o.p; p.inst_info = s->inst_info.p; p.meshes = s->meshes.p;
-        p.vpos = s->vpos.p; p.vnrm = s->vnrm.p; p.indices = s->indices.p;
-        p.materials = s->d_materials.p; p.lights = s->d_lights.p; p.num_lights = uint32_t(s->lights.size());
-        p.tree = s->tree.p; p.tree_nodes = s->tree_nodes;
-        p.lut.texels = c->lut.p; p.filter = c->filter.p;
-        p.cam = s->camera; p.env = s->env;
-        p.spp = pf->samples; p.seed = pf->seed;
-        for (int k = 0; k < 4; ++k) p.bounces[k] = pf->bounces[k];
-        p.caustics = pf->caustics;
-        p.sample_mask = pf->samples <= 1 ? 0u : ((2u << (31 - __builtin_clz(pf->samples - 1u))) - 1u);
-        p.clamp_direct = pf->clamp_direct; p.clamp_indirect = pf->clamp_indirect; p.light_threshold = pf->light_threshold;
-        p.npix = npix; p.first_sample = pf->first_sample;
-        p.ray_o[0] = s->ray_o0.p; p.ray_d[0] = s->ray_d0.p; p.ray_o[1] = s->ray_o1.p; p.ray_d[1] = s->ray_d1.p;
-        p.hit = s->hit.p; p.hit_inst = s->hit_inst.p; p.thr = s->thr.p; p.rad = s->rad.p; p.rng = s->rng.p;
-        p.sa_o = s->sa_o.p; p.sa_d = s->sa_d.p; p.sa_c = s->sa_c.p; p.sb_o = s->sb_o.p; p.sb_d = s->sb_d.p; p.sb_c = s->sb_c.p;
-        p.accum = s->accum.p; p.counters = s->counters.p; p.err = s->err.p; p.work = s->work.p;
-        p.primary_ids = out->primary_ids ? s->ids.p : nullptr;
-        VKB_CUDA(cudaEventRecord(s->ev0, st));
-        for (uint32_t done = 0; done < count; done += wave) {
-            uint32_t ws = std::min(wave, count - done);
-            p.wave_first = pf->first_sample + done;
-            p.wave_samples = ws;
-            p.n_paths = npix * ws;
-            VKB_CUDA(cudaMemcpyAsync(s->counters.p, &p.n_paths, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-            k_camera<<<grid_for(p.n_paths, 256, sms), 256, 0, st>>>(p);
-            const int tgrid = sms * 16, sgrid = sms * 16;
-            for (uint32_t b = 0; b <= pf->bounces[0]; ++b) {
-                int cur = int(b & 1u);
-                if (timed) {
-                    while (s->kernel_events.size() < 2 * (trace_launches + 1)) {
-                        cudaEvent_t e;
-                        VKB_CUDA(cudaEventCreate(&e));
-                        s->kernel_events.push_back(e);
-                    }
-                    VKB_CUDA(cudaEventRecord(s->kernel_events[2 * trace_launches], st));
-                }
-                if (counted) k_trace<false, true><<<tgrid, 128, 0, st>>>(p, cur);
-                else k_trace<false, false><<<tgrid, 128, 0, st>>>(p, cur);
-                if (timed) VKB_CUDA(cudaEventRecord(s->kernel_events[2 * trace_launches + 1], st));
-                trace_launches++;
-                k_reset_queues<<<1, 1, 0, st>>>(s->counters.p, cur ^ 1);
-                k_shade<<<sgrid, 128, 0, st>>>(p, cur);
-                if (counted) k_trace<true, true><<<tgrid, 128, 0, st>>>(p, -1);
-                else k_trace<true, false><<<tgrid, 128, 0, st>>>(p, -1);
-                launches += 4;
-            }
-            k_accumulate<<<grid_for(npix, 256, sms), 256, 0, st>>>(p);
-            launches += 2;
-            VKB_CUDA(cudaGetLastError());
+        std::vector<std::pair<vkb_scene*, vkb_profile>> in{{s, *pf}};
+        std::vector<vkb_output*> outs{out};
+        WaveTotals tot;
+        uint64_t paths = 0;
+        uint32_t hint = pf->wave_samples;
+        if (!hint) {
+            uint32_t count = pf->sample_count ? pf->sample_count : pf->samples - pf->first_sample;
+            size_t npix = size_t(s->camera.width) * s->camera.height;
+            hint = uint32_t(std::max<size_t>(1, std::min<size_t>(count, c->wave_capacity / std::max<size_t>(1, npix))));
         }
-        VKB_CUDA(cudaEventRecord(s->ev1, st));
-        float4* dst;
-        if (out->on_device) dst = reinterpret_cast<float4*>(out->rgba);
-        else { s->out_rgba.alloc(npix); dst = s->out_rgba.p; }
-        k_resolve<<<grid_for(npix, 256, sms), 256, 0, st>>>(npix, s->accum.p, dst);
-        launches += 1;
-        s->launches += launches;
-        unsigned long long work[8] = {};
-        VKB_CUDA(cudaMemcpyAsync(work, s->work.p, sizeof(work), cudaMemcpyDeviceToHost, st));
-        if (!out->on_device) VKB_CUDA(cudaMemcpyAsync(out->rgba, dst, npix * sizeof(float4), cudaMemcpyDeviceToHost, st));
-        if (out->primary_ids) VKB_CUDA(cudaMemcpyAsync(out->primary_ids, s->ids.p, size_t(npix) * 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        uint32_t ctr[16], err = 0;
-        VKB_CUDA(cudaMemcpyAsync(ctr, s->counters.p, sizeof(ctr), cudaMemcpyDeviceToHost, st));
-        VKB_CUDA(cudaMemcpyAsync(&err, s->err.p, sizeof(err), cudaMemcpyDeviceToHost, st));
-        VKB_CUDA(cudaStreamSynchronize(st));
-        float ms = 0.f;
-        VKB_CUDA(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
-        if (stats) {
-            stats->paths = uint64_t(npix) * count;
-            stats->extension_rays = ctr[3];
-            stats->shadow_rays = ctr[4];
-            stats->dropped_light_samples = ctr[5];
-            stats->dropped_path_samples = ctr[6];
-            stats->traversal_overflows = err;
-            stats->render_ms = ms;
-            stats->build_ms = s->build_ms;
-            stats->trace_ms = 0.f;
-            if (timed)
-                for (uint32_t k = 0; k < trace_launches; ++k) {
-                    float e = 0.f;
-                    VKB_CUDA(cudaEventElapsedTime(&e, s->kernel_events[2 * k], s->kernel_events[2 * k + 1]));
-                    stats->trace_ms += e;
+        render_jobs(c, in, outs, pf->flags, hint, tot, paths);
+        s->launches += tot.launches;
+        fill_stats(stats, tot, paths, s->build_ms);
+    });
+}
+
+vkb_status vkb_render_batch(vkb_ctx* c, vkb_job* jobs, uint32_t njobs, uint32_t flags, vkb_stats* stats) {
+    if (!c || (njobs && !jobs)) return fail(VKB_INVALID_ARG, "null context or jobs");
+    return guarded([&] {
+        if (njobs == 0) { if (stats) std::memset(stats, 0, sizeof(*stats)); return; }
+        VKB_CUDA(cudaSetDevice(c->device));
+        std::vector<std::pair<vkb_scene*, vkb_profile>> in(njobs);
+        std::vector<vkb_output*> outs(njobs);
+        for (uint32_t k = 0; k < njobs; ++k) {
+            if (!jobs[k].scene || !jobs[k].out.rgba) throw ArgError{"job " + std::to_string(k) + " has a null scene or output"};
+            if (jobs[k].scene->ctx != c) throw ArgError{"job " + std::to_string(k) + " belongs to another context"};
+            validate_profile(&jobs[k].profile);
+            in[k] = {jobs[k].scene, jobs[k].profile};
+            outs[k] = &jobs[k].out;
+        }
+        WaveTotals tot;
+        uint64_t paths = 0;
+        render_jobs(c, in, outs, flags, 0, tot, paths);
+        fill_stats(stats, tot, paths, 0.f);
+    });
+}
+
+vkb_status vkb_autotune(vkb_ctx* c, vkb_job* jobs, uint32_t njobs, vkb_tune_result* out) {
+    if (!c || !jobs || njobs == 0) return fail(VKB_INVALID_ARG, "null context or no jobs");
+    return guarded([&] {
+        VKB_CUDA(cudaSetDevice(c->device));
+        // Candidates: wave capacity (queue slots) x trace/shade blocks per SM, each timed on
+        // one sample of every job (same work for every candidate).
+        const size_t caps[] = {size_t(2) << 20, size_t(4) << 20, size_t(8) << 20, size_t(16) << 20};
+        const int grids[] = {8, 16, 32};
+        std::vector<std::pair<vkb_scene*, vkb_profile>> in(njobs);
+        std::vector<vkb_output> o(njobs);
+        std::vector<vkb_output*> outs(njobs);
+        size_t max_pix = 0;
+        for (uint32_t k = 0; k < njobs; ++k) {
+            vkb_profile pf = jobs[k].profile;
+            validate_profile(&pf);
+            pf.sample_count = 1;
+            in[k] = {jobs[k].scene, pf};
+            max_pix = std::max(max_pix, size_t(jobs[k].scene->camera.width) * jobs[k].scene->camera.height);
+        }
+        c->staging.alloc(1);
+        size_t best_cap = c->wave_capacity;
+        int best_grid = c->trace_blocks_per_sm;
+        float best_ms = INFINITY;
+        uint32_t tried = 0;
+        for (size_t cap : caps)
+            for (int g : grids) {
+                c->wave_capacity = std::max(cap, max_pix);
+                c->trace_blocks_per_sm = g;
+                // Device outputs into the staging buffer region (results are discarded).
+                size_t total = 0;
+                for (uint32_t k = 0; k < njobs; ++k) total += size_t(in[k].first->camera.width) * in[k].first->camera.height;
+                c->staging.alloc(total);
+                size_t off = 0;
+                for (uint32_t k = 0; k < njobs; ++k) {
+                    o[k] = vkb_output{};
+                    o[k].rgba = reinterpret_cast<float*>(c->staging.p + off);
+                    o[k].on_device = 1;
+                    outs[k] = &o[k];
+                    off += size_t(in[k].first->camera.width) * in[k].first->camera.height;
                 }
-            stats->trace_launches = trace_launches;
-            stats->kernel_launches = launches;
-            stats->nodes_visited = work[0];
-            stats->triangles_tested = work[1];
-            stats->instances_entered = work[2];
-            stats->shadow_nodes_visited = work[3];
-            stats->shadow_triangles_tested = work[4];
-            stats->blas_nodes_visited = work[5];
+                WaveTotals warm, tot;
+                uint64_t paths = 0;
+                render_jobs(c, in, outs, 0, 0, warm, paths);  // captures this shape's graphs
+                render_jobs(c, in, outs, 0, 0, tot, paths);
+                if (out && tried < 16) {
+                    out->capacity[tried] = uint64_t(c->wave_capacity);
+                    out->blocks_per_sm[tried] = uint32_t(g);
+                    out->ms[tried] = tot.render_ms;
+                }
+                ++tried;
+                if (tot.render_ms < best_ms) { best_ms = tot.render_ms; best_cap = c->wave_capacity; best_grid = g; }
+            }
+        c->wave_capacity = best_cap;
+        c->trace_blocks_per_sm = best_grid;
+        if (out) {
+            out->tried = tried;
+            out->best_capacity = uint64_t(best_cap);
+            out->best_blocks_per_sm = uint32_t(best_grid);
+            out->best_ms = best_ms;
         }
     });
 }
@@ -885,6 +1222,161 @@ vkb_status vkb_debug_trace(vkb_scene* s, uint32_t n, const float* rays7, float* 
 
 }  // extern "C"
 
+
+// ================================================================ serving
+// Continuous batching: requests queue on the host; at every wave boundary the server
+// admits queued requests (FIFO) while the job table has room and the device-memory
+// budget holds (resident scenes + shared wavefront + every admitted job's accumulator
+// and output staging), runs one wave over all admitted jobs, and returns finished
+// images.  vork's own kept-alive session serves one request at a time
+// (crates/vork-cli/src/session.rs:1-60, crates/vork-render/src/shot/worker.rs).
+struct vkb_server {
+    vkb_ctx* c = nullptr;
+    uint64_t budget = 0;
+    uint32_t max_jobs = 0;
+    size_t capacity = 0;
+    Wavefront wave;                                   // the server's own queues (renders on the context keep theirs)
+    std::unique_ptr<WaveEngine> eng;
+    struct Pending { uint64_t id; vkb_scene* s; vkb_profile pf; float* host_out; };
+    struct Live { uint64_t id; float* host_out; DBuf<float4> accum, out; uint64_t bytes; };
+    std::deque<Pending> queue;
+    std::map<uint64_t, std::unique_ptr<Live>> live;   // admitted, keyed by id
+    std::map<uint64_t, int> state;                    // 0 queued, 1 running, 2 done
+    uint64_t next_id = 1, used_bytes = 0, peak_bytes = 0, wave_bytes = 0;
+    std::map<vkb_scene*, uint64_t> resident;           // scene -> device bytes
+};
+
+namespace {
+uint64_t scene_bytes(const vkb_scene* s) {
+    return s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas_nodes.n * sizeof(BvhNode) +
+           s->blas_tris.n * sizeof(float4) + s->tlas_nodes.n * sizeof(BvhNode) + s->tlas_leaves.n * sizeof(TlasLeaf) +
+           (s->o2w.n + s->w2o.n) * sizeof(float4);
+}
+uint64_t resident_bytes(const vkb_server* v) {
+    uint64_t b = 0;
+    for (auto& kv : v->resident) b += kv.second;
+    return b;
+}
+}  // namespace
+
+extern "C" {
+
+vkb_status vkb_server_create(vkb_ctx* c, const vkb_server_config* cfg, vkb_server** out) {
+    if (!c || !cfg || !out) return fail(VKB_INVALID_ARG, "null argument");
+    *out = nullptr;
+    auto v = std::make_unique<vkb_server>();
+    vkb_status st = guarded([&] {
+        if (cfg->max_jobs == 0 || cfg->max_jobs > 4096) throw ArgError{"max_jobs must be 1..4096"};
+        VKB_CUDA(cudaSetDevice(c->device));
+        v->c = c;
+        v->budget = cfg->memory_budget_bytes;
+        v->max_jobs = cfg->max_jobs;
+        v->capacity = cfg->wave_capacity ? size_t(cfg->wave_capacity) : c->wave_capacity;
+        v->wave_bytes = uint64_t(v->capacity) * 220u + uint64_t(v->max_jobs) * sizeof(Job);
+        if (v->budget && v->wave_bytes >= v->budget) throw ArgError{"memory budget below the wavefront's own footprint"};
+        v->wave.reserve(v->capacity, v->max_jobs);
+        v->eng = std::make_unique<WaveEngine>(c, v->wave.view(), v->capacity, cfg->flags, true);
+    });
+    if (st != VKB_OK) return st;
+    *out = v.release();
+    return VKB_OK;
+}
+
+vkb_status vkb_server_submit(vkb_server* v, vkb_scene* s, const vkb_profile* pf, float* host_rgba, uint64_t* id) {
+    if (!v || !s || !pf || !host_rgba || !id) return fail(VKB_INVALID_ARG, "null argument");
+    if (s->ctx != v->c) return fail(VKB_INVALID_ARG, "scene belongs to another context");
+    return guarded([&] {
+        validate_profile(pf);
+        uint64_t need = uint64_t(s->camera.width) * s->camera.height * 32u;
+        if (v->budget && v->wave_bytes + scene_bytes(s) + need > v->budget) throw ArgError{"request can never fit the memory budget"};
+        *id = v->next_id++;
+        v->queue.push_back({*id, s, *pf, host_rgba});
+        v->state[*id] = 0;
+    });
+}
+
+vkb_status vkb_server_step(vkb_server* v, vkb_server_status* status) {
+    if (!v) return fail(VKB_INVALID_ARG, "null server");
+    return guarded([&] {
+        vkb_ctx* c = v->c;
+        VKB_CUDA(cudaSetDevice(c->device));
+        WaveEngine& eng = *v->eng;
+        // Admit at the wave boundary.
+        while (!v->queue.empty() && eng.jobs.size() < v->max_jobs) {
+            auto& q = v->queue.front();
+            uint64_t npix = uint64_t(q.s->camera.width) * q.s->camera.height;
+            uint64_t need = npix * 32u;
+            uint64_t scene = v->resident.count(q.s) ? 0u : scene_bytes(q.s);
+            if (v->budget && v->wave_bytes + resident_bytes(v) + scene + v->used_bytes + need > v->budget) break;
+            auto live = std::make_unique<vkb_server::Live>();
+            live->id = q.id; live->host_out = q.host_out; live->bytes = need;
+            live->accum.alloc(npix); live->out.alloc(npix);
+            EngineJob e;
+            e.s = q.s; e.pf = q.pf; e.npix = uint32_t(npix);
+            e.count = q.pf.sample_count ? q.pf.sample_count : q.pf.samples - q.pf.first_sample;
+            e.accum = live->accum.p; e.out_dev = live->out.p;
+            eng.add(e);
+            v->resident[q.s] = scene_bytes(q.s);
+            v->used_bytes += need;
+            v->peak_bytes = std::max(v->peak_bytes, v->wave_bytes + resident_bytes(v) + v->used_bytes);
+            v->state[q.id] = 1;
+            v->live[q.id] = std::move(live);
+            v->queue.pop_front();
+        }
+        uint32_t finished = 0;
+        if (!eng.jobs.empty()) {
+            eng.step();
+            // Finished jobs: resolve, copy out, release.
+            std::vector<uint64_t> ids;
+            for (size_t k = 0; k < eng.jobs.size(); ++k) {
+                if (!eng.finished(k)) continue;
+                eng.resolve(k);
+                for (auto& kv : v->live)
+                    if (kv.second->out.p == eng.jobs[k].out_dev) {
+                        VKB_CUDA(cudaMemcpyAsync(kv.second->host_out, kv.second->out.p, size_t(eng.jobs[k].npix) * sizeof(float4), cudaMemcpyDeviceToHost, c->stream));
+                        ids.push_back(kv.first);
+                    }
+            }
+            VKB_CUDA(cudaStreamSynchronize(c->stream));
+            eng.compact();
+            for (uint64_t id : ids) {
+                v->used_bytes -= v->live[id]->bytes;
+                v->live.erase(id);
+                v->state[id] = 2;
+                ++finished;
+            }
+        }
+        if (status) {
+            status->queued = uint32_t(v->queue.size());
+            status->running = uint32_t(eng.jobs.size());
+            status->finished = finished;
+            status->used_bytes = v->wave_bytes + resident_bytes(v) + v->used_bytes;
+            status->peak_bytes = v->peak_bytes;
+        }
+    });
+}
+
+vkb_status vkb_server_poll(vkb_server* v, uint64_t id, int* state) {
+    if (!v || !state) return fail(VKB_INVALID_ARG, "null argument");
+    auto it = v->state.find(id);
+    if (it == v->state.end()) return fail(VKB_INVALID_ARG, "unknown request id");
+    *state = it->second;
+    return VKB_OK;
+}
+
+vkb_status vkb_server_destroy(vkb_server* v) {
+    if (!v) return VKB_OK;
+    cudaSetDevice(v->c->device);
+    cudaStreamSynchronize(v->c->stream);
+    v->live.clear();
+    v->eng.reset();
+    v->wave.release();
+    delete v;
+    return VKB_OK;
+}
+
+}  // extern "C"
+
 // ================================================================ render without allocation
 //
 // Some callers cannot allocate device memory while they render: a host renderer
@@ -934,23 +1426,22 @@ struct Carver {
 extern "C" vkb_status vkb_render_noalloc(vkb_scene* s, const vkb_profile* pf, vkb_output* out, vkb_stats* stats) {
     if (!s || !pf || !out || !out->rgba) return fail(VKB_INVALID_ARG, "null scene, profile or output");
     return guarded([&] {
-        if (pf->adaptive) throw Unsupported{"adaptive sampling is outside the built subset"};
-        if (pf->samples == 0) throw ArgError{"samples must be positive"};
-        if (pf->first_sample >= pf->samples) throw ArgError{"first_sample beyond samples"};
+        validate_profile(pf);
         uint32_t count = pf->sample_count ? pf->sample_count : pf->samples - pf->first_sample;
-        if (pf->first_sample + count > pf->samples) throw ArgError{"sample range beyond samples"};
-        if (pf->bounces[0] > 250) throw ArgError{"bounce budget above 250"};
         vkb_ctx* c = s->ctx;
         VKB_CUDA(cudaSetDevice(c->device));
         unsigned char* base = noalloc_scratch(c->device);
         cudaStream_t st = c->stream;
-        int sms = c->sms;
         const uint32_t W = s->camera.width, H = s->camera.height, npix = W * H;
-        // Fixed part: counters, error word, traversal counters, accumulator, optional ids and host staging.
+        // Fixed part: counters, error word, traversal counters, job table, accumulator,
+        // optional ids and host-output staging.
         Carver cv{base, 0, NOALLOC_SCRATCH_BYTES};
-        uint32_t* counters = cv.take<uint32_t>(16);
-        uint32_t* err = cv.take<uint32_t>(1);
-        unsigned long long* work = cv.take<unsigned long long>(8);
+        WaveBuffers w;
+        w.counters = cv.take<uint32_t>(16);
+        w.err = cv.take<uint32_t>(1);
+        w.work = cv.take<unsigned long long>(8);
+        w.jobs = cv.take<Job>(1);
+        w.job_capacity = 1;
         float4* accum = cv.take<float4>(npix);
         uint32_t* ids = out->primary_ids ? cv.take<uint32_t>(size_t(npix) * 2) : nullptr;
         float4* staging = out->on_device ? reinterpret_cast<float4*>(out->rgba) : cv.take<float4>(npix);
@@ -960,7 +1451,7 @@ extern "C" vkb_status vkb_render_noalloc(vkb_scene* s, const vkb_profile* pf, vk
         size_t free_bytes = fixed < NOALLOC_SCRATCH_BYTES ? NOALLOC_SCRATCH_BYTES - fixed : 0;
         // 15 regions, each rounded up to 256 bytes.
         size_t slots_fit = free_bytes > 15 * 256 ? (free_bytes - 15 * 256) / per_slot : 0;
-        if (!counters || !err || !work || !accum || (out->primary_ids && !ids) || !staging || slots_fit < npix)
+        if (!w.counters || !w.err || !w.work || !w.jobs || !accum || (out->primary_ids && !ids) || !staging || slots_fit < npix)
             throw ArgError{"vkb_render_noalloc: a " + std::to_string(W) + "x" + std::to_string(H) + " image needs " +
                            std::to_string((fixed + size_t(npix) * per_slot + 15 * 256) >> 10) + " KiB of scratch for one sample per wave; the fixed array holds " +
                            std::to_string(NOALLOC_SCRATCH_BYTES >> 10) + " KiB (use vkb_render)"};
@@ -968,80 +1459,27 @@ extern "C" vkb_status vkb_render_noalloc(vkb_scene* s, const vkb_profile* pf, vk
         if (pf->wave_samples) wave = std::min(wave, pf->wave_samples);
         wave = std::max(1u, wave);
         size_t slots = size_t(npix) * wave;
-        PathParams p{};
-        p.ray_o[0] = cv.take<float4>(slots); p.ray_d[0] = cv.take<float4>(slots);
-        p.ray_o[1] = cv.take<float4>(slots); p.ray_d[1] = cv.take<float4>(slots);
-        p.hit = cv.take<float4>(slots); p.hit_inst = cv.take<uint32_t>(slots);
-        p.thr = cv.take<float4>(slots); p.rad = cv.take<float4>(slots); p.rng = cv.take<uint2>(slots);
-        p.sa_o = cv.take<float4>(slots); p.sa_d = cv.take<float4>(slots); p.sa_c = cv.take<float4>(slots);
-        p.sb_o = cv.take<float4>(slots); p.sb_d = cv.take<float4>(slots); p.sb_c = cv.take<float4>(slots);
-        if (!p.sb_c) throw ArgError{"vkb_render_noalloc: scratch layout overflow"};
-        // The array keeps the previous call's contents: clear what must start at zero.
-        VKB_CUDA(cudaMemsetAsync(accum, 0, npix * sizeof(float4), st));
-        VKB_CUDA(cudaMemsetAsync(counters, 0, 16 * sizeof(uint32_t), st));
-        VKB_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), st));
-        VKB_CUDA(cudaMemsetAsync(work, 0, 8 * sizeof(unsigned long long), st));
-        p.sv = scene_view(s);
-        p.o2w = s->o2w.p; p.w2o = s->w2o.p; p.inst_info = s->inst_info.p; p.meshes = s->meshes.p;
-        p.vpos = s->vpos.p; p.vnrm = s->vnrm.p; p.indices = s->indices.p;
-        p.materials = s->d_materials.p; p.lights = s->d_lights.p; p.num_lights = uint32_t(s->lights.size());
-        p.tree = s->tree.p; p.tree_nodes = s->tree_nodes;
-        p.lut.texels = c->lut.p; p.filter = c->filter.p;
-        p.cam = s->camera; p.env = s->env;
-        p.spp = pf->samples; p.seed = pf->seed;
-        for (int k = 0; k < 4; ++k) p.bounces[k] = pf->bounces[k];
-        p.caustics = pf->caustics;
-        p.sample_mask = pf->samples <= 1 ? 0u : ((2u << (31 - __builtin_clz(pf->samples - 1u))) - 1u);
-        p.clamp_direct = pf->clamp_direct; p.clamp_indirect = pf->clamp_indirect; p.light_threshold = pf->light_threshold;
-        p.npix = npix; p.first_sample = pf->first_sample;
-        p.accum = accum; p.counters = counters; p.err = err; p.work = work;
-        p.primary_ids = ids;
-        uint32_t launches = 0;
-        const bool counted = (pf->flags & VKB_PROFILE_COUNT_TRAVERSAL) != 0;
-        for (uint32_t done = 0; done < count; done += wave) {
-            uint32_t ws = std::min(wave, count - done);
-            p.wave_first = pf->first_sample + done;
-            p.wave_samples = ws;
-            p.n_paths = npix * ws;
-            k_set_count<<<1, 1, 0, st>>>(counters, p.n_paths);
-            k_camera<<<grid_for(p.n_paths, 256, sms), 256, 0, st>>>(p);
-            const int tgrid = sms * 16, sgrid = sms * 16;
-            for (uint32_t b = 0; b <= pf->bounces[0]; ++b) {
-                int cur = int(b & 1u);
-                if (counted) k_trace<false, true><<<tgrid, 128, 0, st>>>(p, cur);
-                else k_trace<false, false><<<tgrid, 128, 0, st>>>(p, cur);
-                k_reset_queues<<<1, 1, 0, st>>>(counters, cur ^ 1);
-                k_shade<<<sgrid, 128, 0, st>>>(p, cur);
-                if (counted) k_trace<true, true><<<tgrid, 128, 0, st>>>(p, -1);
-                else k_trace<true, false><<<tgrid, 128, 0, st>>>(p, -1);
-                launches += 4;
-            }
-            k_accumulate<<<grid_for(npix, 256, sms), 256, 0, st>>>(p);
-            launches += 3;
-            VKB_CUDA(cudaGetLastError());
-        }
-        k_resolve<<<grid_for(npix, 256, sms), 256, 0, st>>>(npix, accum, staging);
-        launches += 1;
-        s->launches += launches;
+        w.capacity = slots;
+        w.ray_o0 = cv.take<float4>(slots); w.ray_d0 = cv.take<float4>(slots);
+        w.ray_o1 = cv.take<float4>(slots); w.ray_d1 = cv.take<float4>(slots);
+        w.hit = cv.take<float4>(slots); w.hit_inst = cv.take<uint32_t>(slots);
+        w.thr = cv.take<float4>(slots); w.rad = cv.take<float4>(slots); w.rng = cv.take<uint2>(slots);
+        w.sa_o = cv.take<float4>(slots); w.sa_d = cv.take<float4>(slots); w.sa_c = cv.take<float4>(slots);
+        w.sb_o = cv.take<float4>(slots); w.sb_d = cv.take<float4>(slots); w.sb_c = cv.take<float4>(slots);
+        w.slot_job = nullptr;  // one job: no per-slot job index
+        if (!w.sb_c) throw ArgError{"vkb_render_noalloc: scratch layout overflow"};
+        // The array keeps the previous call's contents: the engine clears the counters,
+        // the accumulator and the traversal counters before the first wave.
+        std::vector<EngineJob> jobs(1);
+        EngineJob& e = jobs[0];
+        e.s = s; e.pf = *pf; e.npix = npix; e.count = count;
+        e.accum = accum; e.out_dev = staging; e.ids_dev = ids;
+        WaveTotals tot;
+        run_engine(c, jobs, w, slots, pf->flags & VKB_PROFILE_COUNT_TRAVERSAL, false, tot);
         if (!out->on_device) VKB_CUDA(cudaMemcpyAsync(out->rgba, staging, npix * sizeof(float4), cudaMemcpyDeviceToHost, st));
         if (out->primary_ids) VKB_CUDA(cudaMemcpyAsync(out->primary_ids, ids, size_t(npix) * 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        uint32_t ctr[16], e = 0;
-        unsigned long long wk[8];
-        VKB_CUDA(cudaMemcpyAsync(ctr, counters, sizeof(ctr), cudaMemcpyDeviceToHost, st));
-        VKB_CUDA(cudaMemcpyAsync(&e, err, sizeof(e), cudaMemcpyDeviceToHost, st));
-        VKB_CUDA(cudaMemcpyAsync(wk, work, sizeof(wk), cudaMemcpyDeviceToHost, st));
         VKB_CUDA(cudaStreamSynchronize(st));
-        if (stats) {
-            std::memset(stats, 0, sizeof(*stats));
-            stats->paths = uint64_t(npix) * count;
-            stats->extension_rays = ctr[3];
-            stats->shadow_rays = ctr[4];
-            stats->dropped_light_samples = ctr[5];
-            stats->dropped_path_samples = ctr[6];
-            stats->traversal_overflows = e;
-            stats->kernel_launches = launches;
-            stats->nodes_visited = wk[0]; stats->triangles_tested = wk[1]; stats->instances_entered = wk[2];
-            stats->shadow_nodes_visited = wk[3]; stats->shadow_triangles_tested = wk[4];
-        }
+        s->launches += tot.launches;
+        fill_stats(stats, tot, uint64_t(npix) * count, 0.f);
     });
 }

@@ -224,27 +224,38 @@ __global__ void k_tlas_leaves(uint32_t n, const uint32_t* sorted_ids, const floa
 }
 
 // ================================================================ path wavefront
-struct PathParams {
+// One render job: an installed scene, its profile and outputs.  A wave holds, for
+// every job scheduled in it, `wave_samples` consecutive samples of all its pixels in
+// path slots [slot_base, slot_base + npix*wave_samples).  A plain render is a batch
+// of one job; batched renders share every wave among many jobs.
+struct Job {
     SceneView sv;
     const float4* o2w; const float4* w2o; const uint4* inst_info; const MeshInfo* meshes;
     const float4* vpos; const float4* vnrm; const uint32_t* indices;
     const vkb_material* materials; const vkb_light* lights; uint32_t num_lights;
     const LightTreeNode* tree; uint32_t tree_nodes;
-    Lut lut; const float* filter;
     vkb_camera cam; vkb_environment env;
     uint32_t spp, seed, bounces[4], caustics, sample_mask;
     float clamp_direct, clamp_indirect, light_threshold;
-    uint32_t npix, wave_first, wave_samples, n_paths, first_sample;
+    uint32_t npix, first_sample;
+    uint32_t wave_first, wave_samples, slot_base, pixel_base;  // this wave
+    float4* accum; uint32_t* primary_ids; float4* out;
+};
+struct PathParams {
+    Job job0;             // single-job waves read their job from the kernel parameters
+    const Job* jobs; uint32_t njobs;
+    uint32_t* slot_job;   // batched waves: job index of each path slot
+    Lut lut; const float* filter;
     float4* ray_o[2]; float4* ray_d[2];
     float4* hit; uint32_t* hit_inst;
     float4* thr; float4* rad; uint2* rng;
     float4* sa_o; float4* sa_d; float4* sa_c;
     float4* sb_o; float4* sb_d; float4* sb_c;
-    float4* accum;
-    uint32_t* counters;  // [0],[1] ray counts, [2] shadow count, [3] ext rays, [4] shadow rays, [5] dropped light, [6] dropped paths
-    unsigned long long* work;  // instrumented traversal: closest nodes, tris, instances; shadow nodes, tris
+    // [0],[1] ray counts, [2] shadow count, [3] ext rays, [4] shadow rays, [5] dropped light,
+    // [6] dropped paths, [7] path slots of this wave, [8] pixels of this wave's jobs
+    uint32_t* counters;
+    unsigned long long* work;  // instrumented traversal: closest nodes, tris, instances, blas nodes; shadow nodes, tris, blas nodes
     uint32_t* err;
-    uint32_t* primary_ids;
 };
 constexpr uint32_t META_NONFINITE = 0x80000000u;
 constexpr uint32_t SH_TRACE_A = 1u, SH_HAS_B = 2u, SH_TRACE_B = 4u, SH_DIRECT = 8u;
@@ -264,20 +275,40 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
     base = __shfl_sync(mask, base, leader);
     return base + __popc(mask & ((1u << lane) - 1u));
 }
+// The job owning a slot (BATCH) or job 0.
+template <bool BATCH>
+__device__ __forceinline__ uint32_t job_of_slot(const PathParams& p, uint32_t slot) { return BATCH ? __ldg(&p.slot_job[slot]) : 0u; }
+// Largest job whose base (slot_base or pixel_base) is <= x: binary search over the table.
+template <bool PIXELS>
+__device__ __forceinline__ uint32_t find_job(const PathParams& p, uint32_t x) {
+    uint32_t lo = 0, hi = p.njobs;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        uint32_t b = PIXELS ? p.jobs[mid].pixel_base : p.jobs[mid].slot_base;
+        if (b <= x) lo = mid; else hi = mid;
+    }
+    return lo;
+}
 
 // path.slang:1792-1866 up to integrate: sampler, film-filtered pinhole camera ray.
+template <bool BATCH>
 __global__ void k_camera(PathParams p) {
-    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < p.n_paths; slot += gridDim.x * blockDim.x) {
-        uint32_t pixel = slot % p.npix, sidx = p.wave_first + slot / p.npix;
-        uint32_t px = pixel % p.cam.width, py = pixel / p.cam.width;
-        uint32_t pseed = screen_ray_hash(px, py, 0u, p.seed);
-        uint32_t rng = screen_ray_hash(px, py, sidx, p.seed);
-        float4 cs = sample_group(pseed, sidx, p.sample_mask, 0u);
-        float nx = (float(px) + 0.5f + filter_offset(p.filter, cs.x)) / float(p.cam.width) * 2.f + -1.f;
-        float ny = (float(py) + 0.5f + filter_offset(p.filter, cs.y)) / float(p.cam.height) * -2.f + 1.f;
-        float3 fwd = get3(p.cam.forward), eye = get3(p.cam.eye);
-        float3 dir = normalize(fwd + get3(p.cam.right) * (nx / p.cam.proj_x) + get3(p.cam.up) * (ny / p.cam.proj_y));
-        float near_d = p.cam.near_plane / dot(dir, fwd), far_d = p.cam.far_plane / dot(dir, fwd);
+    const uint32_t n = p.counters[7];
+    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
+        uint32_t j = BATCH ? find_job<false>(p, slot) : 0u;
+        const Job& J = BATCH ? p.jobs[j] : p.job0;
+        if (BATCH) p.slot_job[slot] = j;
+        uint32_t local = slot - J.slot_base;
+        uint32_t pixel = local % J.npix, sidx = J.wave_first + local / J.npix;
+        uint32_t px = pixel % J.cam.width, py = pixel / J.cam.width;
+        uint32_t pseed = screen_ray_hash(px, py, 0u, J.seed);
+        uint32_t rng = screen_ray_hash(px, py, sidx, J.seed);
+        float4 cs = sample_group(pseed, sidx, J.sample_mask, 0u);
+        float nx = (float(px) + 0.5f + filter_offset(p.filter, cs.x)) / float(J.cam.width) * 2.f + -1.f;
+        float ny = (float(py) + 0.5f + filter_offset(p.filter, cs.y)) / float(J.cam.height) * -2.f + 1.f;
+        float3 fwd = get3(J.cam.forward), eye = get3(J.cam.eye);
+        float3 dir = normalize(fwd + get3(J.cam.right) * (nx / J.cam.proj_x) + get3(J.cam.up) * (ny / J.cam.proj_y));
+        float near_d = J.cam.near_plane / dot(dir, fwd), far_d = J.cam.far_plane / dot(dir, fwd);
         float3 o = eye + dir * near_d;
         float tmax = fminf(FP32_MAX, fmaxf(0.f, far_d - length(o - eye)));
         p.ray_o[0][slot] = make_float4(o.x, o.y, o.z, tmax);
@@ -305,7 +336,7 @@ __device__ __forceinline__ bool trace_any(const SceneView& sv, float3 o, float3 
     __shared__ int stack_r_[SMEM_STACK * TRACE_BLOCK];                                                  \
     __shared__ float stack_t_[VKB_POP_CULL ? SMEM_STACK * TRACE_BLOCK : 1];                            \
     TraceStack stk{stack_r_ + threadIdx.x, stack_t_ + (VKB_POP_CULL ? threadIdx.x : 0)};
-template <bool ANY, bool COUNT>
+template <bool ANY, bool COUNT, bool BATCH>
 __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace(PathParams p, int cur) {
     VKB_STACK_DECL
     uint32_t n = cur < 0 ? p.counters[2] : p.counters[cur];
@@ -314,38 +345,39 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace(Pat
         else atomicAdd(&p.counters[3], n);
     }
     TraceCount tc;
-    uint32_t loop_end = COUNT ? (n + 31u) / 32u * 32u : n;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < loop_end; i += gridDim.x * blockDim.x) {
-        if (COUNT && i >= n) continue;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         if (!ANY) {
             float4 ro = p.ray_o[cur][i], rd = p.ray_d[cur][i];
+            const SceneView sv = BATCH ? p.jobs[job_of_slot<true>(p, __float_as_uint(rd.w))].sv : p.job0.sv;
             HitRecord h;
-            bool found = trace_any<false, COUNT>(p.sv, f3(ro.x, ro.y, ro.z), f3(rd.x, rd.y, rd.z), ro.w, h, p.err, &tc, stk);
+            bool found = trace_any<false, COUNT>(sv, f3(ro.x, ro.y, ro.z), f3(rd.x, rd.y, rd.z), ro.w, h, p.err, &tc, stk);
             p.hit[i] = found ? make_float4(h.t, h.u, h.v, __uint_as_float(h.prim)) : make_float4(-1.f, 0.f, 0.f, __uint_as_float(0xffffffffu));
             p.hit_inst[i] = found ? h.inst : 0xffffffffu;
         } else {
             float4 so = p.sa_o[i], sd = p.sa_d[i], sc = p.sa_c[i];
             uint32_t slot = __float_as_uint(sd.w), flags = __float_as_uint(sc.w);
+            const Job& J = BATCH ? p.jobs[job_of_slot<true>(p, slot)] : p.job0;
+            const SceneView sv = J.sv;
             HitRecord h;
             float3 total = f3(sc.x, sc.y, sc.z);
-            if ((flags & SH_TRACE_A) && trace_any<true, COUNT>(p.sv, f3(so.x, so.y, so.z), f3(sd.x, sd.y, sd.z), so.w, h, p.err, &tc, stk)) total = f3(0.f);
+            if ((flags & SH_TRACE_A) && trace_any<true, COUNT>(sv, f3(so.x, so.y, so.z), f3(sd.x, sd.y, sd.z), so.w, h, p.err, &tc, stk)) total = f3(0.f);
             if (flags & SH_HAS_B) {
                 float4 bc = p.sb_c[slot];
                 float3 cb = f3(bc.x, bc.y, bc.z);
                 if (flags & SH_TRACE_B) {
                     float4 bo = p.sb_o[slot], bd = p.sb_d[slot];
-                    if (trace_any<true, COUNT>(p.sv, f3(bo.x, bo.y, bo.z), f3(bd.x, bd.y, bd.z), bo.w, h, p.err, &tc, stk)) cb = f3(0.f);
+                    if (trace_any<true, COUNT>(sv, f3(bo.x, bo.y, bo.z), f3(bd.x, bd.y, bd.z), bo.w, h, p.err, &tc, stk)) cb = f3(0.f);
                 }
                 total = total + cb;
             }
             float4 r = p.rad[slot];
             uint32_t dropped = __float_as_uint(r.w);
-            float3 add = clamp_sample(total, (flags & SH_DIRECT) ? p.clamp_direct : p.clamp_indirect, dropped);
+            float3 add = clamp_sample(total, (flags & SH_DIRECT) ? J.clamp_direct : J.clamp_indirect, dropped);
             p.rad[slot] = make_float4(r.x + add.x, r.y + add.y, r.z + add.z, __uint_as_float(dropped));
         }
     }
     if (COUNT) {
-        // Every lane of a warp reaches here (the loop runs whole warps).
+        // Every lane of the block reaches here after its loop.
         flush_count(&p.work[ANY ? 3 : 0], tc.nodes);
         flush_count(&p.work[ANY ? 4 : 1], tc.tris);
         if (!ANY) flush_count(&p.work[2], tc.instances);
@@ -359,7 +391,7 @@ __device__ __forceinline__ float3 tvec(const float4 I[3], float3 x) {
 }
 __device__ __forceinline__ float3 mvec(const float4 M[3], float3 x) { return f3(M[0].x * x.x + M[0].y * x.y + M[0].z * x.z, M[1].x * x.x + M[1].y * x.y + M[1].z * x.z, M[2].x * x.x + M[2].y * x.y + M[2].z * x.z); }
 // hit_geometry.slang:64-138,174-205; hit.slang:86-114; surface.slang:290-333; material.slang:69-79.
-__device__ __forceinline__ Surface hit_surface(const PathParams& p, uint32_t inst, uint32_t prim, float u, float v, float3 dir) {
+__device__ __forceinline__ Surface hit_surface(const Job& p, uint32_t inst, uint32_t prim, float u, float v, float3 dir) {
     Surface s;
     uint4 info = __ldg(&p.inst_info[inst]);
     const MeshInfo& m = p.meshes[info.x];
@@ -441,6 +473,7 @@ __device__ __forceinline__ float3 light_threshold(float3 value, float threshold,
 }
 
 // integrate's per-vertex body (path.slang:1340-1709) for one queued extension hit.
+template <bool BATCH>
 __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
     const int nxt = cur ^ 1;
     uint32_t n = p.counters[cur];
@@ -453,6 +486,7 @@ __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
         if (active) {
             float4 ro = p.ray_o[cur][i], rd = p.ray_d[cur][i];
             slot = __float_as_uint(rd.w);
+            const Job& J = BATCH ? p.jobs[job_of_slot<true>(p, slot)] : p.job0;
             float3 dir = f3(rd.x, rd.y, rd.z);
             float4 hh = p.hit[i];
             uint32_t inst = p.hit_inst[i];
@@ -463,21 +497,22 @@ __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
             uint32_t ray_event = bounce == 0 ? VKB_RAY_CAMERA : ((meta >> 24) & 0x3fu);
             float3 thr = f3(T.x, T.y, T.z), rad = f3(R.x, R.y, R.z);
             uint32_t dropped = __float_as_uint(R.w), rng = rg.x, pseed = rg.y;
-            uint32_t pixel = slot % p.npix, sidx = p.wave_first + slot / p.npix;
-            float limit = bounce == 0 ? p.clamp_direct : p.clamp_indirect;
-            if (p.primary_ids && bounce == 0 && sidx == p.first_sample) {
-                p.primary_ids[2 * pixel] = hh.x >= 0.f ? inst : 0xffffffffu;
-                p.primary_ids[2 * pixel + 1] = hh.x >= 0.f ? __float_as_uint(hh.w) : 0xffffffffu;
+            uint32_t local = slot - J.slot_base;
+            uint32_t pixel = local % J.npix, sidx = J.wave_first + local / J.npix;
+            float limit = bounce == 0 ? J.clamp_direct : J.clamp_indirect;
+            if (J.primary_ids && bounce == 0 && sidx == J.first_sample) {
+                J.primary_ids[2 * pixel] = hh.x >= 0.f ? inst : 0xffffffffu;
+                J.primary_ids[2 * pixel + 1] = hh.x >= 0.f ? __float_as_uint(hh.w) : 0xffffffffu;
             }
             if (!(hh.x >= 0.f)) {
                 // Miss: path.slang:1484-1512 with the constant world light and camera-visible suns.
                 float3 sky;
-                if (ray_event == VKB_RAY_CAMERA && !p.env.camera_sees_environment) sky = get3(p.env.background);
+                if (ray_event == VKB_RAY_CAMERA && !J.env.camera_sees_environment) sky = get3(J.env.background);
                 else {
-                    sky = get3(p.env.radiance);
+                    sky = get3(J.env.radiance);
                     if (ray_event == VKB_RAY_CAMERA)
-                        for (uint32_t l = 0; l < p.num_lights; ++l) {
-                            const vkb_light& L = p.lights[l];
+                        for (uint32_t l = 0; l < J.num_lights; ++l) {
+                            const vkb_light& L = J.lights[l];
                             if (L.position[3] != 0.f || !(L.shadow_offsets[0] & VKB_RAY_CAMERA)) continue;
                             sky = sky + emitter_eval(L, f3(0.f), dir).radiance;
                         }
@@ -485,9 +520,9 @@ __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
                 rad = rad + clamp_sample(thr * sky, limit, dropped);
             } else {
                 uint32_t vtx = bounce;
-                float4 sc = sample_group(pseed, sidx, p.sample_mask, vertex_group(vtx, 0));   // path_scatter
-                Surface s = hit_surface(p, inst, __float_as_uint(hh.w), hh.y, hh.z, dir);
-                const vkb_material& mt = p.materials[__ldg(&p.inst_info[inst]).y];
+                float4 sc = sample_group(pseed, sidx, J.sample_mask, vertex_group(vtx, 0));   // path_scatter
+                Surface s = hit_surface(J, inst, __float_as_uint(hh.w), hh.y, hh.z, dir);
+                const vkb_material& mt = J.materials[__ldg(&J.inst_info[inst]).y];
                 Closure c;
                 c.base_color = get3(mt.base_color); c.base_weight = mt.base_weight; c.base_metalness = mt.base_metalness;
                 c.specular_color = get3(mt.specular_color); c.specular_weight = mt.specular_weight;
@@ -505,19 +540,19 @@ __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
                     float3 va = f3(0.f), vb = f3(0.f);
                     bool trace_a = false, has_b = false, trace_b = false;
                     float3 oa, da, ob, db; float la = 0.f, lb = 0.f;
-                    if (p.num_lights > 0) {
-                        float4 u = sample_group(pseed, sidx, p.sample_mask, vertex_group(vtx, 1));   // path_light
+                    if (J.num_lights > 0) {
+                        float4 u = sample_group(pseed, sidx, J.sample_mask, vertex_group(vtx, 1));   // path_light
                         float probability;
-                        uint32_t li = tree_pick(p.tree, p.tree_nodes, s.world, u.z, u.w, probability);
-                        if (probability > 0.f && li < p.num_lights) {
-                            const vkb_light& L = p.lights[li];
+                        uint32_t li = tree_pick(J.tree, J.tree_nodes, s.world, u.z, u.w, probability);
+                        if (probability > 0.f && li < J.num_lights) {
+                            const vkb_light& L = J.lights[li];
                             uint32_t contribution = L.shadow_offsets[VKB_LIGHT_CONTRIBUTION_WORD];
                             bool shadowed = (L.shadow_offsets[VKB_LIGHT_RAY_WORD] & VKB_LIGHT_RAY_SHADOWED) != 0u;
                             if ((contribution & VKB_LIGHT_LINK_ALL) || L.shadow_offsets[VKB_LIGHT_LINK_WORD]) {
                                 LightSample src = emitter_sample(L, s.world, u.x, u.y);
                                 float3 power = src.delta ? src.radiance : (src.pdf > 0.f ? src.radiance / src.pdf : f3(0.f));
                                 va = analytic_mis_response(c, view, src.dir, s.face, contribution, src.pdf, pr) * power / probability;
-                                va = light_threshold(va, p.light_threshold, rng);
+                                va = light_threshold(va, J.light_threshold, rng);
                                 if (any_nonzero(va) && shadowed) {
                                     oa = path_origin(s, src.dir);
                                     ray_connection(oa, s.world, src.dir, src.distance, da, la);
@@ -528,7 +563,7 @@ __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
                                     EmitterEval e = emitter_eval(L, s.world, smp.dir);
                                     if (e.pdf > 0.f) {
                                         float w = smp.pdf > 0.f ? mis_power(smp.pdf, e.pdf) : 1.f;
-                                        vb = light_threshold(smp.weight * e.radiance * (w / probability), p.light_threshold, rng);
+                                        vb = light_threshold(smp.weight * e.radiance * (w / probability), J.light_threshold, rng);
                                         if (any_nonzero(vb)) {
                                             has_b = true;
                                             if (shadowed) {
@@ -558,11 +593,11 @@ __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
                         rad = rad + clamp_sample(ca + cb, limit, dropped);
                     }
                     // Continuation (path.slang:1683-1708).
-                    bool go = bounce < p.bounces[0];
+                    bool go = bounce < J.bounces[0];
                     uint32_t event = smp.event;
                     if (go) {
-                        if (event == VKB_RAY_DIFFUSE) { if (diffuse++ >= p.bounces[1]) go = false; }
-                        else if (event == VKB_RAY_SPECULAR) { if (glossy++ >= p.bounces[2] || (diffuse > 0 && !(p.caustics & 1u))) go = false; }
+                        if (event == VKB_RAY_DIFFUSE) { if (diffuse++ >= J.bounces[1]) go = false; }
+                        else if (event == VKB_RAY_SPECULAR) { if (glossy++ >= J.bounces[2] || (diffuse > 0 && !(J.caustics & 1u))) go = false; }
                         else go = false;
                     }
                     if (go && !event_hemisphere(event, smp.dir, s.face, s.geometric)) go = false;
@@ -573,7 +608,7 @@ __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
                     }
                     if (go && bounce >= ROULETTE_START) {
                         float survive = clampf(maxc(thr), ROULETTE_MIN, ROULETTE_MAX);
-                        float4 dec = sample_group(pseed, sidx, p.sample_mask, vertex_group(vtx, 4));
+                        float4 dec = sample_group(pseed, sidx, J.sample_mask, vertex_group(vtx, 4));
                         if (dec.z > survive) go = false;
                         else thr = thr / survive;
                     }
@@ -596,33 +631,44 @@ __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
         if (push_shadow) { p.sa_o[si] = sh_o; p.sa_d[si] = sh_d; p.sa_c[si] = sh_c; }
     }
 }
-// Seed the first ray queue's count (the no-alloc render, whose counters live in device scratch).
-__global__ void k_set_count(uint32_t* counters, uint32_t n) { counters[0] = n; }
+// Seed the first ray queue's count from the wave's path-slot count.
+__global__ void k_start_wave(uint32_t* counters) { counters[0] = counters[7]; }
 // Zero the next ray queue and the shadow queue before a shade pass.
 __global__ void k_reset_queues(uint32_t* counters, int nxt) { counters[nxt] = 0u; counters[2] = 0u; }
-// resolve.slang:162-191: add this wave's finished samples to the accumulator.
+// resolve.slang:162-191: add this wave's finished samples to each job's accumulator,
+// one sample at a time in sample order (any wave size gives the same sums).
+template <bool BATCH>
 __global__ void k_accumulate(PathParams p) {
-    for (uint32_t pixel = blockIdx.x * blockDim.x + threadIdx.x; pixel < p.npix; pixel += gridDim.x * blockDim.x) {
-        float4 sum = p.accum[pixel];
+    const uint32_t n = p.counters[8];
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
+        const Job& J = BATCH ? p.jobs[find_job<true>(p, g)] : p.job0;
+        uint32_t pixel = g - J.pixel_base;
+        if (pixel >= J.npix || J.wave_samples == 0) continue;
+        float4 sum = J.accum[pixel];
         uint32_t dl = 0, dp = 0;
-        for (uint32_t k = 0; k < p.wave_samples; ++k) {
-            uint32_t slot = k * p.npix + pixel;
+        for (uint32_t k = 0; k < J.wave_samples; ++k) {
+            uint32_t slot = J.slot_base + k * J.npix + pixel;
             float4 T = p.thr[slot], R = p.rad[slot];
             dl += __float_as_uint(R.w);
-            float3 v = f3(R.x, R.y, R.z) * p.env.exposure;
+            float3 v = f3(R.x, R.y, R.z) * J.env.exposure;
             if ((__float_as_uint(T.w) & META_NONFINITE) || !finite3(v)) { v = f3(0.f); dp++; }
             sum.x += v.x; sum.y += v.y; sum.z += v.z; sum.w += 1.f;
         }
-        p.accum[pixel] = sum;
+        J.accum[pixel] = sum;
         if (dl) atomicAdd(&p.counters[5], dl);
         if (dp) atomicAdd(&p.counters[6], dp);
     }
 }
-__global__ void k_resolve(uint32_t npix, const float4* accum, float4* out) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
-        float4 a = accum[i];
+// Mean image of every job (pixels numbered across jobs by pixel_base).
+template <bool BATCH>
+__global__ void k_resolve(PathParams p, uint32_t total_pixels) {
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total_pixels; g += gridDim.x * blockDim.x) {
+        const Job& J = BATCH ? p.jobs[find_job<true>(p, g)] : p.job0;
+        uint32_t i = g - J.pixel_base;
+        if (i >= J.npix) continue;
+        float4 a = J.accum[i];
         float inv = a.w > 0.f ? 1.f / a.w : 0.f;
-        out[i] = make_float4(a.x * inv, a.y * inv, a.z * inv, a.w > 0.f ? 1.f : 0.f);
+        J.out[i] = make_float4(a.x * inv, a.y * inv, a.z * inv, a.w > 0.f ? 1.f : 0.f);
     }
 }
 // Test entry: sampler groups for arbitrary (pixel, index, group).

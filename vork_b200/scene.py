@@ -443,3 +443,26 @@ def flock_scene(num_birds: int = 1_000_000, seed: int = 0, width: int = 1920, he
     env = environment(radiance=(0.18, 0.26, 0.42))
     sc = Scene([bird, terrain], rows, mesh_ids, mat_ids, materials, [sun], cam, env, name="flock")
     return sc, flock
+
+
+# ----------------------------------------------------------------------------- batched previews
+def preview_jobs(count: int = 256, seed: int = 0, max_side: int = 1024):
+    """Seeded preview jobs: resolution log-uniform 128^2..max_side^2, spp U{4..32},
+    depth U{4..8}, a scene of 1k..200k triangles (log-uniform) from the small
+    configuration's generator (spheres + ground grid), scene seed = job index.
+    Returns [(Scene, spp, depth), ...]."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for j in range(count):
+        side = int(round(math.exp(rng.uniform(math.log(128), math.log(max_side)))))
+        aspect = rng.choice([1.0, 4 / 3, 16 / 9])
+        w = max(16, int(round(side * math.sqrt(aspect))))
+        h = max(16, int(round(side / math.sqrt(aspect))))
+        spp = int(rng.integers(4, 33))
+        depth = int(rng.integers(4, 9))
+        tris = math.exp(rng.uniform(math.log(1000), math.log(200000)))
+        cells = 8 if tris < 20000 else 64
+        n_spheres = max(1, int(round((tris - 2 * cells * cells) / 960)))
+        sc = spheres_scene(num_spheres=n_spheres, seed=j, width=w, height=h, grid_cells=cells)
+        jobs.append((sc, spp, depth))
+    return jobs
