@@ -214,12 +214,16 @@ def run_batch(args, device):
     t0 = time.perf_counter()
     _, st = r.render_batch(items)
     batch_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    r.render_batch(items, flags=4)  # fair scheduling (one sample of every job per wave)
+    fair_s = time.perf_counter() - t0
     line = {"metric": METRIC, "value": paths / batch_s, "unit": "paths/s", "n_gpus": 1, "steps": 1, "warmup": args.warmup,
             "ms_per_step": 1000 * batch_s, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generator; no dataset)",
             "config": {"workload": f"batched previews: {len(items)} jobs, resolution log-uniform 128^2..1024^2, spp U{{4..32}}, "
                                    "depth U{4..8}, 1k-200k-triangle sphere scenes seeded per job", "global_batch": paths},
             "sequential": {"value": paths / seq_s, "unit": "paths/s", "ms": 1000 * seq_s},
+            "fair_schedule": {"value": paths / fair_s, "unit": "paths/s", "ms": 1000 * fair_s},
             "speedup_vs_sequential": seq_s / batch_s, "autotune": {k: tune[k] for k in ("best_capacity", "best_blocks_per_sm", "best_ms")},
             "gpu_launches": st["kernel_launches"], "work": {"extension_rays": st["extension_rays"], "shadow_rays": st["shadow_rays"]}}
     print(json.dumps(line), flush=True)

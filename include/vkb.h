@@ -146,6 +146,12 @@ typedef struct vkb_profile {
 /* Measurement switches of vkb_profile.flags (no reference counterpart: timing hooks). */
 #define VKB_PROFILE_TIME_KERNELS 1u        /* CUDA events around every closest-hit trace launch */
 #define VKB_PROFILE_COUNT_TRAVERSAL 2u     /* instrumented traversal: node and triangle visits */
+/* Wave scheduling of several jobs (vkb_render_batch flags / vkb_server_config.flags):
+ * batches pack each job's remaining samples before the next job (throughput: fewer
+ * scenes per wave keep their BVHs in L2) unless VKB_BATCH_FAIR; servers give every
+ * admitted request a sample per wave (latency) unless VKB_BATCH_PACKED. */
+#define VKB_BATCH_FAIR 4u
+#define VKB_BATCH_PACKED 8u
 
 /* Render output: linear RGBA32F mean image (resolve.slang:162-191). */
 typedef struct vkb_output {

@@ -29,6 +29,8 @@ def test_batch_results_equal_single_renders(renderer):
         a = Profile.reference_transport(prof.bounces[0], prof.samples, sample_count=2)
         b = Profile.reference_transport(prof.bounces[0], prof.samples, seed=9)
         (ia, ib), _ = renderer.render_batch([(inst, a), (inst, b)])
+        (fa, fb), _ = renderer.render_batch([(inst, a), (inst, b)], flags=4)
+        assert np.array_equal(fa, ia) and np.array_equal(fb, ib)
         assert np.array_equal(ia, inst.render(a).image) and np.array_equal(ib, inst.render(b).image)
     finally:
         for inst, _ in items:

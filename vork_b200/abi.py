@@ -67,6 +67,7 @@ class VkbProfile(C.Structure):
 
 
 PROFILE_TIME_KERNELS, PROFILE_COUNT_TRAVERSAL = 1, 2
+BATCH_FAIR, BATCH_PACKED = 4, 8
 NOALLOC_SCRATCH_MIB = 32
 
 

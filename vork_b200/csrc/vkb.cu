@@ -154,7 +154,7 @@ std::vector<LightTreeNode> light_tree(const vkb_light* lights, uint32_t n) {
 // BVH2 nodes in the device layout (both child boxes per node), leaves of up to
 // BLAS_LEAF_MAX triangles referenced as ~((first << 2) | (count - 1)), triangles
 // reordered into leaf order.  The per-frame TLAS keeps the GPU LBVH.
-constexpr uint32_t BLAS_LEAF_MAX = 4;
+constexpr uint32_t BLAS_LEAF_MAX = VKB_BLAS_LEAF_MAX;
 struct SahBlas {
     std::vector<BvhNode> nodes;
     std::vector<uint32_t> order;  // leaf-ordered original triangle ids
@@ -599,8 +599,13 @@ struct WaveEngine {
     bool graphs;
     std::vector<EngineJob> jobs;
     std::vector<Job> table;
+    std::vector<Job> wave_table;        // the jobs of the current wave (uploaded)
     WaveTotals tot;
     std::vector<GraphEntry> captured;   // this engine's wave graphs (they point at its buffers)
+    // Scheduling: fair (one sample of every unfinished job per wave, then more: serving
+    // latency) or packed (each job's remaining samples before the next job: fewer scenes
+    // per wave, so their BVHs stay in L2 -- batch throughput).
+    bool packed = false;
     ~WaveEngine() { for (auto& g : captured) cudaGraphExecDestroy(g.exec); }
     WaveEngine(vkb_ctx* ctx, const WaveBuffers& wb, size_t cap, uint32_t fl, bool use_graphs) : c(ctx), w(wb), capacity(cap), flags(fl), graphs(use_graphs) {
         cudaStream_t st = c->stream;
@@ -627,27 +632,41 @@ struct WaveEngine {
         const uint32_t njobs = uint32_t(jobs.size());
         if (njobs == 0) return false;
         if (njobs > w.job_capacity) throw ArgError{"more active jobs than the job table holds"};
-        const bool batch = njobs > 1;
         const bool timed = (flags & VKB_PROFILE_TIME_KERNELS) != 0, counted = (flags & VKB_PROFILE_COUNT_TRAVERSAL) != 0;
-        const bool use_graph = graphs && batch && !timed;
         std::vector<uint32_t> take(njobs, 0u);
         size_t left = capacity;
         bool any = false;
-        for (uint32_t k = 0; k < njobs; ++k) {
-            EngineJob& e = jobs[k];
-            if (finished(k)) continue;
-            if (size_t(e.npix) <= left || !any) { take[k] = 1; left = size_t(e.npix) <= left ? left - e.npix : 0; any = true; }
+        if (packed) {
+            for (uint32_t k = 0; k < njobs && left > 0; ++k) {
+                EngineJob& e = jobs[k];
+                if (finished(k)) continue;
+                uint32_t n = uint32_t(std::min<size_t>(e.count - e.done, left / e.npix));
+                if (n == 0 && !any) n = 1;      // an image larger than the wave: one sample alone
+                if (n == 0) break;              // keep admission order: later jobs wait
+                take[k] = n; any = true;
+                left = size_t(n) * e.npix <= left ? left - size_t(n) * e.npix : 0;
+            }
+        } else {
+            for (uint32_t k = 0; k < njobs; ++k) {
+                EngineJob& e = jobs[k];
+                if (finished(k)) continue;
+                if (size_t(e.npix) <= left || !any) { take[k] = 1; left = size_t(e.npix) <= left ? left - e.npix : 0; any = true; }
+            }
+            for (uint32_t k = 0; k < njobs; ++k) {
+                if (!take[k]) continue;
+                EngineJob& e = jobs[k];
+                uint32_t more = uint32_t(std::min<size_t>(e.count - e.done - 1, left / e.npix));
+                take[k] += more;
+                left -= size_t(more) * e.npix;
+            }
         }
         if (!any) return false;
+        // The wave's table holds only the jobs that take samples in it, so the camera and
+        // accumulate passes see no idle jobs' pixels.
+        uint32_t n_paths = 0, bounces = 0, total_pixels = 0;
+        wave_table.clear();
         for (uint32_t k = 0; k < njobs; ++k) {
             if (!take[k]) continue;
-            EngineJob& e = jobs[k];
-            uint32_t more = uint32_t(std::min<size_t>(e.count - e.done - 1, left / e.npix));
-            take[k] += more;
-            left -= size_t(more) * e.npix;
-        }
-        uint32_t n_paths = 0, bounces = 0, total_pixels = 0;
-        for (uint32_t k = 0; k < njobs; ++k) {
             EngineJob& e = jobs[k];
             Job& j = table[k];
             e.pixel_base = total_pixels; j.pixel_base = total_pixels; total_pixels += e.npix;
@@ -656,17 +675,21 @@ struct WaveEngine {
             j.slot_base = n_paths;
             n_paths += take[k] * e.npix;
             e.done += take[k];
-            if (take[k]) bounces = std::max(bounces, e.pf.bounces[0]);
+            bounces = std::max(bounces, e.pf.bounces[0]);
+            wave_table.push_back(j);
         }
+        const uint32_t wave_jobs = uint32_t(wave_table.size());
+        const bool batch = wave_jobs > 1;
+        const bool use_graph = graphs && batch && !timed;
         uint32_t wave_counts[2] = {n_paths, total_pixels};
-        VKB_CUDA(cudaMemcpyAsync(w.jobs, table.data(), njobs * sizeof(Job), cudaMemcpyHostToDevice, st));
+        VKB_CUDA(cudaMemcpyAsync(w.jobs, wave_table.data(), wave_jobs * sizeof(Job), cudaMemcpyHostToDevice, st));
         VKB_CUDA(cudaMemcpyAsync(w.counters + 7, wave_counts, sizeof(wave_counts), cudaMemcpyHostToDevice, st));
-        PathParams p = path_params(c, w, njobs);
-        p.job0 = table[0];
+        PathParams p = path_params(c, w, wave_jobs);
+        p.job0 = wave_table[0];
         if (use_graph) {
             uint64_t key = (uint64_t(bounces) << 1) | 1u;
             key = key * 1315423911ull + (counted ? 7u : 3u);
-            key = key * 40503ull + njobs;
+            key = key * 40503ull + wave_jobs;
             key = key * 97ull + uint64_t(c->trace_blocks_per_sm);
             cudaGraphExec_t exec = nullptr;
             for (auto& g : captured) if (g.key == key) exec = g.exec;
@@ -717,8 +740,10 @@ struct WaveEngine {
 };
 
 // Run `jobs` to completion on the wavefront `w` and resolve each into its out_dev.
-void run_engine(vkb_ctx* c, std::vector<EngineJob>& jobs, const WaveBuffers& w, size_t capacity, uint32_t flags, bool graphs, WaveTotals& tot) {
+void run_engine(vkb_ctx* c, std::vector<EngineJob>& jobs, const WaveBuffers& w, size_t capacity, uint32_t flags, bool graphs, WaveTotals& tot,
+                bool packed = false) {
     WaveEngine eng(c, w, capacity, flags, graphs);
+    eng.packed = packed;
     for (auto& e : jobs) eng.add(e);
     VKB_CUDA(cudaEventRecord(c->ev0, c->stream));
     while (eng.step()) {}
@@ -786,7 +811,7 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
         if (outs[k]->primary_ids) { e.ids_dev = c->ids.p + idw; idw += 2 * size_t(e.npix); }
         paths += uint64_t(e.npix) * e.count;
     }
-    run_engine(c, jobs, c->wave.view(), capacity, flags, true, tot);
+    run_engine(c, jobs, c->wave.view(), capacity, flags, true, tot, (flags & VKB_BATCH_FAIR) == 0);
     for (size_t k = 0; k < in.size(); ++k) {
         if (!outs[k]->on_device) VKB_CUDA(cudaMemcpyAsync(outs[k]->rgba, jobs[k].out_dev, size_t(jobs[k].npix) * sizeof(float4), cudaMemcpyDeviceToHost, st));
         if (outs[k]->primary_ids) VKB_CUDA(cudaMemcpyAsync(outs[k]->primary_ids, jobs[k].ids_dev, size_t(jobs[k].npix) * 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -1097,7 +1122,7 @@ vkb_status vkb_autotune(vkb_ctx* c, vkb_job* jobs, uint32_t njobs, vkb_tune_resu
                 }
                 WaveTotals warm, tot;
                 uint64_t paths = 0;
-                render_jobs(c, in, outs, 0, 0, warm, paths);  // captures this shape's graphs
+                render_jobs(c, in, outs, 0, 0, warm, paths);  // warm-up: buffer sizes, caches
                 render_jobs(c, in, outs, 0, 0, tot, paths);
                 if (out && tried < 16) {
                     out->capacity[tried] = uint64_t(c->wave_capacity);
@@ -1276,6 +1301,7 @@ vkb_status vkb_server_create(vkb_ctx* c, const vkb_server_config* cfg, vkb_serve
         if (v->budget && v->wave_bytes >= v->budget) throw ArgError{"memory budget below the wavefront's own footprint"};
         v->wave.reserve(v->capacity, v->max_jobs);
         v->eng = std::make_unique<WaveEngine>(c, v->wave.view(), v->capacity, cfg->flags, true);
+        v->eng->packed = (cfg->flags & VKB_BATCH_PACKED) != 0;
     });
     if (st != VKB_OK) return st;
     *out = v.release();

@@ -136,7 +136,30 @@ __device__ __forceinline__ bool tri_test(const RaySpace& r, float3 v0, float3 v1
     return true;
 }
 
+// Triangles per BLAS leaf (1..4; counts are stored in two bits).  One triangle per leaf
+// measured fastest on the instanced flock frame (the SAH tree then has fewer box tests
+// per ray than multi-triangle leaves save in node visits).
+#ifndef VKB_BLAS_LEAF_MAX
+#define VKB_BLAS_LEAF_MAX 1
+#endif
+static_assert(VKB_BLAS_LEAF_MAX >= 1 && VKB_BLAS_LEAF_MAX <= 4, "leaf counts are stored in two bits");
+
 struct HitRecord { float t, u, v; uint32_t prim, inst; };
+
+// A world ray in global memory (origin and direction as 3 floats each).  Traversal
+// re-reads it when it enters or leaves an instance instead of keeping six registers live
+// across the loop; the volatile loads keep the compiler from caching the values.
+struct RayRef {
+    const float* o;
+    const float* d;
+    __device__ __forceinline__ static float ld(const float* p) {
+        float v;
+        asm volatile("ld.global.nc.f32 %0, [%1];" : "=f"(v) : "l"(p));
+        return v;
+    }
+    __device__ __forceinline__ float3 origin() const { return f3(ld(o), ld(o + 1), ld(o + 2)); }
+    __device__ __forceinline__ float3 dir() const { return f3(ld(d), ld(d + 1), ld(d + 2)); }
+};
 
 struct SceneView {
     const BvhNode* tlas_nodes;
@@ -152,10 +175,10 @@ struct TraceCount { uint32_t nodes = 0, tris = 0, instances = 0, blas_nodes = 0;
 // Closest hit (any == false) or first hit (any == true) of a world ray over the
 // two-level BVH.  Error: overflow/step-limit exits set *err and return the best so far.
 template <bool ANY, bool COUNT = false>
-__device__ __forceinline__ bool trace_ray(const SceneView& s, float3 o, float3 d, float tmax, HitRecord& hit, uint32_t* err,
+__device__ __forceinline__ bool trace_ray(const SceneView& s, RayRef ray, float tmax, HitRecord& hit, uint32_t* err,
                                           TraceCount* count, TraceStack stk) {
     RaySpace rs;
-    make_space(rs, o, d);
+    make_space(rs, ray.origin(), ray.dir());
     int sp = 0;
     float tbest = tmax;
     bool found = false, in_blas = false, cull = false;
@@ -191,6 +214,7 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, float3 o, float3 d
             const TlasLeaf* lf = s.tlas_leaves + (~node);
             float4 r0 = __ldg(&lf->w2o[0]), r1 = __ldg(&lf->w2o[1]), r2 = __ldg(&lf->w2o[2]);
             uint4 info = __ldg(reinterpret_cast<const uint4*>(&lf->instance));
+            const float3 o = ray.origin(), d = ray.dir();
             float3 oo = f3(r0.x * o.x + r0.y * o.y + r0.z * o.z + r0.w, r1.x * o.x + r1.y * o.y + r1.z * o.z + r1.w, r2.x * o.x + r2.y * o.y + r2.z * o.z + r2.w);
             float3 od = f3(r0.x * d.x + r0.y * d.y + r0.z * d.z, r1.x * d.x + r1.y * d.y + r1.z * d.z, r2.x * d.x + r2.y * d.y + r2.z * d.z);
             make_space(rs, oo, od);
@@ -206,8 +230,8 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, float3 o, float3 d
             node = 0;
             continue;
         } else {
-            // BLAS leaf: up to four triangles in leaf order, ~((first << 2) | (count - 1)).
-            uint32_t v = uint32_t(~node), first = v >> 2, cnt = (v & 3u) + 1u;
+            // BLAS leaf: up to VKB_BLAS_LEAF_MAX triangles in leaf order, ~((first << 2) | (count - 1)).
+            uint32_t v = uint32_t(~node), first = v >> 2, cnt = VKB_BLAS_LEAF_MAX == 1 ? 1u : (v & 3u) + 1u;
             for (uint32_t k = 0; k < cnt; ++k) {
                 if (COUNT) count->tris++;
                 const float4* tp = tris + 3u * (tri_base + first + k);
@@ -227,7 +251,7 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, float3 o, float3 d
             node = stk.r[sp * TRACE_BLOCK];
             if (node == SENTINEL) {
                 in_blas = false;
-                make_space(rs, o, d);
+                make_space(rs, ray.origin(), ray.dir());
                 nodes = s.tlas_nodes;
                 continue;
             }

@@ -327,9 +327,9 @@ __device__ __forceinline__ void flush_count(unsigned long long* dst, uint32_t v)
 #define VKB_TRACE_MIN_BLOCKS 8
 #endif
 template <bool ANY, bool COUNT>
-__device__ __forceinline__ bool trace_any(const SceneView& sv, float3 o, float3 d, float tmax, HitRecord& h, uint32_t* err, TraceCount* tc,
+__device__ __forceinline__ bool trace_any(const SceneView& sv, RayRef ray, float tmax, HitRecord& h, uint32_t* err, TraceCount* tc,
                                           TraceStack stk) {
-    return trace_ray<ANY, COUNT>(sv, o, d, tmax, h, err, tc, stk);
+    return trace_ray<ANY, COUNT>(sv, ray, tmax, h, err, tc, stk);
 }
 // This thread's column of the block's shared-memory traversal stack.
 #define VKB_STACK_DECL                                                                                   \
@@ -347,10 +347,10 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace(Pat
     TraceCount tc;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         if (!ANY) {
-            float4 ro = p.ray_o[cur][i], rd = p.ray_d[cur][i];
-            const SceneView sv = BATCH ? p.jobs[job_of_slot<true>(p, __float_as_uint(rd.w))].sv : p.job0.sv;
+            const float tmax = p.ray_o[cur][i].w;
+            const SceneView sv = BATCH ? p.jobs[job_of_slot<true>(p, __float_as_uint(p.ray_d[cur][i].w))].sv : p.job0.sv;
             HitRecord h;
-            bool found = trace_any<false, COUNT>(sv, f3(ro.x, ro.y, ro.z), f3(rd.x, rd.y, rd.z), ro.w, h, p.err, &tc, stk);
+            bool found = trace_any<false, COUNT>(sv, RayRef{&p.ray_o[cur][i].x, &p.ray_d[cur][i].x}, tmax, h, p.err, &tc, stk);
             p.hit[i] = found ? make_float4(h.t, h.u, h.v, __uint_as_float(h.prim)) : make_float4(-1.f, 0.f, 0.f, __uint_as_float(0xffffffffu));
             p.hit_inst[i] = found ? h.inst : 0xffffffffu;
         } else {
@@ -360,13 +360,12 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace(Pat
             const SceneView sv = J.sv;
             HitRecord h;
             float3 total = f3(sc.x, sc.y, sc.z);
-            if ((flags & SH_TRACE_A) && trace_any<true, COUNT>(sv, f3(so.x, so.y, so.z), f3(sd.x, sd.y, sd.z), so.w, h, p.err, &tc, stk)) total = f3(0.f);
+            if ((flags & SH_TRACE_A) && trace_any<true, COUNT>(sv, RayRef{&p.sa_o[i].x, &p.sa_d[i].x}, so.w, h, p.err, &tc, stk)) total = f3(0.f);
             if (flags & SH_HAS_B) {
                 float4 bc = p.sb_c[slot];
                 float3 cb = f3(bc.x, bc.y, bc.z);
                 if (flags & SH_TRACE_B) {
-                    float4 bo = p.sb_o[slot], bd = p.sb_d[slot];
-                    if (trace_any<true, COUNT>(sv, f3(bo.x, bo.y, bo.z), f3(bd.x, bd.y, bd.z), bo.w, h, p.err, &tc, stk)) cb = f3(0.f);
+                    if (trace_any<true, COUNT>(sv, RayRef{&p.sb_o[slot].x, &p.sb_d[slot].x}, p.sb_o[slot].w, h, p.err, &tc, stk)) cb = f3(0.f);
                 }
                 total = total + cb;
             }
@@ -685,7 +684,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_debug_trace(SceneView sv, uint3
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float* r = rays + 7 * i;
         HitRecord h;
-        bool f = trace_any<false, false>(sv, f3(r[0], r[1], r[2]), f3(r[3], r[4], r[5]), r[6], h, err, nullptr, stk);
+        bool f = trace_any<false, false>(sv, RayRef{r, r + 3}, r[6], h, err, nullptr, stk);
         t[i] = f ? h.t : -1.f;
         ids[2 * i] = f ? h.inst : 0xffffffffu; ids[2 * i + 1] = f ? h.prim : 0xffffffffu;
         uv[2 * i] = f ? h.u : 0.f; uv[2 * i + 1] = f ? h.v : 0.f;
