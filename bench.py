@@ -278,6 +278,7 @@ def main():
     ap.add_argument("--requests", type=int, default=32, help="serve: requests per arrival rate")
     ap.add_argument("--rates", default="2,8,32", help="serve: Poisson arrival rates (req/s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tlas", choices=["lbvh", "ploc"], default="lbvh", help="TLAS builder of the frame scene")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -307,6 +308,7 @@ def main():
         dist.barrier()
 
     sc, flock, prof, cfg = workload(args.config, seed=rank)
+    sc.tlas_builder = abi.TLAS_PLOC if args.tlas == "ploc" else abi.TLAS_LBVH
     frames = frames_for(sc, flock, args.warmup + args.steps)
     cam = sc.camera
     npix = cam.width * cam.height
@@ -341,6 +343,7 @@ def main():
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     trace_ms = 0.0
     trace_launches = 0
+    build_ms = 0.0
     latencies = []
     with ClockSampler(local) as clocks:
         ev0.record(stream)
@@ -349,10 +352,14 @@ def main():
             trace_ms += st["trace_ms"]
             trace_launches += st["trace_launches"]
             latencies.append(st["render_ms"] + st["build_ms"])
+            build_ms += st["build_ms"]
         ev1.record(stream)
         sync()
     elapsed_ms = ev0.elapsed_time(ev1)
     launches = s.launch_count - launches0
+    tlas = {"builder": ("PLOC (radius 16)" if args.tlas == "ploc" else "Karras LBVH") + " over 30-bit Morton order, rebuilt every frame",
+            "build_ms_per_frame": build_ms / args.steps,
+            **s.tlas_stats()}
     if dist:
         t = torch.tensor([elapsed_ms], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -402,6 +409,7 @@ def main():
             "e2e": {"value": e2e, "unit": "paths/s", "h2d_bytes_per_step": int(frames[0].nbytes),
                     "d2h_bytes_per_step": int(npix * 16)},
             "gpu_launches": int(launches),
+            "tlas": tlas,
             "clocks": clocks.summary(),
             "work": {k: counted[k] for k in ("extension_rays", "shadow_rays", "nodes_visited", "triangles_tested",
                                              "instances_entered", "blas_nodes_visited", "shadow_nodes_visited", "shadow_triangles_tested",

@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define VKB_ABI_VERSION 1u
+#define VKB_ABI_VERSION 2u
 
 /* Error model: FailureKind exit categories of crates/vork-render/src/failure.rs:21-100,
  * reduced to what a render call can report. */
@@ -124,7 +124,15 @@ typedef struct vkb_scene_desc {
     uint32_t num_lights;
     vkb_camera camera;
     vkb_environment environment;
+    uint32_t tlas_builder;            /* VKB_TLAS_LBVH or VKB_TLAS_PLOC (no reference counterpart: the
+                                         reference's TLAS is built by the graphics driver) */
 } vkb_scene_desc;
+
+/* TLAS builders, both over the instance boxes in Morton order and both refittable:
+ * Karras LBVH (fast build, siblings adjacent in memory) or PLOC (lower surface area
+ * cost; Meister & Bittner 2018). */
+#define VKB_TLAS_LBVH 0u
+#define VKB_TLAS_PLOC 1u
 
 /* PathSettings (path.slang:54; passes/path.rs:16-28,576-607). */
 typedef struct vkb_profile {
@@ -315,6 +323,11 @@ vkb_status vkb_debug_brdf_lut(vkb_ctx* ctx, float* out);
 vkb_status vkb_debug_tlas_morton(vkb_scene* scene, uint32_t* out);
 /* 30-bit Morton codes of one mesh's BLAS build (triangle centroids over the mesh box). */
 vkb_status vkb_debug_blas_morton(vkb_scene* scene, uint32_t mesh, uint32_t* out);
+/* TLAS check (test hook, no reference counterpart): walks the installed TLAS from its
+ * root and reports whether every instance leaf is reached exactly once and every stored
+ * child box contains its subtree (*valid = 1), the deepest leaf, and the tree's surface
+ * area cost (sum of node and leaf box areas over the root box area, unit costs). */
+vkb_status vkb_debug_tlas_stats(vkb_scene* scene, double* sah_cost, uint32_t* max_depth, uint32_t* valid);
 /* Closest hits of n world rays (origin xyz, dir xyz, tmax per ray; host arrays):
  * out_t[n], out_ids[n*2] (instance, triangle; 0xffffffff on miss), out_uv[n*2]. */
 vkb_status vkb_debug_trace(vkb_scene* scene, uint32_t n, const float* rays7, float* out_t,

@@ -1,4 +1,5 @@
 """CUDA path against the oracle and the reference's known answers, through the C ABI."""
+import dataclasses
 import json
 from pathlib import Path
 
@@ -172,10 +173,25 @@ def test_tiny_scenes_and_errors(renderer):
     with pytest.raises(abi.VkbError) as e:
         renderer.install(bad)
     assert e.value.status == abi.VKB_INVALID_ARG
+    # One and two instances under both TLAS builders; an unknown builder is refused.
+    for builder in (abi.TLAS_LBVH, abi.TLAS_PLOC):
+        for k in (1, 2):
+            rows = np.stack([S.rows_from(1.0, (0.0, 0.0, 0.0)), S.rows_from(1.0, (0.5, 0.1, 0.0))])[:k]
+            sk = S.Scene([tri], rows, np.zeros(k, np.uint32), np.zeros(k, np.uint32), [S.material()], [light], cam,
+                         S.environment(), tlas_builder=builder)
+            with renderer.install(sk) as s:
+                assert s.tlas_stats()["valid"]
+                assert np.isfinite(s.render(Profile.reference_transport(4, 2)).image).all()
+    with pytest.raises(abi.VkbError) as e:
+        renderer.install(S.Scene([tri], S.rows_from(1.0, (0, 0, 0))[None], np.zeros(1, np.uint32), np.zeros(1, np.uint32),
+                                 [S.material()], [light], cam, S.environment(), tlas_builder=7))
+    assert e.value.status == abi.VKB_INVALID_ARG
 
 
-def test_tlas_refit_matches_rebuild_and_follows_the_quarter_rule(renderer, small_scene):
+@pytest.mark.parametrize("builder", [abi.TLAS_LBVH, abi.TLAS_PLOC])
+def test_tlas_refit_matches_rebuild_and_follows_the_quarter_rule(renderer, small_scene, builder):
     # rt.rs:1465-1476: refit until the changed object bytes reach a quarter of the object buffer.
+    small_scene = dataclasses.replace(small_scene, tlas_builder=builder)
     rows = small_scene.instance_rows.copy()
     with renderer.install(small_scene) as s:
         base = s.info()
@@ -184,6 +200,7 @@ def test_tlas_refit_matches_rebuild_and_follows_the_quarter_rule(renderer, small
         i1 = s.info()
         assert i1["tlas_refits"] == base["tlas_refits"] + 1 and i1["tlas_rebuilds"] == base["tlas_rebuilds"]
         refit_img = s.render(_small_profile(4)).image
+        assert s.tlas_stats()["valid"]
         s.update_instances(few, policy=1)                         # same rows, forced rebuild
         rebuilt_img = s.render(_small_profile(4)).image
         assert np.array_equal(refit_img, rebuilt_img)
@@ -199,3 +216,43 @@ def test_tlas_refit_matches_rebuild_and_follows_the_quarter_rule(renderer, small
         s.update_instances(big, policy=1)
         b = s.render(_small_profile(4)).image
         assert np.array_equal(a, b)
+
+
+def _crowd_scene(seed=5):
+    """20,000 instances of a 500-triangle sphere: 4,000 coincident at one spot, 6,000 in
+    a dense clump, the rest scattered -- equal merge costs and near-equal Morton codes
+    for the TLAS builder."""
+    rng = np.random.default_rng(seed)
+    mesh = S.geodesic_sphere(5)
+    centers = np.concatenate([np.tile([[5.0, 5.0, 5.0]], (4000, 1)), rng.normal(5.0, 0.3, (6000, 3)),
+                              rng.uniform(0.0, 10.0, (10000, 3))])
+    radii = np.concatenate([np.full(4000, 0.4), rng.uniform(0.02, 0.1, 16000)])
+    rows = np.stack([S.rows_from(float(r), tuple(c)) for r, c in zip(radii, centers)]).astype(np.float32)
+    cam = S.look_at(eye=(5.0, 5.0, -12.0), target=(5.0, 5.0, 5.0), width=96, height=96)
+    return S.Scene([mesh], rows, np.zeros(len(rows), np.uint32), np.zeros(len(rows), np.uint32), [S.material()],
+                   [S.sun_light((0.3, -1.0, 0.2))], cam, S.environment((0.2, 0.2, 0.2)), name="crowd")
+
+
+@pytest.mark.parametrize("builder", [abi.TLAS_LBVH, abi.TLAS_PLOC])
+def test_tlas_over_coincident_and_clustered_instances(renderer, oracle, builder):
+    # Coincident instances tie on t, so which instance is reported may differ; the hit
+    # distance and hit/miss must not.
+    sc = _crowd_scene()
+    sc.tlas_builder = builder
+    o = oracle.OracleScene(sc, fp64=False)
+    rng = np.random.default_rng(3)
+    n = 20000
+    org = rng.uniform(-2, 12, (n, 3))
+    d = rng.normal(size=(n, 3)); d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.concatenate([org, d, np.full((n, 1), 1e30)], 1).astype(np.float32)
+    t_ref, ids_ref, _ = o.trace(rays, fp64=False)
+    with renderer.install(sc) as s:
+        t, ids, _ = s.trace(rays)
+        st = s.tlas_stats()
+        assert st["valid"] and st["max_depth"] < 200 and np.isfinite(st["sah_cost"]), st
+    hit, hit_ref = ids[:, 0] != 0xffffffff, ids_ref[:, 0] != 0xffffffff
+    assert np.mean(hit != hit_ref) <= 1e-3
+    both = hit & hit_ref
+    assert both.sum() > 1000
+    rel = np.abs(t[both] - t_ref[both]) / np.maximum(t_ref[both], 1e-3)
+    assert np.mean(rel > 1e-4) <= 2e-3

@@ -203,6 +203,12 @@ class InstalledScene:
         abi.check(self.r.lib.vkb_debug_blas_morton(self.h, mesh, abi.uptr(out)))
         return out
 
+    def tlas_stats(self) -> dict:
+        """Walk the TLAS (vkb_debug_tlas_stats): validity, deepest leaf, surface area cost."""
+        cost, depth, valid = C.c_double(), C.c_uint32(), C.c_uint32()
+        abi.check(self.r.lib.vkb_debug_tlas_stats(self.h, C.byref(cost), C.byref(depth), C.byref(valid)))
+        return {"valid": bool(valid.value), "max_depth": int(depth.value), "sah_cost": float(cost.value)}
+
     def trace(self, rays7: np.ndarray):
         r = np.ascontiguousarray(rays7, np.float32)
         n = r.shape[0]

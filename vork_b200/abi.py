@@ -56,7 +56,7 @@ class VkbSceneDesc(C.Structure):
                 ("instance_rows", C.POINTER(C.c_float)), ("instance_mesh", C.POINTER(C.c_uint32)),
                 ("instance_material", C.POINTER(C.c_uint32)), ("materials", C.POINTER(VkbMaterial)),
                 ("num_materials", C.c_uint32), ("lights", C.POINTER(VkbLight)), ("num_lights", C.c_uint32),
-                ("camera", VkbCamera), ("environment", VkbEnvironment)]
+                ("camera", VkbCamera), ("environment", VkbEnvironment), ("tlas_builder", C.c_uint32)]
 
 
 class VkbProfile(C.Structure):
@@ -68,6 +68,7 @@ class VkbProfile(C.Structure):
 
 PROFILE_TIME_KERNELS, PROFILE_COUNT_TRAVERSAL = 1, 2
 BATCH_FAIR, BATCH_PACKED = 4, 8
+TLAS_LBVH, TLAS_PLOC = 0, 1
 NOALLOC_SCRATCH_MIB = 32
 
 
@@ -140,6 +141,7 @@ SIGNATURES = {
     "vkb_debug_blas_morton": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32)]),
     "vkb_debug_trace": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_uint32),
                                   C.POINTER(C.c_float)]),
+    "vkb_debug_tlas_stats": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
 }
 
 _lib = None

@@ -8,6 +8,7 @@
 // wavefront buffers its renders reuse.
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <deque>
@@ -40,6 +41,7 @@ struct CudaError {
 
 struct ArgError { std::string msg; };
 struct Unsupported { std::string msg; };
+struct InternalError { std::string msg; };
 
 template <class T> struct DBuf {
     T* p = nullptr;
@@ -267,11 +269,9 @@ struct LbvhScratch {
     }
 };
 
-// Build one LBVH over n boxes into nodes (n-1 internal nodes, or 1 for n == 1).
-// On return scratch.ids_sorted holds the leaf order and scratch.codes the codes in input order.
-void build_lbvh(uint32_t n, const float4* lo, const float4* hi, BvhNode* nodes, LbvhScratch& sc, cudaStream_t s, int sms, uint64_t& launches) {
-    if (n == 0) return;
-    launches += n == 1 ? 3 : 4;
+// Morton codes of n boxes (sc.codes, input order) and the sorted order (sc.ids_sorted).
+void morton_sort(uint32_t n, const float4* lo, const float4* hi, LbvhScratch& sc, cudaStream_t s, int sms, uint64_t& launches) {
+    launches += 3;
     sc.reserve(n, s);
     VKB_CUDA(cudaMemsetAsync(sc.bounds.p, 0xff, 3 * sizeof(uint32_t), s));
     VKB_CUDA(cudaMemsetAsync(sc.bounds.p + 3, 0x00, 3 * sizeof(uint32_t), s));
@@ -279,6 +279,14 @@ void build_lbvh(uint32_t n, const float4* lo, const float4* hi, BvhNode* nodes, 
     k_morton<<<grid_for(n, 256, sms), 256, 0, s>>>(n, lo, hi, sc.bounds.p, sc.codes.p, sc.ids.p);
     size_t bytes = sc.cub_temp.n;
     VKB_CUDA(cub::DeviceRadixSort::SortPairs(sc.cub_temp.p, bytes, sc.codes.p, sc.codes_sorted.p, sc.ids.p, sc.ids_sorted.p, int(n), 0, 30, s));
+}
+
+// Build one LBVH over n boxes into nodes (n-1 internal nodes, or 1 for n == 1).
+// On return scratch.ids_sorted holds the leaf order and scratch.codes the codes in input order.
+void build_lbvh(uint32_t n, const float4* lo, const float4* hi, BvhNode* nodes, LbvhScratch& sc, cudaStream_t s, int sms, uint64_t& launches) {
+    if (n == 0) return;
+    morton_sort(n, lo, hi, sc, s, sms, launches);
+    launches += n == 1 ? 0 : 1;
     if (n == 1) {
         k_single_leaf<<<1, 1, 0, s>>>(lo, hi, nodes);
         return;
@@ -286,6 +294,50 @@ void build_lbvh(uint32_t n, const float4* lo, const float4* hi, BvhNode* nodes, 
     k_karras<<<grid_for(n - 1, 256, sms), 256, 0, s>>>(int(n), sc.codes_sorted.p, nodes, sc.leaf_parent.p, sc.node_parent.p, sc.counters.p);
     k_refit<<<grid_for(n, 256, sms), 256, 0, s>>>(int(n), sc.ids_sorted.p, lo, hi, nodes, sc.leaf_parent.p, sc.node_parent.p, sc.counters.p);
     VKB_CUDA(cudaGetLastError());
+}
+
+// Cluster arrays of the PLOC builder (double-buffered) and its prefix-sum scratch.
+struct PlocScratch {
+    DBuf<float4> clo, chi, clo2, chi2;
+    DBuf<uint32_t> nn, counts;
+    DBuf<unsigned long long> flags, offs;
+    DBuf<unsigned char> cub_temp;
+    void reserve(size_t n, cudaStream_t s) {
+        clo.alloc(n); chi.alloc(n); clo2.alloc(n); chi2.alloc(n); nn.alloc(n); counts.alloc(2); flags.alloc(n); offs.alloc(n);
+        size_t bytes = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, bytes, flags.p, offs.p, int(n), s);
+        cub_temp.alloc(std::max<size_t>(bytes, 1));
+    }
+};
+
+// Build a PLOC tree over n boxes (n >= 2) into nodes[0, n-1), root 0, leaves ~k in
+// Morton order (sc.ids_sorted, from the same sort as the LBVH), with parent links and
+// zeroed counters for refits.  One host round trip per pass (cluster count).
+void build_ploc(uint32_t n, const float4* lo, const float4* hi, BvhNode* nodes, uint32_t* leaf_parent, uint32_t* node_parent,
+                uint32_t* counters, LbvhScratch& sc, PlocScratch& pc, cudaStream_t s, int sms, uint64_t& launches) {
+    pc.reserve(n, s);
+    k_ploc_init<<<grid_for(n, 256, sms), 256, 0, s>>>(n, sc.ids_sorted.p, lo, hi, pc.clo.p, pc.chi.p);
+    launches += 1;
+    uint32_t c = n, next_free = n - 1;
+    float4 *a_lo = pc.clo.p, *a_hi = pc.chi.p, *b_lo = pc.clo2.p, *b_hi = pc.chi2.p;
+    for (uint32_t pass = 0; c > 1; ++pass) {
+        if (pass >= n) throw InternalError{"PLOC made no progress"};
+        k_ploc_nn<<<(c + PLOC_BLOCK - 1) / PLOC_BLOCK, PLOC_BLOCK, 0, s>>>(c, a_lo, a_hi, pc.nn.p);
+        k_ploc_flags<<<grid_for(c, 256, sms), 256, 0, s>>>(c, pc.nn.p, pc.flags.p);
+        size_t bytes = pc.cub_temp.n;
+        VKB_CUDA(cub::DeviceScan::ExclusiveSum(pc.cub_temp.p, bytes, pc.flags.p, pc.offs.p, int(c), s));
+        k_ploc_merge<<<grid_for(c, 256, sms), 256, 0, s>>>(c, pc.nn.p, pc.offs.p, a_lo, a_hi, next_free, nodes, leaf_parent, node_parent,
+                                                           counters, b_lo, b_hi, pc.counts.p);
+        launches += 4;
+        uint32_t counts[2] = {0u, 0u};
+        VKB_CUDA(cudaMemcpyAsync(counts, pc.counts.p, sizeof(counts), cudaMemcpyDeviceToHost, s));
+        VKB_CUDA(cudaStreamSynchronize(s));
+        if (counts[1] == 0 || counts[1] > next_free || counts[0] != c - counts[1]) throw InternalError{"PLOC pass merged no pair"};
+        c = counts[0];
+        next_free -= counts[1];
+        std::swap(a_lo, b_lo); std::swap(a_hi, b_hi);
+    }
+    if (next_free != 0) throw InternalError{"PLOC left unused nodes"};
 }
 
 }  // namespace
@@ -377,6 +429,8 @@ struct vkb_scene {
     DBuf<vkb_light> d_lights;
     DBuf<LightTreeNode> tree;
     LbvhScratch scratch;
+    PlocScratch ploc;
+    uint32_t tlas_builder = VKB_TLAS_LBVH;
     float build_ms = 0.f;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint64_t launches = 0;                    // kernels launched for this scene so far
@@ -395,6 +449,8 @@ template <class F> vkb_status guarded(F&& f) {
         return fail(VKB_INVALID_ARG, e.msg);
     } catch (const Unsupported& e) {
         return fail(VKB_UNSUPPORTED, e.msg);
+    } catch (const InternalError& e) {
+        return fail(VKB_INTERNAL, e.msg);
     } catch (const std::bad_alloc&) {
         return fail(VKB_OUT_OF_MEMORY, "host allocation failed");
     }
@@ -408,7 +464,9 @@ SceneView scene_view(const vkb_scene* s) {
     return v;
 }
 
-// Instance rows -> w2o, world boxes, TLAS (LBVH) and its leaf records.
+// Instance rows -> w2o, world boxes, TLAS and its leaf records.  The TLAS is the
+// Karras LBVH or a PLOC tree over the instance boxes in Morton order (the scene's
+// tlas_builder); both keep parent links for refits.
 void build_tlas(vkb_scene* s) {
     cudaStream_t st = s->ctx->stream;
     int sms = s->ctx->sms;
@@ -416,17 +474,23 @@ void build_tlas(vkb_scene* s) {
     if (n == 0) return;
     VKB_CUDA(cudaEventRecord(s->ev0, st));
     k_instances<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->o2w.p, s->inst_info.p, s->meshes.p, s->w2o.p, s->inst_lo.p, s->inst_hi.p);
-    build_lbvh(n, s->inst_lo.p, s->inst_hi.p, s->tlas_nodes.p, s->scratch, st, sms, s->launches);
+    s->tlas_order.alloc(n); s->tlas_leaf_parent.alloc(n); s->tlas_node_parent.alloc(std::max(1u, n)); s->tlas_counters.alloc(std::max(1u, n));
+    if (s->tlas_builder == VKB_TLAS_LBVH || n == 1) {
+        build_lbvh(n, s->inst_lo.p, s->inst_hi.p, s->tlas_nodes.p, s->scratch, st, sms, s->launches);
+        // Keep the topology for later refits (the LBVH scratch is shared with other builds).
+        if (n > 1) {
+            VKB_CUDA(cudaMemcpyAsync(s->tlas_leaf_parent.p, s->scratch.leaf_parent.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+            VKB_CUDA(cudaMemcpyAsync(s->tlas_node_parent.p, s->scratch.node_parent.p, (n - 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+        }
+    } else {
+        morton_sort(n, s->inst_lo.p, s->inst_hi.p, s->scratch, st, sms, s->launches);
+        build_ploc(n, s->inst_lo.p, s->inst_hi.p, s->tlas_nodes.p, s->tlas_leaf_parent.p, s->tlas_node_parent.p, s->tlas_counters.p,
+                   s->scratch, s->ploc, st, sms, s->launches);
+    }
     s->launches += 2;
     k_tlas_leaves<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->scratch.ids_sorted.p, s->w2o.p, s->inst_info.p, s->meshes.p, s->d_materials.p, s->tlas_leaves.p);
     VKB_CUDA(cudaMemcpyAsync(s->tlas_codes.p, s->scratch.codes.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-    // Keep the topology for later refits (the LBVH scratch is shared with other builds).
-    s->tlas_order.alloc(n); s->tlas_leaf_parent.alloc(n); s->tlas_node_parent.alloc(std::max(1u, n)); s->tlas_counters.alloc(std::max(1u, n));
     VKB_CUDA(cudaMemcpyAsync(s->tlas_order.p, s->scratch.ids_sorted.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-    if (n > 1) {
-        VKB_CUDA(cudaMemcpyAsync(s->tlas_leaf_parent.p, s->scratch.leaf_parent.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-        VKB_CUDA(cudaMemcpyAsync(s->tlas_node_parent.p, s->scratch.node_parent.p, (n - 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-    }
     s->tlas_rebuilds++;
     VKB_CUDA(cudaEventRecord(s->ev1, st));
     VKB_CUDA(cudaEventSynchronize(s->ev1));
@@ -491,6 +555,7 @@ void validate_desc(const vkb_scene_desc* d) {
         if (!(k == 0.f || k == 1.f || k == 2.f || k == 3.f)) throw ArgError{"light kind must be 0..3"};
     }
     if (d->camera.width == 0 || d->camera.height == 0) throw ArgError{"camera resolution is zero"};
+    if (d->tlas_builder > VKB_TLAS_PLOC) throw ArgError{"unknown TLAS builder"};
 }
 
 
@@ -878,6 +943,7 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         VKB_CUDA(cudaEventCreate(&s->ev1));
         s->num_meshes = d->num_meshes;
         s->num_instances = d->num_instances;
+        s->tlas_builder = d->tlas_builder;
         // Concatenate meshes.
         uint32_t nv = 0, nt = 0;
         s->mesh_info.resize(d->num_meshes);
@@ -998,6 +1064,9 @@ vkb_status vkb_scene_destroy(vkb_scene* s) {
     s->tree.release();
     s->scratch.codes.release(); s->scratch.codes_sorted.release(); s->scratch.ids.release(); s->scratch.ids_sorted.release();
     s->scratch.leaf_parent.release(); s->scratch.node_parent.release(); s->scratch.counters.release(); s->scratch.bounds.release(); s->scratch.cub_temp.release();
+    DBuf<float4>* pf4[] = {&s->ploc.clo, &s->ploc.chi, &s->ploc.clo2, &s->ploc.chi2};
+    for (auto* b : pf4) b->release();
+    s->ploc.nn.release(); s->ploc.counts.release(); s->ploc.flags.release(); s->ploc.offs.release(); s->ploc.cub_temp.release();
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     delete s;
@@ -1157,6 +1226,68 @@ vkb_status vkb_scene_info(vkb_scene* s, vkb_scene_info_t* out) {
     out->scene_bytes = dev;
     out->build_ms = s->build_ms;
     return VKB_OK;
+}
+
+vkb_status vkb_debug_tlas_stats(vkb_scene* s, double* sah_cost, uint32_t* max_depth, uint32_t* valid) {
+    if (!s || !sah_cost || !max_depth || !valid) return fail(VKB_INVALID_ARG, "null argument");
+    return guarded([&] {
+        VKB_CUDA(cudaSetDevice(s->ctx->device));
+        VKB_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        const uint32_t n = s->num_instances;
+        *sah_cost = 0.0; *max_depth = 0; *valid = 1;
+        if (n == 0) return;
+        const uint32_t nn = std::max(1u, n - 1);
+        std::vector<BvhNode> nodes(nn);
+        VKB_CUDA(cudaMemcpy(nodes.data(), s->tlas_nodes.p, nn * sizeof(BvhNode), cudaMemcpyDeviceToHost));
+        auto area = [](const float lo[3], const float hi[3]) {
+            double dx = double(hi[0]) - lo[0], dy = double(hi[1]) - lo[1], dz = double(hi[2]) - lo[2];
+            return dx * dy + dy * dz + dz * dx;
+        };
+        struct Item { int ref; uint32_t depth; float lo[3], hi[3]; };
+        auto child = [&](const BvhNode& b, int side, Item& it) {
+            const float4 q = side ? b.b : b.a;
+            it.lo[0] = q.x; it.hi[0] = q.y; it.lo[1] = q.z; it.hi[1] = q.w;
+            it.lo[2] = side ? b.c.z : b.c.x; it.hi[2] = side ? b.c.w : b.c.y;
+            it.ref = side ? b.d.y : b.d.x;
+        };
+        std::vector<uint8_t> seen_leaf(n, 0), seen_node(nn, 0);
+        std::vector<Item> stack;
+        Item root;
+        root.ref = 0; root.depth = 0;
+        for (int k = 0; k < 3; ++k) { root.lo[k] = INFINITY; root.hi[k] = -INFINITY; }
+        {
+            Item a, b;
+            child(nodes[0], 0, a); child(nodes[0], 1, b);
+            for (int k = 0; k < 3; ++k) { root.lo[k] = std::min(a.lo[k], n > 1 ? b.lo[k] : a.lo[k]); root.hi[k] = std::max(a.hi[k], n > 1 ? b.hi[k] : a.hi[k]); }
+        }
+        const double root_area = std::max(area(root.lo, root.hi), 1e-30);
+        stack.push_back(root);
+        double cost = 0.0;
+        while (!stack.empty()) {
+            Item it = stack.back(); stack.pop_back();
+            *max_depth = std::max(*max_depth, it.depth);
+            cost += area(it.lo, it.hi) / root_area;
+            if (it.ref < 0) {
+                uint32_t leaf = uint32_t(~it.ref);
+                if (leaf >= n || seen_leaf[leaf]) { *valid = 0; continue; }
+                seen_leaf[leaf] = 1;
+                continue;
+            }
+            if (uint32_t(it.ref) >= nn || seen_node[it.ref] || it.depth > n) { *valid = 0; continue; }
+            seen_node[it.ref] = 1;
+            const BvhNode& b = nodes[it.ref];
+            for (int side = 0; side < (n > 1 ? 2 : 1); ++side) {
+                Item c;
+                child(b, side, c);
+                c.depth = it.depth + 1;
+                for (int k = 0; k < 3; ++k)
+                    if (!(c.lo[k] >= it.lo[k] && c.hi[k] <= it.hi[k])) *valid = 0;
+                stack.push_back(c);
+            }
+        }
+        for (uint32_t k = 0; k < n; ++k) if (!seen_leaf[k]) *valid = 0;
+        *sah_cost = cost;
+    });
 }
 
 void* vkb_ctx_stream(vkb_ctx* c) { return c ? reinterpret_cast<void*>(c->stream) : nullptr; }

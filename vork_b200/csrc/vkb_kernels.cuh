@@ -189,6 +189,109 @@ __global__ void k_refit(int n, const uint32_t* sorted_ids, const float4* lo, con
         }
     }
 }
+// ---- PLOC (Meister & Bittner 2018, "Parallel Locally-Ordered Clustering for Bounding
+// Volume Hierarchy Construction"): clusters in Morton order; each picks the neighbour
+// within PLOC_RADIUS positions whose merged box has the least surface area; mutual
+// pairs merge into a new node.  Ties are broken by a strict order on pairs, so the
+// closest pair of every pass is mutual and every pass merges.  A cluster is (lo.xyz, ref) / (hi.xyz, -): ref ~k for the k-th leaf in Morton
+// order, else an internal node index.
+constexpr int PLOC_RADIUS = 16;
+constexpr int PLOC_BLOCK = 256;
+__device__ __forceinline__ float merged_area(float3 alo, float3 ahi, float3 blo, float3 bhi) {
+    float dx = fmaxf(ahi.x, bhi.x) - fminf(alo.x, blo.x);
+    float dy = fmaxf(ahi.y, bhi.y) - fminf(alo.y, blo.y);
+    float dz = fmaxf(ahi.z, bhi.z) - fminf(alo.z, blo.z);
+    float a = dx * dy + dy * dz + dz * dx;
+    return a == a ? a : INFINITY;  // a NaN box sorts last, by index like every tie
+}
+__global__ void k_ploc_init(uint32_t n, const uint32_t* sorted_ids, const float4* lo, const float4* hi, float4* clo, float4* chi) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        uint32_t id = sorted_ids[k];
+        float4 a = lo[id], b = hi[id];
+        clo[k] = make_float4(a.x, a.y, a.z, __int_as_float(~int(k)));
+        chi[k] = make_float4(b.x, b.y, b.z, 0.f);
+    }
+}
+// Nearest neighbour of every cluster: one block covers PLOC_BLOCK clusters and stages
+// their boxes plus PLOC_RADIUS on either side in shared memory.  Launch with
+// blockDim.x == PLOC_BLOCK and one block per PLOC_BLOCK clusters.
+__global__ void __launch_bounds__(PLOC_BLOCK) k_ploc_nn(uint32_t c, const float4* clo, const float4* chi, uint32_t* nn) {
+    __shared__ float3 slo[PLOC_BLOCK + 2 * PLOC_RADIUS], shi[PLOC_BLOCK + 2 * PLOC_RADIUS];
+    const int base = int(blockIdx.x) * PLOC_BLOCK - PLOC_RADIUS;
+    for (int t = threadIdx.x; t < PLOC_BLOCK + 2 * PLOC_RADIUS; t += PLOC_BLOCK) {
+        int g = base + t;
+        if (g >= 0 && g < int(c)) {
+            float4 a = clo[g], b = chi[g];
+            slo[t] = f3(a.x, a.y, a.z); shi[t] = f3(b.x, b.y, b.z);
+        }
+    }
+    __syncthreads();
+    const int i = int(blockIdx.x) * PLOC_BLOCK + int(threadIdx.x);
+    if (i >= int(c)) return;
+    const int li = int(threadIdx.x) + PLOC_RADIUS;
+    const float3 alo = slo[li], ahi = shi[li];
+    const int j0 = max(0, i - PLOC_RADIUS), j1 = min(int(c) - 1, i + PLOC_RADIUS);
+    float best = INFINITY;
+    int best_j = -1, best_d = 0, best_m = 0;
+    for (int j = j0; j <= j1; ++j) {
+        if (j == i) continue;
+        float a = merged_area(alo, ahi, slo[j - base], shi[j - base]);
+        int d = abs(i - j), m = min(i, j);
+        // Pair order (area, index distance, parity of the lower index, lower index): a
+        // strict order that pairs equal neighbours as (0,1), (2,3), ... rather than
+        // chaining them all to one cluster.
+        bool better = best_j < 0 || a < best ||
+                      (a == best && (d < best_d || (d == best_d && ((m & 1) < (best_m & 1) || ((m & 1) == (best_m & 1) && m < best_m)))));
+        if (better) { best = a; best_j = j; best_d = d; best_m = m; }
+    }
+    nn[i] = uint32_t(best_j);
+}
+// Per cluster: bit 32 = merges (mutual pair, lower index), bit 0 = survives.
+__global__ void k_ploc_flags(uint32_t c, const uint32_t* nn, unsigned long long* flags) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c; i += gridDim.x * blockDim.x) {
+        uint32_t j = nn[i];
+        bool mutual = nn[j] == i;
+        flags[i] = ((mutual && i < j) ? (1ull << 32) : 0ull) | ((mutual && i > j) ? 0ull : 1ull);
+    }
+}
+// Merge mutual pairs into nodes next_free-1, next_free-2, ... (by exclusive prefix of
+// merges) and compact the surviving clusters; counts = {clusters left, merges}.
+__global__ void k_ploc_merge(uint32_t c, const uint32_t* nn, const unsigned long long* offs, const float4* clo, const float4* chi,
+                             uint32_t next_free, BvhNode* nodes, uint32_t* leaf_parent, uint32_t* node_parent, uint32_t* counters,
+                             float4* clo2, float4* chi2, uint32_t* counts) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c; i += gridDim.x * blockDim.x) {
+        uint32_t j = nn[i];
+        bool mutual = nn[j] == i;
+        bool merge = mutual && i < j, keep = !(mutual && i > j);
+        unsigned long long o = offs[i];
+        if (i == c - 1) {
+            counts[0] = uint32_t(o & 0xffffffffull) + (keep ? 1u : 0u);
+            counts[1] = uint32_t(o >> 32) + (merge ? 1u : 0u);
+        }
+        if (!keep) continue;
+        uint32_t pos = uint32_t(o & 0xffffffffull);
+        float4 alo = clo[i], ahi = chi[i];
+        if (!merge) { clo2[pos] = alo; chi2[pos] = ahi; continue; }
+        // next_free == c - 1 before every pass and a pass merges at most c / 2 pairs, so
+        // the offset is below next_free; the test only keeps a broken caller in bounds.
+        if (uint32_t(o >> 32) >= next_free) continue;
+        float4 blo = clo[j], bhi = chi[j];
+        uint32_t node = next_free - 1u - uint32_t(o >> 32);
+        int ra = __float_as_int(alo.w), rb = __float_as_int(blo.w);
+        BvhNode nd;
+        nd.a = make_float4(alo.x, ahi.x, alo.y, ahi.y);
+        nd.b = make_float4(blo.x, bhi.x, blo.y, bhi.y);
+        nd.c = make_float4(alo.z, ahi.z, blo.z, bhi.z);
+        nd.d = make_int4(ra, rb, 0, 0);
+        nodes[node] = nd;
+        if (ra < 0) leaf_parent[~ra] = node * 2u; else node_parent[ra] = node * 2u;
+        if (rb < 0) leaf_parent[~rb] = node * 2u + 1u; else node_parent[rb] = node * 2u + 1u;
+        counters[node] = 0u;
+        if (node == 0u) node_parent[0] = 0xffffffffu;
+        clo2[pos] = make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), __int_as_float(int(node)));
+        chi2[pos] = make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.f);
+    }
+}
 // A one-primitive tree: root with the leaf on the left and an empty right box.
 __global__ void k_single_leaf(const float4* lo, const float4* hi, BvhNode* nodes) {
     BvhNode n;

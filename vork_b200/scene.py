@@ -260,6 +260,7 @@ class Scene:
     camera: abi.VkbCamera
     environment: abi.VkbEnvironment
     name: str = "scene"
+    tlas_builder: int = abi.TLAS_LBVH
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -299,6 +300,7 @@ class Scene:
         d.num_lights = len(self.lights)
         d.camera = self.camera
         d.environment = self.environment
+        d.tlas_builder = self.tlas_builder
         self._keep = keep
         return d
 
