@@ -323,6 +323,46 @@ vkb_status vkb_debug_brdf_lut(vkb_ctx* ctx, float* out);
 vkb_status vkb_debug_tlas_morton(vkb_scene* scene, uint32_t* out);
 /* 30-bit Morton codes of one mesh's BLAS build (triangle centroids over the mesh box). */
 vkb_status vkb_debug_blas_morton(vkb_scene* scene, uint32_t mesh, uint32_t* out);
+/* ---- Learned radiance cache (no reference counterpart: vork has no learned path
+ * component).  A multiresolution hash encoding (16 levels x 2^19 entries x 2 FP16
+ * features) and a 5-layer, 64-wide BF16 MLP with FP32 accumulation on the tensor cores,
+ * trained online on the tracer's own path vertices; renders through it stop each path at
+ * `query_vertex` and add throughput x the cached outgoing radiance there.  One cache per
+ * installed scene; it owns its parameters, optimizer state and training buffers. */
+typedef struct vkb_cache vkb_cache;
+typedef struct vkb_cache_config {
+    uint32_t train_records;    /* training vertices per vkb_cache_train call (default 65536) */
+    uint32_t train_steps;      /* optimizer steps per call, each over all records (default 4) */
+    uint32_t query_vertex;     /* path vertex (0 = camera hit) answered by the cache (default 2) */
+    uint32_t seed;             /* parameter initialisation and training-path sampling */
+    float lr_mlp, lr_hash;     /* Adam learning rates (defaults 2e-3, 1e-2) */
+    float beta1, beta2, eps;   /* Adam moments (defaults 0.9, 0.99, 1e-10) */
+} vkb_cache_config;
+typedef struct vkb_cache_stats {
+    uint64_t steps;            /* optimizer steps taken so far */
+    uint64_t records;          /* training vertices of the last call */
+    float loss;                /* mean relative-L2 loss of the last step */
+    float train_ms;            /* device time of the last call (paths + steps) */
+} vkb_cache_stats;
+vkb_status vkb_cache_create(vkb_scene* scene, const vkb_cache_config* config, vkb_cache** out);
+vkb_status vkb_cache_destroy(vkb_cache* cache);
+/* Test hooks of the network itself.  Parameters as FP32: MLP row-major [out][in] per
+ * layer (4 x 64x64 then 16x64, rows 3..15 of the last zero), hash table [level][entry][feature]. */
+#define VKB_NRC_MLP_PARAMS 17408u
+#define VKB_NRC_HASH_PARAMS 16777216u
+vkb_status vkb_debug_nrc_set_params(vkb_cache* cache, const float* mlp, const float* hash);
+vkb_status vkb_debug_nrc_get_params(vkb_cache* cache, float* mlp, float* hash);
+/* records: n x 16 floats (position normalised to [0,1]^3, outgoing direction, shading
+ * normal, roughness, metalness, base colour, 2 pad).  x_out: n x 64 network inputs (as
+ * BF16 values), y_out: n x 3 raw outputs. */
+vkb_status vkb_debug_nrc_forward(vkb_cache* cache, uint32_t n, const float* records, float* x_out, float* y_out);
+/* Gradients of the mean relative-L2 loss over n records against targets (n x 3), no
+ * update: mlp_grad (VKB_NRC_MLP_PARAMS), hash_grad (VKB_NRC_HASH_PARAMS, may be NULL), loss. */
+vkb_status vkb_debug_nrc_gradients(vkb_cache* cache, uint32_t n, const float* records, const float* targets, float* mlp_grad,
+                                   float* hash_grad, float* loss);
+/* One optimizer step over n records (the same step vkb_cache_train takes). */
+vkb_status vkb_debug_nrc_step(vkb_cache* cache, uint32_t n, const float* records, const float* targets, float* loss);
+
 /* TLAS check (test hook, no reference counterpart): walks the installed TLAS from its
  * root and reports whether every instance leaf is reached exactly once and every stored
  * child box contains its subtree (*valid = 1), the deepest leaf, and the tree's surface

@@ -1,0 +1,74 @@
+"""Learned radiance cache on the GPU (tcgen05 MLP, hash encoding, training step) against
+the CPU oracle (oracle/nrc.py)."""
+import numpy as np
+import pytest
+
+from oracle import nrc as O
+from vork_b200 import RadianceCache
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def installed(renderer, small_scene):
+    with renderer.install(small_scene) as s:
+        yield s
+
+
+def _targets(rec):
+    p, d = rec[:, 0:3].astype(np.float64), rec[:, 3:6].astype(np.float64)
+    t = np.stack([0.6 + 0.4 * np.sin(3 * p[:, 0] + d[:, 1]), 0.5 + 0.3 * np.cos(4 * p[:, 1]) * p[:, 2],
+                  0.2 + 0.8 * p[:, 2] ** 2], 1)
+    return t.astype(np.float32)
+
+
+def test_forward_matches_oracle(installed):
+    mlp, table = O.random_params(seed=10)
+    with RadianceCache(installed) as k:
+        k.set_params(mlp, table)
+        rec = O.random_records(1000, seed=11)            # 7 full tiles and a ragged one
+        x, y = k.forward(rec)
+    xo = O.encode(rec, table)
+    # Same inputs up to one BF16 step (FP32 vs float64 interpolation before rounding).
+    assert np.all(np.abs(x - xo) <= 2.0 ** -7 * np.abs(xo) + 1e-6)
+    yo, _ = O.forward(x.astype(np.float64), mlp)
+    scale = np.abs(yo).max()
+    assert np.all(np.abs(y - yo) <= 2e-3 * np.abs(yo) + 2e-3 * scale), np.abs(y - yo).max()
+
+
+def test_gradients_match_oracle(installed):
+    mlp, table = O.random_params(seed=12)
+    rec = O.random_records(640, seed=13)
+    target = _targets(rec)
+    with RadianceCache(installed) as k:
+        k.set_params(mlp, table)
+        loss, g, hg = k.gradients(rec, target)
+        x, _ = k.forward(rec)
+    lo, go, ho, _ = O.backward(rec, mlp, table, target, x=x.astype(np.float64))
+    assert abs(loss - lo) <= 1e-3 * lo
+    # Against the oracle that rounds where the GPU rounds: FP32 accumulation order only.
+    for l in range(5):
+        a, b = (l * 4096, l * 4096 + (4096 if l < 4 else 3 * 64))
+        assert np.linalg.norm(g[a:b] - go[a:b]) <= 1e-2 * np.linalg.norm(go[a:b]), l
+    assert not np.any(g[4 * 4096 + 3 * 64:])
+    ho = ho.reshape(-1)
+    assert np.linalg.norm(hg - ho) <= 2e-2 * np.linalg.norm(ho)
+    touched = np.flatnonzero(ho)
+    assert np.all(hg[np.setdiff1d(np.arange(hg.size), touched)[:100000]] == 0)
+    # And against plain float64 (no rounding anywhere): within the BF16 budget.
+    l64, g64, h64, _ = O.backward(rec, mlp, table, target, emulate=False)
+    assert np.linalg.norm(g - g64) <= 0.1 * np.linalg.norm(g64)
+    assert np.linalg.norm(hg - h64.reshape(-1)) <= 0.1 * np.linalg.norm(h64)
+
+
+def test_training_steps_reduce_the_loss(installed):
+    rec = O.random_records(8192, seed=14)
+    target = _targets(rec)
+    with RadianceCache(installed, seed=3) as k:
+        first = k.step(rec, target)
+        for _ in range(150):
+            last = k.step(rec, target)
+        _, y = k.forward(rec)
+    assert np.isfinite(last) and last < 0.1 * first, (first, last)
+    rel = np.abs(y - target) / target
+    assert np.median(rel) < 0.1

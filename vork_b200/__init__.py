@@ -15,7 +15,7 @@ from . import abi
 from .abi import VkbError
 from .scene import Scene
 
-__all__ = ["Profile", "Renderer", "InstalledScene", "render", "VkbError", "Scene"]
+__all__ = ["Profile", "Renderer", "InstalledScene", "RadianceCache", "render", "VkbError", "Scene"]
 
 
 @dataclass
@@ -215,6 +215,64 @@ class InstalledScene:
         t = np.zeros(n, np.float32); ids = np.zeros((n, 2), np.uint32); uv = np.zeros((n, 2), np.float32)
         abi.check(self.r.lib.vkb_debug_trace(self.h, n, abi.fptr(r), abi.fptr(t), abi.uptr(ids), abi.fptr(uv)))
         return t, ids, uv
+
+
+class RadianceCache:
+    """A learned radiance cache bound to an installed scene (vkb_cache_*)."""
+
+    def __init__(self, installed: "InstalledScene", **config):
+        self.scene = installed
+        self.r = installed.r
+        cfg = abi.VkbCacheConfig()
+        for k, v in config.items():
+            setattr(cfg, k, v)
+        h = C.c_void_p()
+        abi.check(self.r.lib.vkb_cache_create(installed.h, C.byref(cfg), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.r.lib.vkb_cache_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_params(self, mlp=None, table=None):
+        m = None if mlp is None else np.ascontiguousarray(mlp, np.float32)
+        t = None if table is None else np.ascontiguousarray(table, np.float32).reshape(-1)
+        abi.check(self.r.lib.vkb_debug_nrc_set_params(self.h, abi.fptr(m) if m is not None else None, abi.fptr(t) if t is not None else None))
+
+    def params(self, table=True):
+        m = np.empty(abi.NRC_MLP_PARAMS, np.float32)
+        t = np.empty(abi.NRC_HASH_PARAMS, np.float32) if table else None
+        abi.check(self.r.lib.vkb_debug_nrc_get_params(self.h, abi.fptr(m), abi.fptr(t) if table else None))
+        return m, t
+
+    def forward(self, records):
+        rec = np.ascontiguousarray(records, np.float32)
+        n = rec.shape[0]
+        x = np.empty((n, 64), np.float32); y = np.empty((n, 3), np.float32)
+        abi.check(self.r.lib.vkb_debug_nrc_forward(self.h, n, abi.fptr(rec), abi.fptr(x), abi.fptr(y)))
+        return x, y
+
+    def gradients(self, records, targets, table=True):
+        rec = np.ascontiguousarray(records, np.float32); tg = np.ascontiguousarray(targets, np.float32)
+        g = np.empty(abi.NRC_MLP_PARAMS, np.float32)
+        hg = np.empty(abi.NRC_HASH_PARAMS, np.float32) if table else None
+        loss = C.c_float()
+        abi.check(self.r.lib.vkb_debug_nrc_gradients(self.h, rec.shape[0], abi.fptr(rec), abi.fptr(tg), abi.fptr(g),
+                                                     abi.fptr(hg) if table else None, C.byref(loss)))
+        return float(loss.value), g, hg
+
+    def step(self, records, targets) -> float:
+        rec = np.ascontiguousarray(records, np.float32); tg = np.ascontiguousarray(targets, np.float32)
+        loss = C.c_float()
+        abi.check(self.r.lib.vkb_debug_nrc_step(self.h, rec.shape[0], abi.fptr(rec), abi.fptr(tg), C.byref(loss)))
+        return float(loss.value)
 
 
 def render(scene: Scene, profile: Profile | None = None, device: int = 0) -> RenderResult:

@@ -66,6 +66,16 @@ class VkbProfile(C.Structure):
                 ("adaptive", C.c_uint32), ("wave_samples", C.c_uint32), ("flags", C.c_uint32)]
 
 
+class VkbCacheConfig(C.Structure):
+    _fields_ = [("train_records", C.c_uint32), ("train_steps", C.c_uint32), ("query_vertex", C.c_uint32), ("seed", C.c_uint32),
+                ("lr_mlp", C.c_float), ("lr_hash", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float)]
+
+
+class VkbCacheStats(C.Structure):
+    _fields_ = [("steps", C.c_uint64), ("records", C.c_uint64), ("loss", C.c_float), ("train_ms", C.c_float)]
+
+
+NRC_MLP_PARAMS, NRC_HASH_PARAMS = 17408, 16777216
 PROFILE_TIME_KERNELS, PROFILE_COUNT_TRAVERSAL = 1, 2
 BATCH_FAIR, BATCH_PACKED = 4, 8
 TLAS_LBVH, TLAS_PLOC = 0, 1
@@ -142,6 +152,14 @@ SIGNATURES = {
     "vkb_debug_trace": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_uint32),
                                   C.POINTER(C.c_float)]),
     "vkb_debug_tlas_stats": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "vkb_cache_create": (C.c_int, [_P, C.c_void_p, C.POINTER(_P)]),
+    "vkb_cache_destroy": (C.c_int, [_P]),
+    "vkb_debug_nrc_set_params": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "vkb_debug_nrc_get_params": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "vkb_debug_nrc_forward": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "vkb_debug_nrc_gradients": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                          C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "vkb_debug_nrc_step": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
 }
 
 _lib = None

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "vkb_kernels.cuh"
+#include "vkb_nrc.cuh"
 
 using namespace vkb;
 
@@ -42,6 +43,7 @@ struct CudaError {
 struct ArgError { std::string msg; };
 struct Unsupported { std::string msg; };
 struct InternalError { std::string msg; };
+struct DeviceTimeout { std::string msg; };
 
 template <class T> struct DBuf {
     T* p = nullptr;
@@ -451,6 +453,8 @@ template <class F> vkb_status guarded(F&& f) {
         return fail(VKB_UNSUPPORTED, e.msg);
     } catch (const InternalError& e) {
         return fail(VKB_INTERNAL, e.msg);
+    } catch (const DeviceTimeout& e) {
+        return fail(VKB_DEVICE_TIMEOUT, e.msg);
     } catch (const std::bad_alloc&) {
         return fail(VKB_OUT_OF_MEMORY, "host allocation failed");
     }
@@ -702,12 +706,14 @@ struct WaveEngine {
         size_t left = capacity;
         bool any = false;
         if (packed) {
+            // First fit in admission order: a job that does not fit what is left is
+            // skipped for this wave and later (smaller) jobs fill the slots.
             for (uint32_t k = 0; k < njobs && left > 0; ++k) {
                 EngineJob& e = jobs[k];
                 if (finished(k)) continue;
                 uint32_t n = uint32_t(std::min<size_t>(e.count - e.done, left / e.npix));
                 if (n == 0 && !any) n = 1;      // an image larger than the wave: one sample alone
-                if (n == 0) break;              // keep admission order: later jobs wait
+                if (n == 0) continue;
                 take[k] = n; any = true;
                 left = size_t(n) * e.npix <= left ? left - size_t(n) * e.npix : 0;
             }
@@ -1640,3 +1646,6 @@ extern "C" vkb_status vkb_render_noalloc(vkb_scene* s, const vkb_profile* pf, vk
         fill_stats(stats, tot, uint64_t(npix) * count, 0.f);
     });
 }
+
+// ================================================================ learned radiance cache
+#include "vkb_cache.cuh"

@@ -1,0 +1,261 @@
+// Host side of the learned radiance cache: parameters, Adam state, training buffers and
+// the C ABI (included at the end of vkb.cu, inside its translation unit).
+#pragma once
+
+struct vkb_cache {
+    vkb_scene* s = nullptr;
+    vkb_cache_config cfg{};
+    uint64_t steps = 0;
+    float last_loss = 0.f, last_train_ms = 0.f;
+    uint64_t last_records = 0;
+    DBuf<float> mlp_master, mlp_m1, mlp_m2;
+    DBuf<__nv_bfloat16> mlp_w;
+    DBuf<float> hash_master, hash_m1, hash_m2;
+    DBuf<__half> table;
+    DBuf<long long> hash_grad;
+    DBuf<float> wpartial, loss_partial, targets, scratch;
+    DBuf<float4> records;
+    DBuf<uint32_t> err;
+};
+
+namespace {
+
+using namespace vkb::nrc;
+
+__global__ void k_nrc_init_hash(uint64_t count, uint32_t seed, float* master, __half* table) {
+    for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < count; p += uint64_t(gridDim.x) * blockDim.x) {
+        uint32_t h = uint32_t(p) * 0x9e3779b9u ^ uint32_t(p >> 32) * 0x85ebca6bu ^ seed * 0xc2b2ae35u;
+        h ^= h >> 16; h *= 0x7feb352du; h ^= h >> 15; h *= 0x846ca68bu; h ^= h >> 16;
+        const float x = (float(h >> 8) * (1.f / 16777216.f) * 2.f - 1.f) * 1e-4f;
+        master[p] = x;
+        table[p] = __float2half_rn(x);
+    }
+}
+__global__ void k_nrc_from_master(uint64_t count, const float* master, __half* table) {
+    for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < count; p += uint64_t(gridDim.x) * blockDim.x)
+        table[p] = __float2half_rn(master[p]);
+}
+__global__ void k_nrc_mlp_from_master(uint32_t count, const float* master, __nv_bfloat16* w) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x) w[p] = __float2bfloat16_rn(master[p]);
+}
+
+void cache_defaults(vkb_cache_config& c) {
+    if (!c.train_records) c.train_records = 65536;
+    if (!c.train_steps) c.train_steps = 4;
+    if (!c.query_vertex) c.query_vertex = 2;
+    if (c.lr_mlp == 0.f) c.lr_mlp = 2e-3f;
+    if (c.lr_hash == 0.f) c.lr_hash = 1e-2f;
+    if (c.beta1 == 0.f) c.beta1 = 0.9f;
+    if (c.beta2 == 0.f) c.beta2 = 0.99f;
+    if (c.eps == 0.f) c.eps = 1e-10f;
+}
+
+// Xavier-uniform MLP weights from a PCG32 stream (rows 3..15 of the output layer zero).
+std::vector<float> mlp_init(uint32_t seed) {
+    std::vector<float> w(MLP_PARAMS, 0.f);
+    uint64_t state = 0x853c49e6748fea9bull + seed, inc = 0xda3e39cb94b95bdbull | 1u;
+    auto next = [&]() {
+        uint64_t old = state;
+        state = old * 6364136223846793005ull + inc;
+        uint32_t xs = uint32_t(((old >> 18u) ^ old) >> 27u), rot = uint32_t(old >> 59u);
+        return (xs >> rot) | (xs << ((32u - rot) & 31u));
+    };
+    for (int l = 0; l < LAYERS; ++l) {
+        const int rows = l == LAYERS - 1 ? 3 : WIDTH;
+        const float a = std::sqrt(6.f / float(WIDTH + rows));
+        for (int o = 0; o < rows; ++o)
+            for (int i = 0; i < WIDTH; ++i) w[size_t(l) * WIDTH * WIDTH + size_t(o) * WIDTH + i] = (float(next() >> 8) * (1.f / 16777216.f) * 2.f - 1.f) * a;
+    }
+    return w;
+}
+
+void nrc_kernel_attributes() {
+    static std::once_flag once;
+    std::call_once(once, [] {
+        VKB_CUDA(cudaFuncSetAttribute(k_nrc_forward<DebugIO>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(FWD_SMEM)));
+        VKB_CUDA(cudaFuncSetAttribute(k_nrc_forward<QueryIO>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(FWD_SMEM)));
+        VKB_CUDA(cudaFuncSetAttribute(k_nrc_train, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TRN_SMEM)));
+    });
+}
+
+void check_nrc_err(vkb_cache* k) {
+    uint32_t e = 0;
+    VKB_CUDA(cudaMemcpyAsync(&e, k->err.p, sizeof(e), cudaMemcpyDeviceToHost, k->s->ctx->stream));
+    VKB_CUDA(cudaStreamSynchronize(k->s->ctx->stream));
+    if (e) {
+        VKB_CUDA(cudaMemsetAsync(k->err.p, 0, sizeof(uint32_t), k->s->ctx->stream));
+        throw DeviceTimeout{"a tensor-core wait of the radiance cache ran out"};
+    }
+}
+
+// Gradients of the loss over `n` device records (already in k->records / k->targets);
+// with lr > 0 also one Adam step.  Returns the mean loss.
+float nrc_step(vkb_cache* k, uint32_t n, bool update, float* mlp_grad_dev, float* hash_grad_dev) {
+    vkb_ctx* c = k->s->ctx;
+    cudaStream_t st = c->stream;
+    nrc_kernel_attributes();
+    const uint32_t tiles = (n + TILE - 1) / TILE;
+    k->wpartial.alloc(size_t(tiles) * MLP_PARAMS);
+    k->loss_partial.alloc(tiles);
+    k_nrc_train<<<tiles, TILE, TRN_SMEM, st>>>(k->records.p, k->targets.p, n, 1.f / float(3u * n), k->mlp_w.p, k->table.p, k->wpartial.p,
+                                               k->hash_grad.p, k->loss_partial.p, k->err.p);
+    AdamParams am{0.f, k->cfg.beta1, k->cfg.beta2, k->cfg.eps, 1.f, 1.f}, ah = am;
+    if (update) {
+        k->steps++;
+        const float bc1 = 1.f - std::pow(k->cfg.beta1, float(k->steps)), bc2 = 1.f - std::pow(k->cfg.beta2, float(k->steps));
+        am = AdamParams{k->cfg.lr_mlp, k->cfg.beta1, k->cfg.beta2, k->cfg.eps, bc1, bc2};
+        ah = AdamParams{k->cfg.lr_hash, k->cfg.beta1, k->cfg.beta2, k->cfg.eps, bc1, bc2};
+    }
+    k_nrc_adam_mlp<<<grid_for(MLP_PARAMS, 256, c->sms), 256, 0, st>>>(tiles, k->wpartial.p, k->mlp_master.p, k->mlp_m1.p, k->mlp_m2.p, k->mlp_w.p,
+                                                                       am, mlp_grad_dev);
+    k_nrc_adam_hash<<<c->sms * 8, 256, 0, st>>>(HASH_PARAMS, k->hash_grad.p, k->hash_master.p, k->hash_m1.p, k->hash_m2.p, k->table.p, ah,
+                                                hash_grad_dev);
+    k->s->launches += 3;
+    VKB_CUDA(cudaGetLastError());
+    std::vector<float> lp(tiles);
+    VKB_CUDA(cudaMemcpyAsync(lp.data(), k->loss_partial.p, tiles * sizeof(float), cudaMemcpyDeviceToHost, st));
+    check_nrc_err(k);
+    double sum = 0.0;
+    for (float x : lp) sum += x;
+    k->last_loss = float(sum / (3.0 * n));
+    return k->last_loss;
+}
+
+void upload_records(vkb_cache* k, uint32_t n, const float* records, const float* targets) {
+    cudaStream_t st = k->s->ctx->stream;
+    k->records.alloc(size_t(n) * 4);
+    VKB_CUDA(cudaMemcpyAsync(k->records.p, records, size_t(n) * RECORD_FLOATS * sizeof(float), cudaMemcpyHostToDevice, st));
+    if (targets) {
+        k->targets.alloc(size_t(n) * 3);
+        VKB_CUDA(cudaMemcpyAsync(k->targets.p, targets, size_t(n) * 3 * sizeof(float), cudaMemcpyHostToDevice, st));
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+vkb_status vkb_cache_create(vkb_scene* s, const vkb_cache_config* config, vkb_cache** out) {
+    if (!s || !out) return fail(VKB_INVALID_ARG, "null scene or output pointer");
+    *out = nullptr;
+    auto* k = new vkb_cache();
+    k->s = s;
+    if (config) k->cfg = *config;
+    cache_defaults(k->cfg);
+    vkb_status st = guarded([&] {
+        if (k->cfg.query_vertex < 1 || k->cfg.query_vertex > 16) throw ArgError{"query_vertex must be 1..16"};
+        VKB_CUDA(cudaSetDevice(s->ctx->device));
+        cudaStream_t str = s->ctx->stream;
+        k->mlp_master.alloc(MLP_PARAMS); k->mlp_m1.alloc(MLP_PARAMS); k->mlp_m2.alloc(MLP_PARAMS); k->mlp_w.alloc(MLP_PARAMS);
+        k->hash_master.alloc(HASH_PARAMS); k->hash_m1.alloc(HASH_PARAMS); k->hash_m2.alloc(HASH_PARAMS);
+        k->table.alloc(HASH_PARAMS); k->hash_grad.alloc(HASH_PARAMS); k->err.alloc(1);
+        VKB_CUDA(cudaMemsetAsync(k->mlp_m1.p, 0, MLP_PARAMS * sizeof(float), str));
+        VKB_CUDA(cudaMemsetAsync(k->mlp_m2.p, 0, MLP_PARAMS * sizeof(float), str));
+        VKB_CUDA(cudaMemsetAsync(k->hash_m1.p, 0, HASH_PARAMS * sizeof(float), str));
+        VKB_CUDA(cudaMemsetAsync(k->hash_m2.p, 0, HASH_PARAMS * sizeof(float), str));
+        VKB_CUDA(cudaMemsetAsync(k->hash_grad.p, 0, HASH_PARAMS * sizeof(long long), str));
+        VKB_CUDA(cudaMemsetAsync(k->err.p, 0, sizeof(uint32_t), str));
+        std::vector<float> w = mlp_init(k->cfg.seed);
+        VKB_CUDA(cudaMemcpyAsync(k->mlp_master.p, w.data(), MLP_PARAMS * sizeof(float), cudaMemcpyHostToDevice, str));
+        k_nrc_mlp_from_master<<<grid_for(MLP_PARAMS, 256, s->ctx->sms), 256, 0, str>>>(MLP_PARAMS, k->mlp_master.p, k->mlp_w.p);
+        k_nrc_init_hash<<<s->ctx->sms * 8, 256, 0, str>>>(HASH_PARAMS, k->cfg.seed, k->hash_master.p, k->table.p);
+        VKB_CUDA(cudaGetLastError());
+        VKB_CUDA(cudaStreamSynchronize(str));
+    });
+    if (st != VKB_OK) { delete k; return st; }
+    *out = k;
+    return VKB_OK;
+}
+
+vkb_status vkb_cache_destroy(vkb_cache* k) {
+    if (!k) return VKB_OK;
+    cudaSetDevice(k->s->ctx->device);
+    cudaStreamSynchronize(k->s->ctx->stream);
+    k->mlp_master.release(); k->mlp_m1.release(); k->mlp_m2.release(); k->mlp_w.release();
+    k->hash_master.release(); k->hash_m1.release(); k->hash_m2.release(); k->table.release(); k->hash_grad.release();
+    k->wpartial.release(); k->loss_partial.release(); k->targets.release(); k->scratch.release(); k->records.release(); k->err.release();
+    delete k;
+    return VKB_OK;
+}
+
+vkb_status vkb_debug_nrc_set_params(vkb_cache* k, const float* mlp, const float* hash) {
+    if (!k) return fail(VKB_INVALID_ARG, "null cache");
+    return guarded([&] {
+        VKB_CUDA(cudaSetDevice(k->s->ctx->device));
+        cudaStream_t st = k->s->ctx->stream;
+        if (mlp) {
+            VKB_CUDA(cudaMemcpyAsync(k->mlp_master.p, mlp, MLP_PARAMS * sizeof(float), cudaMemcpyHostToDevice, st));
+            k_nrc_mlp_from_master<<<grid_for(MLP_PARAMS, 256, k->s->ctx->sms), 256, 0, st>>>(MLP_PARAMS, k->mlp_master.p, k->mlp_w.p);
+        }
+        if (hash) {
+            VKB_CUDA(cudaMemcpyAsync(k->hash_master.p, hash, HASH_PARAMS * sizeof(float), cudaMemcpyHostToDevice, st));
+            k_nrc_from_master<<<k->s->ctx->sms * 8, 256, 0, st>>>(HASH_PARAMS, k->hash_master.p, k->table.p);
+        }
+        VKB_CUDA(cudaGetLastError());
+        VKB_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+vkb_status vkb_debug_nrc_get_params(vkb_cache* k, float* mlp, float* hash) {
+    if (!k) return fail(VKB_INVALID_ARG, "null cache");
+    return guarded([&] {
+        VKB_CUDA(cudaSetDevice(k->s->ctx->device));
+        cudaStream_t st = k->s->ctx->stream;
+        if (mlp) VKB_CUDA(cudaMemcpyAsync(mlp, k->mlp_master.p, MLP_PARAMS * sizeof(float), cudaMemcpyDeviceToHost, st));
+        if (hash) VKB_CUDA(cudaMemcpyAsync(hash, k->hash_master.p, HASH_PARAMS * sizeof(float), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+vkb_status vkb_debug_nrc_forward(vkb_cache* k, uint32_t n, const float* records, float* x_out, float* y_out) {
+    if (!k || (n && (!records || !y_out))) return fail(VKB_INVALID_ARG, "null argument");
+    return guarded([&] {
+        if (n == 0) return;
+        VKB_CUDA(cudaSetDevice(k->s->ctx->device));
+        cudaStream_t st = k->s->ctx->stream;
+        nrc_kernel_attributes();
+        upload_records(k, n, records, nullptr);
+        DBuf<float> x, y;
+        x.alloc(size_t(n) * 64); y.alloc(size_t(n) * 3);
+        DebugIO io{k->records.p, n, x.p, y.p};
+        const uint32_t tiles = (n + TILE - 1) / TILE;
+        k_nrc_forward<DebugIO><<<std::min<uint32_t>(tiles, uint32_t(k->s->ctx->sms) * 4u), TILE, FWD_SMEM, st>>>(io, k->mlp_w.p, k->table.p, k->err.p);
+        VKB_CUDA(cudaGetLastError());
+        check_nrc_err(k);
+        if (x_out) VKB_CUDA(cudaMemcpyAsync(x_out, x.p, size_t(n) * 64 * sizeof(float), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaMemcpyAsync(y_out, y.p, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaStreamSynchronize(st));
+        x.release(); y.release();
+    });
+}
+
+vkb_status vkb_debug_nrc_gradients(vkb_cache* k, uint32_t n, const float* records, const float* targets, float* mlp_grad, float* hash_grad,
+                                   float* loss) {
+    if (!k || !records || !targets || !mlp_grad || n == 0) return fail(VKB_INVALID_ARG, "null argument or no records");
+    return guarded([&] {
+        VKB_CUDA(cudaSetDevice(k->s->ctx->device));
+        cudaStream_t st = k->s->ctx->stream;
+        upload_records(k, n, records, targets);
+        DBuf<float> g, h;
+        g.alloc(MLP_PARAMS);
+        if (hash_grad) h.alloc(HASH_PARAMS);
+        float l = nrc_step(k, n, false, g.p, hash_grad ? h.p : nullptr);
+        VKB_CUDA(cudaMemcpyAsync(mlp_grad, g.p, MLP_PARAMS * sizeof(float), cudaMemcpyDeviceToHost, st));
+        if (hash_grad) VKB_CUDA(cudaMemcpyAsync(hash_grad, h.p, HASH_PARAMS * sizeof(float), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaStreamSynchronize(st));
+        if (loss) *loss = l;
+        g.release(); h.release();
+    });
+}
+
+vkb_status vkb_debug_nrc_step(vkb_cache* k, uint32_t n, const float* records, const float* targets, float* loss) {
+    if (!k || !records || !targets || n == 0) return fail(VKB_INVALID_ARG, "null argument or no records");
+    return guarded([&] {
+        VKB_CUDA(cudaSetDevice(k->s->ctx->device));
+        upload_records(k, n, records, targets);
+        float l = nrc_step(k, n, true, nullptr, nullptr);
+        if (loss) *loss = l;
+    });
+}
+
+}  // extern "C"
