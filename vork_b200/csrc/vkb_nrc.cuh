@@ -6,7 +6,7 @@
 // one thread of the CTA, operands staged in shared memory in the no-swizzle canonical
 // layout, accumulators read back with tcgen05.ld.
 //
-// Network (the oracle's nrc module restates it):
+// Network:
 //   input  x[64]: [0,32) hash grid, 16 levels x 2 features (trilinear); [32,48) real
 //          spherical harmonics of the outgoing direction, bands 0..3; [48,51) shading
 //          normal * 0.5 + 0.5; [51] roughness; [52,55) base colour; [55] metalness;
