@@ -346,6 +346,15 @@ typedef struct vkb_cache_stats {
 } vkb_cache_stats;
 vkb_status vkb_cache_create(vkb_scene* scene, const vkb_cache_config* config, vkb_cache** out);
 vkb_status vkb_cache_destroy(vkb_cache* cache);
+/* One online training round: trace about train_records / 2 training paths through the
+ * scene's camera at reduced resolution (one sample, a fresh seed each call, the
+ * profile's bounce limits), take every vertex from 1 on as a training record whose
+ * target is the path's radiance from there on, and run train_steps optimizer steps. */
+vkb_status vkb_cache_train(vkb_cache* cache, const vkb_profile* profile, vkb_cache_stats* stats);
+/* vkb_render through the cache: paths stop at query_vertex and add throughput x the
+ * cached outgoing radiance there (the plain render is the fallback and the judge of its
+ * error).  Same output and stats as vkb_render. */
+vkb_status vkb_render_cached(vkb_cache* cache, const vkb_profile* profile, vkb_output* out, vkb_stats* stats);
 /* Test hooks of the network itself.  Parameters as FP32: MLP row-major [out][in] per
  * layer (4 x 64x64 then 16x64, rows 3..15 of the last zero), hash table [level][entry][feature]. */
 #define VKB_NRC_MLP_PARAMS 17408u

@@ -241,6 +241,25 @@ class RadianceCache:
     def __exit__(self, *exc):
         self.close()
 
+    def train(self, profile: Profile) -> dict:
+        """One online training round (vkb_cache_train) with the profile's bounce limits and seed."""
+        st = abi.VkbCacheStats()
+        p = profile.c()
+        abi.check(self.r.lib.vkb_cache_train(self.h, C.byref(p), C.byref(st)))
+        return {k: getattr(st, k) for k, _ in abi.VkbCacheStats._fields_}
+
+    def render(self, profile: Profile) -> "RenderResult":
+        """Render the scene through the cache (vkb_render_cached) into a host image."""
+        cam = self.scene.scene.camera
+        img = np.empty((cam.height, cam.width, 4), np.float32)
+        o = abi.VkbOutput()
+        o.rgba = img.ctypes.data_as(C.c_void_p)
+        o.on_device = 0
+        st = abi.VkbStats()
+        p = profile.c()
+        abi.check(self.r.lib.vkb_render_cached(self.h, C.byref(p), C.byref(o), C.byref(st)))
+        return RenderResult(img, {k: getattr(st, k) for k, _ in abi.VkbStats._fields_})
+
     def set_params(self, mlp=None, table=None):
         m = None if mlp is None else np.ascontiguousarray(mlp, np.float32)
         t = None if table is None else np.ascontiguousarray(table, np.float32).reshape(-1)

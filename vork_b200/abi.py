@@ -154,6 +154,8 @@ SIGNATURES = {
     "vkb_debug_tlas_stats": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "vkb_cache_create": (C.c_int, [_P, C.c_void_p, C.POINTER(_P)]),
     "vkb_cache_destroy": (C.c_int, [_P]),
+    "vkb_cache_train": (C.c_int, [_P, C.POINTER(VkbProfile), C.c_void_p]),
+    "vkb_render_cached": (C.c_int, [_P, C.POINTER(VkbProfile), C.POINTER(VkbOutput), C.POINTER(VkbStats)]),
     "vkb_debug_nrc_set_params": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "vkb_debug_nrc_get_params": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "vkb_debug_nrc_forward": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),

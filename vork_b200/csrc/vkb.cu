@@ -568,6 +568,8 @@ void validate_desc(const vkb_scene_desc* d) {
 struct EngineJob {
     vkb_scene* s = nullptr;
     vkb_profile pf{};
+    bool own_camera = false;        // render through `camera` instead of the scene's
+    vkb_camera camera{};
     float4* out_dev = nullptr;      // device destination of the mean image
     uint32_t* ids_dev = nullptr;    // device primary ids (first sample) or null
     float4* accum = nullptr;        // device accumulator, npix
@@ -601,7 +603,7 @@ Job make_job(const EngineJob& e) {
     j.vpos = s->vpos.p; j.vnrm = s->vnrm.p; j.indices = s->indices.p;
     j.materials = s->d_materials.p; j.lights = s->d_lights.p; j.num_lights = uint32_t(s->lights.size());
     j.tree = s->tree.p; j.tree_nodes = s->tree_nodes;
-    j.cam = s->camera; j.env = s->env;
+    j.cam = e.own_camera ? e.camera : s->camera; j.env = s->env;
     j.spp = pf.samples; j.seed = pf.seed;
     for (int k = 0; k < 4; ++k) j.bounces[k] = pf.bounces[k];
     j.caustics = pf.caustics;
@@ -624,10 +626,22 @@ PathParams path_params(const vkb_ctx* c, const WaveBuffers& w, uint32_t njobs) {
     return p;
 }
 
+// A render's radiance-cache hooks: the device side (copied into PathParams) and what
+// the query (mode 1) or target (mode 2) kernel after the bounce loop needs.
+struct CacheLaunch {
+    CacheParams dev{};
+    const __nv_bfloat16* w = nullptr;
+    const __half* table = nullptr;
+    uint32_t* err = nullptr;
+    float* targets = nullptr;
+};
+
 // The kernels of one wave: camera, then per bounce closest-hit trace, shade, shadow trace;
-// then accumulation.  Timed mode records events around every closest-hit trace.
+// then the radiance-cache queries or training targets, if any; then accumulation.  Timed
+// mode records events around every closest-hit trace.
 template <bool BATCH>
-void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counted, bool timed, WaveTotals& tot) {
+void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counted, bool timed, WaveTotals& tot,
+                  const CacheLaunch* cache = nullptr) {
     cudaStream_t st = c->stream;
     const int sms = c->sms, tgrid = sms * c->trace_blocks_per_sm, sgrid = sms * c->trace_blocks_per_sm;
     k_start_wave<<<1, 1, 0, st>>>(p.counters);
@@ -650,6 +664,14 @@ void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counte
         k_shade<BATCH><<<sgrid, 128, 0, st>>>(p, cur);
         if (counted) k_trace<true, true, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p, -1);
         else k_trace<true, false, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p, -1);
+    }
+    if (cache && cache->dev.mode == 1u) {
+        nrc::QueryIO io{cache->dev.rec, p.counters + 9, cache->dev.capacity, cache->dev.slot, p.thr, p.rad};
+        nrc::k_nrc_forward<nrc::QueryIO><<<sms * 4, nrc::TILE, nrc::FWD_SMEM, st>>>(io, cache->w, cache->table, cache->err);
+        tot.launches += 1;
+    } else if (cache && cache->dev.mode == 2u) {
+        nrc::k_nrc_targets<<<sms * 8, 256, 0, st>>>(p.counters + 9, cache->dev.capacity, cache->dev.slot, cache->dev.aux, p.rad, cache->targets);
+        tot.launches += 1;
     }
     k_accumulate<BATCH><<<sms * 8, 256, 0, st>>>(p);
     tot.launches += 3 + 4 * (bounces + 1);
@@ -675,6 +697,7 @@ struct WaveEngine {
     // latency) or packed (each job's remaining samples before the next job: fewer scenes
     // per wave, so their BVHs stay in L2 -- batch throughput).
     bool packed = false;
+    const CacheLaunch* cache = nullptr;   // radiance-cache hooks (single-job renders)
     ~WaveEngine() { for (auto& g : captured) cudaGraphExecDestroy(g.exec); }
     WaveEngine(vkb_ctx* ctx, const WaveBuffers& wb, size_t cap, uint32_t fl, bool use_graphs) : c(ctx), w(wb), capacity(cap), flags(fl), graphs(use_graphs) {
         cudaStream_t st = c->stream;
@@ -757,6 +780,10 @@ struct WaveEngine {
         VKB_CUDA(cudaMemcpyAsync(w.counters + 7, wave_counts, sizeof(wave_counts), cudaMemcpyHostToDevice, st));
         PathParams p = path_params(c, w, wave_jobs);
         p.job0 = wave_table[0];
+        if (cache) {
+            if (batch) throw ArgError{"radiance-cache renders take one job"};
+            p.cache = cache->dev;
+        }
         if (use_graph) {
             uint64_t key = (uint64_t(bounces) << 1) | 1u;
             key = key * 1315423911ull + (counted ? 7u : 3u);
@@ -780,7 +807,7 @@ struct WaveEngine {
         } else if (batch) {
             wave_kernels<true>(c, p, bounces, counted, timed, tot);
         } else {
-            wave_kernels<false>(c, p, bounces, counted, timed, tot);
+            wave_kernels<false>(c, p, bounces, counted, timed, tot, cache);
         }
         VKB_CUDA(cudaGetLastError());
         return true;
@@ -812,9 +839,10 @@ struct WaveEngine {
 
 // Run `jobs` to completion on the wavefront `w` and resolve each into its out_dev.
 void run_engine(vkb_ctx* c, std::vector<EngineJob>& jobs, const WaveBuffers& w, size_t capacity, uint32_t flags, bool graphs, WaveTotals& tot,
-                bool packed = false) {
+                bool packed = false, const CacheLaunch* cache = nullptr) {
     WaveEngine eng(c, w, capacity, flags, graphs);
     eng.packed = packed;
+    eng.cache = cache;
     for (auto& e : jobs) eng.add(e);
     VKB_CUDA(cudaEventRecord(c->ev0, c->stream));
     while (eng.step()) {}
@@ -852,7 +880,7 @@ void fill_stats(vkb_stats* stats, const WaveTotals& t, uint64_t paths, float bui
 
 // Render jobs with the context's own buffers (grown on demand).
 void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile>>& in, std::vector<vkb_output*>& outs, uint32_t flags,
-                 uint32_t wave_samples_hint, WaveTotals& tot, uint64_t& paths) {
+                 uint32_t wave_samples_hint, WaveTotals& tot, uint64_t& paths, const CacheLaunch* cache = nullptr) {
     cudaStream_t st = c->stream;
     size_t total_pixels = 0, max_pix = 0, ids_words = 0, staged = 0;
     for (size_t k = 0; k < in.size(); ++k) {
@@ -882,7 +910,7 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
         if (outs[k]->primary_ids) { e.ids_dev = c->ids.p + idw; idw += 2 * size_t(e.npix); }
         paths += uint64_t(e.npix) * e.count;
     }
-    run_engine(c, jobs, c->wave.view(), capacity, flags, true, tot, (flags & VKB_BATCH_FAIR) == 0);
+    run_engine(c, jobs, c->wave.view(), capacity, flags, true, tot, (flags & VKB_BATCH_FAIR) == 0, cache);
     for (size_t k = 0; k < in.size(); ++k) {
         if (!outs[k]->on_device) VKB_CUDA(cudaMemcpyAsync(outs[k]->rgba, jobs[k].out_dev, size_t(jobs[k].npix) * sizeof(float4), cudaMemcpyDeviceToHost, st));
         if (outs[k]->primary_ids) VKB_CUDA(cudaMemcpyAsync(outs[k]->primary_ids, jobs[k].ids_dev, size_t(jobs[k].npix) * 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));

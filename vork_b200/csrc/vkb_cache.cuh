@@ -16,6 +16,15 @@ struct vkb_cache {
     DBuf<float> wpartial, loss_partial, targets, scratch;
     DBuf<float4> records;
     DBuf<uint32_t> err;
+    // Training paths: per-record path slot and (throughput, radiance) at the vertex; the
+    // low-resolution training render's accumulator and image.
+    DBuf<uint32_t> rec_slot;
+    DBuf<float4> aux, train_accum, train_out;
+    // Render queries: one record and path slot per path slot of a wave.
+    DBuf<float4> qrec;
+    DBuf<uint32_t> qslot;
+    float4 box_lo{}, box_scale{};   // world -> [0,1]^3, fixed at creation (5% margin)
+    uint64_t train_calls = 0;
 };
 
 namespace {
@@ -155,6 +164,25 @@ vkb_status vkb_cache_create(vkb_scene* s, const vkb_cache_config* config, vkb_ca
         VKB_CUDA(cudaMemsetAsync(k->hash_m2.p, 0, HASH_PARAMS * sizeof(float), str));
         VKB_CUDA(cudaMemsetAsync(k->hash_grad.p, 0, HASH_PARAMS * sizeof(long long), str));
         VKB_CUDA(cudaMemsetAsync(k->err.p, 0, sizeof(uint32_t), str));
+        // Normalisation box: the TLAS root box at creation, 5% margin on every side.
+        BvhNode root{};
+        VKB_CUDA(cudaMemcpyAsync(&root, s->tlas_nodes.p, sizeof(BvhNode), cudaMemcpyDeviceToHost, str));
+        VKB_CUDA(cudaStreamSynchronize(str));
+        float lo[3] = {root.a.x, root.a.z, root.c.x}, hi[3] = {root.a.y, root.a.w, root.c.y};
+        if (s->num_instances > 1) {
+            lo[0] = std::min(lo[0], root.b.x); hi[0] = std::max(hi[0], root.b.y);
+            lo[1] = std::min(lo[1], root.b.z); hi[1] = std::max(hi[1], root.b.w);
+            lo[2] = std::min(lo[2], root.c.z); hi[2] = std::max(hi[2], root.c.w);
+        }
+        float ext = 0.f;
+        for (int a = 0; a < 3; ++a) ext = std::max(ext, hi[a] - lo[a]);
+        if (!(ext > 0.f) || !std::isfinite(ext)) throw ArgError{"the scene has no finite extent for the radiance cache"};
+        for (int a = 0; a < 3; ++a) {
+            const float m = 0.05f * std::max(hi[a] - lo[a], 1e-3f * ext);
+            lo[a] -= m; hi[a] += m;
+        }
+        k->box_lo = make_float4(lo[0], lo[1], lo[2], 0.f);
+        k->box_scale = make_float4(1.f / (hi[0] - lo[0]), 1.f / (hi[1] - lo[1]), 1.f / (hi[2] - lo[2]), 0.f);
         std::vector<float> w = mlp_init(k->cfg.seed);
         VKB_CUDA(cudaMemcpyAsync(k->mlp_master.p, w.data(), MLP_PARAMS * sizeof(float), cudaMemcpyHostToDevice, str));
         k_nrc_mlp_from_master<<<grid_for(MLP_PARAMS, 256, s->ctx->sms), 256, 0, str>>>(MLP_PARAMS, k->mlp_master.p, k->mlp_w.p);
@@ -174,8 +202,92 @@ vkb_status vkb_cache_destroy(vkb_cache* k) {
     k->mlp_master.release(); k->mlp_m1.release(); k->mlp_m2.release(); k->mlp_w.release();
     k->hash_master.release(); k->hash_m1.release(); k->hash_m2.release(); k->table.release(); k->hash_grad.release();
     k->wpartial.release(); k->loss_partial.release(); k->targets.release(); k->scratch.release(); k->records.release(); k->err.release();
+    k->rec_slot.release(); k->aux.release(); k->train_accum.release(); k->train_out.release(); k->qrec.release(); k->qslot.release();
     delete k;
     return VKB_OK;
+}
+
+vkb_status vkb_cache_train(vkb_cache* k, const vkb_profile* pf, vkb_cache_stats* stats) {
+    if (!k || !pf) return fail(VKB_INVALID_ARG, "null cache or profile");
+    return guarded([&] {
+        validate_profile(pf);
+        vkb_scene* s = k->s;
+        vkb_ctx* c = s->ctx;
+        VKB_CUDA(cudaSetDevice(c->device));
+        cudaStream_t st = c->stream;
+        nrc_kernel_attributes();
+        VKB_CUDA(cudaEventRecord(c->ev0, st));
+        // Training paths: the scene's camera at a resolution of about train_records / 2
+        // pixels, one sample of a fresh seed per call, full path depth.
+        const vkb_camera& cam = s->camera;
+        const double px = std::max(256.0, double(k->cfg.train_records) / 2.0);
+        const double aspect = double(cam.width) / double(cam.height);
+        const uint32_t tw = std::max(8u, uint32_t(std::lround(std::sqrt(px * aspect)))), th = std::max(8u, uint32_t(std::lround(px / tw)));
+        std::vector<EngineJob> jobs(1);
+        EngineJob& e = jobs[0];
+        e.s = s; e.pf = *pf;
+        e.pf.samples = 1; e.pf.first_sample = 0; e.pf.sample_count = 1; e.pf.wave_samples = 1;
+        e.pf.seed = pf->seed ^ (0x9e3779b9u * uint32_t(k->train_calls + 1) + k->cfg.seed);
+        e.own_camera = true; e.camera = cam; e.camera.width = tw; e.camera.height = th;
+        e.npix = tw * th; e.count = 1;
+        k->train_accum.alloc(e.npix); k->train_out.alloc(e.npix);
+        e.accum = k->train_accum.p; e.out_dev = k->train_out.p;
+        const uint32_t cap = 2u * k->cfg.train_records;
+        k->records.alloc(size_t(cap) * 4); k->rec_slot.alloc(cap); k->aux.alloc(size_t(cap) * 2); k->targets.alloc(size_t(cap) * 3);
+        c->wave.reserve(e.npix, 1);
+        CacheLaunch cl;
+        cl.dev.mode = 2; cl.dev.vertex = 0; cl.dev.capacity = cap;
+        cl.dev.box_lo = k->box_lo; cl.dev.box_scale = k->box_scale;
+        cl.dev.rec = k->records.p; cl.dev.slot = k->rec_slot.p; cl.dev.aux = k->aux.p;
+        cl.w = k->mlp_w.p; cl.table = k->table.p; cl.err = k->err.p; cl.targets = k->targets.p;
+        WaveTotals tot;
+        run_engine(c, jobs, c->wave.view(), e.npix, 0, false, tot, false, &cl);
+        uint32_t count = 0;
+        VKB_CUDA(cudaMemcpyAsync(&count, c->wave.view().counters + 9, sizeof(count), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaStreamSynchronize(st));
+        count = std::min(count, cap);
+        s->launches += tot.launches;
+        k->train_calls++;
+        if (count > 0)
+            for (uint32_t i = 0; i < k->cfg.train_steps; ++i) nrc_step(k, count, true, nullptr, nullptr);
+        VKB_CUDA(cudaEventRecord(c->ev1, st));
+        VKB_CUDA(cudaEventSynchronize(c->ev1));
+        VKB_CUDA(cudaEventElapsedTime(&k->last_train_ms, c->ev0, c->ev1));
+        k->last_records = count;
+        if (stats) {
+            stats->steps = k->steps; stats->records = count; stats->loss = k->last_loss; stats->train_ms = k->last_train_ms;
+        }
+    });
+}
+
+vkb_status vkb_render_cached(vkb_cache* k, const vkb_profile* pf, vkb_output* out, vkb_stats* stats) {
+    if (!k || !pf || !out || !out->rgba) return fail(VKB_INVALID_ARG, "null cache, profile or output");
+    return guarded([&] {
+        validate_profile(pf);
+        vkb_scene* s = k->s;
+        vkb_ctx* c = s->ctx;
+        VKB_CUDA(cudaSetDevice(c->device));
+        nrc_kernel_attributes();
+        const uint32_t count = pf->sample_count ? pf->sample_count : pf->samples - pf->first_sample;
+        const size_t npix = size_t(s->camera.width) * s->camera.height;
+        uint32_t hint = pf->wave_samples;
+        if (!hint) hint = uint32_t(std::max<size_t>(1, std::min<size_t>(count, c->wave_capacity / std::max<size_t>(1, npix))));
+        const size_t capacity = std::max(npix * hint, npix);   // the wave size render_jobs picks for one job
+        k->qrec.alloc(capacity * 4); k->qslot.alloc(capacity);
+        CacheLaunch cl;
+        cl.dev.mode = 1; cl.dev.vertex = k->cfg.query_vertex; cl.dev.capacity = uint32_t(capacity);
+        cl.dev.box_lo = k->box_lo; cl.dev.box_scale = k->box_scale;
+        cl.dev.rec = k->qrec.p; cl.dev.slot = k->qslot.p; cl.dev.aux = nullptr;
+        cl.w = k->mlp_w.p; cl.table = k->table.p; cl.err = k->err.p;
+        std::vector<std::pair<vkb_scene*, vkb_profile>> in{{s, *pf}};
+        std::vector<vkb_output*> outs{out};
+        WaveTotals tot;
+        uint64_t paths = 0;
+        render_jobs(c, in, outs, pf->flags, hint, tot, paths, &cl);
+        check_nrc_err(k);
+        s->launches += tot.launches;
+        fill_stats(stats, tot, paths, s->build_ms);
+    });
 }
 
 vkb_status vkb_debug_nrc_set_params(vkb_cache* k, const float* mlp, const float* hash) {

@@ -4,6 +4,7 @@
 #include <cstdint>
 #include "vkb_device.cuh"
 #include "vkb_bvh.cuh"
+#include <cooperative_groups.h>
 
 namespace vkb {
 
@@ -344,6 +345,19 @@ struct Job {
     uint32_t wave_first, wave_samples, slot_base, pixel_base;  // this wave
     float4* accum; uint32_t* primary_ids; float4* out;
 };
+// Radiance-cache hooks of a wave.  mode 1 (query): a path reaching vertex `vertex`
+// (0 = camera hit) writes a cache record and stops; the query kernel adds throughput x
+// the cached outgoing radiance.  mode 2 (record): every vertex from 1 on writes a
+// record plus the path's throughput and radiance there (training targets follow from
+// the path's final radiance).  counters[9] counts records; `capacity` bounds them.
+struct CacheParams {
+    uint32_t mode, vertex, capacity;
+    float4 box_lo, box_scale;      // world -> [0,1]^3
+    float4* rec;                   // 4 float4 per record
+    uint32_t* slot;                // path slot of each record
+    float4* aux;                   // mode 2: throughput, radiance at the vertex (2 float4 per record)
+};
+
 struct PathParams {
     Job job0;             // single-job waves read their job from the kernel parameters
     const Job* jobs; uint32_t njobs;
@@ -356,9 +370,11 @@ struct PathParams {
     float4* sb_o; float4* sb_d; float4* sb_c;
     // [0],[1] ray counts, [2] shadow count, [3] ext rays, [4] shadow rays, [5] dropped light,
     // [6] dropped paths, [7] path slots of this wave, [8] pixels of this wave's jobs
+    // [9] radiance-cache records of this wave
     uint32_t* counters;
     unsigned long long* work;  // instrumented traversal: closest nodes, tris, instances, blas nodes; shadow nodes, tris, blas nodes
     uint32_t* err;
+    CacheParams cache;
 };
 constexpr uint32_t META_NONFINITE = 0x80000000u;
 constexpr uint32_t SH_TRACE_A = 1u, SH_HAS_B = 2u, SH_TRACE_B = 4u, SH_DIRECT = 8u;
@@ -574,6 +590,30 @@ __device__ __forceinline__ float3 light_threshold(float3 value, float threshold,
     return value;
 }
 
+// One radiance-cache record of this vertex (warp-aggregated append on counters[9]).
+__device__ __noinline__ void cache_append(const PathParams& p, float3 world, float3 view, float3 normal, const Closure& c, uint32_t slot,
+                                          float3 thr, float3 rad) {
+    namespace cg = cooperative_groups;
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(&p.counters[9], g.size());
+    base = g.shfl(base, 0);
+    const uint32_t idx = base + g.thread_rank();
+    if (idx >= p.cache.capacity) return;
+    const float3 q = f3((world.x - p.cache.box_lo.x) * p.cache.box_scale.x, (world.y - p.cache.box_lo.y) * p.cache.box_scale.y,
+                        (world.z - p.cache.box_lo.z) * p.cache.box_scale.z);
+    float4* r = p.cache.rec + 4 * size_t(idx);
+    r[0] = make_float4(q.x, q.y, q.z, view.x);
+    r[1] = make_float4(view.y, view.z, normal.x, normal.y);
+    r[2] = make_float4(normal.z, c.specular_roughness, c.base_metalness, c.base_color.x);
+    r[3] = make_float4(c.base_color.y, c.base_color.z, 0.f, 0.f);
+    p.cache.slot[idx] = slot;
+    if (p.cache.mode == 2u) {
+        p.cache.aux[2 * size_t(idx)] = make_float4(thr.x, thr.y, thr.z, 0.f);
+        p.cache.aux[2 * size_t(idx) + 1] = make_float4(rad.x, rad.y, rad.z, 0.f);
+    }
+}
+
 // integrate's per-vertex body (path.slang:1340-1709) for one queued extension hit.
 template <bool BATCH>
 __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
@@ -632,6 +672,11 @@ __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
                 c.n = s.geometric;
                 boundary_closure_air(c);
                 float3 view = -dir;
+                // Radiance cache: record this vertex, and at the query vertex stop the path
+                // here (the query kernel adds thr x the cached outgoing radiance).
+                const bool cache_query = p.cache.mode == 1u && bounce >= p.cache.vertex;
+                if (cache_query || (p.cache.mode == 2u && bounce >= 1u)) cache_append(p, s.world, view, s.geometric, c, slot, thr, rad);
+                if (!cache_query) {
                 float3 iface = dot(s.geometric, view) > 0.f ? s.geometric : s.face;
                 Prepared pr = transport_prepare(p.lut, c, view, s.geometric, iface);
                 BsdfSample smp = transport_sample(c, view, sc.x, sc.y, sc.z, pr);
@@ -722,6 +767,7 @@ __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
                         meta = (meta & META_NONFINITE) | ((bounce + 1u) & 0xffu) | ((diffuse & 0xffu) << 8) | ((glossy & 0xffu) << 16) | ((event & 0x3fu) << 24);
                     }
                 }
+                }  // !cache_query
             }
             p.thr[slot] = make_float4(thr.x, thr.y, thr.z, __uint_as_float(meta));
             p.rad[slot] = make_float4(rad.x, rad.y, rad.z, __uint_as_float(dropped));
@@ -734,7 +780,7 @@ __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
     }
 }
 // Seed the first ray queue's count from the wave's path-slot count.
-__global__ void k_start_wave(uint32_t* counters) { counters[0] = counters[7]; }
+__global__ void k_start_wave(uint32_t* counters) { counters[0] = counters[7]; counters[9] = 0u; }
 // Zero the next ray queue and the shadow queue before a shade pass.
 __global__ void k_reset_queues(uint32_t* counters, int nxt) { counters[nxt] = 0u; counters[2] = 0u; }
 // resolve.slang:162-191: add this wave's finished samples to each job's accumulator,

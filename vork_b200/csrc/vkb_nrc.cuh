@@ -287,7 +287,7 @@ struct DebugIO {         // records in, encoded inputs and raw outputs out
 };
 struct QueryIO {         // cache queries of a wave: rad[slot] += throughput * max(y, 0)
     static constexpr bool kDebug = false;
-    const float4* rec; const uint32_t* count; const uint32_t* slot; const float4* thr; float4* rad;
+    const float4* rec; const uint32_t* count; uint32_t cap; const uint32_t* slot; const float4* thr; float4* rad;
 };
 
 // Fused query kernel: 128 rows per tile, persistent over tiles.  blockDim.x == TILE.
@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(TILE) k_nrc_forward(IO io, const __nv_bfloat16
     const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(smem + FWD_BAR + 8);
     const uint32_t lane_addr = tmem + ((warp * 32u) << 16);
     uint32_t n;
-    if constexpr (IO::kDebug) n = io.n; else n = *io.count;
+    if constexpr (IO::kDebug) n = io.n; else n = min(*io.count, io.cap);
     const uint32_t tiles = (n + TILE - 1) / TILE;
     uint32_t phase = 0;
     bool ok = true;
@@ -510,6 +510,21 @@ __global__ void __launch_bounds__(TILE) k_nrc_train(const float4* __restrict__ r
     if (!ok && threadIdx.x == 0) atomicOr(err, 1u);
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem, TMEM_COLS_TRN);
+}
+
+// Training targets of recorded vertices: outgoing radiance = (the path's final radiance
+// - its radiance at the vertex) / its throughput at the vertex, per channel.
+__global__ void k_nrc_targets(const uint32_t* count, uint32_t cap, const uint32_t* __restrict__ slot, const float4* __restrict__ aux,
+                              const float4* __restrict__ rad, float* __restrict__ targets) {
+    const uint32_t n = min(*count, cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 t = aux[2 * size_t(i)], r0 = aux[2 * size_t(i) + 1], rf = rad[slot[i]];
+        const float tt[3] = {t.x, t.y, t.z}, d[3] = {rf.x - r0.x, rf.y - r0.y, rf.z - r0.z};
+        for (int c = 0; c < 3; ++c) {
+            float v = tt[c] > 0.f ? d[c] / tt[c] : 0.f;
+            targets[3 * size_t(i) + c] = isfinite(v) ? fminf(fmaxf(v, 0.f), 1e4f) : 0.f;
+        }
+    }
 }
 
 // Adam over the MLP: gradient = sum of the tile partials in tile order; FP32 master
