@@ -78,3 +78,50 @@ def test_training_steps_reduce_the_loss(installed):
     assert np.isfinite(last) and last < 0.1 * first, (first, last)
     rel = np.abs(y - target) / target
     assert np.median(rel) < 0.1
+
+
+def test_online_training_is_deterministic(renderer):
+    # Training records are compacted in (path slot, vertex) order and gradients are
+    # summed in a fixed order, so two caches trained alike hold identical parameters.
+    from vork_b200 import Profile, scene as S
+    with renderer.install(S.spheres_scene(width=96, height=96)) as s:
+        runs = []
+        for _ in range(2):
+            with RadianceCache(s, seed=5, train_records=8192) as k:
+                for i in range(4):
+                    k.train(Profile.reference_transport(4, 1, seed=40 + i))
+                mlp, table = k.params()
+                img = k.render(Profile.reference_transport(4, 4, seed=1)).image
+                runs.append((mlp, table, img))
+        for a, b in zip(runs[0], runs[1]):
+            assert np.array_equal(a, b)
+
+
+def test_trained_cache_recovers_the_radiance_that_truncation_drops(renderer):
+    # The method without the network: paths stopped at vertex 2 with nothing added (the
+    # cache's output zeroed) lose the light of every deeper bounce.  With the trained
+    # network the image mean is back within 1% of the converged plain render.
+    from vork_b200 import Profile, scene as S
+    with renderer.install(S.spheres_scene(width=128, height=128)) as s:
+        ref = s.render(Profile.reference_transport(4, 1024, seed=7)).image[..., :3]
+        plain = s.render(Profile.reference_transport(4, 64, seed=1))
+        with RadianceCache(s, seed=1) as k:
+            mlp, _ = k.params(table=False)
+            k.set_params(np.zeros_like(mlp), None)
+            cut = k.render(Profile.reference_transport(4, 64, seed=1))
+            k.set_params(mlp, None)
+            for i in range(60):
+                k.train(Profile.reference_transport(4, 1, seed=100 + i))
+            cached = k.render(Profile.reference_transport(4, 64, seed=1))
+    err = lambda im: float(im[..., :3].mean() / ref.mean() - 1.0)
+    e_cut, e_cached, e_plain = err(cut.image), err(cached.image), err(plain.image)
+    assert e_cut < -0.02, e_cut
+    assert abs(e_cached) < 0.01 and abs(e_cached) < 0.25 * abs(e_cut), (e_cut, e_cached, e_plain)
+    # Per 16x16 block (noise averaged down) close to the reference, like the plain render.
+    blocks = lambda im: im[..., :3].reshape(8, 16, 8, 16, 3).mean((1, 3))
+    b_ref = blocks(ref)
+    rel = np.sqrt(np.mean((blocks(cached.image) - b_ref) ** 2)) / b_ref.mean()
+    rel_plain = np.sqrt(np.mean((blocks(plain.image) - b_ref) ** 2)) / b_ref.mean()
+    assert rel < max(0.05, 2 * rel_plain), (rel, rel_plain)
+    # Paths end at the query vertex: fewer extension rays than the plain render.
+    assert cached.stats["extension_rays"] < plain.stats["extension_rays"]

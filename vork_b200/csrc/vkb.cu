@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+#include <cub/iterator/counting_input_iterator.cuh>
 
 #include <algorithm>
 #include <deque>
@@ -627,17 +629,16 @@ PathParams path_params(const vkb_ctx* c, const WaveBuffers& w, uint32_t njobs) {
 }
 
 // A render's radiance-cache hooks: the device side (copied into PathParams) and what
-// the query (mode 1) or target (mode 2) kernel after the bounce loop needs.
+// the query kernel after the bounce loop (mode 1) needs.
 struct CacheLaunch {
     CacheParams dev{};
     const __nv_bfloat16* w = nullptr;
     const __half* table = nullptr;
     uint32_t* err = nullptr;
-    float* targets = nullptr;
 };
 
 // The kernels of one wave: camera, then per bounce closest-hit trace, shade, shadow trace;
-// then the radiance-cache queries or training targets, if any; then accumulation.  Timed
+// then the radiance-cache queries, if any; then accumulation.  Timed
 // mode records events around every closest-hit trace.
 template <bool BATCH>
 void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counted, bool timed, WaveTotals& tot,
@@ -668,9 +669,6 @@ void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counte
     if (cache && cache->dev.mode == 1u) {
         nrc::QueryIO io{cache->dev.rec, p.counters + 9, cache->dev.capacity, cache->dev.slot, p.thr, p.rad};
         nrc::k_nrc_forward<nrc::QueryIO><<<sms * 4, nrc::TILE, nrc::FWD_SMEM, st>>>(io, cache->w, cache->table, cache->err);
-        tot.launches += 1;
-    } else if (cache && cache->dev.mode == 2u) {
-        nrc::k_nrc_targets<<<sms * 8, 256, 0, st>>>(p.counters + 9, cache->dev.capacity, cache->dev.slot, cache->dev.aux, p.rad, cache->targets);
         tot.launches += 1;
     }
     k_accumulate<BATCH><<<sms * 8, 256, 0, st>>>(p);

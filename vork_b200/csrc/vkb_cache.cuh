@@ -16,10 +16,11 @@ struct vkb_cache {
     DBuf<float> wpartial, loss_partial, targets, scratch;
     DBuf<float4> records;
     DBuf<uint32_t> err;
-    // Training paths: per-record path slot and (throughput, radiance) at the vertex; the
-    // low-resolution training render's accumulator and image.
-    DBuf<uint32_t> rec_slot;
-    DBuf<float4> aux, train_accum, train_out;
+    // Training paths: records, (throughput, radiance) and flags at fixed positions, the
+    // compacted indices and count; the low-resolution training render's accumulator and image.
+    DBuf<uint32_t> rec_flag, rec_index, rec_count;
+    DBuf<float4> rec_sparse, aux, train_accum, train_out;
+    DBuf<unsigned char> select_temp;
     // Render queries: one record and path slot per path slot of a wave.
     DBuf<float4> qrec;
     DBuf<uint32_t> qslot;
@@ -202,7 +203,8 @@ vkb_status vkb_cache_destroy(vkb_cache* k) {
     k->mlp_master.release(); k->mlp_m1.release(); k->mlp_m2.release(); k->mlp_w.release();
     k->hash_master.release(); k->hash_m1.release(); k->hash_m2.release(); k->table.release(); k->hash_grad.release();
     k->wpartial.release(); k->loss_partial.release(); k->targets.release(); k->scratch.release(); k->records.release(); k->err.release();
-    k->rec_slot.release(); k->aux.release(); k->train_accum.release(); k->train_out.release(); k->qrec.release(); k->qslot.release();
+    k->rec_flag.release(); k->rec_index.release(); k->rec_count.release(); k->rec_sparse.release(); k->aux.release();
+    k->train_accum.release(); k->train_out.release(); k->select_temp.release(); k->qrec.release(); k->qslot.release();
     delete k;
     return VKB_OK;
 }
@@ -232,18 +234,34 @@ vkb_status vkb_cache_train(vkb_cache* k, const vkb_profile* pf, vkb_cache_stats*
         e.npix = tw * th; e.count = 1;
         k->train_accum.alloc(e.npix); k->train_out.alloc(e.npix);
         e.accum = k->train_accum.p; e.out_dev = k->train_out.p;
-        const uint32_t cap = 2u * k->cfg.train_records;
-        k->records.alloc(size_t(cap) * 4); k->rec_slot.alloc(cap); k->aux.alloc(size_t(cap) * 2); k->targets.alloc(size_t(cap) * 3);
+        // Record positions: path slot x vmax + vertex - 1 (vertices 1..bounces[0]).
+        const uint32_t vmax = std::max(1u, pf->bounces[0]);
+        const uint32_t cap = e.npix * vmax;
+        k->rec_sparse.alloc(size_t(cap) * 4); k->aux.alloc(size_t(cap) * 2); k->rec_flag.alloc(cap); k->rec_index.alloc(cap);
+        k->rec_count.alloc(1); k->records.alloc(size_t(cap) * 4); k->targets.alloc(size_t(cap) * 3);
+        VKB_CUDA(cudaMemsetAsync(k->rec_flag.p, 0, size_t(cap) * sizeof(uint32_t), st));
         c->wave.reserve(e.npix, 1);
         CacheLaunch cl;
-        cl.dev.mode = 2; cl.dev.vertex = 0; cl.dev.capacity = cap;
+        cl.dev.mode = 2; cl.dev.vertex = 0; cl.dev.capacity = cap; cl.dev.vmax = vmax;
         cl.dev.box_lo = k->box_lo; cl.dev.box_scale = k->box_scale;
-        cl.dev.rec = k->records.p; cl.dev.slot = k->rec_slot.p; cl.dev.aux = k->aux.p;
-        cl.w = k->mlp_w.p; cl.table = k->table.p; cl.err = k->err.p; cl.targets = k->targets.p;
+        cl.dev.rec = k->rec_sparse.p; cl.dev.slot = nullptr; cl.dev.aux = k->aux.p; cl.dev.flag = k->rec_flag.p;
+        cl.w = k->mlp_w.p; cl.table = k->table.p; cl.err = k->err.p;
         WaveTotals tot;
         run_engine(c, jobs, c->wave.view(), e.npix, 0, false, tot, false, &cl);
+        // The wave's radiance is still in place: compact the flagged positions in order
+        // and gather records and targets.
+        cub::CountingInputIterator<uint32_t> positions(0u);
+        size_t bytes = 0;
+        VKB_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, positions, k->rec_flag.p, k->rec_index.p, k->rec_count.p, int(cap), st));
+        k->select_temp.alloc(std::max<size_t>(bytes, 1));
+        bytes = k->select_temp.n;
+        VKB_CUDA(cub::DeviceSelect::Flagged(k->select_temp.p, bytes, positions, k->rec_flag.p, k->rec_index.p, k->rec_count.p, int(cap), st));
+        k_nrc_gather<<<c->sms * 8, 256, 0, st>>>(k->rec_count.p, cap, k->rec_index.p, vmax, k->rec_sparse.p, k->aux.p, c->wave.view().rad,
+                                                 k->records.p, k->targets.p);
+        tot.launches += 2;
+        VKB_CUDA(cudaGetLastError());
         uint32_t count = 0;
-        VKB_CUDA(cudaMemcpyAsync(&count, c->wave.view().counters + 9, sizeof(count), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaMemcpyAsync(&count, k->rec_count.p, sizeof(count), cudaMemcpyDeviceToHost, st));
         VKB_CUDA(cudaStreamSynchronize(st));
         count = std::min(count, cap);
         s->launches += tot.launches;

@@ -346,16 +346,18 @@ struct Job {
     float4* accum; uint32_t* primary_ids; float4* out;
 };
 // Radiance-cache hooks of a wave.  mode 1 (query): a path reaching vertex `vertex`
-// (0 = camera hit) writes a cache record and stops; the query kernel adds throughput x
-// the cached outgoing radiance.  mode 2 (record): every vertex from 1 on writes a
-// record plus the path's throughput and radiance there (training targets follow from
-// the path's final radiance).  counters[9] counts records; `capacity` bounds them.
+// (0 = camera hit) appends a cache record (counters[9] counts them, `capacity` bounds
+// them) and stops; the query kernel adds throughput x the cached outgoing radiance.
+// mode 2 (record): vertex v >= 1 of the path in slot s writes its record, throughput and
+// radiance at position s * vmax + v - 1 and sets flag[position]; the training set is
+// compacted from the flags in position order, so it does not depend on thread timing.
 struct CacheParams {
-    uint32_t mode, vertex, capacity;
+    uint32_t mode, vertex, capacity, vmax;
     float4 box_lo, box_scale;      // world -> [0,1]^3
     float4* rec;                   // 4 float4 per record
-    uint32_t* slot;                // path slot of each record
+    uint32_t* slot;                // mode 1: path slot of each record
     float4* aux;                   // mode 2: throughput, radiance at the vertex (2 float4 per record)
+    uint32_t* flag;                // mode 2: position holds a record
 };
 
 struct PathParams {
@@ -590,15 +592,22 @@ __device__ __forceinline__ float3 light_threshold(float3 value, float threshold,
     return value;
 }
 
-// One radiance-cache record of this vertex (warp-aggregated append on counters[9]).
+// One radiance-cache record of this vertex: queries append (warp-aggregated on
+// counters[9]); training records go to their fixed position.
 __device__ __noinline__ void cache_append(const PathParams& p, float3 world, float3 view, float3 normal, const Closure& c, uint32_t slot,
-                                          float3 thr, float3 rad) {
-    namespace cg = cooperative_groups;
-    cg::coalesced_group g = cg::coalesced_threads();
-    uint32_t base = 0;
-    if (g.thread_rank() == 0) base = atomicAdd(&p.counters[9], g.size());
-    base = g.shfl(base, 0);
-    const uint32_t idx = base + g.thread_rank();
+                                          uint32_t vertex, float3 thr, float3 rad) {
+    uint32_t idx;
+    if (p.cache.mode == 1u) {
+        namespace cg = cooperative_groups;
+        cg::coalesced_group g = cg::coalesced_threads();
+        uint32_t base = 0;
+        if (g.thread_rank() == 0) base = atomicAdd(&p.counters[9], g.size());
+        base = g.shfl(base, 0);
+        idx = base + g.thread_rank();
+    } else {
+        if (vertex < 1u || vertex > p.cache.vmax) return;
+        idx = slot * p.cache.vmax + vertex - 1u;
+    }
     if (idx >= p.cache.capacity) return;
     const float3 q = f3((world.x - p.cache.box_lo.x) * p.cache.box_scale.x, (world.y - p.cache.box_lo.y) * p.cache.box_scale.y,
                         (world.z - p.cache.box_lo.z) * p.cache.box_scale.z);
@@ -607,10 +616,12 @@ __device__ __noinline__ void cache_append(const PathParams& p, float3 world, flo
     r[1] = make_float4(view.y, view.z, normal.x, normal.y);
     r[2] = make_float4(normal.z, c.specular_roughness, c.base_metalness, c.base_color.x);
     r[3] = make_float4(c.base_color.y, c.base_color.z, 0.f, 0.f);
-    p.cache.slot[idx] = slot;
-    if (p.cache.mode == 2u) {
+    if (p.cache.mode == 1u) {
+        p.cache.slot[idx] = slot;
+    } else {
         p.cache.aux[2 * size_t(idx)] = make_float4(thr.x, thr.y, thr.z, 0.f);
         p.cache.aux[2 * size_t(idx) + 1] = make_float4(rad.x, rad.y, rad.z, 0.f);
+        p.cache.flag[idx] = 1u;
     }
 }
 
@@ -675,7 +686,7 @@ __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
                 // Radiance cache: record this vertex, and at the query vertex stop the path
                 // here (the query kernel adds thr x the cached outgoing radiance).
                 const bool cache_query = p.cache.mode == 1u && bounce >= p.cache.vertex;
-                if (cache_query || (p.cache.mode == 2u && bounce >= 1u)) cache_append(p, s.world, view, s.geometric, c, slot, thr, rad);
+                if (cache_query || (p.cache.mode == 2u && bounce >= 1u)) cache_append(p, s.world, view, s.geometric, c, slot, bounce, thr, rad);
                 if (!cache_query) {
                 float3 iface = dot(s.geometric, view) > 0.f ? s.geometric : s.face;
                 Prepared pr = transport_prepare(p.lut, c, view, s.geometric, iface);

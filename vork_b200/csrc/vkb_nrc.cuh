@@ -512,13 +512,17 @@ __global__ void __launch_bounds__(TILE) k_nrc_train(const float4* __restrict__ r
     if (warp == 0) tmem_dealloc(tmem, TMEM_COLS_TRN);
 }
 
-// Training targets of recorded vertices: outgoing radiance = (the path's final radiance
-// - its radiance at the vertex) / its throughput at the vertex, per channel.
-__global__ void k_nrc_targets(const uint32_t* count, uint32_t cap, const uint32_t* __restrict__ slot, const float4* __restrict__ aux,
-                              const float4* __restrict__ rad, float* __restrict__ targets) {
+// Training set of a recording wave, in position order (indices from the flags): the
+// record itself and its target, the outgoing radiance = (the path's final radiance - its
+// radiance at the vertex) / its throughput at the vertex, per channel.
+__global__ void k_nrc_gather(const uint32_t* __restrict__ count, uint32_t cap, const uint32_t* __restrict__ index, uint32_t vmax,
+                             const float4* __restrict__ rec, const float4* __restrict__ aux, const float4* __restrict__ rad,
+                             float4* __restrict__ out_rec, float* __restrict__ targets) {
     const uint32_t n = min(*count, cap);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 t = aux[2 * size_t(i)], r0 = aux[2 * size_t(i) + 1], rf = rad[slot[i]];
+        const uint32_t q = index[i];
+        for (int k = 0; k < 4; ++k) out_rec[4 * size_t(i) + k] = rec[4 * size_t(q) + k];
+        const float4 t = aux[2 * size_t(q)], r0 = aux[2 * size_t(q) + 1], rf = rad[q / vmax];
         const float tt[3] = {t.x, t.y, t.z}, d[3] = {rf.x - r0.x, rf.y - r0.y, rf.z - r0.z};
         for (int c = 0; c < 3; ++c) {
             float v = tt[c] > 0.f ? d[c] / tt[c] : 0.f;
