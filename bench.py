@@ -34,8 +34,9 @@ def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
-    return {"hbm_gbs": PEAKS_FALLBACK["hbm_gbs"], "source": "fallback"}
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d.get("bf16_tflops", PEAKS_FALLBACK["bf16_tflops"])),
+                "source": "measured"}
+    return {**PEAKS_FALLBACK, "source": "fallback"}
 
 
 def workload(config: str, seed: int = 0):
@@ -267,18 +268,130 @@ def run_serve(args, device):
     r.close()
 
 
+def run_cache(args, device):
+    """Learned radiance cache on the large scene at 1920x1080, 16 spp, depth 8: per frame
+    the TLAS is rebuilt, the cache takes one online training round (2^16 records, 4
+    steps) and renders through it (paths stop at vertex 2); against plain 16-spp renders
+    of the same frames.  Error of both against the plain tracer at 1024 spp of the last
+    frame, and of the 64x64 centre crop against the FP64 oracle."""
+    import torch
+    from vork_b200 import Profile, RadianceCache, Renderer, abi
+    from vork_b200.build import build
+    build()
+    sc, flock, _, _ = workload("large")
+    spp, depth = 16, 8
+    frames = frames_for(sc, flock, args.warmup + args.steps)
+    cam = sc.camera
+    npix = cam.width * cam.height
+    r = Renderer(device)
+    s = r.install(sc)
+    n_inst = frames[0].shape[0]
+    dev_frames = [torch.from_numpy(f).to(f"cuda:{device}") for f in frames]
+    prof = Profile.reference_transport(depth, spp, seed=1)
+    timed = prof.__class__(**{**prof.__dict__, "flags": abi.PROFILE_TIME_KERNELS})
+    k = RadianceCache(s, seed=0)
+    cached_ms, plain_ms, train_ms, build_ms, cache_ms, queries = [], [], [], [], 0.0, 0
+    train_parts = {"paths_ms": 0.0, "steps_ms": 0.0, "host_ms": 0.0}
+    rays_cached = rays_plain = 0
+    with ClockSampler(device) as clocks:
+        for i in range(args.warmup + args.steps):
+            s.update_instances_device(dev_frames[i].data_ptr(), n_inst, 1)
+            b = s.info()["build_ms"]
+            t = k.train(Profile.reference_transport(depth, 1, seed=1000 + i))
+            c = k.render(timed)
+            p = s.render(timed)
+            if i >= args.warmup:
+                build_ms.append(b); train_ms.append(t["train_ms"])
+                for key in train_parts:
+                    train_parts[key] += t[key] / args.steps
+                cached_ms.append(t["train_ms"] + c.stats["render_ms"]); plain_ms.append(p.stats["render_ms"])
+                cache_ms += c.stats["cache_ms"]; queries += c.stats["cache_queries"]
+                rays_cached += c.stats["extension_rays"]; rays_plain += p.stats["extension_rays"]
+    last_cached, last_plain = c.image[..., :3], p.image[..., :3]
+    if args.no_error:   # timing only (profiling runs): no reference renders
+        ref = last_plain
+    else:
+        ref = s.render(Profile.reference_transport(depth, 1024, seed=7)).image[..., :3]
+    conv = last_cached if args.no_error else k.render(Profile.reference_transport(depth, 256, seed=3)).image[..., :3]
+    h16 = cam.height // 16 * 16
+
+    def errs(img):
+        blocks = lambda im: im[:h16].reshape(h16 // 16, 16, cam.width // 16, 16, 3).mean((1, 3))
+        br = blocks(ref)
+        return {"mean_rel_err": float(img.mean() / ref.mean() - 1.0),
+                "rel_rmse_pixels": float(np.sqrt(np.mean((img - ref) ** 2)) / ref.mean()),
+                "rel_rmse_16x16_blocks": float(np.sqrt(np.mean((blocks(img) - br) ** 2)) / br.mean())}
+
+    # FP64 oracle on the 64x64 centre crop of the last frame (plain path tracing, 64 spp).
+    oracle_crop = None
+    try:
+        if args.no_error:
+            raise RuntimeError("skipped (--no-error)")
+        import dataclasses
+        from oracle import pyoracle
+        osc = dataclasses.replace(sc, instance_rows=frames[-1].reshape(-1, 3, 4))
+        o = pyoracle.OracleScene(osc, fp32=False, fp64=True)
+        x0, y0 = cam.width // 2 - 32, cam.height // 2 - 32
+        t0 = time.perf_counter()
+        oimg, _ = o.render(Profile.reference_transport(depth, 64, seed=11).c(), x0, y0, 64, 64, fp64=True, threads=os.cpu_count() or 1)
+        dt = time.perf_counter() - t0
+        o.close()
+        om = float(oimg[..., :3].mean())
+        crop = lambda im: float(im[y0:y0 + 64, x0:x0 + 64].mean())
+        oracle_crop = {"spp": 64, "seconds": dt, "oracle_mean": om, "cached_256spp_rel_err": crop(conv) / om - 1.0,
+                       "plain_1024spp_rel_err": crop(ref) / om - 1.0}
+    except Exception as e:  # reported, never silently dropped
+        oracle_crop = {"error": repr(e)}
+    pk = peaks()
+    steps = args.steps
+    paths = npix * spp * steps
+    value = paths / (sum(cached_ms) / 1000.0)
+    plain_value = paths / (sum(plain_ms) / 1000.0)
+    flops = 2.0 * abi.NRC_MLP_PARAMS * queries
+    tflops = flops / (cache_ms / 1000.0) / 1e12 if cache_ms > 0 else None
+    # Query kernel bytes per query: record 64 + slot 4 + throughput 16 + radiance 32 (read
+    # and write) + 16 levels x 8 corners x 4 B of hash features.
+    qbytes = 64 + 4 + 16 + 32 + 16 * 8 * 4
+    line = {"metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": sum(cached_ms) / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16",
+            "data": "synthetic (seeded generator; no dataset)",
+            "config": {"workload": "learned radiance cache: large scene 1920x1080, 16 spp, depth 8, one training round per frame "
+                                   "(2^16 records, 4 Adam steps) then the cached render (queries at vertex 2); hash grid 16 levels "
+                                   "x 2^19 x 2 FP16, 5x64 BF16 MLP, FP32 accumulation", "global_batch": npix * spp,
+                       "l2_flush": "inputs > L2: 1M-instance TLAS + 2M-tri BLAS + wavefront queues per frame"},
+            "plain": {"value": plain_value, "unit": "paths/s", "ms_per_step": sum(plain_ms) / steps},
+            "speedup_vs_plain": value / plain_value,
+            "per_frame_ms": {"train": sum(train_ms) / steps, "train_parts": train_parts,
+                             "cached_render": sum(cached_ms) / steps - sum(train_ms) / steps,
+                             "plain_render": sum(plain_ms) / steps, "tlas_build": sum(build_ms) / steps},
+            "extension_rays_per_path": {"cached": rays_cached / paths, "plain": rays_plain / paths},
+            "error_vs_plain_1024spp": {"cached_16spp": errs(last_cached), "plain_16spp": errs(last_plain),
+                                       "cached_256spp": errs(conv)},
+            "error_vs_fp64_oracle_crop": oracle_crop,
+            "roofline": {"bound": "tensor", "kernel": "k_nrc_forward<query> (fused hash encoding + 5-layer MLP)",
+                         "achieved": tflops, "peak": pk["bf16_tflops"], "peak_source": pk["source"], "unit": "TFLOP/s",
+                         "frac": (tflops / pk["bf16_tflops"]) if tflops else None, "traffic": None,
+                         "queries": queries, "kernel_ms": cache_ms,
+                         "hbm_view": {"bytes_per_query": qbytes, "achieved_gbs": qbytes * queries / (cache_ms / 1000.0) / 1e9 if cache_ms else None,
+                                      "peak_gbs": pk["hbm_gbs"]}},
+            "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+    k.close(); s.close(); r.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="vkb", choices=["vkb", "reference"])
-    ap.add_argument("--config", default="large", choices=["large", "small", "profile", "batch", "serve"])
+    ap.add_argument("--config", default="large", choices=["large", "small", "profile", "batch", "serve", "cache"])
     ap.add_argument("--jobs", type=int, default=256, help="batch: preview jobs")
     ap.add_argument("--requests", type=int, default=32, help="serve: requests per arrival rate")
     ap.add_argument("--rates", default="2,8,32", help="serve: Poisson arrival rates (req/s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tlas", choices=["lbvh", "ploc"], default="lbvh", help="TLAS builder of the frame scene")
+    ap.add_argument("--no-error", action="store_true", help="cache: skip the reference renders (timing/profiling runs)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -290,6 +403,8 @@ def main():
         return run_batch(args, local)
     if args.config == "serve":
         return run_serve(args, local)
+    if args.config == "cache":
+        return run_cache(args, local)
 
     import torch
     dist = None

@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define VKB_ABI_VERSION 2u
+#define VKB_ABI_VERSION 3u
 
 /* Error model: FailureKind exit categories of crates/vork-render/src/failure.rs:21-100,
  * reduced to what a render call can report. */
@@ -186,6 +186,8 @@ typedef struct vkb_stats {
     uint64_t shadow_nodes_visited;
     uint64_t shadow_triangles_tested;
     uint64_t blas_nodes_visited;   /* closest-hit node visits inside instance BLASes (the rest are TLAS) */
+    float cache_ms;            /* VKB_PROFILE_TIME_KERNELS, vkb_render_cached: radiance-cache query kernel time */
+    uint64_t cache_queries;    /* vkb_render_cached: paths answered by the radiance cache */
 } vkb_stats;
 
 typedef struct vkb_ctx vkb_ctx;
@@ -332,7 +334,7 @@ vkb_status vkb_debug_blas_morton(vkb_scene* scene, uint32_t mesh, uint32_t* out)
 typedef struct vkb_cache vkb_cache;
 typedef struct vkb_cache_config {
     uint32_t train_records;    /* training vertices per vkb_cache_train call (default 65536) */
-    uint32_t train_steps;      /* optimizer steps per call, each over all records (default 4) */
+    uint32_t train_steps;      /* optimizer steps per vkb_cache_train call, over interleaved minibatches of its records (default 4) */
     uint32_t query_vertex;     /* path vertex (0 = camera hit) answered by the cache (default 2) */
     uint32_t seed;             /* parameter initialisation and training-path sampling */
     float lr_mlp, lr_hash;     /* Adam learning rates (defaults 2e-3, 1e-2) */
@@ -343,13 +345,17 @@ typedef struct vkb_cache_stats {
     uint64_t records;          /* training vertices of the last call */
     float loss;                /* mean relative-L2 loss of the last step */
     float train_ms;            /* device time of the last call (paths + steps) */
+    float paths_ms;            /* of which the training paths and the training-set compaction */
+    float steps_ms;            /* of which the optimizer steps */
+    float host_ms;             /* wall time of the call on the host */
 } vkb_cache_stats;
 vkb_status vkb_cache_create(vkb_scene* scene, const vkb_cache_config* config, vkb_cache** out);
 vkb_status vkb_cache_destroy(vkb_cache* cache);
 /* One online training round: trace about train_records / 2 training paths through the
  * scene's camera at reduced resolution (one sample, a fresh seed each call, the
  * profile's bounce limits), take every vertex from 1 on as a training record whose
- * target is the path's radiance from there on, and run train_steps optimizer steps. */
+ * target is the path's radiance from there on, and run train_steps optimizer steps,
+ * step i over records i, i + train_steps, ... (every record once per round). */
 vkb_status vkb_cache_train(vkb_cache* cache, const vkb_profile* profile, vkb_cache_stats* stats);
 /* vkb_render through the cache: paths stop at query_vertex and add throughput x the
  * cached outgoing radiance there (the plain render is the fallback and the judge of its

@@ -72,7 +72,8 @@ class VkbCacheConfig(C.Structure):
 
 
 class VkbCacheStats(C.Structure):
-    _fields_ = [("steps", C.c_uint64), ("records", C.c_uint64), ("loss", C.c_float), ("train_ms", C.c_float)]
+    _fields_ = [("steps", C.c_uint64), ("records", C.c_uint64), ("loss", C.c_float), ("train_ms", C.c_float),
+                ("paths_ms", C.c_float), ("steps_ms", C.c_float), ("host_ms", C.c_float)]
 
 
 NRC_MLP_PARAMS, NRC_HASH_PARAMS = 17408, 16777216
@@ -93,7 +94,7 @@ class VkbStats(C.Structure):
                 ("trace_ms", C.c_float), ("trace_launches", C.c_uint32), ("kernel_launches", C.c_uint32),
                 ("nodes_visited", C.c_uint64), ("triangles_tested", C.c_uint64), ("instances_entered", C.c_uint64),
                 ("shadow_nodes_visited", C.c_uint64), ("shadow_triangles_tested", C.c_uint64),
-                ("blas_nodes_visited", C.c_uint64)]
+                ("blas_nodes_visited", C.c_uint64), ("cache_ms", C.c_float), ("cache_queries", C.c_uint64)]
 
 
 class VkbJob(C.Structure):

@@ -13,6 +13,7 @@
 #include <cub/iterator/counting_input_iterator.cuh>
 
 #include <algorithm>
+#include <chrono>
 #include <deque>
 #include <map>
 #include <memory>
@@ -406,6 +407,7 @@ struct vkb_ctx {
     uint64_t launches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<cudaEvent_t> kernel_events;
+    std::vector<cudaEvent_t> cache_events;    // timed renders: around each radiance-cache query launch
 };
 
 struct vkb_scene {
@@ -578,8 +580,8 @@ struct EngineJob {
     uint32_t npix = 0, count = 0, done = 0, pixel_base = 0;
 };
 struct WaveTotals {
-    uint32_t launches = 0, trace_launches = 0;
-    float trace_ms = 0.f, render_ms = 0.f;
+    uint32_t launches = 0, trace_launches = 0, cache_launches = 0;
+    float trace_ms = 0.f, render_ms = 0.f, cache_ms = 0.f;
     uint32_t counters[16] = {};
     unsigned long long work[8] = {};
     uint32_t err = 0;
@@ -667,8 +669,18 @@ void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counte
         else k_trace<true, false, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p, -1);
     }
     if (cache && cache->dev.mode == 1u) {
-        nrc::QueryIO io{cache->dev.rec, p.counters + 9, cache->dev.capacity, cache->dev.slot, p.thr, p.rad};
+        if (timed) {
+            while (c->cache_events.size() < 2 * (tot.cache_launches + 1)) {
+                cudaEvent_t e;
+                VKB_CUDA(cudaEventCreate(&e));
+                c->cache_events.push_back(e);
+            }
+            VKB_CUDA(cudaEventRecord(c->cache_events[2 * tot.cache_launches], st));
+        }
+        nrc::QueryIO io{cache->dev.rec, p.counters + 9, cache->dev.capacity, cache->dev.slot, p.thr, p.rad, p.work + 7};
         nrc::k_nrc_forward<nrc::QueryIO><<<sms * 4, nrc::TILE, nrc::FWD_SMEM, st>>>(io, cache->w, cache->table, cache->err);
+        if (timed) VKB_CUDA(cudaEventRecord(c->cache_events[2 * tot.cache_launches + 1], st));
+        tot.cache_launches++;
         tot.launches += 1;
     }
     k_accumulate<BATCH><<<sms * 8, 256, 0, st>>>(p);
@@ -727,16 +739,32 @@ struct WaveEngine {
         size_t left = capacity;
         bool any = false;
         if (packed) {
-            // First fit in admission order: a job that does not fit what is left is
-            // skipped for this wave and later (smaller) jobs fill the slots.
-            for (uint32_t k = 0; k < njobs && left > 0; ++k) {
-                EngineJob& e = jobs[k];
-                if (finished(k)) continue;
-                uint32_t n = uint32_t(std::min<size_t>(e.count - e.done, left / e.npix));
-                if (n == 0 && !any) n = 1;      // an image larger than the wave: one sample alone
-                if (n == 0) continue;
-                take[k] = n; any = true;
-                left = size_t(n) * e.npix <= left ? left - size_t(n) * e.npix : 0;
+            // A job whose remaining samples fill at least half a wave takes the wave alone
+            // (the plain single-job kernels, its scene alone in L2).  Otherwise first fit in
+            // admission order over the small jobs: one that does not fit what is left is
+            // skipped for this wave and later ones fill the slots.
+            auto big = [&](uint32_t k) { return size_t(jobs[k].count - jobs[k].done) * jobs[k].npix >= capacity / 2; };
+            uint32_t first = 0;
+            while (first < njobs && finished(first)) ++first;
+            if (first < njobs && big(first)) {
+                EngineJob& e = jobs[first];
+                take[first] = uint32_t(std::max<size_t>(1, std::min<size_t>(e.count - e.done, capacity / e.npix)));
+                any = true;
+            } else {
+                for (uint32_t k = 0; k < njobs && left > 0; ++k) {
+                    EngineJob& e = jobs[k];
+                    if (finished(k) || big(k)) continue;
+                    uint32_t n = uint32_t(std::min<size_t>(e.count - e.done, left / e.npix));
+                    if (n == 0) continue;
+                    take[k] = n; any = true;
+                    left -= size_t(n) * e.npix;
+                }
+                if (!any)   // only big jobs are left: the first of them alone
+                    for (uint32_t k = 0; k < njobs && !any; ++k)
+                        if (!finished(k)) {
+                            take[k] = uint32_t(std::max<size_t>(1, std::min<size_t>(jobs[k].count - jobs[k].done, capacity / jobs[k].npix)));
+                            any = true;
+                        }
             }
         } else {
             for (uint32_t k = 0; k < njobs; ++k) {
@@ -832,6 +860,12 @@ struct WaveEngine {
                 VKB_CUDA(cudaEventElapsedTime(&e, c->kernel_events[2 * k], c->kernel_events[2 * k + 1]));
                 tot.trace_ms += e;
             }
+        if (flags & VKB_PROFILE_TIME_KERNELS)
+            for (uint32_t k = 0; k < tot.cache_launches; ++k) {
+                float e = 0.f;
+                VKB_CUDA(cudaEventElapsedTime(&e, c->cache_events[2 * k], c->cache_events[2 * k + 1]));
+                tot.cache_ms += e;
+            }
     }
 };
 
@@ -874,6 +908,8 @@ void fill_stats(vkb_stats* stats, const WaveTotals& t, uint64_t paths, float bui
     stats->shadow_nodes_visited = t.work[3];
     stats->shadow_triangles_tested = t.work[4];
     stats->blas_nodes_visited = t.work[5];
+    stats->cache_ms = t.cache_ms;
+    stats->cache_queries = t.work[7];
 }
 
 // Render jobs with the context's own buffers (grown on demand).
@@ -951,6 +987,7 @@ vkb_status vkb_close(vkb_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (cudaEvent_t e : c->kernel_events) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->cache_events) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     c->wave.release();

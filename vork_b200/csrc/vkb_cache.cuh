@@ -26,6 +26,10 @@ struct vkb_cache {
     DBuf<uint32_t> qslot;
     float4 box_lo{}, box_scale{};   // world -> [0,1]^3, fixed at creation (5% margin)
     uint64_t train_calls = 0;
+    // Training round: compaction start/end, optimizer steps start/end (no host
+    // synchronisation inside either pair, so they measure device work only).
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    float last_paths_ms = 0.f, last_steps_ms = 0.f, last_host_ms = 0.f;
 };
 
 namespace {
@@ -98,17 +102,35 @@ void check_nrc_err(vkb_cache* k) {
     }
 }
 
-// Gradients of the loss over `n` device records (already in k->records / k->targets);
-// with lr > 0 also one Adam step.  Returns the mean loss.
-float nrc_step(vkb_cache* k, uint32_t n, bool update, float* mlp_grad_dev, float* hash_grad_dev) {
+// Mean loss of the last step (over its n records) from the per-tile partials; also
+// raises a timed-out tensor-core wait.  Synchronises.
+float nrc_read_loss(vkb_cache* k, uint32_t n) {
+    cudaStream_t st = k->s->ctx->stream;
+    const uint32_t tiles = (n + TILE - 1) / TILE;
+    std::vector<float> lp(tiles);
+    VKB_CUDA(cudaMemcpyAsync(lp.data(), k->loss_partial.p, tiles * sizeof(float), cudaMemcpyDeviceToHost, st));
+    check_nrc_err(k);
+    double sum = 0.0;
+    for (float x : lp) sum += x;
+    k->last_loss = float(sum / (3.0 * n));
+    return k->last_loss;
+}
+
+// Gradients of the loss over the device records offset, offset + stride, ... below
+// `total` (already in k->records / k->targets); with `update` also one Adam step.  With
+// `read_loss` returns the step's mean loss (one host round trip), else 0.
+float nrc_step(vkb_cache* k, uint32_t total, bool update, float* mlp_grad_dev, float* hash_grad_dev, uint32_t offset = 0,
+               uint32_t stride = 1, bool read_loss = true) {
     vkb_ctx* c = k->s->ctx;
     cudaStream_t st = c->stream;
     nrc_kernel_attributes();
+    const uint32_t n = offset < total ? (total - offset + stride - 1) / stride : 0u;
+    if (n == 0) return 0.f;
     const uint32_t tiles = (n + TILE - 1) / TILE;
     k->wpartial.alloc(size_t(tiles) * MLP_PARAMS);
     k->loss_partial.alloc(tiles);
-    k_nrc_train<<<tiles, TILE, TRN_SMEM, st>>>(k->records.p, k->targets.p, n, 1.f / float(3u * n), k->mlp_w.p, k->table.p, k->wpartial.p,
-                                               k->hash_grad.p, k->loss_partial.p, k->err.p);
+    k_nrc_train<<<tiles, TILE, TRN_SMEM, st>>>(k->records.p, k->targets.p, n, offset, stride, 1.f / float(3u * n), k->mlp_w.p, k->table.p,
+                                               k->wpartial.p, k->hash_grad.p, k->loss_partial.p, k->err.p);
     AdamParams am{0.f, k->cfg.beta1, k->cfg.beta2, k->cfg.eps, 1.f, 1.f}, ah = am;
     if (update) {
         k->steps++;
@@ -122,13 +144,8 @@ float nrc_step(vkb_cache* k, uint32_t n, bool update, float* mlp_grad_dev, float
                                                 hash_grad_dev);
     k->s->launches += 3;
     VKB_CUDA(cudaGetLastError());
-    std::vector<float> lp(tiles);
-    VKB_CUDA(cudaMemcpyAsync(lp.data(), k->loss_partial.p, tiles * sizeof(float), cudaMemcpyDeviceToHost, st));
-    check_nrc_err(k);
-    double sum = 0.0;
-    for (float x : lp) sum += x;
-    k->last_loss = float(sum / (3.0 * n));
-    return k->last_loss;
+    if (!read_loss) return 0.f;
+    return nrc_read_loss(k, n);
 }
 
 void upload_records(vkb_cache* k, uint32_t n, const float* records, const float* targets) {
@@ -156,6 +173,7 @@ vkb_status vkb_cache_create(vkb_scene* s, const vkb_cache_config* config, vkb_ca
         if (k->cfg.query_vertex < 1 || k->cfg.query_vertex > 16) throw ArgError{"query_vertex must be 1..16"};
         VKB_CUDA(cudaSetDevice(s->ctx->device));
         cudaStream_t str = s->ctx->stream;
+        for (auto& e : k->ev) VKB_CUDA(cudaEventCreate(&e));
         k->mlp_master.alloc(MLP_PARAMS); k->mlp_m1.alloc(MLP_PARAMS); k->mlp_m2.alloc(MLP_PARAMS); k->mlp_w.alloc(MLP_PARAMS);
         k->hash_master.alloc(HASH_PARAMS); k->hash_m1.alloc(HASH_PARAMS); k->hash_m2.alloc(HASH_PARAMS);
         k->table.alloc(HASH_PARAMS); k->hash_grad.alloc(HASH_PARAMS); k->err.alloc(1);
@@ -203,6 +221,7 @@ vkb_status vkb_cache_destroy(vkb_cache* k) {
     k->mlp_master.release(); k->mlp_m1.release(); k->mlp_m2.release(); k->mlp_w.release();
     k->hash_master.release(); k->hash_m1.release(); k->hash_m2.release(); k->table.release(); k->hash_grad.release();
     k->wpartial.release(); k->loss_partial.release(); k->targets.release(); k->scratch.release(); k->records.release(); k->err.release();
+    for (auto& e : k->ev) if (e) cudaEventDestroy(e);
     k->rec_flag.release(); k->rec_index.release(); k->rec_count.release(); k->rec_sparse.release(); k->aux.release();
     k->train_accum.release(); k->train_out.release(); k->select_temp.release(); k->qrec.release(); k->qslot.release();
     delete k;
@@ -218,7 +237,7 @@ vkb_status vkb_cache_train(vkb_cache* k, const vkb_profile* pf, vkb_cache_stats*
         VKB_CUDA(cudaSetDevice(c->device));
         cudaStream_t st = c->stream;
         nrc_kernel_attributes();
-        VKB_CUDA(cudaEventRecord(c->ev0, st));
+        const auto host0 = std::chrono::steady_clock::now();
         // Training paths: the scene's camera at a resolution of about train_records / 2
         // pixels, one sample of a fresh seed per call, full path depth.
         const vkb_camera& cam = s->camera;
@@ -250,6 +269,7 @@ vkb_status vkb_cache_train(vkb_cache* k, const vkb_profile* pf, vkb_cache_stats*
         run_engine(c, jobs, c->wave.view(), e.npix, 0, false, tot, false, &cl);
         // The wave's radiance is still in place: compact the flagged positions in order
         // and gather records and targets.
+        VKB_CUDA(cudaEventRecord(k->ev[0], st));
         cub::CountingInputIterator<uint32_t> positions(0u);
         size_t bytes = 0;
         VKB_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, positions, k->rec_flag.p, k->rec_index.p, k->rec_count.p, int(cap), st));
@@ -260,20 +280,31 @@ vkb_status vkb_cache_train(vkb_cache* k, const vkb_profile* pf, vkb_cache_stats*
                                                  k->records.p, k->targets.p);
         tot.launches += 2;
         VKB_CUDA(cudaGetLastError());
+        VKB_CUDA(cudaEventRecord(k->ev[1], st));
         uint32_t count = 0;
         VKB_CUDA(cudaMemcpyAsync(&count, k->rec_count.p, sizeof(count), cudaMemcpyDeviceToHost, st));
         VKB_CUDA(cudaStreamSynchronize(st));
         count = std::min(count, cap);
         s->launches += tot.launches;
         k->train_calls++;
-        if (count > 0)
-            for (uint32_t i = 0; i < k->cfg.train_steps; ++i) nrc_step(k, count, true, nullptr, nullptr);
-        VKB_CUDA(cudaEventRecord(c->ev1, st));
-        VKB_CUDA(cudaEventSynchronize(c->ev1));
-        VKB_CUDA(cudaEventElapsedTime(&k->last_train_ms, c->ev0, c->ev1));
+        // train_steps interleaved minibatches: step i takes records i, i + steps, ... (each
+        // spread over the whole image), so one round visits every record once.
+        VKB_CUDA(cudaEventRecord(k->ev[2], st));
+        const uint32_t steps = std::min(k->cfg.train_steps, std::max(1u, count));
+        for (uint32_t i = 0; i < steps && count > 0; ++i) nrc_step(k, count, true, nullptr, nullptr, i, steps, false);
+        VKB_CUDA(cudaEventRecord(k->ev[3], st));
+        VKB_CUDA(cudaEventSynchronize(k->ev[3]));
+        if (count > 0) nrc_read_loss(k, (count - (steps - 1) + steps - 1) / steps);   // records of the last step (offset steps - 1)
+        float compact_ms = 0.f;
+        VKB_CUDA(cudaEventElapsedTime(&compact_ms, k->ev[0], k->ev[1]));
+        VKB_CUDA(cudaEventElapsedTime(&k->last_steps_ms, k->ev[2], k->ev[3]));
+        k->last_paths_ms = tot.render_ms + compact_ms;
+        k->last_train_ms = k->last_paths_ms + k->last_steps_ms;
+        k->last_host_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - host0).count();
         k->last_records = count;
         if (stats) {
             stats->steps = k->steps; stats->records = count; stats->loss = k->last_loss; stats->train_ms = k->last_train_ms;
+            stats->paths_ms = k->last_paths_ms; stats->steps_ms = k->last_steps_ms; stats->host_ms = k->last_host_ms;
         }
     });
 }

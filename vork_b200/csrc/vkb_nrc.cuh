@@ -288,6 +288,7 @@ struct DebugIO {         // records in, encoded inputs and raw outputs out
 struct QueryIO {         // cache queries of a wave: rad[slot] += throughput * max(y, 0)
     static constexpr bool kDebug = false;
     const float4* rec; const uint32_t* count; uint32_t cap; const uint32_t* slot; const float4* thr; float4* rad;
+    unsigned long long* queries;   // += queries answered
 };
 
 // Fused query kernel: 128 rows per tile, persistent over tiles.  blockDim.x == TILE.
@@ -308,6 +309,9 @@ __global__ void __launch_bounds__(TILE) k_nrc_forward(IO io, const __nv_bfloat16
     const uint32_t lane_addr = tmem + ((warp * 32u) << 16);
     uint32_t n;
     if constexpr (IO::kDebug) n = io.n; else n = min(*io.count, io.cap);
+    if constexpr (!IO::kDebug) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(io.queries, (unsigned long long)n);
+    }
     const uint32_t tiles = (n + TILE - 1) / TILE;
     uint32_t phase = 0;
     bool ok = true;
@@ -373,7 +377,9 @@ __global__ void __launch_bounds__(TILE) k_nrc_forward(IO io, const __nv_bfloat16
 // cores (delta * W row GEMMs and delta^T * input weight-gradient GEMMs), per-tile
 // weight-gradient partials (summed in tile order by the optimizer: deterministic), and
 // the hash-table gradient scattered as fixed-point int64 atomics.  blockDim.x == TILE.
+// Rows i < n of this step are records offset + i * stride (interleaved minibatches).
 __global__ void __launch_bounds__(TILE) k_nrc_train(const float4* __restrict__ rec, const float* __restrict__ target, uint32_t n,
+                                                   uint32_t offset, uint32_t stride,
                                                    float inv_count, const __nv_bfloat16* __restrict__ w, const __half* __restrict__ table,
                                                    float* __restrict__ wgrad_partial, long long* __restrict__ hash_grad,
                                                    float* __restrict__ loss_partial, uint32_t* err) {
@@ -386,10 +392,11 @@ __global__ void __launch_bounds__(TILE) k_nrc_train(const float4* __restrict__ r
     if (threadIdx.x == 0) mbar_init(mbar, 1);
     for (int l = 0; l < LAYERS; ++l) stage_weights(layer_weights(w, l), layer_rows(l), smem + l * W_BYTES);
     const uint32_t i = blockIdx.x * TILE + row;
+    const size_t ri = size_t(offset) + size_t(i) * stride;
     const bool valid = i < n;
     Record r{};
     float v[64];
-    if (valid) { r = load_record(rec, i); encode(r, table, v); }
+    if (valid) { r = load_record(rec, uint32_t(ri)); encode(r, table, v); }
     else for (int k = 0; k < 64; ++k) v[k] = 0.f;
     store_row(tiles, row, v);
     fence_async_smem();
@@ -432,7 +439,7 @@ __global__ void __launch_bounds__(TILE) k_nrc_train(const float4* __restrict__ r
     float loss = 0.f;
     if (valid && ok) {
         for (int c = 0; c < 3; ++c) {
-            const float t = target[3 * size_t(i) + c], d = y[c] - t, den = y[c] * y[c] + LOSS_EPS;
+            const float t = target[3 * ri + c], d = y[c] - t, den = y[c] * y[c] + LOSS_EPS;
             loss += d * d / den;
             g[c] = 2.f * d / den * inv_count;
         }
