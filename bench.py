@@ -139,23 +139,29 @@ def cpu_baseline(config: str, seconds: float = 12.0):
     cam = sc.camera
     threads = os.cpu_count() or 1
     p = Profile.reference_transport(prof.bounces[0], prof.samples, sample_count=1)
-    w, h = 64, 32
-    x0, y0 = cam.width // 2 - w // 2, cam.height // 2 - h // 2
-    o.render(p.c(), x0, y0, 8, 8, fp64=False, threads=threads)  # bakes the oracle's BRDF atlas once
-    t0 = time.perf_counter()
-    o.render(p.c(), x0, y0, w, h, fp64=False, threads=threads)
-    dt = time.perf_counter() - t0
-    # Grow the crop to about `seconds` of work.
-    scale = max(1.0, seconds / max(dt, 1e-3))
-    w2 = min(cam.width, int(w * scale ** 0.5) // 8 * 8 or 8)
-    h2 = min(cam.height, int(h * scale ** 0.5) // 8 * 8 or 8)
-    x0, y0 = cam.width // 2 - w2 // 2, cam.height // 2 - h2 // 2
-    t0 = time.perf_counter()
-    o.render(p.c(), x0, y0, w2, h2, fp64=False, threads=threads)
-    dt = time.perf_counter() - t0
+    x0, y0 = cam.width // 2 - 4, cam.height // 2 - 4
+    o.render(p.c(), x0, y0, 8, 8, fp64=False, threads=threads)  # bakes the oracle's BRDF atlas, starts the threads
+    # Grow the crop, then the samples per pixel once it is the whole frame, until one
+    # measured render takes about `seconds`.
+    w, h, spp = 64, 32, 1
+    for _ in range(8):
+        x0, y0 = cam.width // 2 - w // 2, cam.height // 2 - h // 2
+        p = Profile.reference_transport(prof.bounces[0], prof.samples, sample_count=spp)
+        t0 = time.perf_counter()
+        o.render(p.c(), x0, y0, w, h, fp64=False, threads=threads)
+        dt = time.perf_counter() - t0
+        if dt >= 0.5 * seconds:
+            break
+        scale = min(64.0, seconds / max(dt, 1e-3))
+        w2 = min(cam.width, max(8, int(w * scale ** 0.5) // 8 * 8))
+        h2 = min(cam.height, max(8, int(h * scale ** 0.5) // 8 * 8))
+        spp2 = max(1, min(prof.samples, int(spp * scale * w * h / (w2 * h2))))
+        if (w2, h2, spp2) == (w, h, spp):
+            break
+        w, h, spp = w2, h2, spp2
     o.close()
-    return {"value": w2 * h2 / dt, "unit": "paths/s", "cores": threads, "kind": "port",
-            "sample": f"{w2}x{h2} centre crop of the same frame at 1 spp (of {prof.samples}), depth {prof.bounces[0]}, "
+    return {"value": w * h * spp / dt, "unit": "paths/s", "cores": threads, "kind": "port",
+            "sample": f"{w}x{h} centre crop of the same frame at {spp} spp (of {prof.samples}), depth {prof.bounces[0]}, "
                       f"FP32 C++ restatement, {threads} threads, {dt:.1f} s"}
 
 
@@ -205,18 +211,23 @@ def run_batch(args, device):
     items = [(r.install(sc), Profile.reference_transport(depth, spp)) for sc, spp, depth in jobs]
     paths = sum(i.scene.camera.width * i.scene.camera.height * p.samples for i, p in items)
     tune = r.autotune(items)
+    # Host images written in place by both arms, allocated and touched up front (fresh
+    # pages would add their first-touch faults to whichever arm writes them first).
+    outs = [np.zeros((i.scene.camera.height, i.scene.camera.width, 4), np.float32) for i, _ in items]
     for _ in range(max(1, args.warmup)):
-        r.render_batch(items[: min(8, len(items))])
+        r.render_batch(items, outs=outs)
+        for (inst, prof), o in zip(items[:8], outs):
+            inst.render(prof, out=o)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for inst, prof in items:
-        inst.render(prof)
+    for (inst, prof), o in zip(items, outs):
+        inst.render(prof, out=o)
     seq_s = time.perf_counter() - t0
     t0 = time.perf_counter()
-    _, st = r.render_batch(items)
+    _, st = r.render_batch(items, outs=outs)
     batch_s = time.perf_counter() - t0
     t0 = time.perf_counter()
-    r.render_batch(items, flags=4)  # fair scheduling (one sample of every job per wave)
+    r.render_batch(items, flags=4, outs=outs)  # fair scheduling (one sample of every job per wave)
     fair_s = time.perf_counter() - t0
     line = {"metric": METRIC, "value": paths / batch_s, "unit": "paths/s", "n_gpus": 1, "steps": 1, "warmup": args.warmup,
             "ms_per_step": 1000 * batch_s, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -278,7 +289,9 @@ def run_cache(args, device):
     from vork_b200 import Profile, RadianceCache, Renderer, abi
     from vork_b200.build import build
     build()
-    sc, flock, _, _ = workload("large")
+    from vork_b200 import scene as S
+    w, h = (int(v) for v in args.res.lower().split("x"))
+    sc, flock = S.flock_scene(seed=0, width=w, height=h)
     spp, depth = 16, 8
     frames = frames_for(sc, flock, args.warmup + args.steps)
     cam = sc.camera
@@ -355,7 +368,7 @@ def run_cache(args, device):
     line = {"metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
             "ms_per_step": sum(cached_ms) / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16",
             "data": "synthetic (seeded generator; no dataset)",
-            "config": {"workload": "learned radiance cache: large scene 1920x1080, 16 spp, depth 8, one training round per frame "
+            "config": {"workload": f"learned radiance cache: large scene {w}x{h}, 16 spp, depth 8, one training round per frame "
                                    "(2^16 records, 4 Adam steps) then the cached render (queries at vertex 2); hash grid 16 levels "
                                    "x 2^19 x 2 FP16, 5x64 BF16 MLP, FP32 accumulation", "global_batch": npix * spp,
                        "l2_flush": "inputs > L2: 1M-instance TLAS + 2M-tri BLAS + wavefront queues per frame"},
@@ -392,6 +405,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tlas", choices=["lbvh", "ploc"], default="lbvh", help="TLAS builder of the frame scene")
     ap.add_argument("--no-error", action="store_true", help="cache: skip the reference renders (timing/profiling runs)")
+    ap.add_argument("--res", default="1920x1080", help="cache: frame resolution (smaller for profiling captures)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))

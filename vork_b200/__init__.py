@@ -88,15 +88,17 @@ class Renderer:
                                                     count, stream, abi.uptr(out)))
         return out
 
-    def render_batch(self, items, flags: int = 0):
+    def render_batch(self, items, flags: int = 0, outs=None):
         """Render [(InstalledScene, Profile), ...] together (vkb_render_batch): one shared
-        wavefront, per-job images identical to InstalledScene.render."""
+        wavefront, per-job images identical to InstalledScene.render.  `outs`, when given,
+        are the (H, W, 4) float32 host images to fill (else new ones are made)."""
         n = len(items)
         jobs = (abi.VkbJob * max(1, n))()
         images = []
         for k, (inst, prof) in enumerate(items):
             cam = inst.scene.camera
-            img = np.empty((cam.height, cam.width, 4), np.float32)
+            img = outs[k] if outs is not None else np.empty((cam.height, cam.width, 4), np.float32)
+            assert img.shape == (cam.height, cam.width, 4) and img.dtype == np.float32 and img.flags.c_contiguous
             images.append(img)
             jobs[k].scene = inst.h
             jobs[k].profile = prof.c()
