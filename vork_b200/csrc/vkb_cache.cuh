@@ -270,7 +270,7 @@ vkb_status vkb_cache_train(vkb_cache* k, const vkb_profile* pf, vkb_cache_stats*
         // The wave's radiance is still in place: compact the flagged positions in order
         // and gather records and targets.
         VKB_CUDA(cudaEventRecord(k->ev[0], st));
-        cub::CountingInputIterator<uint32_t> positions(0u);
+        thrust::counting_iterator<uint32_t> positions(0u);
         size_t bytes = 0;
         VKB_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, positions, k->rec_flag.p, k->rec_index.p, k->rec_count.p, int(cap), st));
         k->select_temp.alloc(std::max<size_t>(bytes, 1));
