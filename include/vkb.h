@@ -29,7 +29,7 @@ typedef enum vkb_status {
     VKB_INVALID_ARG = 1,      /* malformed descriptor or profile (failure.rs "scene") */
     VKB_OUT_OF_MEMORY = 2,    /* device allocation refused (gpu_memory.rs device_limit) */
     VKB_DEVICE_TIMEOUT = 3,   /* a bounded device loop or host wait ran out */
-    VKB_NONFINITE = 4,        /* reserved: non-finite scene input */
+    VKB_NONFINITE = 4,        /* non-finite input (an image given to vkb_display) */
     VKB_INTERNAL = 5,         /* CUDA runtime error; message via vkb_last_error() */
     VKB_UNSUPPORTED = 6       /* a profile feature outside the built subset */
 } vkb_status;
@@ -325,6 +325,30 @@ vkb_status vkb_debug_brdf_lut(vkb_ctx* ctx, float* out);
 vkb_status vkb_debug_tlas_morton(vkb_scene* scene, uint32_t* out);
 /* 30-bit Morton codes of one mesh's BLAS build (triangle centroids over the mesh box). */
 vkb_status vkb_debug_blas_morton(vkb_scene* scene, uint32_t mesh, uint32_t* out);
+/* ---- Display stage (crates/vork-render/shaders/resolve.slang:13,140-160 and the std/standard
+ * view, libraries/std/standard.slang:1-33 with libraries/std/view.slang:3-25): linear Rec.709
+ * RGBA (a vkb_render result) -> display code values for an sRGB, Display P3, Rec.2100 PQ or
+ * Rec.2100 HLG destination, quantised to 8 or 16 bits like the resolve stage's unorm store
+ * (no dither, as the reference's Render::dither = false) or returned as float codes. */
+#define VKB_DISPLAY_SRGB 0u
+#define VKB_DISPLAY_P3 1u
+#define VKB_DISPLAY_REC2100_PQ 2u
+#define VKB_DISPLAY_REC2100_HLG 3u
+typedef struct vkb_display_params {
+    uint32_t display;          /* VKB_DISPLAY_* */
+    float exposure;            /* stops (std/standard `exposure`, default 0) */
+    float gamma;               /* creative gamma on the code values (std/standard `gamma`, default 1) */
+    float peak_luminance;      /* Rec.2100 destinations: display peak, cd/m^2 (1000) */
+    float reference_white;     /* Rec.2100 destinations: cd/m^2 of unit scene white (100) */
+    uint32_t bits;             /* 8 (uchar4), 16 (ushort4) or 32 (float4 code values) per pixel */
+    uint32_t unassociate;      /* 1: colour divided by alpha first (resolve.slang:140-145) */
+    uint32_t reserved;
+} vkb_display_params;
+/* width x height RGBA float pixels (host or device) -> `out` (host or device), row-major.
+ * Non-finite input pixels are written as zero and the call returns VKB_NONFINITE. */
+vkb_status vkb_display(vkb_ctx* ctx, const vkb_display_params* params, const float* rgba, int rgba_on_device, uint32_t width,
+                       uint32_t height, void* out, int out_on_device);
+
 /* ---- Learned radiance cache (no reference counterpart: vork has no learned path
  * component).  A multiresolution hash encoding (16 levels x 2^19 entries x 2 FP16
  * features) and a 5-layer, 64-wide BF16 MLP with FP32 accumulation on the tensor cores,

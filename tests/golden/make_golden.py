@@ -4,6 +4,11 @@ reference_kats.json: known answers copied, by parsing the text of the reference'
 tests, from crates/vork-render/src/path_sampler.rs:84-91 (Joe-Kuo dimension-4 direction
 numbers and the first Sobol points in eighths) and
 crates/vork-render/src/environment/brdf_tests.rs:97-104 (BRDF atlas texels).
+display_standard.npz: Blender 5.2.1 "Standard" view samples computed directly by
+OpenColorIO, read from crates/vork-render/data/device-reference.json (family "standard",
+displays Display P3, Rec.2100-PQ and Rec.2100-HLG at 1000 cd/m2 peak, 100 cd/m2 white;
+the reference checks its std/standard view against them in
+crates/vork-render/src/display_program_tests.rs:126-150,205-235).
 sampler_harness.npz: the four sampler groups of the reference's GPU parity harness
 (path_sampler.rs:266-276: 64*47 invocations, index id%300 of 300, pixel
 (id/300*7, id/300*13+1), stream 0x5eed, vertex id%5), computed by the oracle's
@@ -18,6 +23,16 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REF = Path("/root/reference/crates/vork-render/src")
+
+
+def display_kats():
+    data = json.loads((REF.parent / "data" / "device-reference.json").read_text())
+    out = {}
+    for row in data["standard"]:
+        key = row["display"].replace(".", "").replace("-", "_").replace(" ", "_").lower()
+        out[key + "_input"] = np.asarray([s["input"] for s in row["samples"]], np.float64)
+        out[key + "_output"] = np.asarray([s["output"] for s in row["samples"]], np.float64)
+    return out
 
 
 def reference_kats():
@@ -58,4 +73,5 @@ def sampler_harness():
 if __name__ == "__main__":
     (HERE / "reference_kats.json").write_text(json.dumps(reference_kats(), indent=1) + "\n")
     np.savez_compressed(HERE / "sampler_harness.npz", **sampler_harness())
-    print("wrote", HERE / "reference_kats.json", HERE / "sampler_harness.npz")
+    np.savez_compressed(HERE / "display_standard.npz", **display_kats())
+    print("wrote", HERE / "reference_kats.json", HERE / "sampler_harness.npz", HERE / "display_standard.npz")

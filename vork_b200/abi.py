@@ -77,6 +77,12 @@ class VkbCacheStats(C.Structure):
 
 
 NRC_MLP_PARAMS, NRC_HASH_PARAMS = 17408, 16777216
+DISPLAY_SRGB, DISPLAY_P3, DISPLAY_REC2100_PQ, DISPLAY_REC2100_HLG = 0, 1, 2, 3
+
+
+class VkbDisplayParams(C.Structure):
+    _fields_ = [("display", C.c_uint32), ("exposure", C.c_float), ("gamma", C.c_float), ("peak_luminance", C.c_float),
+                ("reference_white", C.c_float), ("bits", C.c_uint32), ("unassociate", C.c_uint32), ("reserved", C.c_uint32)]
 PROFILE_TIME_KERNELS, PROFILE_COUNT_TRAVERSAL = 1, 2
 BATCH_FAIR, BATCH_PACKED = 4, 8
 TLAS_LBVH, TLAS_PLOC = 0, 1
@@ -153,6 +159,7 @@ SIGNATURES = {
     "vkb_debug_trace": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_uint32),
                                   C.POINTER(C.c_float)]),
     "vkb_debug_tlas_stats": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "vkb_display": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_uint32, C.c_void_p, C.c_int]),
     "vkb_cache_create": (C.c_int, [_P, C.c_void_p, C.POINTER(_P)]),
     "vkb_cache_destroy": (C.c_int, [_P]),
     "vkb_cache_train": (C.c_int, [_P, C.POINTER(VkbProfile), C.c_void_p]),

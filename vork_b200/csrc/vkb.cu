@@ -26,6 +26,7 @@
 
 #include "vkb_kernels.cuh"
 #include "vkb_nrc.cuh"
+#include "vkb_display.cuh"
 
 using namespace vkb;
 
@@ -1294,6 +1295,49 @@ vkb_status vkb_scene_info(vkb_scene* s, vkb_scene_info_t* out) {
     dev += s->tlas_nodes.n * sizeof(BvhNode) + s->tlas_leaves.n * sizeof(TlasLeaf) + (s->o2w.n + s->w2o.n) * sizeof(float4);
     out->scene_bytes = dev;
     out->build_ms = s->build_ms;
+    return VKB_OK;
+}
+
+vkb_status vkb_display(vkb_ctx* c, const vkb_display_params* prm, const float* rgba, int rgba_on_device, uint32_t width, uint32_t height,
+                       void* out, int out_on_device) {
+    if (!c || !prm || !rgba || !out) return fail(VKB_INVALID_ARG, "null argument");
+    if (prm->display > VKB_DISPLAY_REC2100_HLG) return fail(VKB_INVALID_ARG, "unknown display");
+    if (prm->bits != 8 && prm->bits != 16 && prm->bits != 32) return fail(VKB_INVALID_ARG, "bits must be 8, 16 or 32");
+    if (!(prm->gamma > 0.f) || !std::isfinite(prm->exposure)) return fail(VKB_INVALID_ARG, "gamma must be positive and exposure finite");
+    if (prm->display >= VKB_DISPLAY_REC2100_PQ && !(prm->peak_luminance > 0.f && prm->reference_white > 0.f))
+        return fail(VKB_INVALID_ARG, "Rec.2100 needs a positive peak luminance and reference white");
+    uint32_t bad = 0;
+    vkb_status st = guarded([&] {
+        VKB_CUDA(cudaSetDevice(c->device));
+        cudaStream_t s = c->stream;
+        const size_t n = size_t(width) * height;
+        if (n == 0) return;
+        const size_t out_bytes = n * (prm->bits / 8u) * 4u;
+        DBuf<float4> in;
+        DBuf<unsigned char> o;
+        DBuf<uint32_t> flag;
+        const float4* src = reinterpret_cast<const float4*>(rgba);
+        if (!rgba_on_device) { in.upload(reinterpret_cast<const float4*>(rgba), n, s); src = in.p; }
+        void* dst = out;
+        if (!out_on_device) { o.alloc(out_bytes); dst = o.p; }
+        flag.alloc(1);
+        VKB_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(uint32_t), s));
+        DisplayParams d;
+        d.display = prm->display; d.bits = prm->bits; d.unassociate = prm->unassociate ? 1u : 0u;
+        d.exposure_scale = std::exp2(prm->exposure); d.inv_gamma = 1.f / prm->gamma;
+        d.peak = prm->peak_luminance > 0.f ? prm->peak_luminance : 1000.f;
+        d.white = prm->reference_white > 0.f ? prm->reference_white : 100.f;
+        const double rel = std::log2(double(d.peak) / 1000.0);
+        d.hlg_gamma = float(d.peak >= 400.f && d.peak <= 2000.f ? 1.2 + .42 * .30102999566 * rel : 1.2 * std::pow(1.111, rel));
+        k_display<<<grid_for(uint32_t(n), 256, c->sms), 256, 0, s>>>(uint32_t(n), src, d, dst, flag.p);
+        VKB_CUDA(cudaGetLastError());
+        if (!out_on_device) VKB_CUDA(cudaMemcpyAsync(out, o.p, out_bytes, cudaMemcpyDeviceToHost, s));
+        VKB_CUDA(cudaMemcpyAsync(&bad, flag.p, sizeof(bad), cudaMemcpyDeviceToHost, s));
+        VKB_CUDA(cudaStreamSynchronize(s));
+        c->launches += 1;
+    });
+    if (st != VKB_OK) return st;
+    if (bad) return fail(VKB_NONFINITE, "non-finite pixels were written as zero");
     return VKB_OK;
 }
 
