@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define VKB_ABI_VERSION 3u
+#define VKB_ABI_VERSION 4u
 
 /* Error model: FailureKind exit categories of crates/vork-render/src/failure.rs:21-100,
  * reduced to what a render call can report. */
@@ -146,9 +146,11 @@ typedef struct vkb_profile {
     float clamp_direct;        /* clamp.x (0 = off) */
     float clamp_indirect;      /* clamp.y (0 = off) */
     float light_threshold;     /* adaptive.z: stochastic light-sample kill */
-    uint32_t adaptive;         /* must be 0: adaptive stopping is outside the built subset */
-    uint32_t wave_samples;     /* samples per wavefront wave (0 = automatic) */
+    uint32_t adaptive;         /* 1: adaptive stopping (path.slang:1792-1837), vkb_render of a whole exposure only */
+    uint32_t wave_samples;     /* samples per wavefront wave (0 = automatic; 1 with adaptive stopping) */
     uint32_t flags;            /* VKB_PROFILE_* measurement switches (0 for production renders) */
+    float adaptive_threshold;  /* adaptive.x: relative standard error to stop at (0 = 0.01) */
+    uint32_t adaptive_min_samples; /* sampling.w: samples before stopping (0 = max(16, sqrt(samples))) */
 } vkb_profile;
 
 /* Measurement switches of vkb_profile.flags (no reference counterpart: timing hooks). */
@@ -188,6 +190,7 @@ typedef struct vkb_stats {
     uint64_t blas_nodes_visited;   /* closest-hit node visits inside instance BLASes (the rest are TLAS) */
     float cache_ms;            /* VKB_PROFILE_TIME_KERNELS, vkb_render_cached: radiance-cache query kernel time */
     uint64_t cache_queries;    /* vkb_render_cached: paths answered by the radiance cache */
+    uint64_t samples_skipped;  /* adaptive stopping: pixel samples not traced (stopped pixels) */
 } vkb_stats;
 
 typedef struct vkb_ctx vkb_ctx;

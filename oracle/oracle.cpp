@@ -1396,8 +1396,102 @@ template <class R> V3<R> integrate(Ctx<R>& cx, uint32_t px, uint32_t py, uint32_
 
 struct OracleScene { void* s32 = nullptr; void* s64 = nullptr; };
 
+// Adaptive stopping (path.slang:1792-1837, 1963-1966), sample-major over the whole image:
+// per pixel Welford moments of the RGBA sample values (a dropped sample is zero RGBA),
+// settled once every channel's standard error of the mean is within threshold x
+// max(|mean|, 0.01) from the minimum sample on, stopped once it and its 3x3
+// neighbourhood were settled at the previous sample; a stopped pixel adds its mean to
+// the accumulator for the remaining samples.  Arithmetic in float, as the shader's.
+template <class R> void render_adaptive(const Scene<R>& s, const vkb_profile& pf, uint32_t w, uint32_t h, float* rgba, uint32_t threads,
+                                        uint64_t* stats) {
+    const uint32_t n = w * h, count = pf.samples;
+    const float thr = pf.adaptive_threshold > 0.f ? pf.adaptive_threshold : 0.01f;
+    const uint32_t minimum = pf.adaptive_min_samples ? pf.adaptive_min_samples : std::max(16u, uint32_t(std::sqrt(float(pf.samples))));
+    std::vector<float> mean(4 * size_t(n), 0.f), m2(4 * size_t(n), 0.f);
+    std::vector<double> sum(3 * size_t(n), 0.0);
+    std::vector<uint32_t> state(n, 0u);
+    std::vector<uint8_t> skip(n, 0);
+    std::mutex mu;
+    for (uint32_t i = 0; i < count; ++i) {
+        // Decide (reads neighbours' previous parity bit only).
+        std::vector<uint32_t> next = state;
+        for (uint32_t p = 0; p < n; ++p) {
+            uint32_t st = state[p];
+            if (st & 4u) { skip[p] = 1; continue; }
+            skip[p] = 0;
+            bool settled = false;
+            if (i >= minimum) {
+                const float a1 = float(std::max(i - 1u, 1u)), a2 = float(i);
+                settled = true;
+                for (int c = 0; c < 4; ++c) {
+                    const float e = std::sqrt(std::max(m2[4 * size_t(p) + c] / a1 / a2, 0.f));
+                    settled = settled && e <= thr * std::max(std::fabs(mean[4 * size_t(p) + c]), .01f);
+                }
+            }
+            const uint32_t bit = 1u << (i & 1u), prev = 1u << ((i & 1u) ^ 1u);
+            bool done = settled;
+            const int x = int(p % w), y = int(p / w);
+            for (int dy = -1; dy <= 1 && done; ++dy)
+                for (int dx = -1; dx <= 1 && done; ++dx) {
+                    const int nx = std::min(std::max(x + dx, 0), int(w) - 1), ny = std::min(std::max(y + dy, 0), int(h) - 1);
+                    done = (state[size_t(ny) * w + size_t(nx)] & prev) != 0u;
+                }
+            st = settled ? (st | bit) : (st & ~bit);
+            if (done) { st |= 4u; skip[p] = 1; }
+            next[p] = st;
+        }
+        state.swap(next);
+        // Trace the live pixels of this sample.
+        std::atomic<uint32_t> row{0};
+        auto work = [&] {
+            Ctx<R> cx{s, pf};
+            for (uint32_t y; (y = row.fetch_add(1)) < h;)
+                for (uint32_t x = 0; x < w; ++x) {
+                    const size_t p = size_t(y) * w + x;
+                    float* m = &mean[4 * p];
+                    if (skip[p]) { for (int c = 0; c < 3; ++c) sum[3 * p + c] += m[c]; continue; }
+                    const uint64_t before = cx.dropped_path;
+                    const V3<R> v = integrate(cx, x, y, i, nullptr);
+                    const float val[4] = {float(v.x), float(v.y), float(v.z), cx.dropped_path != before ? 0.f : 1.f};
+                    for (int c = 0; c < 3; ++c) sum[3 * p + c] += val[c];
+                    float* q = &m2[4 * p];
+                    const float inv = 1.f / float(i + 1u);
+                    for (int c = 0; c < 4; ++c) {
+                        const float d = val[c] - m[c];
+                        m[c] = m[c] + d * inv;
+                        q[c] += d * (val[c] - m[c]);
+                    }
+                }
+            std::lock_guard<std::mutex> g(mu);
+            if (stats) { stats[0] += cx.ext_rays; stats[1] += cx.shadow_rays; stats[2] += cx.dropped_path; stats[3] += cx.dropped_light; }
+        };
+        if (threads <= 1) work();
+        else {
+            std::vector<std::thread> ts;
+            for (uint32_t t = 0; t < threads; ++t) ts.emplace_back(work);
+            for (auto& t : ts) t.join();
+        }
+    }
+    for (uint32_t p = 0; p < n; ++p) {
+        float* o = rgba + 4 * size_t(p);
+        for (int c = 0; c < 3; ++c) o[c] = float(sum[3 * size_t(p) + c] / double(count));
+        o[3] = 1.f;
+    }
+}
+
 template <class R> void render_impl(const Scene<R>& s, const vkb_profile& pf, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,
                                     float* rgba, uint32_t* ids, uint32_t threads, uint64_t* stats) {
+    if (pf.adaptive) {
+        // Whole image, whole exposure: the stop rule reads image-edge-clamped neighbours.
+        if (x0 != 0 || y0 != 0 || w != s.cam.width || h != s.cam.height || pf.first_sample != 0 ||
+            (pf.sample_count && pf.sample_count != pf.samples))
+        {   // refused (pyoracle checks first): the image reads NaN
+            for (size_t k = 0; k < size_t(w) * h * 4; ++k) rgba[k] = std::numeric_limits<float>::quiet_NaN();
+            return;
+        }
+        render_adaptive(s, pf, w, h, rgba, threads, stats);
+        return;
+    }
     uint32_t first = pf.first_sample, count = pf.sample_count ? pf.sample_count : pf.samples - pf.first_sample;
     std::atomic<uint32_t> next{0};
     std::mutex mu;

@@ -160,6 +160,9 @@ class OracleScene:
         cam = self.scene.camera
         w = cam.width if w is None else w
         h = cam.height if h is None else h
+        if profile.adaptive and ((x0, y0, w, h) != (0, 0, cam.width, cam.height) or profile.first_sample
+                                 or profile.sample_count not in (0, profile.samples)):
+            raise ValueError("the adaptive oracle renders a whole image and a whole exposure")
         threads = threads or os.cpu_count() or 1
         out = np.zeros((h, w, 4), np.float32)
         idbuf = np.zeros((h, w, 2), np.uint32) if ids else None

@@ -163,9 +163,10 @@ def test_tiny_scenes_and_errors(renderer):
     with renderer.install(sc) as s:
         img = s.render(Profile.reference_transport(4, 4)).image
         assert np.isfinite(img).all() and img[..., :3].max() > 0
-        with pytest.raises(abi.VkbError) as e:
-            s.render(Profile(samples=4, adaptive=True))
+        with pytest.raises(abi.VkbError) as e:     # adaptive stopping needs the whole exposure
+            s.render(Profile(samples=4, adaptive=True, first_sample=1))
         assert e.value.status == abi.VKB_UNSUPPORTED
+        assert np.isfinite(s.render(Profile(samples=4, adaptive=True)).image).all()
         with pytest.raises(abi.VkbError):
             s.render(Profile(samples=4, first_sample=9))
     bad = S.Scene([tri], S.rows_from(1.0, (0, 0, 0))[None], np.array([3], np.uint32), np.zeros(1, np.uint32), [S.material()],
@@ -256,3 +257,31 @@ def test_tlas_over_coincident_and_clustered_instances(renderer, oracle, builder)
     assert both.sum() > 1000
     rel = np.abs(t[both] - t_ref[both]) / np.maximum(t_ref[both], 1e-3)
     assert np.mean(rel > 1e-4) <= 2e-3
+
+
+def test_adaptive_stopping_matches_the_oracle(renderer, oracle):
+    # path.slang:1792-1837: per-sample stopping with the 3x3 rule, whole image; the GPU
+    # (one sample per wave) and the FP32 oracle (sample-major) take the same decisions up
+    # to float differences in the moments, so the traced work and the image agree closely.
+    sc = S.spheres_scene(width=96, height=96)
+    prof = Profile.reference_transport(4, 64, adaptive=True, adaptive_threshold=0.05)
+    o = oracle.OracleScene(sc, fp32=True, fp64=False)
+    ref, st_ref = o.render(prof.c(), fp64=False)
+    with renderer.install(sc) as s:
+        res = s.render(prof)
+        plain = s.render(Profile.reference_transport(4, 64))
+        again = s.render(prof)
+    assert np.array_equal(res.image, again.image)
+    st = res.stats
+    assert st["samples_skipped"] > 0.05 * 96 * 96 * 64
+    assert abs(st["extension_rays"] / st_ref["extension_rays"] - 1) < 0.02
+    assert st["extension_rays"] < plain.stats["extension_rays"]
+    m, mr = res.image[..., :3].mean((0, 1)), ref[..., :3].mean((0, 1))
+    assert np.all(np.abs(m / mr - 1) < 0.01), (m, mr)
+    with pytest.raises(abi.VkbError) as e:
+        s2 = renderer.install(sc)
+        try:
+            s2.render(Profile.reference_transport(4, 64, adaptive=True, first_sample=8))
+        finally:
+            s2.close()
+    assert e.value.status == abi.VKB_UNSUPPORTED

@@ -35,6 +35,8 @@ class Profile:
     clamp_indirect: float = 10.0
     light_threshold: float = 0.01
     adaptive: bool = False
+    adaptive_threshold: float = 0.0
+    adaptive_min_samples: int = 0
     first_sample: int = 0
     sample_count: int = 0
     wave_samples: int = 0
@@ -52,6 +54,7 @@ class Profile:
         p.transparent, p.caustics = self.transparent, self.caustics
         p.clamp_direct, p.clamp_indirect, p.light_threshold = self.clamp_direct, self.clamp_indirect, self.light_threshold
         p.adaptive = 1 if self.adaptive else 0
+        p.adaptive_threshold, p.adaptive_min_samples = self.adaptive_threshold, self.adaptive_min_samples
         p.wave_samples = self.wave_samples
         p.flags = self.flags
         return p

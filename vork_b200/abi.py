@@ -63,7 +63,8 @@ class VkbProfile(C.Structure):
     _fields_ = [("samples", C.c_uint32), ("first_sample", C.c_uint32), ("sample_count", C.c_uint32), ("seed", C.c_uint32),
                 ("bounces", C.c_uint32 * 4), ("transparent", C.c_uint32), ("caustics", C.c_uint32),
                 ("clamp_direct", C.c_float), ("clamp_indirect", C.c_float), ("light_threshold", C.c_float),
-                ("adaptive", C.c_uint32), ("wave_samples", C.c_uint32), ("flags", C.c_uint32)]
+                ("adaptive", C.c_uint32), ("wave_samples", C.c_uint32), ("flags", C.c_uint32),
+                ("adaptive_threshold", C.c_float), ("adaptive_min_samples", C.c_uint32)]
 
 
 class VkbCacheConfig(C.Structure):
@@ -100,7 +101,8 @@ class VkbStats(C.Structure):
                 ("trace_ms", C.c_float), ("trace_launches", C.c_uint32), ("kernel_launches", C.c_uint32),
                 ("nodes_visited", C.c_uint64), ("triangles_tested", C.c_uint64), ("instances_entered", C.c_uint64),
                 ("shadow_nodes_visited", C.c_uint64), ("shadow_triangles_tested", C.c_uint64),
-                ("blas_nodes_visited", C.c_uint64), ("cache_ms", C.c_float), ("cache_queries", C.c_uint64)]
+                ("blas_nodes_visited", C.c_uint64), ("cache_ms", C.c_float), ("cache_queries", C.c_uint64),
+                ("samples_skipped", C.c_uint64)]
 
 
 class VkbJob(C.Structure):

@@ -409,6 +409,8 @@ struct vkb_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<cudaEvent_t> kernel_events;
     std::vector<cudaEvent_t> cache_events;    // timed renders: around each radiance-cache query launch
+    DBuf<float4> ad_mean, ad_m2;              // adaptive stopping: per-pixel moments
+    DBuf<uint32_t> ad_state;                  // and parity/stop bits
 };
 
 struct vkb_scene {
@@ -575,6 +577,9 @@ struct EngineJob {
     vkb_profile pf{};
     bool own_camera = false;        // render through `camera` instead of the scene's
     vkb_camera camera{};
+    float4* ad_mean = nullptr;      // adaptive stopping: per-pixel moments and state
+    float4* ad_m2 = nullptr;
+    uint32_t* ad_state = nullptr;
     float4* out_dev = nullptr;      // device destination of the mean image
     uint32_t* ids_dev = nullptr;    // device primary ids (first sample) or null
     float4* accum = nullptr;        // device accumulator, npix
@@ -589,7 +594,8 @@ struct WaveTotals {
 };
 
 void validate_profile(const vkb_profile* pf) {
-    if (pf->adaptive) throw Unsupported{"adaptive sampling is outside the built subset"};
+    if (pf->adaptive > 1u) throw ArgError{"adaptive must be 0 or 1"};
+    if (pf->adaptive && !(pf->adaptive_threshold >= 0.f)) throw ArgError{"adaptive_threshold must be non-negative"};
     if (pf->samples == 0) throw ArgError{"samples must be positive"};
     if (pf->first_sample >= pf->samples) throw ArgError{"first_sample beyond samples"};
     uint32_t count = pf->sample_count ? pf->sample_count : pf->samples - pf->first_sample;
@@ -617,6 +623,10 @@ Job make_job(const EngineJob& e) {
     j.npix = e.npix; j.first_sample = pf.first_sample;
     j.pixel_base = e.pixel_base;
     j.accum = e.accum; j.primary_ids = e.ids_dev; j.out = e.out_dev;
+    j.adaptive = (pf.adaptive && e.ad_state) ? 1u : 0u;   // only where the caller gave it moment buffers
+    j.adaptive_threshold = pf.adaptive_threshold > 0.f ? pf.adaptive_threshold : 0.01f;
+    j.adaptive_min = pf.adaptive_min_samples ? pf.adaptive_min_samples : std::max(16u, uint32_t(std::sqrt(float(pf.samples))));
+    j.ad_mean = e.ad_mean; j.ad_m2 = e.ad_m2; j.ad_state = e.ad_state;
     return j;
 }
 
@@ -648,7 +658,9 @@ void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counte
                   const CacheLaunch* cache = nullptr) {
     cudaStream_t st = c->stream;
     const int sms = c->sms, tgrid = sms * c->trace_blocks_per_sm, sgrid = sms * c->trace_blocks_per_sm;
-    k_start_wave<<<1, 1, 0, st>>>(p.counters);
+    const bool adaptive = !BATCH && p.job0.adaptive;
+    if (adaptive) k_adaptive_decide<<<grid_for(p.job0.npix, 256, sms), 256, 0, st>>>(p);
+    k_start_wave<<<1, 1, 0, st>>>(p.counters, adaptive ? 1u : 0u);
     k_camera<BATCH><<<sms * 8, 256, 0, st>>>(p);
     for (uint32_t b = 0; b <= bounces; ++b) {
         int cur = int(b & 1u);
@@ -685,7 +697,7 @@ void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counte
         tot.launches += 1;
     }
     k_accumulate<BATCH><<<sms * 8, 256, 0, st>>>(p);
-    tot.launches += 3 + 4 * (bounces + 1);
+    tot.launches += 3 + 4 * (bounces + 1) + (adaptive ? 1 : 0);
 }
 
 // A wavefront that runs jobs wave by wave.  Each wave gives one sample to every
@@ -911,6 +923,7 @@ void fill_stats(vkb_stats* stats, const WaveTotals& t, uint64_t paths, float bui
     stats->blas_nodes_visited = t.work[5];
     stats->cache_ms = t.cache_ms;
     stats->cache_queries = t.work[7];
+    stats->samples_skipped = t.counters[10];
 }
 
 // Render jobs with the context's own buffers (grown on demand).
@@ -924,6 +937,19 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
         total_pixels += npix; max_pix = std::max(max_pix, npix);
         if (outs[k]->primary_ids) ids_words += 2 * npix;
         if (!outs[k]->on_device) staged += npix;
+    }
+    bool adaptive = false;
+    for (const auto& job : in) adaptive = adaptive || job.second.adaptive;
+    if (adaptive) {
+        // path.slang stops pixels sample by sample against their neighbours' previous
+        // sample: one job, one sample per wave, the whole exposure in this call.
+        const vkb_profile& pf = in[0].second;
+        if (in.size() != 1 || cache) throw Unsupported{"adaptive stopping renders one job through vkb_render"};
+        if (pf.first_sample != 0 || (pf.sample_count && pf.sample_count != pf.samples))
+            throw Unsupported{"adaptive stopping renders a whole exposure (first_sample 0, every sample)"};
+        wave_samples_hint = 1;
+        c->ad_mean.alloc(max_pix); c->ad_m2.alloc(max_pix); c->ad_state.alloc(max_pix);
+        VKB_CUDA(cudaMemsetAsync(c->ad_state.p, 0, max_pix * sizeof(uint32_t), st));
     }
     size_t capacity = c->wave_capacity;
     if (in.size() == 1 && wave_samples_hint) capacity = max_pix * wave_samples_hint;
@@ -943,6 +969,7 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
         if (outs[k]->on_device) e.out_dev = reinterpret_cast<float4*>(outs[k]->rgba);
         else { e.out_dev = c->staging.p + stg; stg += e.npix; }
         if (outs[k]->primary_ids) { e.ids_dev = c->ids.p + idw; idw += 2 * size_t(e.npix); }
+        if (adaptive) { e.ad_mean = c->ad_mean.p; e.ad_m2 = c->ad_m2.p; e.ad_state = c->ad_state.p; }
         paths += uint64_t(e.npix) * e.count;
     }
     run_engine(c, jobs, c->wave.view(), capacity, flags, true, tot, (flags & VKB_BATCH_FAIR) == 0, cache);
@@ -992,7 +1019,7 @@ vkb_status vkb_close(vkb_ctx* c) {
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     c->wave.release();
-    c->accum.release(); c->staging.release(); c->ids.release();
+    c->accum.release(); c->staging.release(); c->ids.release(); c->ad_mean.release(); c->ad_m2.release(); c->ad_state.release();
     c->lut.release(); c->filter.release();
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -1235,6 +1262,7 @@ vkb_status vkb_autotune(vkb_ctx* c, vkb_job* jobs, uint32_t njobs, vkb_tune_resu
             vkb_profile pf = jobs[k].profile;
             validate_profile(&pf);
             pf.sample_count = 1;
+            pf.adaptive = 0;   // timing one sample of every job
             in[k] = {jobs[k].scene, pf};
             max_pix = std::max(max_pix, size_t(jobs[k].scene->camera.width) * jobs[k].scene->camera.height);
         }
@@ -1557,6 +1585,7 @@ vkb_status vkb_server_submit(vkb_server* v, vkb_scene* s, const vkb_profile* pf,
     if (s->ctx != v->c) return fail(VKB_INVALID_ARG, "scene belongs to another context");
     return guarded([&] {
         validate_profile(pf);
+        if (pf->adaptive) throw Unsupported{"adaptive stopping renders through vkb_render"};
         uint64_t need = uint64_t(s->camera.width) * s->camera.height * 32u;
         if (v->budget && v->wave_bytes + scene_bytes(s) + need > v->budget) throw ArgError{"request can never fit the memory budget"};
         *id = v->next_id++;
@@ -1697,6 +1726,7 @@ extern "C" vkb_status vkb_render_noalloc(vkb_scene* s, const vkb_profile* pf, vk
     if (!s || !pf || !out || !out->rgba) return fail(VKB_INVALID_ARG, "null scene, profile or output");
     return guarded([&] {
         validate_profile(pf);
+        if (pf->adaptive) throw Unsupported{"adaptive stopping renders through vkb_render"};
         uint32_t count = pf->sample_count ? pf->sample_count : pf->samples - pf->first_sample;
         vkb_ctx* c = s->ctx;
         VKB_CUDA(cudaSetDevice(c->device));

@@ -247,7 +247,7 @@ vkb_status vkb_cache_train(vkb_cache* k, const vkb_profile* pf, vkb_cache_stats*
         std::vector<EngineJob> jobs(1);
         EngineJob& e = jobs[0];
         e.s = s; e.pf = *pf;
-        e.pf.samples = 1; e.pf.first_sample = 0; e.pf.sample_count = 1; e.pf.wave_samples = 1;
+        e.pf.samples = 1; e.pf.first_sample = 0; e.pf.sample_count = 1; e.pf.wave_samples = 1; e.pf.adaptive = 0;
         e.pf.seed = pf->seed ^ (0x9e3779b9u * uint32_t(k->train_calls + 1) + k->cfg.seed);
         e.own_camera = true; e.camera = cam; e.camera.width = tw; e.camera.height = th;
         e.npix = tw * th; e.count = 1;

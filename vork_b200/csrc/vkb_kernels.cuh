@@ -344,7 +344,14 @@ struct Job {
     uint32_t npix, first_sample;
     uint32_t wave_first, wave_samples, slot_base, pixel_base;  // this wave
     float4* accum; uint32_t* primary_ids; float4* out;
+    // Adaptive sampling (path.slang:1792-1837,1963-1966): per-pixel moments (mean, M2 of
+    // the accumulated RGBA values) and a state word (bit 0/1: settled at an even/odd
+    // sample, bit 2: stopped); one sample per wave.
+    uint32_t adaptive, adaptive_min;
+    float adaptive_threshold;
+    float4* ad_mean; float4* ad_m2; uint32_t* ad_state;
 };
+constexpr uint32_t AD_STOPPED = 4u;
 // Radiance-cache hooks of a wave.  mode 1 (query): a path reaching vertex `vertex`
 // (0 = camera hit) appends a cache record (counters[9] counts them, `capacity` bounds
 // them) and stops; the query kernel adds throughput x the cached outgoing radiance.
@@ -372,7 +379,7 @@ struct PathParams {
     float4* sb_o; float4* sb_d; float4* sb_c;
     // [0],[1] ray counts, [2] shadow count, [3] ext rays, [4] shadow rays, [5] dropped light,
     // [6] dropped paths, [7] path slots of this wave, [8] pixels of this wave's jobs
-    // [9] radiance-cache records of this wave
+    // [9] radiance-cache records of this wave, [10] adaptive pixel-samples skipped
     uint32_t* counters;
     unsigned long long* work;  // instrumented traversal: closest nodes, tris, instances, blas nodes; shadow nodes, tris, blas nodes
     uint32_t* err;
@@ -432,11 +439,25 @@ __global__ void k_camera(PathParams p) {
         float near_d = J.cam.near_plane / dot(dir, fwd), far_d = J.cam.far_plane / dot(dir, fwd);
         float3 o = eye + dir * near_d;
         float tmax = fminf(FP32_MAX, fmaxf(0.f, far_d - length(o - eye)));
-        p.ray_o[0][slot] = make_float4(o.x, o.y, o.z, tmax);
-        p.ray_d[0][slot] = make_float4(dir.x, dir.y, dir.z, __uint_as_float(slot));
         p.thr[slot] = make_float4(1.f, 1.f, 1.f, __uint_as_float(0u));
         p.rad[slot] = make_float4(0.f, 0.f, 0.f, __uint_as_float(0u));
         p.rng[slot] = make_uint2(rng, pseed);
+        if (!BATCH && J.adaptive) {
+            // Stopped pixels trace nothing: the camera rays of the others are compacted.
+            const bool live = (J.ad_state[pixel] & AD_STOPPED) == 0u;
+            namespace cg = cooperative_groups;
+            if (live) {
+                cg::coalesced_group g = cg::coalesced_threads();
+                uint32_t base = 0;
+                if (g.thread_rank() == 0) base = atomicAdd(&p.counters[0], g.size());
+                const uint32_t ri = g.shfl(base, 0) + g.thread_rank();
+                p.ray_o[0][ri] = make_float4(o.x, o.y, o.z, tmax);
+                p.ray_d[0][ri] = make_float4(dir.x, dir.y, dir.z, __uint_as_float(slot));
+            }
+            continue;
+        }
+        p.ray_o[0][slot] = make_float4(o.x, o.y, o.z, tmax);
+        p.ray_d[0][slot] = make_float4(dir.x, dir.y, dir.z, __uint_as_float(slot));
     }
 }
 __device__ __forceinline__ void flush_count(unsigned long long* dst, uint32_t v) {
@@ -791,7 +812,52 @@ __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
     }
 }
 // Seed the first ray queue's count from the wave's path-slot count.
-__global__ void k_start_wave(uint32_t* counters) { counters[0] = counters[7]; counters[9] = 0u; }
+__global__ void k_start_wave(uint32_t* counters, uint32_t append_camera) {
+    counters[0] = append_camera ? 0u : counters[7];
+    counters[9] = 0u;
+}
+// Adaptive sampling, before the wave of sample index i = wave_first (path.slang:1797-1835):
+// reset at i = 0; from the minimum on a pixel is settled when every channel's standard
+// error of the mean is within threshold x max(|mean|, 0.01); it publishes that in its
+// parity slot (i & 1) and stops once it and its whole 3x3 neighbourhood were settled at
+// the previous sample (slot (i & 1) ^ 1, which nothing writes during this kernel).
+__global__ void k_adaptive_decide(PathParams p) {
+    const Job& J = p.job0;
+    const uint32_t i = J.wave_first, w = J.cam.width, h = J.cam.height;
+    uint32_t skipped = 0;
+    for (uint32_t px = blockIdx.x * blockDim.x + threadIdx.x; px < J.npix; px += gridDim.x * blockDim.x) {
+        uint32_t st = J.ad_state[px];
+        if (i == 0u) {
+            st &= ~AD_STOPPED;
+            J.ad_mean[px] = make_float4(0.f, 0.f, 0.f, 0.f);
+            J.ad_m2[px] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        if (st & AD_STOPPED) { ++skipped; continue; }
+        bool settled = false;
+        if (i >= J.adaptive_min) {
+            const float4 m = J.ad_mean[px], v = J.ad_m2[px];
+            const float a1 = float(max(i - 1u, 1u)), a2 = float(i);
+            const float e[4] = {sqrtf(fmaxf(v.x / a1 / a2, 0.f)), sqrtf(fmaxf(v.y / a1 / a2, 0.f)), sqrtf(fmaxf(v.z / a1 / a2, 0.f)),
+                                sqrtf(fmaxf(v.w / a1 / a2, 0.f))};
+            const float a[4] = {m.x, m.y, m.z, m.w};
+            settled = true;
+            for (int c = 0; c < 4; ++c) settled = settled && e[c] <= J.adaptive_threshold * fmaxf(fabsf(a[c]), .01f);
+        }
+        const uint32_t bit = 1u << (i & 1u), prev = 1u << ((i & 1u) ^ 1u);
+        bool done = settled;
+        const int x = int(px % w), y = int(px / w);
+        for (int dy = -1; dy <= 1 && done; ++dy)
+            for (int dx = -1; dx <= 1 && done; ++dx) {
+                const int nx = min(max(x + dx, 0), int(w) - 1), ny = min(max(y + dy, 0), int(h) - 1);
+                done = (J.ad_state[uint32_t(ny) * w + uint32_t(nx)] & prev) != 0u;
+            }
+        st = settled ? (st | bit) : (st & ~bit);
+        if (done) { st |= AD_STOPPED; ++skipped; }
+        J.ad_state[px] = st;   // neighbours read only the other parity bit of this word
+    }
+    for (int off = 16; off > 0; off >>= 1) skipped += __shfl_xor_sync(0xffffffffu, skipped, off);
+    if ((threadIdx.x & 31u) == 0u && skipped) atomicAdd(&p.counters[10], skipped);
+}
 // Zero the next ray queue and the shadow queue before a shade pass.
 __global__ void k_reset_queues(uint32_t* counters, int nxt) { counters[nxt] = 0u; counters[2] = 0u; }
 // resolve.slang:162-191: add this wave's finished samples to each job's accumulator,
@@ -805,6 +871,30 @@ __global__ void k_accumulate(PathParams p) {
         if (pixel >= J.npix || J.wave_samples == 0) continue;
         float4 sum = J.accum[pixel];
         uint32_t dl = 0, dp = 0;
+        if (!BATCH && J.adaptive) {
+            // One sample per wave: a stopped pixel adds its stopped mean; a live one its
+            // value, which also updates its moments (Welford, path.slang:1963-1965; a
+            // dropped non-finite sample is the zero RGBA value).
+            const uint32_t slot = J.slot_base + pixel;
+            const float4 m = J.ad_mean[pixel];
+            if (J.ad_state[pixel] & AD_STOPPED) {
+                sum.x += m.x; sum.y += m.y; sum.z += m.z; sum.w += 1.f;
+            } else {
+                float4 T = p.thr[slot], R = p.rad[slot];
+                dl += __float_as_uint(R.w);
+                float3 v = f3(R.x, R.y, R.z) * J.env.exposure;
+                float alpha = 1.f;
+                if ((__float_as_uint(T.w) & META_NONFINITE) || !finite3(v)) { v = f3(0.f); alpha = 0.f; dp++; }
+                sum.x += v.x; sum.y += v.y; sum.z += v.z; sum.w += 1.f;
+                const float inv = 1.f / float(J.wave_first + 1u);
+                const float4 d = make_float4(v.x - m.x, v.y - m.y, v.z - m.z, alpha - m.w);
+                const float4 nm = make_float4(m.x + d.x * inv, m.y + d.y * inv, m.z + d.z * inv, m.w + d.w * inv);
+                float4 m2 = J.ad_m2[pixel];
+                m2.x += d.x * (v.x - nm.x); m2.y += d.y * (v.y - nm.y); m2.z += d.z * (v.z - nm.z); m2.w += d.w * (alpha - nm.w);
+                J.ad_mean[pixel] = nm;
+                J.ad_m2[pixel] = m2;
+            }
+        } else
         for (uint32_t k = 0; k < J.wave_samples; ++k) {
             uint32_t slot = J.slot_base + k * J.npix + pixel;
             float4 T = p.thr[slot], R = p.rad[slot];
