@@ -263,7 +263,8 @@ def run_serve(args, device):
     results = []
     for i, rate in enumerate(float(x) for x in args.rates.split(",")):
         reqs = request_mix(args.requests, len(scenes), seed=i, frames=24, spp_range=(8, 128), bounces=8)
-        with Server(r, memory_budget_bytes=160 << 30, max_jobs=256) as srv:
+        flags = {"srpt": 0, "fair": 4, "packed": 8}[args.schedule]
+        with Server(r, memory_budget_bytes=160 << 30, max_jobs=256, flags=flags) as srv:
             results.append(poisson_load(srv, scenes, reqs, rate=rate, seed=i, timeout_s=900))
     best = max(results, key=lambda x: x["throughput_paths_s"])
     line = {"metric": METRIC, "value": best["throughput_paths_s"], "unit": "paths/s", "n_gpus": 1, "steps": len(results),
@@ -271,7 +272,7 @@ def run_serve(args, device):
             "dtype": "f32", "data": "synthetic (seeded generator; no dataset)",
             "config": {"workload": f"serving: {args.requests} requests per rate, rates {args.rates} req/s, 80% stills / 20% 24-frame "
                                    "sequences, spp U{8..128}, 5 resident scenes (4 sphere scenes 256..1080 lines, 1M-instance flock "
-                                   "at 640x360), 160 GB budget, continuous batching"},
+                                   f"at 640x360), 160 GB budget, continuous batching, {args.schedule} wave schedule"},
             "latency": results}
     print(json.dumps(line), flush=True)
     for s in scenes:
@@ -406,6 +407,7 @@ def main():
     ap.add_argument("--tlas", choices=["lbvh", "ploc"], default="lbvh", help="TLAS builder of the frame scene")
     ap.add_argument("--no-error", action="store_true", help="cache: skip the reference renders (timing/profiling runs)")
     ap.add_argument("--res", default="1920x1080", help="cache: frame resolution (smaller for profiling captures)")
+    ap.add_argument("--schedule", default="srpt", choices=["srpt", "fair", "packed"], help="serve: wave schedule")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))

@@ -158,8 +158,9 @@ typedef struct vkb_profile {
 #define VKB_PROFILE_COUNT_TRAVERSAL 2u     /* instrumented traversal: node and triangle visits */
 /* Wave scheduling of several jobs (vkb_render_batch flags / vkb_server_config.flags):
  * batches pack each job's remaining samples before the next job (throughput: fewer
- * scenes per wave keep their BVHs in L2) unless VKB_BATCH_FAIR; servers give every
- * admitted request a sample per wave (latency) unless VKB_BATCH_PACKED. */
+ * scenes per wave keep their BVHs in L2) unless VKB_BATCH_FAIR; servers give the waves to
+ * the admitted requests with the least remaining work first (latency), or one sample of
+ * every request per wave with VKB_BATCH_FAIR, or pack like batches with VKB_BATCH_PACKED. */
 #define VKB_BATCH_FAIR 4u
 #define VKB_BATCH_PACKED 8u
 

@@ -716,10 +716,11 @@ struct WaveEngine {
     std::vector<Job> wave_table;        // the jobs of the current wave (uploaded)
     WaveTotals tot;
     std::vector<GraphEntry> captured;   // this engine's wave graphs (they point at its buffers)
-    // Scheduling: fair (one sample of every unfinished job per wave, then more: serving
-    // latency) or packed (each job's remaining samples before the next job: fewer scenes
-    // per wave, so their BVHs stay in L2 -- batch throughput).
-    bool packed = false;
+    // Scheduling: fair (one sample of every unfinished job per wave, then more), packed
+    // (each job's remaining samples before the next job: fewer scenes per wave, so their
+    // BVHs stay in L2 -- batch throughput), or shortest remaining work first (the jobs
+    // with the fewest paths left take their samples first -- serving latency).
+    bool packed = false, srpt = false;
     const CacheLaunch* cache = nullptr;   // radiance-cache hooks (single-job renders)
     ~WaveEngine() { for (auto& g : captured) cudaGraphExecDestroy(g.exec); }
     WaveEngine(vkb_ctx* ctx, const WaveBuffers& wb, size_t cap, uint32_t fl, bool use_graphs) : c(ctx), w(wb), capacity(cap), flags(fl), graphs(use_graphs) {
@@ -751,7 +752,23 @@ struct WaveEngine {
         std::vector<uint32_t> take(njobs, 0u);
         size_t left = capacity;
         bool any = false;
-        if (packed) {
+        if (srpt) {
+            // Shortest remaining work first: every job, in order of the paths it has left
+            // (admission order on ties), takes as many samples as still fit.
+            std::vector<uint32_t> order;
+            for (uint32_t k = 0; k < njobs; ++k) if (!finished(k)) order.push_back(k);
+            std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+                return uint64_t(jobs[a].count - jobs[a].done) * jobs[a].npix < uint64_t(jobs[b].count - jobs[b].done) * jobs[b].npix;
+            });
+            for (uint32_t k : order) {
+                EngineJob& e = jobs[k];
+                uint32_t n = uint32_t(std::min<size_t>(e.count - e.done, left / e.npix));
+                if (n == 0 && !any) n = 1;
+                if (n == 0) continue;
+                take[k] = n; any = true;
+                left = size_t(n) * e.npix <= left ? left - size_t(n) * e.npix : 0;
+            }
+        } else if (packed) {
             // A job whose remaining samples fill at least half a wave takes the wave alone
             // (the plain single-job kernels, its scene alone in L2).  Otherwise first fit in
             // admission order over the small jobs: one that does not fit what is left is
@@ -1574,6 +1591,7 @@ vkb_status vkb_server_create(vkb_ctx* c, const vkb_server_config* cfg, vkb_serve
         v->wave.reserve(v->capacity, v->max_jobs);
         v->eng = std::make_unique<WaveEngine>(c, v->wave.view(), v->capacity, cfg->flags, true);
         v->eng->packed = (cfg->flags & VKB_BATCH_PACKED) != 0;
+        v->eng->srpt = !v->eng->packed && (cfg->flags & VKB_BATCH_FAIR) == 0;
     });
     if (st != VKB_OK) return st;
     *out = v.release();
