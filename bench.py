@@ -393,6 +393,45 @@ def run_cache(args, device):
     k.close(); s.close(); r.close()
 
 
+def max_over_ranks(value: float, dist, device=None) -> float:
+    """The largest of every rank's value (NCCL needs a CUDA tensor, gloo a host one)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_dry(args, rank, world):
+    """The multi-rank host logic of the replicas bench without a GPU (gloo): rendezvous,
+    a different seeded workload per rank, barrier, a stand-in step time per rank, the
+    max over ranks and one JSON line from rank 0."""
+    import datetime
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+        dist.barrier()
+    sc, _, prof, cfg = workload("small", seed=rank)
+    paths_per_step = sc.camera.width * sc.camera.height * prof.samples
+    elapsed_ms = args.steps * 10.0 * (1 + rank)          # stand-in device time of this rank
+    elapsed = max_over_ranks(elapsed_ms, dist)
+    digest = float(np.asarray(sc.instance_rows, np.float64).sum())
+    digests = [digest]
+    if dist is not None:
+        out = [None] * world
+        dist.all_gather_object(out, digest)
+        digests = out
+    if rank == 0:
+        print(json.dumps({"dry_run": True, "n_gpus": world, "steps": args.steps, "ms_per_step": elapsed / args.steps,
+                          "value": world * args.steps * paths_per_step / (elapsed / 1000.0), "unit": "paths/s",
+                          "scaling": "weak", "rank_workload_digests": digests, "config": cfg}), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -408,11 +447,14 @@ def main():
     ap.add_argument("--no-error", action="store_true", help="cache: skip the reference renders (timing/profiling runs)")
     ap.add_argument("--res", default="1920x1080", help="cache: frame resolution (smaller for profiling captures)")
     ap.add_argument("--schedule", default="srpt", choices=["srpt", "fair", "packed"], help="serve: wave schedule")
+    ap.add_argument("--dry-run", action="store_true", help="multi-rank host logic on CPU (gloo), no GPU work")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.dry_run:
+        return run_dry(args, rank, world)
     if args.impl == "reference":
         return run_reference(args, rank)
     if args.config == "batch":
@@ -491,10 +533,7 @@ def main():
     tlas = {"builder": ("PLOC (radius 16)" if args.tlas == "ploc" else "Karras LBVH") + " over 30-bit Morton order, rebuilt every frame",
             "build_ms_per_frame": build_ms / args.steps,
             **s.tlas_stats()}
-    if dist:
-        t = torch.tensor([elapsed_ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(elapsed_ms, dist, f"cuda:{local}")
     value = world * args.steps * paths_per_step / (elapsed_ms / 1000.0)
 
     # e2e: pinned host rows in, host image out, through the C ABI (copies inside the call).
@@ -505,10 +544,7 @@ def main():
         s.render(prof, out=host_image.numpy())
     sync()
     e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dist, f"cuda:{local}")
     e2e = world * args.steps * paths_per_step / e2e_s
 
     if rank == 0:
