@@ -122,10 +122,11 @@ class ClockSampler:
 
 def roofline_bytes(stats: dict) -> float:
     """Algorithmic bytes of the closest-hit trace kernels of one render: every node visit
-    loads one 64-byte BVH2 node, every triangle test one 48-byte triangle, every instance
-    entry one 64-byte TLAS leaf record; every ray reads its 32-byte queue entry and writes
-    a 20-byte hit record."""
-    return (stats["nodes_visited"] * 64 + stats["triangles_tested"] * 48 + stats["instances_entered"] * 64
+    loads 112 bytes of one 128-byte 4-wide node (the ray's near and far face planes of
+    the three axes, 6 x 16 bytes, and the four child references), every triangle test one
+    48-byte triangle, every instance entry one 64-byte TLAS leaf record; every ray reads
+    its 32-byte queue entry and writes a 20-byte hit record."""
+    return (stats["nodes_visited"] * 112 + stats["triangles_tested"] * 48 + stats["instances_entered"] * 64
             + stats["extension_rays"] * (32 + 20))
 
 

@@ -262,6 +262,28 @@ struct SahBlas {
     }
 };
 
+// 4-wide BLAS from the binary SAH tree (root 0): the 4-wide children of one node are
+// allocated together, depth first.
+std::vector<Bvh4Node> collapse_blas(const std::vector<BvhNode>& n2) {
+    std::vector<Bvh4Node> out(1);
+    std::vector<std::pair<int, int>> todo{{0, 0}};  // (binary node, 4-wide node)
+    while (!todo.empty()) {
+        auto [b, q] = todo.back();
+        todo.pop_back();
+        Bvh4Node node = collapse_node(n2.data(), n2[b]);
+        int* child = reinterpret_cast<int*>(&node.child);
+        for (int k = 0; k < 4; ++k) {
+            if (child[k] < 0) continue;
+            const int idx = int(out.size());
+            out.emplace_back();
+            todo.push_back({child[k], idx});
+            child[k] = idx;
+        }
+        out[q] = node;
+    }
+    return out;
+}
+
 // Scratch of one LBVH build, reused across builds.
 struct LbvhScratch {
     DBuf<uint32_t> codes, codes_sorted, ids, ids_sorted, leaf_parent, node_parent, counters, bounds;
@@ -432,7 +454,9 @@ struct vkb_scene {
     uint64_t motion_bytes = 0, tlas_rebuilds = 0, tlas_refits = 0;
     DBuf<uint4> inst_info;
     DBuf<MeshInfo> meshes;
-    DBuf<BvhNode> blas_nodes, tlas_nodes;
+    DBuf<BvhNode> tlas_nodes;                 // binary TLAS (built, refitted; SAH statistics)
+    DBuf<Bvh4Node> blas4, tlas4;              // 4-wide traversal nodes (TLAS sparse: index = binary node)
+    DBuf<uint8_t> tlas_odd;                   // depth parity of the binary TLAS nodes
     DBuf<TlasLeaf> tlas_leaves;
     DBuf<vkb_material> d_materials;
     DBuf<vkb_light> d_lights;
@@ -469,8 +493,8 @@ template <class F> vkb_status guarded(F&& f) {
 
 SceneView scene_view(const vkb_scene* s) {
     SceneView v;
-    v.tlas_nodes = s->tlas_nodes.p; v.tlas_leaves = s->tlas_leaves.p;
-    v.blas_nodes = s->blas_nodes.p; v.blas_tris = s->blas_tris.p;
+    v.tlas_nodes = s->tlas4.p; v.tlas_leaves = s->tlas_leaves.p;
+    v.blas_nodes = s->blas4.p; v.blas_tris = s->blas_tris.p;
     v.num_instances = s->num_instances;
     return v;
 }
@@ -498,8 +522,12 @@ void build_tlas(vkb_scene* s) {
         build_ploc(n, s->inst_lo.p, s->inst_hi.p, s->tlas_nodes.p, s->tlas_leaf_parent.p, s->tlas_node_parent.p, s->tlas_counters.p,
                    s->scratch, s->ploc, st, sms, s->launches);
     }
-    s->launches += 2;
+    s->launches += 4;
     k_tlas_leaves<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->scratch.ids_sorted.p, s->w2o.p, s->inst_info.p, s->meshes.p, s->d_materials.p, s->tlas_leaves.p);
+    const uint32_t ni = n > 1 ? n - 1 : 1u;
+    if (n > 1) k_bvh_parity<<<grid_for(ni, 256, sms), 256, 0, st>>>(ni, s->tlas_node_parent.p, s->tlas_odd.p);
+    else VKB_CUDA(cudaMemsetAsync(s->tlas_odd.p, 0, 1, st));
+    k_collapse4<<<grid_for(ni, 256, sms), 256, 0, st>>>(ni, s->tlas_nodes.p, s->tlas_odd.p, s->tlas4.p);
     VKB_CUDA(cudaMemcpyAsync(s->tlas_codes.p, s->scratch.codes.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     VKB_CUDA(cudaMemcpyAsync(s->tlas_order.p, s->scratch.ids_sorted.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     s->tlas_rebuilds++;
@@ -524,7 +552,9 @@ void refit_tlas(vkb_scene* s) {
                                                        s->tlas_node_parent.p, s->tlas_counters.p);
     }
     k_tlas_leaves<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->tlas_order.p, s->w2o.p, s->inst_info.p, s->meshes.p, s->d_materials.p, s->tlas_leaves.p);
-    s->launches += 3;
+    const uint32_t ni = n > 1 ? n - 1 : 1u;
+    k_collapse4<<<grid_for(ni, 256, sms), 256, 0, st>>>(ni, s->tlas_nodes.p, s->tlas_odd.p, s->tlas4.p);
+    s->launches += 4;
     VKB_CUDA(cudaGetLastError());
     VKB_CUDA(cudaEventRecord(s->ev1, st));
     VKB_CUDA(cudaEventSynchronize(s->ev1));
@@ -1086,21 +1116,19 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         s->vpos.upload(pos.data(), pos.size(), str);
         s->vnrm.upload(nrm.data(), nrm.size(), str);
         s->indices.upload(idx.data(), idx.size(), str);
-        // BLAS per mesh: node offsets first (n-1 internal nodes, at least 1).
-        uint32_t node_total = 0;
-        for (auto& mi : s->mesh_info) { mi.node_offset = node_total; node_total += std::max(1u, mi.num_triangles > 1 ? mi.num_triangles - 1u : 1u); }
-        s->blas_nodes.alloc(std::max(1u, node_total));
+        // BLAS per mesh: binary SAH tree, collapsed to 4-wide nodes (mesh node_offset into those).
         s->blas_tris.alloc(std::max<size_t>(1, size_t(nt) * 3));
         uint32_t max_tris = 0;
         for (auto& mi : s->mesh_info) max_tris = std::max(max_tris, mi.num_triangles);
         s->tri_lo.alloc(std::max(1u, max_tris)); s->tri_hi.alloc(std::max(1u, max_tris));
         VKB_CUDA(cudaEventRecord(s->ev0, str));
-        std::vector<BvhNode> all_nodes(std::max(1u, node_total));
+        std::vector<Bvh4Node> all_nodes;
         std::vector<float4> all_tris(std::max<size_t>(1, size_t(nt) * 3));
         for (uint32_t m = 0; m < d->num_meshes; ++m) {
-            const MeshInfo& mi = s->mesh_info[m];
+            MeshInfo& mi = s->mesh_info[m];
             const vkb_mesh& me = d->meshes[m];
             uint32_t n = mi.num_triangles;
+            mi.node_offset = uint32_t(all_nodes.size());
             if (n == 0) continue;
             std::vector<float> lo(3 * size_t(n)), hi(3 * size_t(n)), cen(3 * size_t(n));
             for (uint32_t t = 0; t < n; ++t)
@@ -1112,7 +1140,9 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
             SahBlas sah;
             sah.run(n, lo.data(), hi.data(), cen.data());
             if (sah.nodes.size() > std::max(1u, n > 1 ? n - 1 : 1u)) throw ArgError{"BLAS node count above its bound"};
-            std::copy(sah.nodes.begin(), sah.nodes.end(), all_nodes.begin() + mi.node_offset);
+            std::vector<Bvh4Node> wide = collapse_blas(sah.nodes);
+            if (all_nodes.size() + wide.size() > size_t(INT32_MAX)) throw ArgError{"BLAS node count above its bound"};
+            all_nodes.insert(all_nodes.end(), wide.begin(), wide.end());
             for (uint32_t k = 0; k < n; ++k) {
                 uint32_t t = sah.order[k];
                 const float* p0 = me.positions + 3 * me.indices[3 * t];
@@ -1126,7 +1156,9 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
                 all_tris[o + 2] = make_float4(p2[0], p2[1], p2[2], 0.f);
             }
         }
-        VKB_CUDA(cudaMemcpyAsync(s->blas_nodes.p, all_nodes.data(), all_nodes.size() * sizeof(BvhNode), cudaMemcpyHostToDevice, str));
+        if (all_nodes.empty()) all_nodes.emplace_back();
+        s->blas4.alloc(all_nodes.size());
+        VKB_CUDA(cudaMemcpyAsync(s->blas4.p, all_nodes.data(), all_nodes.size() * sizeof(Bvh4Node), cudaMemcpyHostToDevice, str));
         VKB_CUDA(cudaMemcpyAsync(s->blas_tris.p, all_tris.data(), all_tris.size() * sizeof(float4), cudaMemcpyHostToDevice, str));
         VKB_CUDA(cudaStreamSynchronize(str));
         VKB_CUDA(cudaEventRecord(s->ev1, str));
@@ -1153,6 +1185,8 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         s->w2o.alloc(size_t(n) * 3);
         s->inst_lo.alloc(n); s->inst_hi.alloc(n);
         s->tlas_nodes.alloc(std::max(1u, n > 1 ? n - 1 : 1u));
+        s->tlas4.alloc(std::max(1u, n > 1 ? n - 1 : 1u));
+        s->tlas_odd.alloc(std::max(1u, n > 1 ? n - 1 : 1u));
         s->tlas_leaves.alloc(std::max(1u, n));
         s->tlas_codes.alloc(std::max(1u, n));
         VKB_CUDA(cudaStreamSynchronize(str));
@@ -1174,7 +1208,7 @@ vkb_status vkb_scene_destroy(vkb_scene* s) {
     for (auto* b : f4) b->release();
     s->indices.release(); s->tlas_codes.release();
     s->tlas_order.release(); s->tlas_leaf_parent.release(); s->tlas_node_parent.release(); s->tlas_counters.release(); s->inst_info.release(); s->meshes.release();
-    s->blas_nodes.release(); s->tlas_nodes.release(); s->tlas_leaves.release(); s->d_materials.release(); s->d_lights.release();
+    s->blas4.release(); s->tlas4.release(); s->tlas_odd.release(); s->tlas_nodes.release(); s->tlas_leaves.release(); s->d_materials.release(); s->d_lights.release();
     s->tree.release();
     s->scratch.codes.release(); s->scratch.codes_sorted.release(); s->scratch.ids.release(); s->scratch.ids_sorted.release();
     s->scratch.leaf_parent.release(); s->scratch.node_parent.release(); s->scratch.counters.release(); s->scratch.bounds.release(); s->scratch.cub_temp.release();
@@ -1336,8 +1370,8 @@ vkb_status vkb_scene_info(vkb_scene* s, vkb_scene_info_t* out) {
     out->tlas_refits = s->tlas_refits;
     out->motion_bytes = s->motion_bytes;
     size_t dev = 0;
-    dev += s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas_nodes.n * sizeof(BvhNode) + s->blas_tris.n * sizeof(float4);
-    dev += s->tlas_nodes.n * sizeof(BvhNode) + s->tlas_leaves.n * sizeof(TlasLeaf) + (s->o2w.n + s->w2o.n) * sizeof(float4);
+    dev += s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas4.n * sizeof(Bvh4Node) + s->blas_tris.n * sizeof(float4);
+    dev += s->tlas_nodes.n * sizeof(BvhNode) + s->tlas4.n * sizeof(Bvh4Node) + s->tlas_odd.n + s->tlas_leaves.n * sizeof(TlasLeaf) + (s->o2w.n + s->w2o.n) * sizeof(float4);
     out->scene_bytes = dev;
     out->build_ms = s->build_ms;
     return VKB_OK;
@@ -1518,9 +1552,17 @@ vkb_status vkb_debug_trace(vkb_scene* s, uint32_t n, const float* rays7, float* 
     return guarded([&] {
         VKB_CUDA(cudaSetDevice(s->ctx->device));
         cudaStream_t st = s->ctx->stream;
-        DBuf<float> r, t, uv;
+        DBuf<float4> r;
+        DBuf<float> t, uv;
         DBuf<uint32_t> ids, err;
-        r.upload(rays7, size_t(n) * 7, st);
+        // origins (xyz, tmax) in [0, n), directions in [n, 2n)
+        std::vector<float4> rays4(2 * size_t(n));
+        for (uint32_t i = 0; i < n; ++i) {
+            const float* q = rays7 + 7 * size_t(i);
+            rays4[i] = make_float4(q[0], q[1], q[2], q[6]);
+            rays4[n + i] = make_float4(q[3], q[4], q[5], 0.f);
+        }
+        r.upload(rays4.data(), rays4.size(), st);
         t.alloc(n); uv.alloc(size_t(n) * 2); ids.alloc(size_t(n) * 2); err.alloc(1);
         VKB_CUDA(cudaMemsetAsync(err.p, 0, sizeof(uint32_t), st));
         if (n) k_debug_trace<<<grid_for(n, 128, s->ctx->sms), 128, 0, st>>>(scene_view(s), n, r.p, t.p, ids.p, uv.p, err.p);
@@ -1562,8 +1604,8 @@ struct vkb_server {
 
 namespace {
 uint64_t scene_bytes(const vkb_scene* s) {
-    return s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas_nodes.n * sizeof(BvhNode) +
-           s->blas_tris.n * sizeof(float4) + s->tlas_nodes.n * sizeof(BvhNode) + s->tlas_leaves.n * sizeof(TlasLeaf) +
+    return s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas4.n * sizeof(Bvh4Node) +
+           s->blas_tris.n * sizeof(float4) + s->tlas_nodes.n * sizeof(BvhNode) + s->tlas4.n * sizeof(Bvh4Node) + s->tlas_odd.n + s->tlas_leaves.n * sizeof(TlasLeaf) +
            (s->o2w.n + s->w2o.n) * sizeof(float4);
 }
 uint64_t resident_bytes(const vkb_server* v) {

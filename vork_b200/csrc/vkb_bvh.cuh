@@ -5,9 +5,10 @@
 // The reference builds these inside the Vulkan driver (crates/vork-render/src/rt.rs:
 // Rays::new :1098-1289 for BLAS batches, FrameRays::new :1339-1385 and encode /
 // rebuild_tlas :1387-1476 for the instance TLAS); its traversal is RayQuery::Proceed
-// (shaders/path.slang:155-189, :641-684).  Traversal here is a two-level stack walk
-// over 64-byte BVH2 nodes holding both child boxes, with watertight triangle tests
-// (Woop, Benthin & Wald, JCGT 2013), bounded stack and iteration count.
+// (shaders/path.slang:155-189, :641-684).  Both levels are built as binary trees and
+// collapsed to 4-wide nodes of one 128-byte line (FP32 child boxes as planes); traversal
+// is a two-level stack walk over those, nearest child first, with watertight triangle
+// tests (Woop, Benthin & Wald, JCGT 2013), bounded stack and iteration count.
 #pragma once
 #include <cstdint>
 #include "vkb_device.cuh"
@@ -19,6 +20,16 @@ namespace vkb {
 // c = (L.lo.z, L.hi.z, R.lo.z, R.hi.z), d = (left, right, -, -).  A child reference
 // >= 0 is an internal node, < 0 is ~(sorted leaf index).
 struct alignas(16) BvhNode { float4 a, b, c; int4 d; };
+
+// Four child boxes of a 4-wide node as planes (component k = child slot k), one 128-byte
+// line per node: plane 2a is the low face of axis a, plane 2a+1 the high face, so a ray
+// reads its near face of axis a at 2a + (direction negative) and its far face at the
+// other.  child = (c0, c1, c2, c3) as in BvhNode; an unused slot has the empty box
+// lo = +inf, hi = -inf, which every ray misses.  Traversal runs on these nodes; they are
+// collapsed from the binary trees (every internal node at even depth takes its children
+// and the children of its internal children).
+struct alignas(16) Bvh4Node { float4 plane[6]; int4 child; int4 pad; };
+static_assert(sizeof(Bvh4Node) == 128, "one 128-byte line per 4-wide node");
 
 // One TLAS leaf, in Morton order: the instance's world->object rows and what its BLAS needs.
 struct alignas(16) TlasLeaf { float4 w2o[3]; uint32_t instance, node_offset, tri_offset, flags; };
@@ -34,14 +45,11 @@ constexpr int TRACE_STACK = 64;
 #ifndef VKB_SMEM_STACK
 #define VKB_SMEM_STACK 48
 #endif
-#ifndef VKB_POP_CULL
-#define VKB_POP_CULL 0
-#endif
 // Traversal stacks live in shared memory as [entry][thread]: lane l of a 128-thread
 // block always touches bank l, whatever depth each lane is at (no bank conflicts).
 constexpr int SMEM_STACK = VKB_SMEM_STACK;
 constexpr int TRACE_BLOCK = 128;
-struct TraceStack { int* r; float* t; };
+struct TraceStack { int* r; };
 constexpr uint32_t TRACE_STEP_LIMIT = 1u << 16;
 constexpr int SENTINEL = 0x7fffffff;
 
@@ -73,24 +81,25 @@ __device__ __forceinline__ float float_unflip(uint32_t u) { return __uint_as_flo
 
 // ---------------------------------------------------------------- traversal
 struct RaySpace {
-    float3 o, d, idir, ood;     // origin, direction, 1/d, o/d
-    int kx, ky, kz;             // watertight shear permutation
+    float3 o, idir, ood;        // origin, 1/d, o/d
+    uint32_t k;                 // watertight shear permutation: kx | ky << 2 | kz << 4
     float sx, sy, sz;
 };
 __device__ __forceinline__ float safe_rcp(float x) { return 1.f / (fabsf(x) > 1e-20f ? x : copysignf(1e-20f, x)); }
 __device__ __forceinline__ float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
 __device__ __forceinline__ void make_space(RaySpace& r, float3 o, float3 d) {
-    r.o = o; r.d = d;
+    r.o = o;
     r.idir = f3(safe_rcp(d.x), safe_rcp(d.y), safe_rcp(d.z));
     r.ood = f3(o.x * r.idir.x, o.y * r.idir.y, o.z * r.idir.z);
     float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
-    r.kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
-    r.kx = r.kz + 1 == 3 ? 0 : r.kz + 1;
-    r.ky = r.kx + 1 == 3 ? 0 : r.kx + 1;
-    float dz = comp(d, r.kz);
-    if (dz < 0.f) { int t = r.kx; r.kx = r.ky; r.ky = t; }
-    r.sx = comp(d, r.kx) / dz;
-    r.sy = comp(d, r.ky) / dz;
+    int kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    int kx = kz + 1 == 3 ? 0 : kz + 1;
+    int ky = kx + 1 == 3 ? 0 : kx + 1;
+    float dz = comp(d, kz);
+    if (dz < 0.f) { int t = kx; kx = ky; ky = t; }
+    r.k = uint32_t(kx) | uint32_t(ky) << 2 | uint32_t(kz) << 4;
+    r.sx = comp(d, kx) / dz;
+    r.sy = comp(d, ky) / dz;
     r.sz = 1.f / dz;
 }
 // Slab test of both children of a node; returns entry distances (or +inf on miss).
@@ -109,14 +118,31 @@ __device__ __forceinline__ void node_boxes(const BvhNode& n, const RaySpace& r, 
     tl = lmin <= lmax * 1.00000024f ? lmin : __int_as_float(0x7f800000);
     tr = rmin <= rmax * 1.00000024f ? rmin : __int_as_float(0x7f800000);
 }
+// Three-input float min / max (sm_100 instructions; no NaN reaches them here).
+__device__ __forceinline__ float max3f(float a, float b, float c) { float r; asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c)); return r; }
+__device__ __forceinline__ float min3f(float a, float b, float c) { float r; asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c)); return r; }
+// Entry distance key of child slot k of a 4-wide node from the ray's near and far faces:
+// float bits of the entry distance (>= 0, so unsigned order is distance order) with the
+// slot in the two low bits, or ~0u on a miss.
+__device__ __forceinline__ uint32_t slot_key(float nx, float ny, float nz, float fx, float fy, float fz, const RaySpace& r, float tmax, uint32_t k) {
+    float tn = max3f(fmaf(nx, r.idir.x, -r.ood.x), fmaf(ny, r.idir.y, -r.ood.y), fmaxf(fmaf(nz, r.idir.z, -r.ood.z), 0.f));
+    float tf = min3f(fmaf(fx, r.idir.x, -r.ood.x), fmaf(fy, r.idir.y, -r.ood.y), fminf(fmaf(fz, r.idir.z, -r.ood.z), tmax));
+    return tn <= tf * 1.00000024f ? ((__float_as_uint(tn) & ~3u) | k) : 0xffffffffu;
+}
+__device__ __forceinline__ void key_order(uint32_t& a, uint32_t& b) { uint32_t l = min(a, b); b = max(a, b); a = l; }
+__device__ __forceinline__ int slot_child(const int4& c, uint32_t key) {
+    uint32_t k = key & 3u;
+    return k == 0u ? c.x : (k == 1u ? c.y : (k == 2u ? c.z : c.w));
+}
 // Watertight ray/triangle test. cull: accept front faces only (counter-clockwise
 // winding seen from the ray origin).  Returns t and barycentrics of vertices 1, 2.
 __device__ __forceinline__ bool tri_test(const RaySpace& r, float3 v0, float3 v1, float3 v2, bool cull, float tbest, float& t, float& b1, float& b2) {
+    const int kx = int(r.k & 3u), ky = int((r.k >> 2) & 3u), kz = int(r.k >> 4);
     float3 A = v0 - r.o, B = v1 - r.o, C = v2 - r.o;
-    float Az = comp(A, r.kz), Bz = comp(B, r.kz), Cz = comp(C, r.kz);
-    float Ax = comp(A, r.kx) - r.sx * Az, Ay = comp(A, r.ky) - r.sy * Az;
-    float Bx = comp(B, r.kx) - r.sx * Bz, By = comp(B, r.ky) - r.sy * Bz;
-    float Cx = comp(C, r.kx) - r.sx * Cz, Cy = comp(C, r.ky) - r.sy * Cz;
+    float Az = comp(A, kz), Bz = comp(B, kz), Cz = comp(C, kz);
+    float Ax = comp(A, kx) - r.sx * Az, Ay = comp(A, ky) - r.sy * Az;
+    float Bx = comp(B, kx) - r.sx * Bz, By = comp(B, ky) - r.sy * Bz;
+    float Cx = comp(C, kx) - r.sx * Cz, Cy = comp(C, ky) - r.sy * Cz;
     float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
     if (U == 0.f || V == 0.f || W == 0.f) {
         double cxby = double(Cx) * double(By), cybx = double(Cy) * double(Bx);
@@ -146,25 +172,28 @@ static_assert(VKB_BLAS_LEAF_MAX >= 1 && VKB_BLAS_LEAF_MAX <= 4, "leaf counts are
 
 struct HitRecord { float t, u, v; uint32_t prim, inst; };
 
-// A world ray in global memory (origin and direction as 3 floats each).  Traversal
-// re-reads it when it enters or leaves an instance instead of keeping six registers live
-// across the loop; the volatile loads keep the compiler from caching the values.
+// A world ray in global memory: entry i of an origin queue and a direction queue (xyz of
+// float4).  Traversal re-reads it when it enters or leaves an instance instead of keeping
+// six registers live across the loop; the volatile loads keep the compiler from caching
+// the values, and the queue bases are the same for every thread (uniform registers).
 struct RayRef {
-    const float* o;
-    const float* d;
-    __device__ __forceinline__ static float ld(const float* p) {
-        float v;
-        asm volatile("ld.global.nc.f32 %0, [%1];" : "=f"(v) : "l"(p));
-        return v;
+    const float4* o;
+    const float4* d;
+    uint32_t i;
+    __device__ __forceinline__ static float3 ld3(const float4* p) {
+        float x, y, z;
+        asm volatile("ld.global.nc.f32 %0, [%3];\n\tld.global.nc.f32 %1, [%3+4];\n\tld.global.nc.f32 %2, [%3+8];"
+                     : "=f"(x), "=f"(y), "=f"(z) : "l"(p));
+        return f3(x, y, z);
     }
-    __device__ __forceinline__ float3 origin() const { return f3(ld(o), ld(o + 1), ld(o + 2)); }
-    __device__ __forceinline__ float3 dir() const { return f3(ld(d), ld(d + 1), ld(d + 2)); }
+    __device__ __forceinline__ float3 origin() const { return ld3(o + i); }
+    __device__ __forceinline__ float3 dir() const { return ld3(d + i); }
 };
 
 struct SceneView {
-    const BvhNode* tlas_nodes;
+    const Bvh4Node* tlas_nodes;
     const TlasLeaf* tlas_leaves;
-    const BvhNode* blas_nodes;
+    const Bvh4Node* blas_nodes;
     const float4* blas_tris;     // 3 per triangle (Morton order within a mesh); v0.w = original triangle id
     uint32_t num_instances;
 };
@@ -182,7 +211,7 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, RayRef ray, float 
     int sp = 0;
     float tbest = tmax;
     bool found = false, in_blas = false, cull = false;
-    const BvhNode* nodes = s.tlas_nodes;
+    const Bvh4Node* nodes = s.tlas_nodes;
     const float4* tris = s.blas_tris;
     uint32_t tri_base = 0, cur_instance = 0;
     int node = 0;
@@ -191,24 +220,29 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, RayRef ray, float 
         if (steps >= TRACE_STEP_LIMIT) { atomicOr(err, 2u); break; }
         if (node >= 0) {
             if (COUNT) { count->nodes++; if (in_blas) count->blas_nodes++; }
-            BvhNode n;
             const float4* p = reinterpret_cast<const float4*>(nodes + node);
-            n.a = __ldg(p); n.b = __ldg(p + 1); n.c = __ldg(p + 2);
-            n.d = __ldg(reinterpret_cast<const int4*>(p + 3));
-            float tl, tr;
-            node_boxes(n, rs, tbest, tl, tr);
-            bool hl = tl != __int_as_float(0x7f800000), hr = tr != __int_as_float(0x7f800000);
-            if (hl && hr) {
-                bool lfirst = tl <= tr;
-                if (sp >= SMEM_STACK) { atomicOr(err, 1u); break; }
-                stk.r[sp * TRACE_BLOCK] = lfirst ? n.d.y : n.d.x;
-                if (VKB_POP_CULL) stk.t[sp * TRACE_BLOCK] = lfirst ? tr : tl;
-                ++sp;
-                node = lfirst ? n.d.x : n.d.y;
+            const uint32_t sx = __float_as_uint(rs.idir.x) >> 31, sy = __float_as_uint(rs.idir.y) >> 31, sz = __float_as_uint(rs.idir.z) >> 31;
+            const float4 nx = __ldg(p + sx), fx = __ldg(p + (sx ^ 1u));
+            const float4 ny = __ldg(p + 2u + sy), fy = __ldg(p + (3u - sy));
+            const float4 nz = __ldg(p + 4u + sz), fz = __ldg(p + (5u - sz));
+            const int4 ch = __ldg(reinterpret_cast<const int4*>(p + 6));
+            uint32_t k0 = slot_key(nx.x, ny.x, nz.x, fx.x, fy.x, fz.x, rs, tbest, 0u);
+            uint32_t k1 = slot_key(nx.y, ny.y, nz.y, fx.y, fy.y, fz.y, rs, tbest, 1u);
+            uint32_t k2 = slot_key(nx.z, ny.z, nz.z, fx.z, fy.z, fz.z, rs, tbest, 2u);
+            uint32_t k3 = slot_key(nx.w, ny.w, nz.w, fx.w, fy.w, fz.w, rs, tbest, 3u);
+            // Nearest first: a five-exchange sorting network on the keys.
+            key_order(k0, k1); key_order(k2, k3); key_order(k0, k2); key_order(k1, k3); key_order(k1, k2);
+            if (k0 != 0xffffffffu) {
+                if (k1 != 0xffffffffu) {
+                    const int pushes = 1 + (k2 != 0xffffffffu) + (k3 != 0xffffffffu);
+                    if (sp + pushes > SMEM_STACK) { atomicOr(err, 1u); break; }
+                    if (k3 != 0xffffffffu) { stk.r[sp * TRACE_BLOCK] = slot_child(ch, k3); ++sp; }
+                    if (k2 != 0xffffffffu) { stk.r[sp * TRACE_BLOCK] = slot_child(ch, k2); ++sp; }
+                    stk.r[sp * TRACE_BLOCK] = slot_child(ch, k1); ++sp;
+                }
+                node = slot_child(ch, k0);
                 continue;
             }
-            if (hl) { node = n.d.x; continue; }
-            if (hr) { node = n.d.y; continue; }
         } else if (!in_blas) {
             if (COUNT) count->instances++;
             const TlasLeaf* lf = s.tlas_leaves + (~node);
@@ -224,7 +258,6 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, RayRef ray, float 
             cull = !ANY && (info.w & LEAF_CULL_BACKFACES);
             if (sp >= SMEM_STACK) { atomicOr(err, 1u); break; }
             stk.r[sp * TRACE_BLOCK] = SENTINEL;
-            if (VKB_POP_CULL) stk.t[sp * TRACE_BLOCK] = 0.f;
             ++sp;
             in_blas = true;
             node = 0;
@@ -244,18 +277,17 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, RayRef ray, float 
                 }
             }
         }
-        // pop (with VKB_POP_CULL, an entry farther than the closest hit so far is skipped without a fetch)
-        for (;;) {
+        // pop
+        if (sp == 0) return found;
+        --sp;
+        node = stk.r[sp * TRACE_BLOCK];
+        while (node == SENTINEL) {
+            in_blas = false;
+            make_space(rs, ray.origin(), ray.dir());
+            nodes = s.tlas_nodes;
             if (sp == 0) return found;
             --sp;
             node = stk.r[sp * TRACE_BLOCK];
-            if (node == SENTINEL) {
-                in_blas = false;
-                make_space(rs, ray.origin(), ray.dir());
-                nodes = s.tlas_nodes;
-                continue;
-            }
-            if (!VKB_POP_CULL || stk.t[sp * TRACE_BLOCK] <= tbest) break;
         }
     }
     return found;

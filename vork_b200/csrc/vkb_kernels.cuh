@@ -302,6 +302,54 @@ __global__ void k_single_leaf(const float4* lo, const float4* hi, BvhNode* nodes
     n.d = make_int4(~0, ~0, 0, 0);
     nodes[0] = n;
 }
+// ---- 4-wide traversal nodes from a binary tree (parent links, root 0 with parent ~0u).
+// Depth parity of every internal node, by walking its parent links to the root.
+__global__ void k_bvh_parity(uint32_t n_internal, const uint32_t* node_parent, uint8_t* odd) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_internal; i += gridDim.x * blockDim.x) {
+        uint32_t d = 0, j = i;
+        for (uint32_t guard = 0; guard < n_internal; ++guard) {
+            uint32_t pr = node_parent[j];
+            if (pr == 0xffffffffu) break;
+            j = pr >> 1;
+            ++d;
+        }
+        odd[i] = uint8_t(d & 1u);
+    }
+}
+// Child slot k of a 4-wide node: box planes and reference.
+__device__ __host__ __forceinline__ void set_slot(Bvh4Node& q, int k, float lx, float hx, float ly, float hy, float lz, float hz, int ref) {
+    float* pl = reinterpret_cast<float*>(q.plane);
+    pl[0 * 4 + k] = lx; pl[1 * 4 + k] = hx; pl[2 * 4 + k] = ly; pl[3 * 4 + k] = hy; pl[4 * 4 + k] = lz; pl[5 * 4 + k] = hz;
+    reinterpret_cast<int*>(&q.child)[k] = ref;
+}
+// The slots of the 4-wide node for binary node b: each leaf child keeps its slot, each
+// internal child gives its own two children (internal references stay binary indices).
+__device__ __host__ __forceinline__ Bvh4Node collapse_node(const BvhNode* n2, const BvhNode& b) {
+    Bvh4Node q;
+    int k = 0;
+    const int refs[2] = {b.d.x, b.d.y};
+    const float box[2][6] = {{b.a.x, b.a.y, b.a.z, b.a.w, b.c.x, b.c.y}, {b.b.x, b.b.y, b.b.z, b.b.w, b.c.z, b.c.w}};
+    for (int side = 0; side < 2; ++side) {
+        if (refs[side] >= 0) {
+            const BvhNode c = n2[refs[side]];
+            set_slot(q, k++, c.a.x, c.a.y, c.a.z, c.a.w, c.c.x, c.c.y, c.d.x);
+            set_slot(q, k++, c.b.x, c.b.y, c.b.z, c.b.w, c.c.z, c.c.w, c.d.y);
+        } else {
+            set_slot(q, k++, box[side][0], box[side][1], box[side][2], box[side][3], box[side][4], box[side][5], refs[side]);
+        }
+    }
+    for (; k < 4; ++k) set_slot(q, k, INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY, ~0);
+    q.pad = make_int4(0, 0, 0, 0);
+    return q;
+}
+// Every even-depth internal node i of the binary tree becomes 4-wide node i (the odd
+// depths are folded into their parents; their slots stay unused).
+__global__ void k_collapse4(uint32_t n_internal, const BvhNode* n2, const uint8_t* odd, Bvh4Node* n4) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_internal; i += gridDim.x * blockDim.x) {
+        if (odd[i]) continue;
+        n4[i] = collapse_node(n2, n2[i]);
+    }
+}
 // Triangles of one mesh in Morton order, v0.w = original triangle id.
 __global__ void k_sorted_tris(uint32_t n, const uint32_t* sorted_ids, const uint32_t* idx, const float4* pos, float4* tris) {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -476,8 +524,7 @@ __device__ __forceinline__ bool trace_any(const SceneView& sv, RayRef ray, float
 // This thread's column of the block's shared-memory traversal stack.
 #define VKB_STACK_DECL                                                                                   \
     __shared__ int stack_r_[SMEM_STACK * TRACE_BLOCK];                                                  \
-    __shared__ float stack_t_[VKB_POP_CULL ? SMEM_STACK * TRACE_BLOCK : 1];                            \
-    TraceStack stk{stack_r_ + threadIdx.x, stack_t_ + (VKB_POP_CULL ? threadIdx.x : 0)};
+    TraceStack stk{stack_r_ + threadIdx.x};
 template <bool ANY, bool COUNT, bool BATCH>
 __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace(PathParams p, int cur) {
     VKB_STACK_DECL
@@ -487,12 +534,12 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace(Pat
         else atomicAdd(&p.counters[3], n);
     }
     TraceCount tc;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    auto trace_one = [&](uint32_t i) {
         if (!ANY) {
             const float tmax = p.ray_o[cur][i].w;
             const SceneView sv = BATCH ? p.jobs[job_of_slot<true>(p, __float_as_uint(p.ray_d[cur][i].w))].sv : p.job0.sv;
             HitRecord h;
-            bool found = trace_any<false, COUNT>(sv, RayRef{&p.ray_o[cur][i].x, &p.ray_d[cur][i].x}, tmax, h, p.err, &tc, stk);
+            bool found = trace_any<false, COUNT>(sv, RayRef{p.ray_o[cur], p.ray_d[cur], i}, tmax, h, p.err, &tc, stk);
             p.hit[i] = found ? make_float4(h.t, h.u, h.v, __uint_as_float(h.prim)) : make_float4(-1.f, 0.f, 0.f, __uint_as_float(0xffffffffu));
             p.hit_inst[i] = found ? h.inst : 0xffffffffu;
         } else {
@@ -502,12 +549,12 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace(Pat
             const SceneView sv = J.sv;
             HitRecord h;
             float3 total = f3(sc.x, sc.y, sc.z);
-            if ((flags & SH_TRACE_A) && trace_any<true, COUNT>(sv, RayRef{&p.sa_o[i].x, &p.sa_d[i].x}, so.w, h, p.err, &tc, stk)) total = f3(0.f);
+            if ((flags & SH_TRACE_A) && trace_any<true, COUNT>(sv, RayRef{p.sa_o, p.sa_d, i}, so.w, h, p.err, &tc, stk)) total = f3(0.f);
             if (flags & SH_HAS_B) {
                 float4 bc = p.sb_c[slot];
                 float3 cb = f3(bc.x, bc.y, bc.z);
                 if (flags & SH_TRACE_B) {
-                    if (trace_any<true, COUNT>(sv, RayRef{&p.sb_o[slot].x, &p.sb_d[slot].x}, p.sb_o[slot].w, h, p.err, &tc, stk)) cb = f3(0.f);
+                    if (trace_any<true, COUNT>(sv, RayRef{p.sb_o, p.sb_d, slot}, p.sb_o[slot].w, h, p.err, &tc, stk)) cb = f3(0.f);
                 }
                 total = total + cb;
             }
@@ -516,6 +563,16 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace(Pat
             float3 add = clamp_sample(total, (flags & SH_DIRECT) ? J.clamp_direct : J.clamp_indirect, dropped);
             p.rad[slot] = make_float4(r.x + add.x, r.y + add.y, r.z + add.z, __uint_as_float(dropped));
         }
+    };
+    // Whole warps take the next 32 consecutive queue entries from a counter, so warps
+    // that finish early take more and the launch ends without a tail of lone warps.
+    uint32_t* fetch = &p.counters[ANY ? 12 : 11];
+    for (;;) {
+        uint32_t base = 0;
+        if ((threadIdx.x & 31u) == 0u) base = atomicAdd(fetch, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        if (base + (threadIdx.x & 31u) < n) trace_one(base + (threadIdx.x & 31u));
     }
     if (COUNT) {
         // Every lane of the block reaches here after its loop.
@@ -815,6 +872,8 @@ __global__ void __launch_bounds__(128) k_shade(PathParams p, int cur) {
 __global__ void k_start_wave(uint32_t* counters, uint32_t append_camera) {
     counters[0] = append_camera ? 0u : counters[7];
     counters[9] = 0u;
+    counters[11] = 0u;   // trace fetch counters (closest, shadow)
+    counters[12] = 0u;
 }
 // Adaptive sampling, before the wave of sample index i = wave_first (path.slang:1797-1835):
 // reset at i = 0; from the minimum on a pixel is settled when every channel's standard
@@ -859,7 +918,7 @@ __global__ void k_adaptive_decide(PathParams p) {
     if ((threadIdx.x & 31u) == 0u && skipped) atomicAdd(&p.counters[10], skipped);
 }
 // Zero the next ray queue and the shadow queue before a shade pass.
-__global__ void k_reset_queues(uint32_t* counters, int nxt) { counters[nxt] = 0u; counters[2] = 0u; }
+__global__ void k_reset_queues(uint32_t* counters, int nxt) { counters[nxt] = 0u; counters[2] = 0u; counters[11] = 0u; counters[12] = 0u; }
 // resolve.slang:162-191: add this wave's finished samples to each job's accumulator,
 // one sample at a time in sample order (any wave size gives the same sums).
 template <bool BATCH>
@@ -929,12 +988,11 @@ __global__ void k_sampler_groups(uint32_t n, const uint32_t* px, const uint32_t*
     }
 }
 // Test entry: closest hits of arbitrary world rays.
-__global__ void __launch_bounds__(TRACE_BLOCK) k_debug_trace(SceneView sv, uint32_t n, const float* rays, float* t, uint32_t* ids, float* uv, uint32_t* err) {
+__global__ void __launch_bounds__(TRACE_BLOCK) k_debug_trace(SceneView sv, uint32_t n, const float4* rays, float* t, uint32_t* ids, float* uv, uint32_t* err) {
     VKB_STACK_DECL
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float* r = rays + 7 * i;
         HitRecord h;
-        bool f = trace_any<false, false>(sv, RayRef{r, r + 3}, r[6], h, err, nullptr, stk);
+        bool f = trace_any<false, false>(sv, RayRef{rays, rays + n, i}, rays[i].w, h, err, nullptr, stk);
         t[i] = f ? h.t : -1.f;
         ids[2 * i] = f ? h.inst : 0xffffffffu; ids[2 * i + 1] = f ? h.prim : 0xffffffffu;
         uv[2 * i] = f ? h.u : 0.f; uv[2 * i + 1] = f ? h.v : 0.f;
