@@ -702,14 +702,14 @@ void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counte
             }
             VKB_CUDA(cudaEventRecord(c->kernel_events[2 * tot.trace_launches], st));
         }
-        if (counted) k_trace<false, true, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p, cur);
-        else k_trace<false, false, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p, cur);
+        if (counted) k_trace<true, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p, cur);
+        else k_trace<false, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p, cur);
         if (timed) VKB_CUDA(cudaEventRecord(c->kernel_events[2 * tot.trace_launches + 1], st));
         tot.trace_launches++;
         k_reset_queues<<<1, 1, 0, st>>>(p.counters, cur ^ 1);
         k_shade<BATCH><<<sgrid, 128, 0, st>>>(p, cur);
-        if (counted) k_trace<true, true, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p, -1);
-        else k_trace<true, false, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p, -1);
+        if (counted) k_trace_shadow<true, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
+        else k_trace_shadow<false, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
     }
     if (cache && cache->dev.mode == 1u) {
         if (timed) {

@@ -201,23 +201,31 @@ struct SceneView {
 // Traversal work of one ray (instrumented builds only): node visits, triangle tests, instance entries.
 struct TraceCount { uint32_t nodes = 0, tris = 0, instances = 0, blas_nodes = 0; };
 
-// Closest hit (any == false) or first hit (any == true) of a world ray over the
-// two-level BVH.  Error: overflow/step-limit exits set *err and return the best so far.
+// Traversal state of one ray: closest hit (ANY == false) or first hit (ANY == true) over
+// the two-level BVH, advanced one step (a 4-wide node, an instance entry, a BLAS leaf,
+// then a pop) at a time.  Error: overflow/step-limit exits set *err and end the ray with
+// the best hit so far.
 template <bool ANY, bool COUNT = false>
-__device__ __forceinline__ bool trace_ray(const SceneView& s, RayRef ray, float tmax, HitRecord& hit, uint32_t* err,
-                                          TraceCount* count, TraceStack stk) {
+struct TraceLane {
     RaySpace rs;
-    make_space(rs, ray.origin(), ray.dir());
-    int sp = 0;
-    float tbest = tmax;
-    bool found = false, in_blas = false, cull = false;
-    const Bvh4Node* nodes = s.tlas_nodes;
-    const float4* tris = s.blas_tris;
-    uint32_t tri_base = 0, cur_instance = 0;
-    int node = 0;
-    if (s.num_instances == 0) return false;
-    for (uint32_t steps = 0;; ++steps) {
-        if (steps >= TRACE_STEP_LIMIT) { atomicOr(err, 2u); break; }
+    float tbest;
+    int node, sp;
+    bool found, in_blas, cull;
+    const Bvh4Node* nodes;
+    uint32_t tri_base, cur_instance, steps;
+    HitRecord hit;
+
+    // Returns false when there is nothing to traverse.
+    __device__ __forceinline__ bool start(const SceneView& s, RayRef ray, float tmax) {
+        make_space(rs, ray.origin(), ray.dir());
+        tbest = tmax; node = 0; sp = 0; steps = 0;
+        found = false; in_blas = false; cull = false;
+        nodes = s.tlas_nodes; tri_base = 0; cur_instance = 0;
+        return s.num_instances != 0;
+    }
+    // One step; returns true when the ray is finished (hit/found hold the result).
+    __device__ __forceinline__ bool step(const SceneView& s, RayRef ray, uint32_t* err, TraceCount* count, TraceStack stk) {
+        if (++steps >= TRACE_STEP_LIMIT) { atomicOr(err, 2u); return true; }
         if (node >= 0) {
             if (COUNT) { count->nodes++; if (in_blas) count->blas_nodes++; }
             const float4* p = reinterpret_cast<const float4*>(nodes + node);
@@ -235,13 +243,13 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, RayRef ray, float 
             if (k0 != 0xffffffffu) {
                 if (k1 != 0xffffffffu) {
                     const int pushes = 1 + (k2 != 0xffffffffu) + (k3 != 0xffffffffu);
-                    if (sp + pushes > SMEM_STACK) { atomicOr(err, 1u); break; }
+                    if (sp + pushes > SMEM_STACK) { atomicOr(err, 1u); return true; }
                     if (k3 != 0xffffffffu) { stk.r[sp * TRACE_BLOCK] = slot_child(ch, k3); ++sp; }
                     if (k2 != 0xffffffffu) { stk.r[sp * TRACE_BLOCK] = slot_child(ch, k2); ++sp; }
                     stk.r[sp * TRACE_BLOCK] = slot_child(ch, k1); ++sp;
                 }
                 node = slot_child(ch, k0);
-                continue;
+                return false;
             }
         } else if (!in_blas) {
             if (COUNT) count->instances++;
@@ -256,18 +264,18 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, RayRef ray, float 
             nodes = s.blas_nodes + info.y;
             tri_base = info.z;
             cull = !ANY && (info.w & LEAF_CULL_BACKFACES);
-            if (sp >= SMEM_STACK) { atomicOr(err, 1u); break; }
+            if (sp >= SMEM_STACK) { atomicOr(err, 1u); return true; }
             stk.r[sp * TRACE_BLOCK] = SENTINEL;
             ++sp;
             in_blas = true;
             node = 0;
-            continue;
+            return false;
         } else {
             // BLAS leaf: up to VKB_BLAS_LEAF_MAX triangles in leaf order, ~((first << 2) | (count - 1)).
             uint32_t v = uint32_t(~node), first = v >> 2, cnt = VKB_BLAS_LEAF_MAX == 1 ? 1u : (v & 3u) + 1u;
             for (uint32_t k = 0; k < cnt; ++k) {
                 if (COUNT) count->tris++;
-                const float4* tp = tris + 3u * (tri_base + first + k);
+                const float4* tp = s.blas_tris + 3u * (tri_base + first + k);
                 float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
                 float t, b1, b2;
                 if (tri_test(rs, f3(v0.x, v0.y, v0.z), f3(v1.x, v1.y, v1.z), f3(v2.x, v2.y, v2.z), cull, tbest, t, b1, b2)) {
@@ -278,19 +286,29 @@ __device__ __forceinline__ bool trace_ray(const SceneView& s, RayRef ray, float 
             }
         }
         // pop
-        if (sp == 0) return found;
+        if (sp == 0) return true;
         --sp;
         node = stk.r[sp * TRACE_BLOCK];
         while (node == SENTINEL) {
             in_blas = false;
             make_space(rs, ray.origin(), ray.dir());
             nodes = s.tlas_nodes;
-            if (sp == 0) return found;
+            if (sp == 0) return true;
             --sp;
             node = stk.r[sp * TRACE_BLOCK];
         }
+        return false;
     }
-    return found;
+};
+
+template <bool ANY, bool COUNT = false>
+__device__ __forceinline__ bool trace_ray(const SceneView& s, RayRef ray, float tmax, HitRecord& hit, uint32_t* err,
+                                          TraceCount* count, TraceStack stk) {
+    TraceLane<ANY, COUNT> L;
+    if (!L.start(s, ray, tmax)) return false;
+    while (!L.step(s, ray, err, count, stk)) {}
+    hit = L.hit;
+    return L.found;
 }
 
 }  // namespace vkb

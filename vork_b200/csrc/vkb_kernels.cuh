@@ -525,61 +525,152 @@ __device__ __forceinline__ bool trace_any(const SceneView& sv, RayRef ray, float
 #define VKB_STACK_DECL                                                                                   \
     __shared__ int stack_r_[SMEM_STACK * TRACE_BLOCK];                                                  \
     TraceStack stk{stack_r_ + threadIdx.x};
-template <bool ANY, bool COUNT, bool BATCH>
+// Lanes of a warp refill together once at most this many are still tracing.
+#ifndef VKB_TRACE_REFILL
+#define VKB_TRACE_REFILL 20
+#endif
+static_assert(VKB_TRACE_REFILL >= 1 && VKB_TRACE_REFILL <= 31, "refill threshold in lanes");
+// Closest hits of the queued rays with lane refill: each lane carries one ray's
+// traversal state; once at most VKB_TRACE_REFILL lanes of a warp are still tracing, the
+// idle lanes take the next rays of the queue together (one atomic per warp), so a warp
+// does not run on with a few long rays while its other lanes wait (measured: a warp's
+// lanes otherwise spend ~60% of its steps idle behind its longest ray).  Refilling
+// each lane as soon as it finishes is slower: the refill code then runs on single lanes.
+template <bool COUNT, bool BATCH>
 __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace(PathParams p, int cur) {
     VKB_STACK_DECL
-    uint32_t n = cur < 0 ? p.counters[2] : p.counters[cur];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        if (ANY) atomicAdd(&p.counters[4], n);
-        else atomicAdd(&p.counters[3], n);
-    }
+    const uint32_t n = p.counters[cur];
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.counters[3], n);
+    const uint32_t lane = threadIdx.x & 31u;
     TraceCount tc;
-    auto trace_one = [&](uint32_t i) {
-        if (!ANY) {
-            const float tmax = p.ray_o[cur][i].w;
-            const SceneView sv = BATCH ? p.jobs[job_of_slot<true>(p, __float_as_uint(p.ray_d[cur][i].w))].sv : p.job0.sv;
-            HitRecord h;
-            bool found = trace_any<false, COUNT>(sv, RayRef{p.ray_o[cur], p.ray_d[cur], i}, tmax, h, p.err, &tc, stk);
-            p.hit[i] = found ? make_float4(h.t, h.u, h.v, __uint_as_float(h.prim)) : make_float4(-1.f, 0.f, 0.f, __uint_as_float(0xffffffffu));
-            p.hit_inst[i] = found ? h.inst : 0xffffffffu;
-        } else {
-            float4 so = p.sa_o[i], sd = p.sa_d[i], sc = p.sa_c[i];
-            uint32_t slot = __float_as_uint(sd.w), flags = __float_as_uint(sc.w);
-            const Job& J = BATCH ? p.jobs[job_of_slot<true>(p, slot)] : p.job0;
-            const SceneView sv = J.sv;
-            HitRecord h;
-            float3 total = f3(sc.x, sc.y, sc.z);
-            if ((flags & SH_TRACE_A) && trace_any<true, COUNT>(sv, RayRef{p.sa_o, p.sa_d, i}, so.w, h, p.err, &tc, stk)) total = f3(0.f);
-            if (flags & SH_HAS_B) {
-                float4 bc = p.sb_c[slot];
-                float3 cb = f3(bc.x, bc.y, bc.z);
-                if (flags & SH_TRACE_B) {
-                    if (trace_any<true, COUNT>(sv, RayRef{p.sb_o, p.sb_d, slot}, p.sb_o[slot].w, h, p.err, &tc, stk)) cb = f3(0.f);
-                }
-                total = total + cb;
-            }
-            float4 r = p.rad[slot];
-            uint32_t dropped = __float_as_uint(r.w);
-            float3 add = clamp_sample(total, (flags & SH_DIRECT) ? J.clamp_direct : J.clamp_indirect, dropped);
-            p.rad[slot] = make_float4(r.x + add.x, r.y + add.y, r.z + add.z, __uint_as_float(dropped));
-        }
-    };
-    // Whole warps take the next 32 consecutive queue entries from a counter, so warps
-    // that finish early take more and the launch ends without a tail of lone warps.
-    uint32_t* fetch = &p.counters[ANY ? 12 : 11];
+    TraceLane<false, COUNT> L;
+    constexpr uint32_t NONE = 0xffffffffu;
+    uint32_t ray = NONE, job = 0;
+    bool drained = false;
     for (;;) {
-        uint32_t base = 0;
-        if ((threadIdx.x & 31u) == 0u) base = atomicAdd(fetch, 32u);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= n) break;
-        if (base + (threadIdx.x & 31u) < n) trace_one(base + (threadIdx.x & 31u));
+        uint32_t act = __ballot_sync(0xffffffffu, ray != NONE);
+        if (!drained && uint32_t(__popc(act)) <= uint32_t(VKB_TRACE_REFILL)) {
+            const uint32_t idle = ~act;
+            uint32_t base = 0;
+            if (lane == 0u) base = atomicAdd(&p.counters[11], uint32_t(__popc(idle)));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            drained = base + uint32_t(__popc(idle)) >= n;
+            if (ray == NONE) {
+                const uint32_t r = base + uint32_t(__popc(idle & ((1u << lane) - 1u)));
+                if (r < n) {
+                    if (BATCH) job = job_of_slot<true>(p, __float_as_uint(p.ray_d[cur][r].w));
+                    if (L.start(BATCH ? p.jobs[job].sv : p.job0.sv, RayRef{p.ray_o[cur], p.ray_d[cur], r}, p.ray_o[cur][r].w)) {
+                        ray = r;
+                    } else {
+                        p.hit[r] = make_float4(-1.f, 0.f, 0.f, __uint_as_float(0xffffffffu));
+                        p.hit_inst[r] = 0xffffffffu;
+                    }
+                }
+            }
+            act = __ballot_sync(0xffffffffu, ray != NONE);
+        }
+        if (act == 0u) {
+            if (drained) break;
+            continue;
+        }
+        bool done = false;
+        if (ray != NONE) {
+            if constexpr (BATCH) done = L.step(p.jobs[job].sv, RayRef{p.ray_o[cur], p.ray_d[cur], ray}, p.err, &tc, stk);
+            else done = L.step(p.job0.sv, RayRef{p.ray_o[cur], p.ray_d[cur], ray}, p.err, &tc, stk);
+        }
+        if (done) {
+            p.hit[ray] = L.found ? make_float4(L.hit.t, L.hit.u, L.hit.v, __uint_as_float(L.hit.prim)) : make_float4(-1.f, 0.f, 0.f, __uint_as_float(0xffffffffu));
+            p.hit_inst[ray] = L.found ? L.hit.inst : 0xffffffffu;
+            ray = NONE;
+        }
     }
     if (COUNT) {
-        // Every lane of the block reaches here after its loop.
-        flush_count(&p.work[ANY ? 3 : 0], tc.nodes);
-        flush_count(&p.work[ANY ? 4 : 1], tc.tris);
-        if (!ANY) flush_count(&p.work[2], tc.instances);
-        flush_count(&p.work[ANY ? 6 : 5], tc.blas_nodes);
+        flush_count(&p.work[0], tc.nodes);
+        flush_count(&p.work[1], tc.tris);
+        flush_count(&p.work[2], tc.instances);
+        flush_count(&p.work[5], tc.blas_nodes);
+    }
+}
+
+// Shadow entries with lane refill (as k_trace): a lane carries one entry through its
+// ray A, then its ray B (the second estimator's, when present and traced), then adds
+// the unoccluded contributions to the slot's radiance.
+template <bool COUNT, bool BATCH>
+__global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace_shadow(PathParams p) {
+    VKB_STACK_DECL
+    const uint32_t n = p.counters[2];
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.counters[4], n);
+    const uint32_t lane = threadIdx.x & 31u;
+    TraceCount tc;
+    TraceLane<true, COUNT> L;
+    constexpr uint32_t NONE = 0xffffffffu;
+    uint32_t e = NONE, rid = 0, phase = 0, occ = 0, job = 0;
+    // Starts entry e's next ray from phase ph on; false when the entry has no ray left.
+    auto begin = [&](uint32_t ph) -> bool {
+        const uint32_t flags = __float_as_uint(p.sa_c[e].w);
+        if (ph == 0u) {
+            if ((flags & SH_TRACE_A) && L.start(BATCH ? p.jobs[job].sv : p.job0.sv, RayRef{p.sa_o, p.sa_d, e}, p.sa_o[e].w)) { phase = 0u; rid = e; return true; }
+        }
+        if ((flags & SH_HAS_B) && (flags & SH_TRACE_B)) {
+            const uint32_t slot = __float_as_uint(p.sa_d[e].w);
+            if (L.start(BATCH ? p.jobs[job].sv : p.job0.sv, RayRef{p.sb_o, p.sb_d, slot}, p.sb_o[slot].w)) { phase = 1u; rid = slot; return true; }
+        }
+        return false;
+    };
+    auto finish = [&]() {
+        const float4 sc = p.sa_c[e];
+        const uint32_t slot = __float_as_uint(p.sa_d[e].w), flags = __float_as_uint(sc.w);
+        float3 total = (occ & 1u) ? f3(0.f) : f3(sc.x, sc.y, sc.z);
+        if (flags & SH_HAS_B) {
+            const float4 bc = p.sb_c[slot];
+            if (!(occ & 2u)) total = total + f3(bc.x, bc.y, bc.z);
+        }
+        const float4 r = p.rad[slot];
+        uint32_t dropped = __float_as_uint(r.w);
+        const Job& J = BATCH ? p.jobs[job] : p.job0;
+        const float3 add = clamp_sample(total, (flags & SH_DIRECT) ? J.clamp_direct : J.clamp_indirect, dropped);
+        p.rad[slot] = make_float4(r.x + add.x, r.y + add.y, r.z + add.z, __uint_as_float(dropped));
+        e = NONE;
+    };
+    bool drained = false;
+    for (;;) {
+        uint32_t act = __ballot_sync(0xffffffffu, e != NONE);
+        if (!drained && uint32_t(__popc(act)) <= uint32_t(VKB_TRACE_REFILL)) {
+            const uint32_t idle = ~act;
+            uint32_t base = 0;
+            if (lane == 0u) base = atomicAdd(&p.counters[12], uint32_t(__popc(idle)));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            drained = base + uint32_t(__popc(idle)) >= n;
+            if (e == NONE) {
+                const uint32_t r = base + uint32_t(__popc(idle & ((1u << lane) - 1u)));
+                if (r < n) {
+                    e = r;
+                    occ = 0u;
+                    if (BATCH) job = job_of_slot<true>(p, __float_as_uint(p.sa_d[r].w));
+                    if (!begin(0u)) finish();
+                }
+            }
+            act = __ballot_sync(0xffffffffu, e != NONE);
+        }
+        if (act == 0u) {
+            if (drained) break;
+            continue;
+        }
+        bool done = false;
+        if (e != NONE) {
+            const RayRef ray{phase ? p.sb_o : p.sa_o, phase ? p.sb_d : p.sa_d, rid};
+            if constexpr (BATCH) done = L.step(p.jobs[job].sv, ray, p.err, &tc, stk);
+            else done = L.step(p.job0.sv, ray, p.err, &tc, stk);
+        }
+        if (done) {
+            if (L.found) occ |= phase ? 2u : 1u;
+            if (phase != 0u || !begin(1u)) finish();
+        }
+    }
+    if (COUNT) {
+        flush_count(&p.work[3], tc.nodes);
+        flush_count(&p.work[4], tc.tris);
+        flush_count(&p.work[6], tc.blas_nodes);
     }
 }
 
