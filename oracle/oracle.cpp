@@ -1555,8 +1555,11 @@ void box_morton(uint32_t n, const float* lo, const float* hi, uint32_t* out) {
     }
 }
 // World box of an instance: the 8 transformed corners of its mesh box, each
-// component ((m0*x + m1*y) + m2*z) + m3 in fp32.
-void instance_box(const float* rows, const float mlo[3], const float mhi[3], float lo[3], float hi[3]) {
+// component ((m0*x + m1*y) + m2*z) + m3 in fp32, intersected with the box of the
+// transformed bounding sphere (centre ((m0*cx + m1*cy) + m2*cz) + m3, half extent
+// r * sqrt((m0*m0 + m1*m1) + m2*m2) widened by 1e-5 relative plus 1e-6 of
+// (|centre| + |m3| + extent)); sph[3] < 0 means no sphere.
+void instance_box(const float* rows, const float mlo[3], const float mhi[3], const float sph[4], float lo[3], float hi[3]) {
     for (int a = 0; a < 3; ++a) { lo[a] = INFINITY; hi[a] = -INFINITY; }
     for (int k = 0; k < 8; ++k) {
         float p[3] = {k & 1 ? mhi[0] : mlo[0], k & 2 ? mhi[1] : mlo[1], k & 4 ? mhi[2] : mlo[2]};
@@ -1568,11 +1571,40 @@ void instance_box(const float* rows, const float mlo[3], const float mhi[3], flo
             lo[a] = std::min(lo[a], v); hi[a] = std::max(hi[a], v);
         }
     }
+    if (sph[3] >= 0.f) {
+        for (int a = 0; a < 3; ++a) {
+            const float* m = rows + 4 * a;
+            float cw = m[0] * sph[0];
+            cw = cw + m[1] * sph[1];
+            cw = cw + m[2] * sph[2];
+            cw = cw + m[3];
+            float nn = m[0] * m[0];
+            nn = nn + m[1] * m[1];
+            nn = nn + m[2] * m[2];
+            const float ext = sph[3] * std::sqrt(nn);
+            const float mag = (std::fabs(cw) + std::fabs(m[3])) + ext;
+            const float half = ext * 1.00001f + mag * 1e-6f;
+            lo[a] = std::max(lo[a], cw - half);
+            hi[a] = std::min(hi[a], cw + half);
+        }
+    }
 }
-void mesh_box(const vkb_mesh& m, float lo[3], float hi[3]) {
+// Box and bounding sphere (about the box centre, radius = largest vertex distance in
+// f64 rounded up to fp32; radius -1 without vertices) of a mesh.
+void mesh_box(const vkb_mesh& m, float lo[3], float hi[3], float sph[4]) {
     for (int a = 0; a < 3; ++a) { lo[a] = INFINITY; hi[a] = -INFINITY; }
     for (uint32_t i = 0; i < m.num_vertices; ++i)
         for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], m.positions[3 * i + a]); hi[a] = std::max(hi[a], m.positions[3 * i + a]); }
+    if (m.num_vertices == 0) { sph[0] = sph[1] = sph[2] = 0.f; sph[3] = -1.f; return; }
+    float c[3];
+    for (int a = 0; a < 3; ++a) c[a] = 0.5f * (lo[a] + hi[a]);
+    double r2 = 0.0;
+    for (uint32_t i = 0; i < m.num_vertices; ++i) {
+        double dx = double(m.positions[3 * i]) - c[0], dy = double(m.positions[3 * i + 1]) - c[1], dz = double(m.positions[3 * i + 2]) - c[2];
+        r2 = std::max(r2, dx * dx + dy * dy + dz * dz);
+    }
+    sph[0] = c[0]; sph[1] = c[1]; sph[2] = c[2];
+    sph[3] = std::nextafter(float(std::sqrt(r2)), INFINITY);
 }
 
 }  // namespace
@@ -1691,11 +1723,11 @@ void oracle_render(void* h, int fp64, const vkb_profile* pf, uint32_t x0, uint32
 // Morton codes of the TLAS build (instance boxes) and of one mesh's BLAS build (triangle boxes).
 void oracle_tlas_morton(const vkb_scene_desc* d, uint32_t* out) {
     std::vector<float> lo(3 * size_t(d->num_instances)), hi(3 * size_t(d->num_instances));
-    std::vector<float> mlo(3 * size_t(d->num_meshes)), mhi(3 * size_t(d->num_meshes));
-    for (uint32_t m = 0; m < d->num_meshes; ++m) mesh_box(d->meshes[m], &mlo[3 * m], &mhi[3 * m]);
+    std::vector<float> mlo(3 * size_t(d->num_meshes)), mhi(3 * size_t(d->num_meshes)), msph(4 * size_t(d->num_meshes));
+    for (uint32_t m = 0; m < d->num_meshes; ++m) mesh_box(d->meshes[m], &mlo[3 * m], &mhi[3 * m], &msph[4 * m]);
     for (uint32_t i = 0; i < d->num_instances; ++i) {
         uint32_t m = d->instance_mesh[i];
-        instance_box(d->instance_rows + 12 * size_t(i), &mlo[3 * m], &mhi[3 * m], &lo[3 * i], &hi[3 * i]);
+        instance_box(d->instance_rows + 12 * size_t(i), &mlo[3 * m], &mhi[3 * m], &msph[4 * m], &lo[3 * i], &hi[3 * i]);
     }
     box_morton(d->num_instances, lo.data(), hi.data(), out);
 }

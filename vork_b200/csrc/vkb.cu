@@ -262,6 +262,21 @@ struct SahBlas {
     }
 };
 
+// Bounding sphere of a mesh about its box centre (c = (lo + hi) / 2 in fp32): the radius
+// is the largest vertex distance, in f64, rounded up to fp32; radius -1 for no vertices.
+void mesh_sphere(const float* pos, uint32_t nv, const float lo[3], const float hi[3], float out[4]) {
+    if (nv == 0) { out[0] = out[1] = out[2] = 0.f; out[3] = -1.f; return; }
+    float c[3];
+    for (int a = 0; a < 3; ++a) c[a] = 0.5f * (lo[a] + hi[a]);
+    double r2 = 0.0;
+    for (uint32_t i = 0; i < nv; ++i) {
+        double dx = double(pos[3 * i]) - c[0], dy = double(pos[3 * i + 1]) - c[1], dz = double(pos[3 * i + 2]) - c[2];
+        r2 = std::max(r2, dx * dx + dy * dy + dz * dz);
+    }
+    out[0] = c[0]; out[1] = c[1]; out[2] = c[2];
+    out[3] = std::nextafter(float(std::sqrt(r2)), INFINITY);
+}
+
 // 4-wide BLAS from the binary SAH tree (root 0): the 4-wide children of one node are
 // allocated together, depth first.
 std::vector<Bvh4Node> collapse_blas(const std::vector<BvhNode>& n2) {
@@ -1099,6 +1114,7 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
             for (uint32_t i = 0; i < d->meshes[m].num_vertices; ++i)
                 for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], d->meshes[m].positions[3 * i + a]); hi[a] = std::max(hi[a], d->meshes[m].positions[3 * i + a]); }
             for (int a = 0; a < 3; ++a) { mi.lo[a] = lo[a]; mi.hi[a] = hi[a]; }
+            mesh_sphere(d->meshes[m].positions, d->meshes[m].num_vertices, lo, hi, mi.sphere);
             nv += d->meshes[m].num_vertices; nt += d->meshes[m].num_triangles;
         }
         s->total_tris = nt;

@@ -38,7 +38,8 @@ constexpr uint32_t LEAF_CULL_BACKFACES = 1u;
 struct MeshInfo {
     uint32_t node_offset, tri_offset, index_offset, vertex_offset;
     uint32_t num_triangles, pad0, pad1, pad2;
-    float lo[4], hi[4];
+    float lo[4], hi[4];      // object-space box (xyz)
+    float sphere[4];         // bounding sphere about the box centre: centre xyz, radius (< 0: none)
 };
 
 constexpr int TRACE_STACK = 64;
