@@ -531,7 +531,7 @@ def main():
         sync()
     elapsed_ms = ev0.elapsed_time(ev1)
     launches = s.launch_count - launches0
-    tlas = {"builder": ("PLOC (radius 16)" if args.tlas == "ploc" else "Karras LBVH") + " over 30-bit Morton order, rebuilt every frame",
+    tlas = {"builder": ("PLOC (radius 16)" if args.tlas == "ploc" else "Karras LBVH") + " over 30-bit Morton order (bit 30: boxes wider than a quarter of the centroid spread, split at the root), rebuilt every frame",
             "build_ms_per_frame": build_ms / args.steps,
             **s.tlas_stats()}
     elapsed_ms = max_over_ranks(elapsed_ms, dist, f"cuda:{local}")

@@ -1540,7 +1540,9 @@ inline uint32_t morton3(const float c[3], const float lo[3], const float ext[3])
     }
     return (expand_bits(q[0]) << 2) | (expand_bits(q[1]) << 1) | expand_bits(q[2]);
 }
-void box_morton(uint32_t n, const float* lo, const float* hi, uint32_t* out) {
+// split_large: bit 30 over the code of a box wider on some axis than a quarter of the
+// centroid box's widest extent (the TLAS build's root split).
+void box_morton(uint32_t n, const float* lo, const float* hi, uint32_t* out, bool split_large = false) {
     float slo[3] = {INFINITY, INFINITY, INFINITY}, shi[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (uint32_t i = 0; i < n; ++i)
         for (int a = 0; a < 3; ++a) {
@@ -1548,10 +1550,12 @@ void box_morton(uint32_t n, const float* lo, const float* hi, uint32_t* out) {
             slo[a] = std::min(slo[a], c); shi[a] = std::max(shi[a], c);
         }
     float ext[3] = {shi[0] - slo[0], shi[1] - slo[1], shi[2] - slo[2]};
+    const float big = std::max(ext[0], std::max(ext[1], ext[2])) * 0.25f;
     for (uint32_t i = 0; i < n; ++i) {
         float c[3];
         for (int a = 0; a < 3; ++a) c[a] = (lo[3 * i + a] + hi[3 * i + a]) * 0.5f;
-        out[i] = morton3(c, slo, ext);
+        const float w = std::max(hi[3 * i] - lo[3 * i], std::max(hi[3 * i + 1] - lo[3 * i + 1], hi[3 * i + 2] - lo[3 * i + 2]));
+        out[i] = morton3(c, slo, ext) | (split_large && w > big ? 1u << 30 : 0u);
     }
 }
 // World box of an instance: the 8 transformed corners of its mesh box, each
@@ -1729,7 +1733,7 @@ void oracle_tlas_morton(const vkb_scene_desc* d, uint32_t* out) {
         uint32_t m = d->instance_mesh[i];
         instance_box(d->instance_rows + 12 * size_t(i), &mlo[3 * m], &mhi[3 * m], &msph[4 * m], &lo[3 * i], &hi[3 * i]);
     }
-    box_morton(d->num_instances, lo.data(), hi.data(), out);
+    box_morton(d->num_instances, lo.data(), hi.data(), out, true);
 }
 void oracle_blas_morton(const vkb_scene_desc* d, uint32_t mesh, uint32_t* out) {
     const vkb_mesh& m = d->meshes[mesh];

@@ -307,7 +307,7 @@ struct LbvhScratch {
         codes.alloc(n); codes_sorted.alloc(n); ids.alloc(n); ids_sorted.alloc(n);
         leaf_parent.alloc(n); node_parent.alloc(std::max<size_t>(n, 1)); counters.alloc(std::max<size_t>(n, 1)); bounds.alloc(6);
         size_t bytes = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, bytes, codes.p, codes_sorted.p, ids.p, ids_sorted.p, int(n), 0, 30, s);
+        cub::DeviceRadixSort::SortPairs(nullptr, bytes, codes.p, codes_sorted.p, ids.p, ids_sorted.p, int(n), 0, 31, s);
         cub_temp.alloc(std::max<size_t>(bytes, 1));
     }
 };
@@ -319,9 +319,9 @@ void morton_sort(uint32_t n, const float4* lo, const float4* hi, LbvhScratch& sc
     VKB_CUDA(cudaMemsetAsync(sc.bounds.p, 0xff, 3 * sizeof(uint32_t), s));
     VKB_CUDA(cudaMemsetAsync(sc.bounds.p + 3, 0x00, 3 * sizeof(uint32_t), s));
     k_centroid_box<<<grid_for(n, 256, sms), 256, 0, s>>>(n, lo, hi, sc.bounds.p);
-    k_morton<<<grid_for(n, 256, sms), 256, 0, s>>>(n, lo, hi, sc.bounds.p, sc.codes.p, sc.ids.p);
+    k_morton<<<grid_for(n, 256, sms), 256, 0, s>>>(n, lo, hi, sc.bounds.p, sc.codes.p, sc.ids.p, true);
     size_t bytes = sc.cub_temp.n;
-    VKB_CUDA(cub::DeviceRadixSort::SortPairs(sc.cub_temp.p, bytes, sc.codes.p, sc.codes_sorted.p, sc.ids.p, sc.ids_sorted.p, int(n), 0, 30, s));
+    VKB_CUDA(cub::DeviceRadixSort::SortPairs(sc.cub_temp.p, bytes, sc.codes.p, sc.codes_sorted.p, sc.ids.p, sc.ids_sorted.p, int(n), 0, 31, s));
 }
 
 // Build one LBVH over n boxes into nodes (n-1 internal nodes, or 1 for n == 1).
@@ -1557,7 +1557,7 @@ vkb_status vkb_debug_blas_morton(vkb_scene* s, uint32_t mesh, uint32_t* out) {
         VKB_CUDA(cudaMemsetAsync(s->scratch.bounds.p, 0xff, 3 * sizeof(uint32_t), st));
         VKB_CUDA(cudaMemsetAsync(s->scratch.bounds.p + 3, 0x00, 3 * sizeof(uint32_t), st));
         k_centroid_box<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->tri_lo.p, s->tri_hi.p, s->scratch.bounds.p);
-        k_morton<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->tri_lo.p, s->tri_hi.p, s->scratch.bounds.p, s->scratch.codes.p, s->scratch.ids.p);
+        k_morton<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->tri_lo.p, s->tri_hi.p, s->scratch.bounds.p, s->scratch.codes.p, s->scratch.ids.p, false);
         VKB_CUDA(cudaMemcpyAsync(out, s->scratch.codes.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         VKB_CUDA(cudaStreamSynchronize(st));
     });

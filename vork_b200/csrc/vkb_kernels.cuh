@@ -143,12 +143,19 @@ __global__ void k_centroid_box(uint32_t n, const float4* lo, const float4* hi, u
     if ((threadIdx.x & 31) == 0)
         for (int k = 0; k < 3; ++k) { atomicMin(&bounds[k], mn[k]); atomicMax(&bounds[3 + k], mx[k]); }
 }
-__global__ void k_morton(uint32_t n, const float4* lo, const float4* hi, const uint32_t* bounds, uint32_t* codes, uint32_t* ids) {
+// split_large: a box wider on some axis than a quarter of the centroid box's widest
+// extent gets bit 30 over its 30-bit code, so the hierarchy's root split separates such
+// boxes (a terrain instance) from the rest and their size does not inflate the boxes
+// of every node on their Morton path.
+__global__ void k_morton(uint32_t n, const float4* lo, const float4* hi, const uint32_t* bounds, uint32_t* codes, uint32_t* ids, bool split_large) {
     float3 slo = f3(float_unflip(bounds[0]), float_unflip(bounds[1]), float_unflip(bounds[2]));
     float3 shi = f3(float_unflip(bounds[3]), float_unflip(bounds[4]), float_unflip(bounds[5]));
     float3 ext = f3(__fsub_rn(shi.x, slo.x), __fsub_rn(shi.y, slo.y), __fsub_rn(shi.z, slo.z));
+    const float big = __fmul_rn(fmaxf(ext.x, fmaxf(ext.y, ext.z)), 0.25f);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        codes[i] = morton_code(lo[i], hi[i], slo, ext);
+        const float4 l = lo[i], h = hi[i];
+        const float w = fmaxf(__fsub_rn(h.x, l.x), fmaxf(__fsub_rn(h.y, l.y), __fsub_rn(h.z, l.z)));
+        codes[i] = morton_code(l, h, slo, ext) | (split_large && w > big ? 1u << 30 : 0u);
         ids[i] = i;
     }
 }
