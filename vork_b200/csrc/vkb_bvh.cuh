@@ -42,15 +42,31 @@ struct MeshInfo {
     float sphere[4];         // bounding sphere about the box centre: centre xyz, radius (< 0: none)
 };
 
-constexpr int TRACE_STACK = 64;
 #ifndef VKB_SMEM_STACK
-#define VKB_SMEM_STACK 48
+#define VKB_SMEM_STACK 24
 #endif
-// Traversal stacks live in shared memory as [entry][thread]: lane l of a 128-thread
-// block always touches bank l, whatever depth each lane is at (no bank conflicts).
+#ifndef VKB_SPILL_STACK
+#define VKB_SPILL_STACK 40
+#endif
+// Traversal stacks: the first SMEM_STACK entries live in shared memory as
+// [entry][thread] (lane l of a 128-thread block always touches bank l, whatever depth
+// each lane is at: no bank conflicts); deeper entries go to a per-thread local array of
+// SPILL_STACK entries.  Shared memory not taken by stacks serves as L1 for the nodes.
 constexpr int SMEM_STACK = VKB_SMEM_STACK;
+constexpr int SPILL_STACK = VKB_SPILL_STACK;
+constexpr int STACK_CAP = SMEM_STACK + SPILL_STACK;
 constexpr int TRACE_BLOCK = 128;
-struct TraceStack { int* r; };
+struct TraceStack {
+    int* r;
+    int* spill;
+    __device__ __forceinline__ void put(int i, int v) {
+        if (SPILL_STACK == 0 || i < SMEM_STACK) r[i * TRACE_BLOCK] = v;
+        else spill[i - SMEM_STACK] = v;
+    }
+    __device__ __forceinline__ int get(int i) const {
+        return (SPILL_STACK == 0 || i < SMEM_STACK) ? r[i * TRACE_BLOCK] : spill[i - SMEM_STACK];
+    }
+};
 constexpr uint32_t TRACE_STEP_LIMIT = 1u << 16;
 constexpr int SENTINEL = 0x7fffffff;
 
@@ -244,10 +260,10 @@ struct TraceLane {
             if (k0 != 0xffffffffu) {
                 if (k1 != 0xffffffffu) {
                     const int pushes = 1 + (k2 != 0xffffffffu) + (k3 != 0xffffffffu);
-                    if (sp + pushes > SMEM_STACK) { atomicOr(err, 1u); return true; }
-                    if (k3 != 0xffffffffu) { stk.r[sp * TRACE_BLOCK] = slot_child(ch, k3); ++sp; }
-                    if (k2 != 0xffffffffu) { stk.r[sp * TRACE_BLOCK] = slot_child(ch, k2); ++sp; }
-                    stk.r[sp * TRACE_BLOCK] = slot_child(ch, k1); ++sp;
+                    if (sp + pushes > STACK_CAP) { atomicOr(err, 1u); return true; }
+                    if (k3 != 0xffffffffu) { stk.put(sp, slot_child(ch, k3)); ++sp; }
+                    if (k2 != 0xffffffffu) { stk.put(sp, slot_child(ch, k2)); ++sp; }
+                    stk.put(sp, slot_child(ch, k1)); ++sp;
                 }
                 node = slot_child(ch, k0);
                 return false;
@@ -265,8 +281,8 @@ struct TraceLane {
             nodes = s.blas_nodes + info.y;
             tri_base = info.z;
             cull = !ANY && (info.w & LEAF_CULL_BACKFACES);
-            if (sp >= SMEM_STACK) { atomicOr(err, 1u); return true; }
-            stk.r[sp * TRACE_BLOCK] = SENTINEL;
+            if (sp >= STACK_CAP) { atomicOr(err, 1u); return true; }
+            stk.put(sp, SENTINEL);
             ++sp;
             in_blas = true;
             node = 0;
@@ -289,14 +305,14 @@ struct TraceLane {
         // pop
         if (sp == 0) return true;
         --sp;
-        node = stk.r[sp * TRACE_BLOCK];
+        node = stk.get(sp);
         while (node == SENTINEL) {
             in_blas = false;
             make_space(rs, ray.origin(), ray.dir());
             nodes = s.tlas_nodes;
             if (sp == 0) return true;
             --sp;
-            node = stk.r[sp * TRACE_BLOCK];
+            node = stk.get(sp);
         }
         return false;
     }

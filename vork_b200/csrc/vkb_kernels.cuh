@@ -552,7 +552,8 @@ __device__ __forceinline__ bool trace_any(const SceneView& sv, RayRef ray, float
 // This thread's column of the block's shared-memory traversal stack.
 #define VKB_STACK_DECL                                                                                   \
     __shared__ int stack_r_[SMEM_STACK * TRACE_BLOCK];                                                  \
-    TraceStack stk{stack_r_ + threadIdx.x};
+    int stack_spill_[SPILL_STACK > 0 ? SPILL_STACK : 1];                                                \
+    TraceStack stk{stack_r_ + threadIdx.x, stack_spill_};
 // Lanes of a warp refill together once at most this many are still tracing.
 #ifndef VKB_TRACE_REFILL
 #define VKB_TRACE_REFILL 20
