@@ -148,8 +148,9 @@ __device__ __forceinline__ uint32_t slot_key(float nx, float ny, float nz, float
 }
 __device__ __forceinline__ void key_order(uint32_t& a, uint32_t& b) { uint32_t l = min(a, b); b = max(a, b); a = l; }
 __device__ __forceinline__ int slot_child(const int4& c, uint32_t key) {
-    uint32_t k = key & 3u;
-    return k == 0u ? c.x : (k == 1u ? c.y : (k == 2u ? c.z : c.w));
+    const bool odd = (key & 1u) != 0u;
+    const int lo = odd ? c.y : c.x, hi = odd ? c.w : c.z;
+    return (key & 2u) ? hi : lo;
 }
 // Watertight ray/triangle test. cull: accept front faces only (counter-clockwise
 // winding seen from the ray origin).  Returns t and barycentrics of vertices 1, 2.
@@ -260,10 +261,17 @@ struct TraceLane {
             if (k0 != 0xffffffffu) {
                 if (k1 != 0xffffffffu) {
                     const int pushes = 1 + (k2 != 0xffffffffu) + (k3 != 0xffffffffu);
-                    if (sp + pushes > STACK_CAP) { atomicOr(err, 1u); return true; }
-                    if (k3 != 0xffffffffu) { stk.put(sp, slot_child(ch, k3)); ++sp; }
-                    if (k2 != 0xffffffffu) { stk.put(sp, slot_child(ch, k2)); ++sp; }
-                    stk.put(sp, slot_child(ch, k1)); ++sp;
+                    if (sp + pushes <= SMEM_STACK) {
+                        // all in shared memory: one bound check for the three
+                        if (k3 != 0xffffffffu) { stk.r[sp * TRACE_BLOCK] = slot_child(ch, k3); ++sp; }
+                        if (k2 != 0xffffffffu) { stk.r[sp * TRACE_BLOCK] = slot_child(ch, k2); ++sp; }
+                        stk.r[sp * TRACE_BLOCK] = slot_child(ch, k1); ++sp;
+                    } else {
+                        if (sp + pushes > STACK_CAP) { atomicOr(err, 1u); return true; }
+                        if (k3 != 0xffffffffu) { stk.put(sp, slot_child(ch, k3)); ++sp; }
+                        if (k2 != 0xffffffffu) { stk.put(sp, slot_child(ch, k2)); ++sp; }
+                        stk.put(sp, slot_child(ch, k1)); ++sp;
+                    }
                 }
                 node = slot_child(ch, k0);
                 return false;
