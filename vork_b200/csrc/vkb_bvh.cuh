@@ -244,6 +244,8 @@ struct TraceLane {
     // One step; returns true when the ray is finished (hit/found hold the result).
     __device__ __forceinline__ bool step(const SceneView& s, RayRef ray, uint32_t* err, TraceCount* count, TraceStack stk) {
         if (++steps >= TRACE_STEP_LIMIT) { atomicOr(err, 2u); return true; }
+        bool respace = false;
+        float3 so, sd;
         if (node >= 0) {
             if (COUNT) { count->nodes++; if (in_blas) count->blas_nodes++; }
             const float4* p = reinterpret_cast<const float4*>(nodes + node);
@@ -282,9 +284,8 @@ struct TraceLane {
             float4 r0 = __ldg(&lf->w2o[0]), r1 = __ldg(&lf->w2o[1]), r2 = __ldg(&lf->w2o[2]);
             uint4 info = __ldg(reinterpret_cast<const uint4*>(&lf->instance));
             const float3 o = ray.origin(), d = ray.dir();
-            float3 oo = f3(r0.x * o.x + r0.y * o.y + r0.z * o.z + r0.w, r1.x * o.x + r1.y * o.y + r1.z * o.z + r1.w, r2.x * o.x + r2.y * o.y + r2.z * o.z + r2.w);
-            float3 od = f3(r0.x * d.x + r0.y * d.y + r0.z * d.z, r1.x * d.x + r1.y * d.y + r1.z * d.z, r2.x * d.x + r2.y * d.y + r2.z * d.z);
-            make_space(rs, oo, od);
+            so = f3(r0.x * o.x + r0.y * o.y + r0.z * o.z + r0.w, r1.x * o.x + r1.y * o.y + r1.z * o.z + r1.w, r2.x * o.x + r2.y * o.y + r2.z * o.z + r2.w);
+            sd = f3(r0.x * d.x + r0.y * d.y + r0.z * d.z, r1.x * d.x + r1.y * d.y + r1.z * d.z, r2.x * d.x + r2.y * d.y + r2.z * d.z);
             cur_instance = info.x;
             nodes = s.blas_nodes + info.y;
             tri_base = info.z;
@@ -294,7 +295,7 @@ struct TraceLane {
             ++sp;
             in_blas = true;
             node = 0;
-            return false;
+            respace = true;
         } else {
             // BLAS leaf: up to VKB_BLAS_LEAF_MAX triangles in leaf order, ~((first << 2) | (count - 1)).
             uint32_t v = uint32_t(~node), first = v >> 2, cnt = VKB_BLAS_LEAF_MAX == 1 ? 1u : (v & 3u) + 1u;
@@ -310,18 +311,24 @@ struct TraceLane {
                 }
             }
         }
-        // pop
-        if (sp == 0) return true;
-        --sp;
-        node = stk.get(sp);
-        while (node == SENTINEL) {
-            in_blas = false;
-            make_space(rs, ray.origin(), ray.dir());
-            nodes = s.tlas_nodes;
+        if (!respace) {
+            // pop; leaving an instance (its sentinel) goes back to the world ray
             if (sp == 0) return true;
             --sp;
             node = stk.get(sp);
+            if (node != SENTINEL) return false;
+            while (node == SENTINEL) {
+                in_blas = false;
+                nodes = s.tlas_nodes;
+                if (sp == 0) return true;
+                --sp;
+                node = stk.get(sp);
+            }
+            so = ray.origin();
+            sd = ray.dir();
         }
+        // the one ray-space set-up of a step (instance entry or exit)
+        make_space(rs, so, sd);
         return false;
     }
 };
