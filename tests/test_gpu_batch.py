@@ -42,7 +42,7 @@ def test_autotune_picks_a_candidate_and_keeps_results(renderer):
     try:
         before = [inst.render(p).image for inst, p in items]
         r = renderer.autotune(items)
-        assert r["best_ms"] > 0 and len(r["tried"]) == 12
+        assert r["best_ms"] > 0 and len(r["tried"]) == 15   # 5 capacities x 3 grids
         assert r["best_capacity"] in [c for c, _, _ in r["tried"]]
         after, _ = renderer.render_batch(items)
         for x, y in zip(before, after):

@@ -440,8 +440,8 @@ struct vkb_ctx {
     Wavefront wave;
     DBuf<float4> accum, staging;        // per-render accumulators and host-output staging (all jobs of a call)
     DBuf<uint32_t> ids;                 // primary ids of the jobs that asked for them
-    size_t wave_capacity = 8u << 20;    // path slots per wave (autotuned)
-    int trace_blocks_per_sm = 16;       // trace/shade grid = SMs x this (autotuned)
+    size_t wave_capacity = 32u << 20;   // path slots per wave (autotuned); 7.4 GB of queues when full
+    int trace_blocks_per_sm = 64;       // trace/shade grid = SMs x this (autotuned)
     uint64_t launches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<cudaEvent_t> kernel_events;
@@ -1319,8 +1319,8 @@ vkb_status vkb_autotune(vkb_ctx* c, vkb_job* jobs, uint32_t njobs, vkb_tune_resu
         VKB_CUDA(cudaSetDevice(c->device));
         // Candidates: wave capacity (queue slots) x trace/shade blocks per SM, each timed on
         // one sample of every job (same work for every candidate).
-        const size_t caps[] = {size_t(2) << 20, size_t(4) << 20, size_t(8) << 20, size_t(16) << 20};
-        const int grids[] = {8, 16, 32};
+        const size_t caps[] = {size_t(2) << 20, size_t(4) << 20, size_t(8) << 20, size_t(16) << 20, size_t(32) << 20};
+        const int grids[] = {16, 32, 64};
         std::vector<std::pair<vkb_scene*, vkb_profile>> in(njobs);
         std::vector<vkb_output> o(njobs);
         std::vector<vkb_output*> outs(njobs);

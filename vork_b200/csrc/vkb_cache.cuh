@@ -289,8 +289,17 @@ vkb_status vkb_cache_train(vkb_cache* k, const vkb_profile* pf, vkb_cache_stats*
         k->train_calls++;
         // train_steps interleaved minibatches: step i takes records i, i + steps, ... (each
         // spread over the whole image), so one round visits every record once.
-        VKB_CUDA(cudaEventRecord(k->ev[2], st));
         const uint32_t steps = std::min(k->cfg.train_steps, std::max(1u, count));
+        {
+            // Per-tile partials of the largest step, grown here (a power of two of tiles, so
+            // rarely) rather than inside the timed steps: a reallocation synchronises.
+            const size_t tiles = (size_t((count + steps - 1) / steps) + TILE - 1) / TILE;
+            size_t t2 = 1;
+            while (t2 < tiles) t2 <<= 1;
+            k->wpartial.alloc(t2 * MLP_PARAMS);
+            k->loss_partial.alloc(t2);
+        }
+        VKB_CUDA(cudaEventRecord(k->ev[2], st));
         for (uint32_t i = 0; i < steps && count > 0; ++i) nrc_step(k, count, true, nullptr, nullptr, i, steps, false);
         VKB_CUDA(cudaEventRecord(k->ev[3], st));
         VKB_CUDA(cudaEventSynchronize(k->ev[3]));
