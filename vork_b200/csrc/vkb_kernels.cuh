@@ -792,8 +792,10 @@ __device__ __forceinline__ float3 light_threshold(float3 value, float threshold,
 
 // One radiance-cache record of this vertex: queries append (warp-aggregated on
 // counters[9]); training records go to their fixed position.
-__device__ __noinline__ void cache_append(const PathParams& p, float3 world, float3 view, float3 normal, const Closure& c, uint32_t slot,
-                                          uint32_t vertex, float3 thr, float3 rad) {
+// The closure values it stores come by value, so the caller's closure need not have an
+// address (a reference to it kept the closure in local memory).
+__device__ __noinline__ void cache_append(const PathParams& p, float3 world, float3 view, float3 normal, float roughness, float metalness,
+                                          float3 base_color, uint32_t slot, uint32_t vertex, float3 thr, float3 rad) {
     uint32_t idx;
     if (p.cache.mode == 1u) {
         namespace cg = cooperative_groups;
@@ -812,8 +814,8 @@ __device__ __noinline__ void cache_append(const PathParams& p, float3 world, flo
     float4* r = p.cache.rec + 4 * size_t(idx);
     r[0] = make_float4(q.x, q.y, q.z, view.x);
     r[1] = make_float4(view.y, view.z, normal.x, normal.y);
-    r[2] = make_float4(normal.z, c.specular_roughness, c.base_metalness, c.base_color.x);
-    r[3] = make_float4(c.base_color.y, c.base_color.z, 0.f, 0.f);
+    r[2] = make_float4(normal.z, roughness, metalness, base_color.x);
+    r[3] = make_float4(base_color.y, base_color.z, 0.f, 0.f);
     if (p.cache.mode == 1u) {
         p.cache.slot[idx] = slot;
     } else {
@@ -824,11 +826,11 @@ __device__ __noinline__ void cache_append(const PathParams& p, float3 world, flo
 }
 
 // integrate's per-vertex body (path.slang:1340-1709) for one queued extension hit.
-template <bool BATCH>
 // The parameter block is __grid_constant__: `J = p.job0` then refers to it in place
 // (a plain by-value parameter that is referenced gets copied to a 736-byte local frame
 // per thread); 4 blocks of 128 per SM (128 registers, a small spill) measured faster
 // than 3 blocks at 158 registers.
+template <bool BATCH>
 __global__ void __launch_bounds__(128, 4) k_shade(const __grid_constant__ PathParams p, int cur) {
     const int nxt = cur ^ 1;
     uint32_t n = p.counters[cur];
@@ -888,7 +890,7 @@ __global__ void __launch_bounds__(128, 4) k_shade(const __grid_constant__ PathPa
                 // Radiance cache: record this vertex, and at the query vertex stop the path
                 // here (the query kernel adds thr x the cached outgoing radiance).
                 const bool cache_query = p.cache.mode == 1u && bounce >= p.cache.vertex;
-                if (cache_query || (p.cache.mode == 2u && bounce >= 1u)) cache_append(p, s.world, view, s.geometric, c, slot, bounce, thr, rad);
+                if (cache_query || (p.cache.mode == 2u && bounce >= 1u)) cache_append(p, s.world, view, s.geometric, c.specular_roughness, c.base_metalness, c.base_color, slot, bounce, thr, rad);
                 if (!cache_query) {
                 float3 iface = dot(s.geometric, view) > 0.f ? s.geometric : s.face;
                 Prepared pr = transport_prepare(p.lut, c, view, s.geometric, iface);
