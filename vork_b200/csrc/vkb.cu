@@ -461,7 +461,8 @@ struct vkb_scene {
     vkb_camera camera{};
     vkb_environment env{};
     uint32_t tree_nodes = 0;
-    std::vector<float> host_rows;  // last rows from the host, for the changed-bytes count
+    DBuf<float4> o2w_next;                    // rows of an update, compared with o2w on the device
+    DBuf<unsigned long long> changed;         // its changed-bytes count
     // device scene
     DBuf<float4> vpos, vnrm, blas_tris, o2w, w2o, inst_lo, inst_hi, tri_lo, tri_hi;
     DBuf<uint32_t> indices, tlas_codes;
@@ -1197,7 +1198,6 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         for (uint32_t i = 0; i < n; ++i) info[i] = make_uint4(d->instance_mesh[i], d->instance_material[i], 0u, 0u);
         s->inst_info.upload(info.data(), n, str);
         s->o2w.upload(reinterpret_cast<const float4*>(d->instance_rows), size_t(n) * 3, str);
-        s->host_rows.assign(d->instance_rows, d->instance_rows + size_t(n) * 12);
         s->w2o.alloc(size_t(n) * 3);
         s->inst_lo.alloc(n); s->inst_hi.alloc(n);
         s->tlas_nodes.alloc(std::max(1u, n > 1 ? n - 1 : 1u));
@@ -1220,8 +1220,9 @@ vkb_status vkb_scene_destroy(vkb_scene* s) {
     if (!s) return VKB_OK;
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->ctx->stream);
-    DBuf<float4>* f4[] = {&s->vpos, &s->vnrm, &s->blas_tris, &s->o2w, &s->w2o, &s->inst_lo, &s->inst_hi, &s->tri_lo, &s->tri_hi};
+    DBuf<float4>* f4[] = {&s->vpos, &s->vnrm, &s->blas_tris, &s->o2w, &s->o2w_next, &s->w2o, &s->inst_lo, &s->inst_hi, &s->tri_lo, &s->tri_hi};
     for (auto* b : f4) b->release();
+    s->changed.release();
     s->indices.release(); s->tlas_codes.release();
     s->tlas_order.release(); s->tlas_leaf_parent.release(); s->tlas_node_parent.release(); s->tlas_counters.release(); s->inst_info.release(); s->meshes.release();
     s->blas4.release(); s->tlas4.release(); s->tlas_odd.release(); s->tlas_nodes.release(); s->tlas_leaves.release(); s->d_materials.release(); s->d_lights.release();
@@ -1243,17 +1244,21 @@ vkb_status vkb_scene_update_instances(vkb_scene* s, const float* rows, uint32_t 
     if (policy < 0 || policy > 2) return fail(VKB_INVALID_ARG, "policy must be 0, 1 or 2");
     return guarded([&] {
         VKB_CUDA(cudaSetDevice(s->ctx->device));
-        // Changed bytes: rows that differ from the installed ones (host copy kept per scene).
-        uint64_t changed = 0;
-        if (s->host_rows.size() == size_t(n) * 12) {
-            for (uint32_t i = 0; i < n; ++i)
-                if (std::memcmp(&s->host_rows[12 * size_t(i)], rows + 12 * size_t(i), 48) != 0) changed += 48;
-        } else {
-            changed = uint64_t(n) * 48u;
-        }
-        s->host_rows.assign(rows, rows + size_t(n) * 12);
+        // Changed bytes: rows that differ from the installed ones, counted on the device
+        // (the new rows go up once; only the count comes back).
+        cudaStream_t st = s->ctx->stream;
+        s->o2w_next.alloc(size_t(n) * 3);
+        s->changed.alloc(1);
+        VKB_CUDA(cudaMemcpyAsync(s->o2w_next.p, rows, size_t(n) * 3 * sizeof(float4), cudaMemcpyHostToDevice, st));
+        VKB_CUDA(cudaMemsetAsync(s->changed.p, 0, sizeof(unsigned long long), st));
+        k_changed_rows<<<grid_for(n, 256, s->ctx->sms), 256, 0, st>>>(n, reinterpret_cast<const uint4*>(s->o2w_next.p),
+                                                                      reinterpret_cast<const uint4*>(s->o2w.p), s->changed.p);
+        s->launches += 1;
+        unsigned long long changed = 0;
+        VKB_CUDA(cudaMemcpyAsync(&changed, s->changed.p, sizeof(changed), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaStreamSynchronize(st));
         if (changed == 0 && policy == 0) return;
-        s->o2w.upload(reinterpret_cast<const float4*>(rows), size_t(n) * 3, s->ctx->stream);
+        VKB_CUDA(cudaMemcpyAsync(s->o2w.p, s->o2w_next.p, size_t(n) * 3 * sizeof(float4), cudaMemcpyDeviceToDevice, st));
         update_tlas(s, changed, policy);
     });
 }
@@ -1265,7 +1270,7 @@ vkb_status vkb_scene_update_instances_device(vkb_scene* s, const float* rows, ui
     return guarded([&] {
         VKB_CUDA(cudaSetDevice(s->ctx->device));
         VKB_CUDA(cudaMemcpyAsync(s->o2w.p, rows, size_t(n) * 3 * sizeof(float4), cudaMemcpyDeviceToDevice, s->ctx->stream));
-        s->host_rows.clear();  // device rows: every row counts as changed
+        // device rows: every row counts as changed
         update_tlas(s, uint64_t(n) * 48u, policy);
     });
 }

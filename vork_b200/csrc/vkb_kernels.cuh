@@ -127,6 +127,20 @@ __global__ void k_instances(uint32_t n, const float4* o2w, const uint4* info, co
         w2o[3 * i + 2] = make_float4(i20, i21, i22, -(i20 * r0.w + i21 * r1.w + i22 * r2.w));
     }
 }
+// Changed object bytes of an instance update (rt.rs:1465-1476 counts the object bytes
+// that differ): 48 for every 3x4 row block whose bits differ from the installed one.
+__global__ void k_changed_rows(uint32_t n, const uint4* next, const uint4* cur, unsigned long long* changed) {
+    unsigned long long local = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint4 a0 = next[3 * i], a1 = next[3 * i + 1], a2 = next[3 * i + 2];
+        const uint4 b0 = cur[3 * i], b1 = cur[3 * i + 1], b2 = cur[3 * i + 2];
+        const uint32_t d = (a0.x ^ b0.x) | (a0.y ^ b0.y) | (a0.z ^ b0.z) | (a0.w ^ b0.w) | (a1.x ^ b1.x) | (a1.y ^ b1.y) | (a1.z ^ b1.z) |
+                           (a1.w ^ b1.w) | (a2.x ^ b2.x) | (a2.y ^ b2.y) | (a2.z ^ b2.z) | (a2.w ^ b2.w);
+        if (d) local += 48ull;
+    }
+    for (int off = 16; off > 0; off >>= 1) local += __shfl_xor_sync(0xffffffffu, local, off);
+    if ((threadIdx.x & 31u) == 0u && local) atomicAdd(changed, local);
+}
 // Centroid box: bounds[0..2] flipped minima, bounds[3..5] flipped maxima.
 __global__ void k_centroid_box(uint32_t n, const float4* lo, const float4* hi, uint32_t* bounds) {
     uint32_t mn[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, mx[3] = {0u, 0u, 0u};
