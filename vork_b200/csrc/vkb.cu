@@ -464,7 +464,7 @@ struct vkb_scene {
     DBuf<float4> o2w_next;                    // rows of an update, compared with o2w on the device
     DBuf<unsigned long long> changed;         // its changed-bytes count
     // device scene
-    DBuf<float4> vpos, vnrm, blas_tris, o2w, w2o, inst_lo, inst_hi, tri_lo, tri_hi;
+    DBuf<float4> vpos, vnrm, blas_tris, tri_nrm, o2w, w2o, inst_lo, inst_hi, tri_lo, tri_hi;
     DBuf<uint32_t> indices, tlas_codes;
     DBuf<uint32_t> tlas_order, tlas_leaf_parent, tlas_node_parent, tlas_counters;  // TLAS topology kept for refits
     uint64_t motion_bytes = 0, tlas_rebuilds = 0, tlas_refits = 0;
@@ -657,7 +657,7 @@ Job make_job(const EngineJob& e) {
     Job j{};
     j.sv = scene_view(s);
     j.o2w = s->o2w.p; j.w2o = s->w2o.p; j.inst_info = s->inst_info.p; j.meshes = s->meshes.p;
-    j.vpos = s->vpos.p; j.vnrm = s->vnrm.p; j.indices = s->indices.p;
+    j.tri_nrm = s->tri_nrm.p;
     j.materials = s->d_materials.p; j.lights = s->d_lights.p; j.num_lights = uint32_t(s->lights.size());
     j.tree = s->tree.p; j.tree_nodes = s->tree_nodes;
     j.cam = e.own_camera ? e.camera : s->camera; j.env = s->env;
@@ -1140,7 +1140,7 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         s->tri_lo.alloc(std::max(1u, max_tris)); s->tri_hi.alloc(std::max(1u, max_tris));
         VKB_CUDA(cudaEventRecord(s->ev0, str));
         std::vector<Bvh4Node> all_nodes;
-        std::vector<float4> all_tris(std::max<size_t>(1, size_t(nt) * 3));
+        std::vector<float4> all_tris(std::max<size_t>(1, size_t(nt) * 3)), all_nrm(std::max<size_t>(1, size_t(nt) * 3));
         for (uint32_t m = 0; m < d->num_meshes; ++m) {
             MeshInfo& mi = s->mesh_info[m];
             const vkb_mesh& me = d->meshes[m];
@@ -1171,12 +1171,17 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
                 all_tris[o] = make_float4(p0[0], p0[1], p0[2], tid);
                 all_tris[o + 1] = make_float4(p1[0], p1[1], p1[2], 0.f);
                 all_tris[o + 2] = make_float4(p2[0], p2[1], p2[2], 0.f);
+                for (int c = 0; c < 3; ++c) {
+                    const float* nv = me.normals ? me.normals + 3 * me.indices[3 * t + c] : nullptr;
+                    all_nrm[o + c] = nv ? make_float4(nv[0], nv[1], nv[2], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
             }
         }
         if (all_nodes.empty()) all_nodes.emplace_back();
         s->blas4.alloc(all_nodes.size());
         VKB_CUDA(cudaMemcpyAsync(s->blas4.p, all_nodes.data(), all_nodes.size() * sizeof(Bvh4Node), cudaMemcpyHostToDevice, str));
         VKB_CUDA(cudaMemcpyAsync(s->blas_tris.p, all_tris.data(), all_tris.size() * sizeof(float4), cudaMemcpyHostToDevice, str));
+        s->tri_nrm.upload(all_nrm.data(), all_nrm.size(), str);
         VKB_CUDA(cudaStreamSynchronize(str));
         VKB_CUDA(cudaEventRecord(s->ev1, str));
         s->meshes.upload(s->mesh_info.data(), s->mesh_info.size(), str);
@@ -1220,7 +1225,7 @@ vkb_status vkb_scene_destroy(vkb_scene* s) {
     if (!s) return VKB_OK;
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->ctx->stream);
-    DBuf<float4>* f4[] = {&s->vpos, &s->vnrm, &s->blas_tris, &s->o2w, &s->o2w_next, &s->w2o, &s->inst_lo, &s->inst_hi, &s->tri_lo, &s->tri_hi};
+    DBuf<float4>* f4[] = {&s->vpos, &s->vnrm, &s->blas_tris, &s->tri_nrm, &s->o2w, &s->o2w_next, &s->w2o, &s->inst_lo, &s->inst_hi, &s->tri_lo, &s->tri_hi};
     for (auto* b : f4) b->release();
     s->changed.release();
     s->indices.release(); s->tlas_codes.release();
@@ -1391,7 +1396,7 @@ vkb_status vkb_scene_info(vkb_scene* s, vkb_scene_info_t* out) {
     out->tlas_refits = s->tlas_refits;
     out->motion_bytes = s->motion_bytes;
     size_t dev = 0;
-    dev += s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas4.n * sizeof(Bvh4Node) + s->blas_tris.n * sizeof(float4);
+    dev += s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas4.n * sizeof(Bvh4Node) + (s->blas_tris.n + s->tri_nrm.n) * sizeof(float4);
     dev += s->tlas_nodes.n * sizeof(BvhNode) + s->tlas4.n * sizeof(Bvh4Node) + s->tlas_odd.n + s->tlas_leaves.n * sizeof(TlasLeaf) + (s->o2w.n + s->w2o.n) * sizeof(float4);
     out->scene_bytes = dev;
     out->build_ms = s->build_ms;
@@ -1626,7 +1631,7 @@ struct vkb_server {
 namespace {
 uint64_t scene_bytes(const vkb_scene* s) {
     return s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas4.n * sizeof(Bvh4Node) +
-           s->blas_tris.n * sizeof(float4) + s->tlas_nodes.n * sizeof(BvhNode) + s->tlas4.n * sizeof(Bvh4Node) + s->tlas_odd.n + s->tlas_leaves.n * sizeof(TlasLeaf) +
+           (s->blas_tris.n + s->tri_nrm.n) * sizeof(float4) + s->tlas_nodes.n * sizeof(BvhNode) + s->tlas4.n * sizeof(Bvh4Node) + s->tlas_odd.n + s->tlas_leaves.n * sizeof(TlasLeaf) +
            (s->o2w.n + s->w2o.n) * sizeof(float4);
 }
 uint64_t resident_bytes(const vkb_server* v) {

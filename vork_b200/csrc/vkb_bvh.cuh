@@ -194,7 +194,9 @@ __device__ __forceinline__ bool tri_test(const RaySpace& r, float3 v0, float3 v1
 #endif
 static_assert(VKB_BLAS_LEAF_MAX >= 1 && VKB_BLAS_LEAF_MAX <= 4, "leaf counts are stored in two bits");
 
-struct HitRecord { float t, u, v; uint32_t prim, inst; };
+// tri: the hit triangle's position in BLAS leaf order (global index into blas_tris; its
+// original id is blas_tris[3 * tri].w), inst: the original instance id.
+struct HitRecord { float t, u, v; uint32_t tri, inst; };
 
 // A world ray in global memory: entry i of an origin queue and a direction queue (xyz of
 // float4).  Traversal re-reads it when it enters or leaves an instance instead of keeping
@@ -314,7 +316,7 @@ struct TraceLane {
                 float t, b1, b2;
                 if (tri_test(rs, f3(v0.x, v0.y, v0.z), f3(v1.x, v1.y, v1.z), f3(v2.x, v2.y, v2.z), cull, tbest, t, b1, b2)) {
                     tbest = t; found = true;
-                    hit.t = t; hit.u = b1; hit.v = b2; hit.prim = __float_as_uint(v0.w); hit.inst = cur_instance;
+                    hit.t = t; hit.u = b1; hit.v = b2; hit.tri = tri_base + first + k; hit.inst = cur_instance;
                     if (ANY) return true;
                 }
             }

@@ -425,7 +425,7 @@ __global__ void k_tlas_leaves(uint32_t n, const uint32_t* sorted_ids, const floa
 struct Job {
     SceneView sv;
     const float4* o2w; const float4* w2o; const uint4* inst_info; const MeshInfo* meshes;
-    const float4* vpos; const float4* vnrm; const uint32_t* indices;
+    const float4* tri_nrm;   // vertex normals of every triangle in BLAS leaf order (3 per triangle, beside sv.blas_tris)
     const vkb_material* materials; const vkb_light* lights; uint32_t num_lights;
     const LightTreeNode* tree; uint32_t tree_nodes;
     vkb_camera cam; vkb_environment env;
@@ -622,7 +622,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace(Pat
             else done = L.step(p.job0.sv, RayRef{p.ray_o[cur], p.ray_d[cur], ray}, p.err, &tc, stk);
         }
         if (done) {
-            p.hit[ray] = L.found ? make_float4(L.hit.t, L.hit.u, L.hit.v, __uint_as_float(L.hit.prim)) : make_float4(-1.f, 0.f, 0.f, __uint_as_float(0xffffffffu));
+            p.hit[ray] = L.found ? make_float4(L.hit.t, L.hit.u, L.hit.v, __uint_as_float(L.hit.tri)) : make_float4(-1.f, 0.f, 0.f, __uint_as_float(0xffffffffu));
             p.hit_inst[ray] = L.found ? L.hit.inst : 0xffffffffu;
             ray = NONE;
         }
@@ -723,16 +723,19 @@ __device__ __forceinline__ float3 tvec(const float4 I[3], float3 x) {
 }
 __device__ __forceinline__ float3 mvec(const float4 M[3], float3 x) { return f3(M[0].x * x.x + M[0].y * x.y + M[0].z * x.z, M[1].x * x.x + M[1].y * x.y + M[1].z * x.z, M[2].x * x.x + M[2].y * x.y + M[2].z * x.z); }
 // hit_geometry.slang:64-138,174-205; hit.slang:86-114; surface.slang:290-333; material.slang:69-79.
-__device__ __forceinline__ Surface hit_surface(const Job& p, uint32_t inst, uint32_t prim, float u, float v, float3 dir) {
+// The triangle's corners come from the BLAS leaf-order copies (positions in blas_tris,
+// normals in tri_nrm, the index buffer's vertex order), so they need no index lookup
+// first: the same values as indices -> vertices, one dependent load fewer.
+__device__ __forceinline__ Surface hit_surface(const Job& p, uint32_t inst, uint32_t tri, float u, float v, float3 dir) {
     Surface s;
     uint4 info = __ldg(&p.inst_info[inst]);
     const MeshInfo& m = p.meshes[info.x];
     float4 M[3] = {__ldg(&p.o2w[3 * inst]), __ldg(&p.o2w[3 * inst + 1]), __ldg(&p.o2w[3 * inst + 2])};
     float4 I[3] = {__ldg(&p.w2o[3 * inst]), __ldg(&p.w2o[3 * inst + 1]), __ldg(&p.w2o[3 * inst + 2])};
-    uint32_t base = m.index_offset + 3u * prim;
-    uint32_t i0 = m.vertex_offset + __ldg(&p.indices[base]), i1 = m.vertex_offset + __ldg(&p.indices[base + 1]), i2 = m.vertex_offset + __ldg(&p.indices[base + 2]);
-    float4 q0 = __ldg(&p.vpos[i0]), q1 = __ldg(&p.vpos[i1]), q2 = __ldg(&p.vpos[i2]);
-    float4 m0 = __ldg(&p.vnrm[i0]), m1 = __ldg(&p.vnrm[i1]), m2 = __ldg(&p.vnrm[i2]);
+    const float4* tp = p.sv.blas_tris + 3u * size_t(tri);
+    const float4* np = p.tri_nrm + 3u * size_t(tri);
+    float4 q0 = __ldg(tp), q1 = __ldg(tp + 1), q2 = __ldg(tp + 2);
+    float4 m0 = __ldg(np), m1 = __ldg(np + 1), m2 = __ldg(np + 2);
     float3 P[3] = {f3(q0.x, q0.y, q0.z), f3(q1.x, q1.y, q1.z), f3(q2.x, q2.y, q2.z)};
     float3 N[3] = {f3(m0.x, m0.y, m0.z), f3(m1.x, m1.y, m1.z), f3(m2.x, m2.y, m2.z)};
     float b[3] = {1.f - u - v, u, v};
@@ -873,7 +876,7 @@ __global__ void __launch_bounds__(128, 4) k_shade(const __grid_constant__ PathPa
             float limit = bounce == 0 ? J.clamp_direct : J.clamp_indirect;
             if (J.primary_ids && bounce == 0 && sidx == J.first_sample) {
                 J.primary_ids[2 * pixel] = hh.x >= 0.f ? inst : 0xffffffffu;
-                J.primary_ids[2 * pixel + 1] = hh.x >= 0.f ? __float_as_uint(hh.w) : 0xffffffffu;
+                J.primary_ids[2 * pixel + 1] = hh.x >= 0.f ? __float_as_uint(__ldg(&J.sv.blas_tris[3u * size_t(__float_as_uint(hh.w))]).w) : 0xffffffffu;
             }
             if (!(hh.x >= 0.f)) {
                 // Miss: path.slang:1484-1512 with the constant world light and camera-visible suns.
@@ -1134,7 +1137,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_debug_trace(SceneView sv, uint3
         HitRecord h;
         bool f = trace_any<false, false>(sv, RayRef{rays, rays + n, i}, rays[i].w, h, err, nullptr, stk);
         t[i] = f ? h.t : -1.f;
-        ids[2 * i] = f ? h.inst : 0xffffffffu; ids[2 * i + 1] = f ? h.prim : 0xffffffffu;
+        ids[2 * i] = f ? h.inst : 0xffffffffu; ids[2 * i + 1] = f ? __float_as_uint(__ldg(&sv.blas_tris[3u * size_t(h.tri)]).w) : 0xffffffffu;
         uv[2 * i] = f ? h.u : 0.f; uv[2 * i + 1] = f ? h.v : 0.f;
     }
 }
