@@ -723,7 +723,7 @@ void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counte
         if (timed) VKB_CUDA(cudaEventRecord(c->kernel_events[2 * tot.trace_launches + 1], st));
         tot.trace_launches++;
         k_reset_queues<<<1, 1, 0, st>>>(p.counters, cur ^ 1);
-        k_shade<BATCH><<<sgrid, 128, 0, st>>>(p, cur);
+        k_shade<BATCH><<<sgrid, 256, 0, st>>>(p, cur);
         if (counted) k_trace_shadow<true, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
         else k_trace_shadow<false, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
     }
