@@ -238,7 +238,7 @@ typedef struct vkb_job {
 vkb_status vkb_render_batch(vkb_ctx* ctx, vkb_job* jobs, uint32_t njobs, uint32_t flags, vkb_stats* stats);
 
 /* Autotuner of the wavefront: times one sample of `jobs` for every candidate wave
- * capacity (path slots per wave: 2, 4, 8, 16, 32 Mi) and trace/shade grid (16, 32, 64
+ * capacity (path slots per wave: 2, 4, 8, 16, 32 Mi) and trace/shade grid (32, 64, 128
  * blocks per SM) and keeps the fastest for this context's later renders. */
 typedef struct vkb_tune_result {
     uint32_t tried;

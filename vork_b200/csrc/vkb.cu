@@ -441,7 +441,7 @@ struct vkb_ctx {
     DBuf<float4> accum, staging;        // per-render accumulators and host-output staging (all jobs of a call)
     DBuf<uint32_t> ids;                 // primary ids of the jobs that asked for them
     size_t wave_capacity = 32u << 20;   // path slots per wave (autotuned); 7.4 GB of queues when full
-    int trace_blocks_per_sm = 64;       // trace/shade grid = SMs x this (autotuned)
+    int trace_blocks_per_sm = 128;      // trace/shade grid = SMs x this (autotuned)
     uint64_t launches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<cudaEvent_t> kernel_events;
@@ -723,7 +723,7 @@ void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counte
         if (timed) VKB_CUDA(cudaEventRecord(c->kernel_events[2 * tot.trace_launches + 1], st));
         tot.trace_launches++;
         k_reset_queues<<<1, 1, 0, st>>>(p.counters, cur ^ 1);
-        k_shade<BATCH><<<sgrid, 256, 0, st>>>(p, cur);
+        k_shade<BATCH><<<sgrid, 512, 0, st>>>(p, cur);
         if (counted) k_trace_shadow<true, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
         else k_trace_shadow<false, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
     }
@@ -1330,7 +1330,7 @@ vkb_status vkb_autotune(vkb_ctx* c, vkb_job* jobs, uint32_t njobs, vkb_tune_resu
         // Candidates: wave capacity (queue slots) x trace/shade blocks per SM, each timed on
         // one sample of every job (same work for every candidate).
         const size_t caps[] = {size_t(2) << 20, size_t(4) << 20, size_t(8) << 20, size_t(16) << 20, size_t(32) << 20};
-        const int grids[] = {16, 32, 64};
+        const int grids[] = {32, 64, 128};
         std::vector<std::pair<vkb_scene*, vkb_profile>> in(njobs);
         std::vector<vkb_output> o(njobs);
         std::vector<vkb_output*> outs(njobs);
