@@ -1725,14 +1725,18 @@ void oracle_render(void* h, int fp64, const vkb_profile* pf, uint32_t x0, uint32
     else render_impl(*static_cast<Scene<float>*>(o->s32), *pf, x0, y0, w, hgt, rgba, ids, threads, stats);
 }
 // Morton codes of the TLAS build (instance boxes) and of one mesh's BLAS build (triangle boxes).
-void oracle_tlas_morton(const vkb_scene_desc* d, uint32_t* out) {
-    std::vector<float> lo(3 * size_t(d->num_instances)), hi(3 * size_t(d->num_instances));
+// World boxes of the TLAS leaves (xyz lo, xyz hi per instance), as the build computes them.
+void oracle_instance_boxes(const vkb_scene_desc* d, float* lo, float* hi) {
     std::vector<float> mlo(3 * size_t(d->num_meshes)), mhi(3 * size_t(d->num_meshes)), msph(4 * size_t(d->num_meshes));
     for (uint32_t m = 0; m < d->num_meshes; ++m) mesh_box(d->meshes[m], &mlo[3 * m], &mhi[3 * m], &msph[4 * m]);
     for (uint32_t i = 0; i < d->num_instances; ++i) {
         uint32_t m = d->instance_mesh[i];
         instance_box(d->instance_rows + 12 * size_t(i), &mlo[3 * m], &mhi[3 * m], &msph[4 * m], &lo[3 * i], &hi[3 * i]);
     }
+}
+void oracle_tlas_morton(const vkb_scene_desc* d, uint32_t* out) {
+    std::vector<float> lo(3 * size_t(d->num_instances)), hi(3 * size_t(d->num_instances));
+    oracle_instance_boxes(d, lo.data(), hi.data());
     box_morton(d->num_instances, lo.data(), hi.data(), out, true);
 }
 void oracle_blas_morton(const vkb_scene_desc* d, uint32_t mesh, uint32_t* out) {

@@ -53,6 +53,7 @@ def lib():
         l.oracle_render.argtypes = [P, C.c_int, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, f32p, u32p, C.c_uint32,
                                     C.POINTER(C.c_uint64)]
         l.oracle_tlas_morton.argtypes = [P, u32p]
+        l.oracle_instance_boxes.argtypes = [P, f32p, f32p]
         l.oracle_blas_morton.argtypes = [P, C.c_uint32, u32p]
         _lib = l
     return _lib
@@ -176,6 +177,13 @@ class OracleScene:
         out = np.zeros(self.desc.num_instances, np.uint32)
         lib().oracle_tlas_morton(C.cast(C.byref(self.desc), C.c_void_p), _p(out, C.c_uint32))
         return out
+
+    def instance_boxes(self):
+        """(lo, hi): the TLAS leaf world boxes, (n, 3) float32 each."""
+        n = self.desc.num_instances
+        lo = np.zeros((n, 3), np.float32); hi = np.zeros((n, 3), np.float32)
+        lib().oracle_instance_boxes(C.cast(C.byref(self.desc), C.c_void_p), _p(lo, C.c_float), _p(hi, C.c_float))
+        return lo, hi
 
     def blas_morton(self, mesh):
         out = np.zeros(self.scene.meshes[mesh].num_triangles, np.uint32)
