@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define VKB_ABI_VERSION 4u
+#define VKB_ABI_VERSION 5u
 
 /* Error model: FailureKind exit categories of crates/vork-render/src/failure.rs:21-100,
  * reduced to what a render call can report. */
@@ -220,10 +220,24 @@ vkb_status vkb_scene_update_instances(vkb_scene* scene, const float* rows, uint3
 /* The same with rows already in device memory of the context's GPU (no host copy). */
 vkb_status vkb_scene_update_instances_device(vkb_scene* scene, const float* device_rows, uint32_t num_instances, int policy);
 
+/* A frame slot over an installed scene (FrameRays::new per frame, rt.rs:1339-1385, over the
+ * BLASes of one install; InstalledScene::create_frame_slot, crates/vork-render/src/install.rs:3303):
+ * a scene that shares `base`'s meshes, BLASes, materials, lights and light tree and owns its
+ * own instance rows and TLAS, starting from base's current rows.  Updating a fork's
+ * instances (vkb_scene_update_instances*) leaves base and other forks unchanged, so frames
+ * of an animated sequence render while other requests use base.  Forks of forks are
+ * refused; base must outlive its forks (vkb_scene_destroy refuses a scene with live forks). */
+vkb_status vkb_scene_fork(vkb_scene* base, vkb_scene** out);
+
 /* passes::path::record + resolve (passes/path.rs:539-724; resolve.slang:162-191): renders
  * samples [first_sample, first_sample+sample_count) of `profile` and writes the mean
  * over them. stats may be NULL. */
 vkb_status vkb_render(vkb_scene* scene, const vkb_profile* profile, vkb_output* out, vkb_stats* stats);
+/* vkb_render through `camera` (its resolution included) instead of the scene's own camera
+ * (the per-shot camera of Shot::render, crates/vork-render/src/shot.rs:31-72); NULL = the
+ * scene's camera.  out->rgba holds camera->width * camera->height * 4 floats. */
+vkb_status vkb_render_view(vkb_scene* scene, const vkb_camera* camera, const vkb_profile* profile, vkb_output* out,
+                           vkb_stats* stats);
 
 /* Batched previews: many render jobs (each its own installed scene of this context,
  * profile and output) share every wavefront wave; each wave's kernel sequence is
@@ -273,6 +287,11 @@ typedef struct vkb_server_status {
 vkb_status vkb_server_create(vkb_ctx* ctx, const vkb_server_config* cfg, vkb_server** out);
 /* host_rgba (width*height*4 floats) must stay valid until the request is done. */
 vkb_status vkb_server_submit(vkb_server* server, vkb_scene* scene, const vkb_profile* profile, float* host_rgba, uint64_t* id);
+/* vkb_server_submit through `camera` (NULL: the scene's camera); host_rgba holds
+ * camera->width * camera->height * 4 floats.  The scene (and a fork's base) must stay
+ * installed until the request is done. */
+vkb_status vkb_server_submit_view(vkb_server* server, vkb_scene* scene, const vkb_camera* camera, const vkb_profile* profile,
+                                  float* host_rgba, uint64_t* id);
 vkb_status vkb_server_step(vkb_server* server, vkb_server_status* status);
 /* state: 0 queued, 1 running, 2 done (its host_rgba holds the mean image). */
 vkb_status vkb_server_poll(vkb_server* server, uint64_t id, int* state);
@@ -415,6 +434,10 @@ vkb_status vkb_debug_tlas_stats(vkb_scene* scene, double* sah_cost, uint32_t* ma
  * out_t[n], out_ids[n*2] (instance, triangle; 0xffffffff on miss), out_uv[n*2]. */
 vkb_status vkb_debug_trace(vkb_scene* scene, uint32_t n, const float* rays7, float* out_t,
                            uint32_t* out_ids, float* out_uv);
+/* Occlusion of n world rays by the shadow-ray traversal (straight_shadow_transmittance's
+ * ACCEPT_FIRST_HIT_AND_END_SEARCH query, shaders/path.slang:630-684: first hit ends the
+ * walk, no back-face culling): out_occluded[n] = 1 when a surface lies within tmax. */
+vkb_status vkb_debug_occluded(vkb_scene* scene, uint32_t n, const float* rays7, uint32_t* out_occluded);
 
 #ifdef __cplusplus
 }

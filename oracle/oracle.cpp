@@ -452,7 +452,10 @@ template <class R> struct Lut {
         return lerp(fetch(ax + lx, ay + ly, 0), fetch(bx + lx, by + ly, 0), at - R(first));
     }
 };
-template <class R> const Lut<R>& lut() { static Lut<R> l; return l; }
+template <class R> Lut<R>& lut_mut() { static Lut<R> l; return l; }
+template <class R> const Lut<R>& lut() { return lut_mut<R>(); }
+// Baked texels of each precision, kept while a caller's atlas replaces them.
+template <class R> std::vector<float>& lut_baked() { static std::vector<float> b; return b; }
 
 // ---------------------------------------------------------------- closure + BSDF (shaders/bsdf*.slang subset)
 template <class R> struct Closure {
@@ -1613,6 +1616,21 @@ void mesh_box(const vkb_mesh& m, float lo[3], float hi[3], float sph[4]) {
 
 }  // namespace
 
+// Replace the atlas both precisions read with `texels` (BRDF_SIZE x BRDF_HEIGHT x 4
+// floats, e.g. the device bake) so a transport comparison does not also measure the
+// bake; NULL restores the oracle's own bake.
+template <class R> void set_lut(const float* texels) {
+    Lut<R>& l = lut_mut<R>();
+    std::vector<float>& b = lut_baked<R>();
+    if (texels) {
+        if (b.empty()) b = l.texels;
+        std::copy(texels, texels + l.texels.size(), l.texels.begin());
+    } else if (!b.empty()) {
+        l.texels = b;
+        b.clear();
+    }
+}
+
 extern "C" {
 
 uint32_t oracle_version(void) { return 1u; }
@@ -1646,6 +1664,7 @@ void oracle_brdf_lut(int fp64, float* out) {
     else { const Lut<float>& l = lut<float>(); std::copy(l.texels.begin(), l.texels.end(), out); }
 }
 float oracle_half_round(float x) { return half_to_float(float_to_half(x)); }
+void oracle_set_lut(const float* texels) { set_lut<float>(texels); set_lut<double>(texels); }
 // Emitter evaluation (for the reference's light_connection_tests invariants).
 void oracle_emitter_sample(const vkb_light* light, const double* world, const double* u, double* out_dir, double* out_radiance, double* out_pdf, double* out_distance) {
     LightV<double> L = light_values<double>(*light);

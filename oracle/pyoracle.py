@@ -55,6 +55,7 @@ def lib():
         l.oracle_tlas_morton.argtypes = [P, u32p]
         l.oracle_instance_boxes.argtypes = [P, f32p, f32p]
         l.oracle_blas_morton.argtypes = [P, C.c_uint32, u32p]
+        l.oracle_set_lut.argtypes = [f32p]
         _lib = l
     return _lib
 
@@ -99,6 +100,23 @@ def brdf_lut(fp64=False):
     return out
 
 
+class atlas:
+    """Within the block the oracle reads `texels` ((2240, 128, 4) float32, e.g. the
+    device-baked atlas) instead of its own bake, so a transport comparison measures the
+    transport alone; the bake itself is compared on its own."""
+
+    def __init__(self, texels):
+        self.texels = np.ascontiguousarray(texels, np.float32)
+        assert self.texels.shape == (2240, 128, 4)
+
+    def __enter__(self):
+        lib().oracle_set_lut(_p(self.texels, C.c_float))
+        return self
+
+    def __exit__(self, *exc):
+        lib().oracle_set_lut(None)
+
+
 def emitter_sample(light, world, u):
     w = np.asarray(world, np.float64); uu = np.asarray(u, np.float64)
     d = np.zeros(3); r = np.zeros(3); pdf = C.c_double(); dist = C.c_double()
@@ -141,12 +159,20 @@ class OracleScene:
         except Exception:
             pass
 
-    def trace(self, rays7: np.ndarray, fp64=True, any_hit=False):
+    def trace(self, rays7: np.ndarray, fp64=True, any_hit=False, threads=None):
+        """Closest (or any) hits of (origin, dir, tmax) rays, in chunks over host threads."""
+        from concurrent.futures import ThreadPoolExecutor
         r = np.ascontiguousarray(rays7, np.float32)
         n = r.shape[0]
         t = np.zeros(n, np.float32); ids = np.zeros((n, 2), np.uint32); uv = np.zeros((n, 2), np.float32)
-        lib().oracle_trace(self.h, 1 if fp64 else 0, n, _p(r, C.c_float), 1 if any_hit else 0, _p(t, C.c_float), _p(ids, C.c_uint32),
-                           _p(uv, C.c_float))
+
+        def chunk(a, b):
+            lib().oracle_trace(self.h, 1 if fp64 else 0, b - a, _p(r[a:b], C.c_float), 1 if any_hit else 0, _p(t[a:b], C.c_float),
+                               _p(ids[a:b], C.c_uint32), _p(uv[a:b], C.c_float))
+        threads = threads or os.cpu_count() or 1
+        step = max(1024, -(-n // (4 * threads)))
+        with ThreadPoolExecutor(threads) as ex:
+            list(ex.map(lambda a: chunk(a, min(n, a + step)), range(0, n, step)))
         return t, ids, uv
 
     def camera_rays(self, profile, index, x0=0, y0=0, w=None, h=None):

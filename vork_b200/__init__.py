@@ -144,17 +144,29 @@ class RenderResult:
 class InstalledScene:
     """Renderer::install + FrameRays (lib.rs:1322-1470; rt.rs:1098-1385) for one scene."""
 
-    def __init__(self, renderer: Renderer, scene: Scene):
+    def __init__(self, renderer: Renderer, scene: Scene, _handle=None):
         self.r = renderer
         self.scene = scene
+        if _handle is not None:       # a fork: the base's descriptor describes it
+            self.desc = None
+            self.h = _handle
+            return
         self.desc = scene.desc()
         h = C.c_void_p()
         abi.check(renderer.lib.vkb_scene_create(renderer.h, C.byref(self.desc), C.byref(h)))
         self.h = h
 
+    def fork(self) -> "InstalledScene":
+        """A frame slot (vkb_scene_fork): shares this scene's meshes, BLASes, materials and
+        lights, owns its instance rows and TLAS (starting from this scene's rows)."""
+        h = C.c_void_p()
+        abi.check(self.r.lib.vkb_scene_fork(self.h, C.byref(h)))
+        return InstalledScene(self.r, self.scene, _handle=h)
+
     def close(self):
+        """Release the scene (a base with live forks is refused: close the forks first)."""
         if self.h:
-            self.r.lib.vkb_scene_destroy(self.h)
+            abi.check(self.r.lib.vkb_scene_destroy(self.h))
             self.h = None
 
     def __enter__(self):
@@ -179,8 +191,11 @@ class InstalledScene:
     def launch_count(self) -> int:
         return int(self.r.lib.vkb_scene_launch_count(self.h))
 
-    def render(self, profile: Profile, ids: bool = False, out: np.ndarray | None = None, device_ptr: int | None = None) -> RenderResult:
-        cam = self.scene.camera
+    def render(self, profile: Profile, ids: bool = False, out: np.ndarray | None = None, device_ptr: int | None = None,
+               camera: abi.VkbCamera | None = None) -> RenderResult:
+        """Render under `profile` (vkb_render), or through `camera` instead of the scene's
+        own (vkb_render_view: its resolution sets the image's)."""
+        cam = camera if camera is not None else self.scene.camera
         o = abi.VkbOutput()
         img = None
         if device_ptr is not None:
@@ -194,12 +209,15 @@ class InstalledScene:
         o.primary_ids = abi.uptr(idbuf) if ids else None
         st = abi.VkbStats()
         p = profile.c()
-        abi.check(self.r.lib.vkb_render(self.h, C.byref(p), C.byref(o), C.byref(st)))
+        if camera is not None:
+            abi.check(self.r.lib.vkb_render_view(self.h, C.cast(C.byref(camera), C.c_void_p), C.byref(p), C.byref(o), C.byref(st)))
+        else:
+            abi.check(self.r.lib.vkb_render(self.h, C.byref(p), C.byref(o), C.byref(st)))
         stats = {k: getattr(st, k) for k, _ in abi.VkbStats._fields_}
         return RenderResult(img, stats, idbuf)
 
     def tlas_morton(self):
-        out = np.zeros(self.desc.num_instances, np.uint32)
+        out = np.zeros(self.scene.instance_rows.shape[0], np.uint32)
         abi.check(self.r.lib.vkb_debug_tlas_morton(self.h, abi.uptr(out)))
         return out
 
@@ -220,6 +238,13 @@ class InstalledScene:
         t = np.zeros(n, np.float32); ids = np.zeros((n, 2), np.uint32); uv = np.zeros((n, 2), np.float32)
         abi.check(self.r.lib.vkb_debug_trace(self.h, n, abi.fptr(r), abi.fptr(t), abi.uptr(ids), abi.fptr(uv)))
         return t, ids, uv
+
+    def occluded(self, rays7: np.ndarray) -> np.ndarray:
+        """Any-hit occlusion of (origin, dir, tmax) rays by the shadow-ray traversal: (n,) bool."""
+        r = np.ascontiguousarray(rays7, np.float32)
+        out = np.zeros(r.shape[0], np.uint32)
+        abi.check(self.r.lib.vkb_debug_occluded(self.h, r.shape[0], abi.fptr(r), abi.uptr(out)))
+        return out.astype(bool)
 
 
 class RadianceCache:

@@ -142,6 +142,9 @@ SIGNATURES = {
     "vkb_scene_update_instances_device": (C.c_int, [_P, C.c_void_p, C.c_uint32, C.c_int]),
     "vkb_render": (C.c_int, [_P, C.POINTER(VkbProfile), C.POINTER(VkbOutput), C.POINTER(VkbStats)]),
     "vkb_render_noalloc": (C.c_int, [_P, C.POINTER(VkbProfile), C.POINTER(VkbOutput), C.POINTER(VkbStats)]),
+    "vkb_render_view": (C.c_int, [_P, C.c_void_p, C.POINTER(VkbProfile), C.POINTER(VkbOutput), C.POINTER(VkbStats)]),
+    "vkb_scene_fork": (C.c_int, [_P, C.POINTER(_P)]),
+    "vkb_server_submit_view": (C.c_int, [_P, _P, C.c_void_p, C.POINTER(VkbProfile), C.POINTER(C.c_float), C.POINTER(C.c_uint64)]),
     "vkb_scene_info": (C.c_int, [_P, C.POINTER(VkbSceneInfo)]),
     "vkb_server_create": (C.c_int, [_P, C.POINTER(VkbServerConfig), C.POINTER(_P)]),
     "vkb_server_submit": (C.c_int, [_P, _P, C.POINTER(VkbProfile), C.POINTER(C.c_float), C.POINTER(C.c_uint64)]),
@@ -160,6 +163,7 @@ SIGNATURES = {
     "vkb_debug_blas_morton": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32)]),
     "vkb_debug_trace": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_uint32),
                                   C.POINTER(C.c_float)]),
+    "vkb_debug_occluded": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_uint32)]),
     "vkb_debug_tlas_stats": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "vkb_display": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_uint32, C.c_void_p, C.c_int]),
     "vkb_cache_create": (C.c_int, [_P, C.c_void_p, C.POINTER(_P)]),

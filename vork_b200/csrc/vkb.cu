@@ -483,6 +483,10 @@ struct vkb_scene {
     float build_ms = 0.f;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint64_t launches = 0;                    // kernels launched for this scene so far
+    // A fork (vkb_scene_fork) shares its base's meshes, BLASes, materials, lights and light
+    // tree and owns only its instances and TLAS; a base counts its live forks.
+    vkb_scene* base = nullptr;
+    uint32_t forks = 0;
 };
 
 namespace {
@@ -613,6 +617,14 @@ void validate_desc(const vkb_scene_desc* d) {
     }
     if (d->camera.width == 0 || d->camera.height == 0) throw ArgError{"camera resolution is zero"};
     if (d->tlas_builder > VKB_TLAS_PLOC) throw ArgError{"unknown TLAS builder"};
+}
+
+
+void validate_camera(const vkb_camera& cam) {
+    if (cam.width == 0 || cam.height == 0) throw ArgError{"camera resolution is zero"};
+    if (uint64_t(cam.width) * cam.height > (uint64_t(1) << 28)) throw ArgError{"camera resolution above 2^28 pixels"};
+    const float* f = &cam.eye[0];
+    for (int k = 0; k < 16; ++k) if (!std::isfinite(f[k])) throw ArgError{"camera has a non-finite field"};
 }
 
 
@@ -991,11 +1003,13 @@ void fill_stats(vkb_stats* stats, const WaveTotals& t, uint64_t paths, float bui
 
 // Render jobs with the context's own buffers (grown on demand).
 void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile>>& in, std::vector<vkb_output*>& outs, uint32_t flags,
-                 uint32_t wave_samples_hint, WaveTotals& tot, uint64_t& paths, const CacheLaunch* cache = nullptr) {
+                 uint32_t wave_samples_hint, WaveTotals& tot, uint64_t& paths, const CacheLaunch* cache = nullptr,
+                 const std::vector<const vkb_camera*>* cams = nullptr) {
     cudaStream_t st = c->stream;
+    auto camera_of = [&](size_t k) -> const vkb_camera& { return (cams && (*cams)[k]) ? *(*cams)[k] : in[k].first->camera; };
     size_t total_pixels = 0, max_pix = 0, ids_words = 0, staged = 0;
     for (size_t k = 0; k < in.size(); ++k) {
-        const vkb_camera& cam = in[k].first->camera;
+        const vkb_camera& cam = camera_of(k);
         size_t npix = size_t(cam.width) * cam.height;
         total_pixels += npix; max_pix = std::max(max_pix, npix);
         if (outs[k]->primary_ids) ids_words += 2 * npix;
@@ -1026,7 +1040,8 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
     for (size_t k = 0; k < in.size(); ++k) {
         EngineJob& e = jobs[k];
         e.s = in[k].first; e.pf = in[k].second;
-        e.npix = e.s->camera.width * e.s->camera.height;
+        if (cams && (*cams)[k]) { e.own_camera = true; e.camera = *(*cams)[k]; }
+        e.npix = camera_of(k).width * camera_of(k).height;
         e.count = e.pf.sample_count ? e.pf.sample_count : e.pf.samples - e.pf.first_sample;
         e.accum = c->accum.p + acc; acc += e.npix;
         if (outs[k]->on_device) e.out_dev = reinterpret_cast<float4*>(outs[k]->rgba);
@@ -1221,10 +1236,66 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
     return VKB_OK;
 }
 
+vkb_status vkb_scene_fork(vkb_scene* b, vkb_scene** out) {
+    if (!b || !out) return fail(VKB_INVALID_ARG, "null scene or output pointer");
+    if (b->base) return fail(VKB_INVALID_ARG, "fork of a fork: fork the base scene");
+    *out = nullptr;
+    vkb_scene* s = new vkb_scene();
+    s->ctx = b->ctx;
+    vkb_status st = guarded([&] {
+        VKB_CUDA(cudaSetDevice(b->ctx->device));
+        cudaStream_t str = b->ctx->stream;
+        VKB_CUDA(cudaEventCreate(&s->ev0));
+        VKB_CUDA(cudaEventCreate(&s->ev1));
+        s->num_meshes = b->num_meshes; s->num_instances = b->num_instances; s->total_tris = b->total_tris;
+        s->mesh_info = b->mesh_info; s->inst_mesh = b->inst_mesh; s->inst_mat = b->inst_mat;
+        s->materials = b->materials; s->lights = b->lights; s->camera = b->camera; s->env = b->env;
+        s->tree_nodes = b->tree_nodes; s->tlas_builder = b->tlas_builder;
+        // Shared, read-only: geometry, BLASes, materials, lights, light tree.
+        s->vpos = b->vpos; s->vnrm = b->vnrm; s->blas_tris = b->blas_tris; s->tri_nrm = b->tri_nrm;
+        s->indices = b->indices; s->meshes = b->meshes; s->blas4 = b->blas4;
+        s->d_materials = b->d_materials; s->d_lights = b->d_lights; s->tree = b->tree;
+        s->base = b;
+        b->forks++;
+        // Owned: the base's current instance rows and records, and a TLAS over them.
+        uint32_t n = b->num_instances;
+        s->inst_info.alloc(std::max(1u, n));
+        s->o2w.alloc(std::max<size_t>(1, size_t(n) * 3));
+        if (n) {
+            VKB_CUDA(cudaMemcpyAsync(s->inst_info.p, b->inst_info.p, n * sizeof(uint4), cudaMemcpyDeviceToDevice, str));
+            VKB_CUDA(cudaMemcpyAsync(s->o2w.p, b->o2w.p, size_t(n) * 3 * sizeof(float4), cudaMemcpyDeviceToDevice, str));
+        }
+        s->w2o.alloc(std::max<size_t>(1, size_t(n) * 3));
+        s->inst_lo.alloc(std::max(1u, n)); s->inst_hi.alloc(std::max(1u, n));
+        s->tlas_nodes.alloc(std::max(1u, n > 1 ? n - 1 : 1u));
+        s->tlas4.alloc(std::max(1u, n > 1 ? n - 1 : 1u));
+        s->tlas_odd.alloc(std::max(1u, n > 1 ? n - 1 : 1u));
+        s->tlas_leaves.alloc(std::max(1u, n));
+        s->tlas_codes.alloc(std::max(1u, n));
+        build_tlas(s);
+    });
+    if (st != VKB_OK) { vkb_scene_destroy(s); return st; }
+    *out = s;
+    return VKB_OK;
+}
+
 vkb_status vkb_scene_destroy(vkb_scene* s) {
     if (!s) return VKB_OK;
+    if (s->forks) return fail(VKB_INVALID_ARG, "scene has live forks: destroy them first");
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->ctx->stream);
+    if (s->base) {
+        // Shared with the base scene: not this fork's to free.
+        DBuf<float4>* shared4[] = {&s->vpos, &s->vnrm, &s->blas_tris, &s->tri_nrm};
+        for (auto* b : shared4) { b->p = nullptr; b->n = 0; }
+        s->indices.p = nullptr; s->indices.n = 0;
+        s->meshes.p = nullptr; s->meshes.n = 0;
+        s->blas4.p = nullptr; s->blas4.n = 0;
+        s->d_materials.p = nullptr; s->d_materials.n = 0;
+        s->d_lights.p = nullptr; s->d_lights.n = 0;
+        s->tree.p = nullptr; s->tree.n = 0;
+        s->base->forks--;
+    }
     DBuf<float4>* f4[] = {&s->vpos, &s->vnrm, &s->blas_tris, &s->tri_nrm, &s->o2w, &s->o2w_next, &s->w2o, &s->inst_lo, &s->inst_hi, &s->tri_lo, &s->tri_hi};
     for (auto* b : f4) b->release();
     s->changed.release();
@@ -1297,6 +1368,31 @@ vkb_status vkb_render(vkb_scene* s, const vkb_profile* pf, vkb_output* out, vkb_
             hint = uint32_t(std::max<size_t>(1, std::min<size_t>(count, c->wave_capacity / std::max<size_t>(1, npix))));
         }
         render_jobs(c, in, outs, pf->flags, hint, tot, paths);
+        s->launches += tot.launches;
+        fill_stats(stats, tot, paths, s->build_ms);
+    });
+}
+
+vkb_status vkb_render_view(vkb_scene* s, const vkb_camera* cam, const vkb_profile* pf, vkb_output* out, vkb_stats* stats) {
+    if (!cam) return vkb_render(s, pf, out, stats);
+    if (!s || !pf || !out || !out->rgba) return fail(VKB_INVALID_ARG, "null scene, profile or output");
+    return guarded([&] {
+        validate_profile(pf);
+        validate_camera(*cam);
+        vkb_ctx* c = s->ctx;
+        VKB_CUDA(cudaSetDevice(c->device));
+        std::vector<std::pair<vkb_scene*, vkb_profile>> in{{s, *pf}};
+        std::vector<vkb_output*> outs{out};
+        std::vector<const vkb_camera*> cams{cam};
+        WaveTotals tot;
+        uint64_t paths = 0;
+        uint32_t hint = pf->wave_samples;
+        if (!hint) {
+            uint32_t count = pf->sample_count ? pf->sample_count : pf->samples - pf->first_sample;
+            size_t npix = size_t(cam->width) * cam->height;
+            hint = uint32_t(std::max<size_t>(1, std::min<size_t>(count, c->wave_capacity / std::max<size_t>(1, npix))));
+        }
+        render_jobs(c, in, outs, pf->flags, hint, tot, paths, nullptr, &cams);
         s->launches += tot.launches;
         fill_stats(stats, tot, paths, s->build_ms);
     });
@@ -1602,6 +1698,34 @@ vkb_status vkb_debug_trace(vkb_scene* s, uint32_t n, const float* rays7, float* 
     });
 }
 
+vkb_status vkb_debug_occluded(vkb_scene* s, uint32_t n, const float* rays7, uint32_t* out_occluded) {
+    if (!s || (n && (!rays7 || !out_occluded))) return fail(VKB_INVALID_ARG, "null argument");
+    return guarded([&] {
+        VKB_CUDA(cudaSetDevice(s->ctx->device));
+        cudaStream_t st = s->ctx->stream;
+        DBuf<float4> r;
+        DBuf<uint32_t> occ, err;
+        std::vector<float4> rays4(2 * size_t(n));
+        for (uint32_t i = 0; i < n; ++i) {
+            const float* q = rays7 + 7 * size_t(i);
+            rays4[i] = make_float4(q[0], q[1], q[2], q[6]);
+            rays4[n + i] = make_float4(q[3], q[4], q[5], 0.f);
+        }
+        r.upload(rays4.data(), rays4.size(), st);
+        occ.alloc(n); err.alloc(1);
+        VKB_CUDA(cudaMemsetAsync(err.p, 0, sizeof(uint32_t), st));
+        if (n) {
+            k_debug_occluded<<<grid_for(n, 128, s->ctx->sms), 128, 0, st>>>(scene_view(s), n, r.p, occ.p, err.p);
+            VKB_CUDA(cudaMemcpyAsync(out_occluded, occ.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        }
+        uint32_t e = 0;
+        VKB_CUDA(cudaMemcpyAsync(&e, err.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        VKB_CUDA(cudaStreamSynchronize(st));
+        r.release(); occ.release(); err.release();
+        if (e) throw InternalError{"any-hit traversal overflowed its stack or step cap"};
+    });
+}
+
 }  // extern "C"
 
 
@@ -1619,7 +1743,7 @@ struct vkb_server {
     size_t capacity = 0;
     Wavefront wave;                                   // the server's own queues (renders on the context keep theirs)
     std::unique_ptr<WaveEngine> eng;
-    struct Pending { uint64_t id; vkb_scene* s; vkb_profile pf; float* host_out; };
+    struct Pending { uint64_t id; vkb_scene* s; vkb_profile pf; float* host_out; bool own_camera; vkb_camera cam; };
     struct Live { uint64_t id; float* host_out; DBuf<float4> accum, out; uint64_t bytes; };
     std::deque<Pending> queue;
     std::map<uint64_t, std::unique_ptr<Live>> live;   // admitted, keyed by id
@@ -1629,10 +1753,13 @@ struct vkb_server {
 };
 
 namespace {
+// Device bytes a scene holds itself (a fork: its instances and TLAS only).
 uint64_t scene_bytes(const vkb_scene* s) {
-    return s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas4.n * sizeof(Bvh4Node) +
-           (s->blas_tris.n + s->tri_nrm.n) * sizeof(float4) + s->tlas_nodes.n * sizeof(BvhNode) + s->tlas4.n * sizeof(Bvh4Node) + s->tlas_odd.n + s->tlas_leaves.n * sizeof(TlasLeaf) +
-           (s->o2w.n + s->w2o.n) * sizeof(float4);
+    uint64_t own = s->tlas_nodes.n * sizeof(BvhNode) + s->tlas4.n * sizeof(Bvh4Node) + s->tlas_odd.n + s->tlas_leaves.n * sizeof(TlasLeaf) +
+                   (s->o2w.n + s->w2o.n) * sizeof(float4) + s->inst_info.n * sizeof(uint4);
+    if (s->base) return own;
+    return own + s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas4.n * sizeof(Bvh4Node) +
+           (s->blas_tris.n + s->tri_nrm.n) * sizeof(float4);
 }
 uint64_t resident_bytes(const vkb_server* v) {
     uint64_t b = 0;
@@ -1666,18 +1793,26 @@ vkb_status vkb_server_create(vkb_ctx* c, const vkb_server_config* cfg, vkb_serve
     return VKB_OK;
 }
 
-vkb_status vkb_server_submit(vkb_server* v, vkb_scene* s, const vkb_profile* pf, float* host_rgba, uint64_t* id) {
+vkb_status vkb_server_submit_view(vkb_server* v, vkb_scene* s, const vkb_camera* cam, const vkb_profile* pf, float* host_rgba, uint64_t* id) {
     if (!v || !s || !pf || !host_rgba || !id) return fail(VKB_INVALID_ARG, "null argument");
     if (s->ctx != v->c) return fail(VKB_INVALID_ARG, "scene belongs to another context");
     return guarded([&] {
         validate_profile(pf);
+        if (cam) validate_camera(*cam);
         if (pf->adaptive) throw Unsupported{"adaptive stopping renders through vkb_render"};
-        uint64_t need = uint64_t(s->camera.width) * s->camera.height * 32u;
-        if (v->budget && v->wave_bytes + scene_bytes(s) + need > v->budget) throw ArgError{"request can never fit the memory budget"};
+        const vkb_camera& c = cam ? *cam : s->camera;
+        uint64_t need = uint64_t(c.width) * c.height * 32u;
+        const uint64_t sb = scene_bytes(s) + (s->base ? scene_bytes(s->base) : 0u);
+        if (v->budget && v->wave_bytes + sb + need > v->budget) throw ArgError{"request can never fit the memory budget"};
+        if (uint64_t(c.width) * c.height > v->capacity) throw ArgError{"request image larger than a wave"};
         *id = v->next_id++;
-        v->queue.push_back({*id, s, *pf, host_rgba});
+        v->queue.push_back({*id, s, *pf, host_rgba, cam != nullptr, c});
         v->state[*id] = 0;
     });
+}
+
+vkb_status vkb_server_submit(vkb_server* v, vkb_scene* s, const vkb_profile* pf, float* host_rgba, uint64_t* id) {
+    return vkb_server_submit_view(v, s, nullptr, pf, host_rgba, id);
 }
 
 vkb_status vkb_server_step(vkb_server* v, vkb_server_status* status) {
@@ -1686,22 +1821,31 @@ vkb_status vkb_server_step(vkb_server* v, vkb_server_status* status) {
         vkb_ctx* c = v->c;
         VKB_CUDA(cudaSetDevice(c->device));
         WaveEngine& eng = *v->eng;
+        // Scenes held under the budget: those of the admitted requests (and a fork's base).
+        v->resident.clear();
+        for (const EngineJob& e : eng.jobs) {
+            v->resident[e.s] = scene_bytes(e.s);
+            if (e.s->base) v->resident[e.s->base] = scene_bytes(e.s->base);
+        }
         // Admit at the wave boundary.
         while (!v->queue.empty() && eng.jobs.size() < v->max_jobs) {
             auto& q = v->queue.front();
-            uint64_t npix = uint64_t(q.s->camera.width) * q.s->camera.height;
+            uint64_t npix = uint64_t(q.cam.width) * q.cam.height;
             uint64_t need = npix * 32u;
             uint64_t scene = v->resident.count(q.s) ? 0u : scene_bytes(q.s);
+            if (q.s->base && !v->resident.count(q.s->base)) scene += scene_bytes(q.s->base);
             if (v->budget && v->wave_bytes + resident_bytes(v) + scene + v->used_bytes + need > v->budget) break;
             auto live = std::make_unique<vkb_server::Live>();
             live->id = q.id; live->host_out = q.host_out; live->bytes = need;
             live->accum.alloc(npix); live->out.alloc(npix);
             EngineJob e;
             e.s = q.s; e.pf = q.pf; e.npix = uint32_t(npix);
+            e.own_camera = q.own_camera; e.camera = q.cam;
             e.count = q.pf.sample_count ? q.pf.sample_count : q.pf.samples - q.pf.first_sample;
             e.accum = live->accum.p; e.out_dev = live->out.p;
             eng.add(e);
             v->resident[q.s] = scene_bytes(q.s);
+            if (q.s->base) v->resident[q.s->base] = scene_bytes(q.s->base);
             v->used_bytes += need;
             v->peak_bytes = std::max(v->peak_bytes, v->wave_bytes + resident_bytes(v) + v->used_bytes);
             v->state[q.id] = 1;

@@ -1141,5 +1141,14 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_debug_trace(SceneView sv, uint3
         uv[2 * i] = f ? h.u : 0.f; uv[2 * i + 1] = f ? h.v : 0.f;
     }
 }
+// Occlusion of n world rays by the shadow rays' any-hit traversal (first hit ends the
+// walk, no back-face culling): occluded[i] = 1 when anything lies within (0, tmax).
+__global__ void __launch_bounds__(TRACE_BLOCK) k_debug_occluded(SceneView sv, uint32_t n, const float4* rays, uint32_t* occluded, uint32_t* err) {
+    VKB_STACK_DECL
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        HitRecord h;
+        occluded[i] = trace_any<true, false>(sv, RayRef{rays, rays + n, i}, rays[i].w, h, err, nullptr, stk) ? 1u : 0u;
+    }
+}
 
 }  // namespace vkb
