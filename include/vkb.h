@@ -167,8 +167,16 @@ typedef struct vkb_profile {
 /* Render output: linear RGBA32F mean image (resolve.slang:162-191). */
 typedef struct vkb_output {
     float* rgba;               /* width*height*4 */
-    uint32_t on_device;        /* 1: rgba is a device pointer on the context's GPU */
+    uint32_t on_device;        /* 1: rgba (and the guide planes) are device pointers on the context's GPU */
     uint32_t* primary_ids;     /* optional, width*height*2 (instance, triangle) of sample first_sample; 0xffffffff on miss */
+    /* Optional denoiser guides (path.slang:1549-1571 written per sample, summed per pixel as
+     * path.slang:1956-1963 does), as means over the rendered samples, width*height*4 each:
+     * guide_albedo = the camera hit's response to a uniform white world (diffuse + reflected,
+     * clamped to [0,1]) in rgb and its coverage (fraction of samples that hit) in w;
+     * guide_normal = the camera hit's shading normal in xyz, 0 in w.  A miss or a dropped
+     * sample adds zero.  vkb_render / vkb_render_view without adaptive stopping only. */
+    float* guide_albedo;
+    float* guide_normal;
 } vkb_output;
 
 typedef struct vkb_stats {
@@ -320,16 +328,18 @@ uint64_t vkb_scene_launch_count(vkb_scene* scene);
 /* Render without allocating (no counterpart in the reference: it exists for callers
  * that cannot allocate device memory while they render, e.g. a host renderer whose
  * own memory manager owns every device allocation, or a serving loop with a fixed
- * footprint).  Same semantics and results as vkb_render, but every wavefront queue,
- * accumulator and counter lives in one fixed device array of VKB_NOALLOC_SCRATCH_MIB
- * MiB that each GPU loading the library holds until process exit; no cudaMalloc or
- * cudaFree is called.  An image needs about 236 bytes per pixel for one sample per
- * wave (16 accumulator + 220 queue bytes, +16 with host output, +8 with primary_ids);
- * larger images are rejected with VKB_INVALID_ARG.  The first call on a device looks
- * up the array's device address with that device current: make that first call
- * before any stream capture.  All calls share the array and it keeps the previous
- * call's contents: calls that overlap on the GPU (another stream, another thread)
- * race, so serialise them.  VKB_PROFILE_TIME_KERNELS is ignored (no events). */
+ * footprint).  Same semantics, results and stats as vkb_render, but every wavefront
+ * queue, accumulator and counter lives in one fixed device array of
+ * VKB_NOALLOC_SCRATCH_MIB MiB that each GPU loading the library holds until process
+ * exit; no cudaMalloc or cudaFree is called.  One sample per wave needs about 252 bytes
+ * per pixel with host output (16 accumulator + 220 queue + 16 staging; ~133k pixels),
+ * 260 with host output and primary_ids (~129k), 236 with device output (~142k), 244
+ * with device output and primary_ids (~137k); larger images are rejected with
+ * VKB_INVALID_ARG.  Each call looks up the array's device address with the device
+ * current: make the first call on a device before any stream capture.  All calls share
+ * the array and it keeps the previous call's contents: calls that overlap on the GPU
+ * (another stream, another thread) race, so serialise them.  VKB_PROFILE_TIME_KERNELS
+ * is ignored (no events). */
 #define VKB_NOALLOC_SCRATCH_MIB 32u
 vkb_status vkb_render_noalloc(vkb_scene* scene, const vkb_profile* profile, vkb_output* out, vkb_stats* stats);
 

@@ -1314,9 +1314,37 @@ template <class R> V3<R> next_event(Ctx<R>& cx, const HitSurf<R>& hs, const Clos
     }
     return value;
 }
+// Denoiser guide albedo of the camera hit (path.slang:1549-1571): the surface's response
+// to a uniform white world, diffuse + reflected, from surface_radiance_at
+// (surface_lighting.slang:260-300): diffuse = direct_diffuse * pi (bsdf_response.slang:
+// 82-96), reflected = specular_reflectance(specular_response(c, view), brdf_moments(nv,
+// roughness)) (bsdf_response.slang:47-77) with the closure's own normal; clamped to
+// [0, 1] (the closure weight is 1: one closure, no opacity).
+template <class R> V3<R> guide_albedo(const Closure<R>& c, V3<R> view) {
+    V3<R> n = c.n;
+    R nv = std::max(dot(n, view), R(0.0001));
+    R m[3];
+    lut<R>().moments(nv, c.specular_roughness, m);
+    V3<R> diffuse = direct_diffuse(c, view) * R(PI);
+    R f0 = fresnel(R(1), dielectric_ior(c));
+    R grazing = f0 != 0 ? m[1] : R(0);
+    V3<R> reflected = (V3<R>(f0, f0, f0) * m[0] + V3<R>(grazing, grazing, grazing)) * c.specular_color;
+    if (c.base_metalness > 0) {
+        V3<R> metal = c.base_color * c.base_weight;
+        V3<R> corr = metal_edge_correction(metal, c.specular_color);
+        V3<R> comp = metal_compensation(c, view);
+        V3<R> mr = (V3<R>(1, 1, 1) + comp) * c.specular_weight * vmax(metal * m[0] + V3<R>(m[1], m[1], m[1]) - corr * m[2], V3<R>());
+        reflected = lerp3(reflected, mr, c.base_metalness);
+    }
+    V3<R> a = diffuse + reflected;
+    return V3<R>(clampr(a.x, R(0), R(1)), clampr(a.y, R(0), R(1)), clampr(a.z, R(0), R(1)));
+}
+
 // One camera sample: path_pixel (path.slang:1792-1968) + integrate (:1313-1709) for
-// opaque OpenPBR surfaces, analytic lights and a constant environment.
-template <class R> V3<R> integrate(Ctx<R>& cx, uint32_t px, uint32_t py, uint32_t index, uint32_t* ids) {
+// opaque OpenPBR surfaces, analytic lights and a constant environment.  guide (8 values,
+// optional): the camera hit's guide albedo + coverage and guide normal + 0, zero on a
+// miss or a dropped sample (path.slang:1946-1950).
+template <class R> V3<R> integrate(Ctx<R>& cx, uint32_t px, uint32_t py, uint32_t index, uint32_t* ids, R* guide = nullptr) {
     const Scene<R>& s = cx.s;
     const vkb_profile& pf = cx.prof;
     Sampler sm = make_sampler(px, py, index, pf.samples, pf.seed);
@@ -1364,6 +1392,11 @@ template <class R> V3<R> integrate(Ctx<R>& cx, uint32_t px, uint32_t py, uint32_
         boundary_closure_air(c);
         groups = 0xffffffffu;                                             // objects[].metadata.x: every link group
         V3<R> view = -dir;
+        if (guide && bounce == 0) {
+            V3<R> a = guide_albedo(c, view);
+            guide[0] = a.x; guide[1] = a.y; guide[2] = a.z; guide[3] = 1;
+            guide[4] = c.n.x; guide[5] = c.n.y; guide[6] = c.n.z; guide[7] = 0;
+        }
         V3<R> iface = dot(hs.geometric, view) > 0 ? hs.geometric : hs.face;
         Prepared<R> pr = transport_prepare(c, view, hs.geometric, iface);
         BsdfSample<R> smp = transport_sample(c, view, R(sc[0]), R(sc[1]), R(sc[2]), pr);
@@ -1393,7 +1426,11 @@ template <class R> V3<R> integrate(Ctx<R>& cx, uint32_t px, uint32_t py, uint32_
     cx.dropped_light += dropped;
     V3<R> result = radiance * R(s.env.exposure);
     if (!finite3(result)) nonfinite = true;
-    if (nonfinite) { cx.dropped_path++; return V3<R>(); }
+    if (nonfinite) {
+        cx.dropped_path++;
+        if (guide) for (int k = 0; k < 8; ++k) guide[k] = 0;
+        return V3<R>();
+    }
     return result;
 }
 
@@ -1483,7 +1520,7 @@ template <class R> void render_adaptive(const Scene<R>& s, const vkb_profile& pf
 }
 
 template <class R> void render_impl(const Scene<R>& s, const vkb_profile& pf, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,
-                                    float* rgba, uint32_t* ids, uint32_t threads, uint64_t* stats) {
+                                    float* rgba, uint32_t* ids, uint32_t threads, uint64_t* stats, float* guides = nullptr) {
     if (pf.adaptive) {
         // Whole image, whole exposure: the stop rule reads image-edge-clamped neighbours.
         if (x0 != 0 || y0 != 0 || w != s.cam.width || h != s.cam.height || pf.first_sample != 0 ||
@@ -1503,11 +1540,17 @@ template <class R> void render_impl(const Scene<R>& s, const vkb_profile& pf, ui
         for (uint32_t row; (row = next.fetch_add(1)) < h;) {
             for (uint32_t x = 0; x < w; ++x) {
                 V3<R> sum;
+                R gsum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
                 uint32_t* pid = ids ? ids + (size_t(row) * w + x) * 2 : nullptr;
-                for (uint32_t k = 0; k < count; ++k)
-                    sum = sum + integrate(cx, x0 + x, y0 + row, first + k, k == 0 ? pid : nullptr);
+                for (uint32_t k = 0; k < count; ++k) {
+                    R g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                    sum = sum + integrate(cx, x0 + x, y0 + row, first + k, k == 0 ? pid : nullptr, guides ? g : nullptr);
+                    for (int c = 0; c < 8; ++c) gsum[c] += g[c];
+                }
                 float* o = rgba + (size_t(row) * w + x) * 4;
                 o[0] = float(sum.x / R(count)); o[1] = float(sum.y / R(count)); o[2] = float(sum.z / R(count)); o[3] = 1.f;
+                if (guides)
+                    for (int c = 0; c < 8; ++c) guides[(size_t(row) * w + x) * 8 + c] = float(gsum[c] / R(count));
             }
         }
         std::lock_guard<std::mutex> g(mu);
@@ -1737,11 +1780,17 @@ void oracle_camera_rays(void* h, const vkb_profile* pf, uint32_t index, uint32_t
         }
 }
 // Render a crop. stats (optional, 4 u64): extension rays, shadow rays, dropped path samples, dropped light samples.
+// guides (optional, w*hgt*8): per pixel the mean guide albedo + coverage and the mean
+// guide normal + 0 over the rendered samples.
 void oracle_render(void* h, int fp64, const vkb_profile* pf, uint32_t x0, uint32_t y0, uint32_t w, uint32_t hgt,
-                   float* rgba, uint32_t* ids, uint32_t threads, uint64_t* stats) {
+                   float* rgba, uint32_t* ids, uint32_t threads, uint64_t* stats, float* guides) {
     OracleScene* o = static_cast<OracleScene*>(h);
-    if (fp64) render_impl(*static_cast<Scene<double>*>(o->s64), *pf, x0, y0, w, hgt, rgba, ids, threads, stats);
-    else render_impl(*static_cast<Scene<float>*>(o->s32), *pf, x0, y0, w, hgt, rgba, ids, threads, stats);
+    if (guides && pf->adaptive) {   // refused (pyoracle checks first): guides read NaN
+        for (size_t k = 0; k < size_t(w) * hgt * 8; ++k) guides[k] = std::numeric_limits<float>::quiet_NaN();
+        guides = nullptr;
+    }
+    if (fp64) render_impl(*static_cast<Scene<double>*>(o->s64), *pf, x0, y0, w, hgt, rgba, ids, threads, stats, guides);
+    else render_impl(*static_cast<Scene<float>*>(o->s32), *pf, x0, y0, w, hgt, rgba, ids, threads, stats, guides);
 }
 // Morton codes of the TLAS build (instance boxes) and of one mesh's BLAS build (triangle boxes).
 // World boxes of the TLAS leaves (xyz lo, xyz hi per instance), as the build computes them.

@@ -51,7 +51,7 @@ def lib():
         l.oracle_trace.argtypes = [P, C.c_int, C.c_uint32, f32p, C.c_int, f32p, u32p, f32p]
         l.oracle_camera_rays.argtypes = [P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, f32p]
         l.oracle_render.argtypes = [P, C.c_int, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, f32p, u32p, C.c_uint32,
-                                    C.POINTER(C.c_uint64)]
+                                    C.POINTER(C.c_uint64), f32p]
         l.oracle_tlas_morton.argtypes = [P, u32p]
         l.oracle_instance_boxes.argtypes = [P, f32p, f32p]
         l.oracle_blas_morton.argtypes = [P, C.c_uint32, u32p]
@@ -183,7 +183,9 @@ class OracleScene:
         lib().oracle_camera_rays(self.h, C.cast(C.byref(profile), C.c_void_p), index, x0, y0, w, h, _p(out, C.c_float))
         return out
 
-    def render(self, profile, x0=0, y0=0, w=None, h=None, fp64=True, threads=None, ids=False):
+    def render(self, profile, x0=0, y0=0, w=None, h=None, fp64=True, threads=None, ids=False, guides=False):
+        """(image, stats), or (image, ids, stats) with ids; with guides=True also the
+        (h, w, 2, 4) guide planes (mean albedo + coverage, mean normal) appended."""
         cam = self.scene.camera
         w = cam.width if w is None else w
         h = cam.height if h is None else h
@@ -193,11 +195,15 @@ class OracleScene:
         threads = threads or os.cpu_count() or 1
         out = np.zeros((h, w, 4), np.float32)
         idbuf = np.zeros((h, w, 2), np.uint32) if ids else None
+        if guides and profile.adaptive:
+            raise ValueError("guides are rendered without adaptive stopping")
+        gbuf = np.zeros((h, w, 2, 4), np.float32) if guides else None
         stats = (C.c_uint64 * 4)()
         lib().oracle_render(self.h, 1 if fp64 else 0, C.cast(C.byref(profile), C.c_void_p), x0, y0, w, h, _p(out, C.c_float),
-                            _p(idbuf, C.c_uint32) if ids else None, threads, stats)
+                            _p(idbuf, C.c_uint32) if ids else None, threads, stats, _p(gbuf, C.c_float) if guides else None)
         st = {"extension_rays": stats[0], "shadow_rays": stats[1], "dropped_path_samples": stats[2], "dropped_light_samples": stats[3]}
-        return (out, idbuf, st) if ids else (out, st)
+        res = (out, idbuf, st) if ids else (out, st)
+        return res + (gbuf,) if guides else res
 
     def tlas_morton(self):
         out = np.zeros(self.desc.num_instances, np.uint32)

@@ -48,6 +48,29 @@ def test_noalloc_render_matches_render_on_two_calls():
         assert np.array_equal(img, s.render(part).image)
 
 
+def test_noalloc_allocates_nothing_on_a_fresh_renderer():
+    # The property the entry point exists for: on a renderer that has never rendered
+    # (so no wavefront of its own exists), a no-allocation render leaves the device's
+    # free memory unchanged, and is still right.  A first renderer loads the library's
+    # device code (lazy module loading allocates for code, not for the render).
+    import torch
+    sc = S.spheres_scene(width=128, height=96)
+    prof = Profile.reference_transport(4, 16)
+    with Renderer(0) as warm, warm.install(sc) as s:
+        _noalloc(s, prof)
+    with Renderer(0) as r, r.install(sc) as s:
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info(0)
+        img, _, st = _noalloc(s, prof)
+        img2, _, _ = _noalloc(s, prof)
+        torch.cuda.synchronize()
+        free1, _ = torch.cuda.mem_get_info(0)
+        # vkb_render would have reserved 128 x 96 x 16 path slots (~43 MB) here.
+        assert free0 - free1 < (1 << 20), (free0, free1)
+        assert np.array_equal(img, img2) and st.paths == 128 * 96 * 16 and st.kernel_launches > 0
+        assert np.array_equal(img, s.render(prof).image)
+
+
 def test_noalloc_rejects_images_beyond_its_scratch():
     big = S.spheres_scene(width=1024, height=1024)
     with Renderer(0) as r, r.install(big) as s:

@@ -139,6 +139,8 @@ class RenderResult:
     image: np.ndarray          # (H, W, 4) linear RGBA32F mean
     stats: dict
     primary_ids: np.ndarray | None = None
+    guide_albedo: np.ndarray | None = None   # (H, W, 4): mean guide albedo (rgb) and coverage (w)
+    guide_normal: np.ndarray | None = None   # (H, W, 4): mean shading normal (xyz), 0
 
 
 class InstalledScene:
@@ -192,9 +194,10 @@ class InstalledScene:
         return int(self.r.lib.vkb_scene_launch_count(self.h))
 
     def render(self, profile: Profile, ids: bool = False, out: np.ndarray | None = None, device_ptr: int | None = None,
-               camera: abi.VkbCamera | None = None) -> RenderResult:
+               camera: abi.VkbCamera | None = None, guides: bool = False) -> RenderResult:
         """Render under `profile` (vkb_render), or through `camera` instead of the scene's
-        own (vkb_render_view: its resolution sets the image's)."""
+        own (vkb_render_view: its resolution sets the image's); `guides` also returns the
+        denoiser guide planes (host output only)."""
         cam = camera if camera is not None else self.scene.camera
         o = abi.VkbOutput()
         img = None
@@ -207,6 +210,14 @@ class InstalledScene:
             o.on_device = 0
         idbuf = np.empty((cam.height, cam.width, 2), np.uint32) if ids else None
         o.primary_ids = abi.uptr(idbuf) if ids else None
+        ga = gn = None
+        if guides:
+            if device_ptr is not None:
+                raise ValueError("guide planes are returned in host memory: render to a host image")
+            ga = np.empty((cam.height, cam.width, 4), np.float32)
+            gn = np.empty((cam.height, cam.width, 4), np.float32)
+            o.guide_albedo = ga.ctypes.data_as(C.c_void_p)
+            o.guide_normal = gn.ctypes.data_as(C.c_void_p)
         st = abi.VkbStats()
         p = profile.c()
         if camera is not None:
@@ -214,7 +225,7 @@ class InstalledScene:
         else:
             abi.check(self.r.lib.vkb_render(self.h, C.byref(p), C.byref(o), C.byref(st)))
         stats = {k: getattr(st, k) for k, _ in abi.VkbStats._fields_}
-        return RenderResult(img, stats, idbuf)
+        return RenderResult(img, stats, idbuf, ga, gn)
 
     def tlas_morton(self):
         out = np.zeros(self.scene.instance_rows.shape[0], np.uint32)

@@ -91,7 +91,8 @@ NOALLOC_SCRATCH_MIB = 32
 
 
 class VkbOutput(C.Structure):
-    _fields_ = [("rgba", C.c_void_p), ("on_device", C.c_uint32), ("primary_ids", C.POINTER(C.c_uint32))]
+    _fields_ = [("rgba", C.c_void_p), ("on_device", C.c_uint32), ("primary_ids", C.POINTER(C.c_uint32)),
+                ("guide_albedo", C.c_void_p), ("guide_normal", C.c_void_p)]
 
 
 class VkbStats(C.Structure):

@@ -396,6 +396,7 @@ struct WaveBuffers {
     uint2* rng = nullptr;
     unsigned long long* work = nullptr;
     Job* jobs = nullptr;
+    float4* guide = nullptr;   // guide renders: 2 float4 per path slot
 };
 // The context's own wavefront storage (grown on demand, reused by every render).
 struct Wavefront {
@@ -448,6 +449,7 @@ struct vkb_ctx {
     std::vector<cudaEvent_t> cache_events;    // timed renders: around each radiance-cache query launch
     DBuf<float4> ad_mean, ad_m2;              // adaptive stopping: per-pixel moments
     DBuf<uint32_t> ad_state;                  // and parity/stop bits
+    DBuf<float4> guide_slots, guide_accum, guide_staging;   // denoiser-guide renders
 };
 
 struct vkb_scene {
@@ -641,6 +643,9 @@ struct EngineJob {
     float4* out_dev = nullptr;      // device destination of the mean image
     uint32_t* ids_dev = nullptr;    // device primary ids (first sample) or null
     float4* accum = nullptr;        // device accumulator, npix
+    float4* guide_accum = nullptr;  // guide renders: 2 x npix sums; mean planes (device) or null
+    float4* guide_albedo = nullptr;
+    float4* guide_normal = nullptr;
     uint32_t npix = 0, count = 0, done = 0, pixel_base = 0;
 };
 struct WaveTotals {
@@ -685,6 +690,7 @@ Job make_job(const EngineJob& e) {
     j.adaptive_threshold = pf.adaptive_threshold > 0.f ? pf.adaptive_threshold : 0.01f;
     j.adaptive_min = pf.adaptive_min_samples ? pf.adaptive_min_samples : std::max(16u, uint32_t(std::sqrt(float(pf.samples))));
     j.ad_mean = e.ad_mean; j.ad_m2 = e.ad_m2; j.ad_state = e.ad_state;
+    j.guide_accum = e.guide_accum; j.guide_albedo = e.guide_albedo; j.guide_normal = e.guide_normal;
     return j;
 }
 
@@ -696,6 +702,7 @@ PathParams path_params(const vkb_ctx* c, const WaveBuffers& w, uint32_t njobs) {
     p.hit = w.hit; p.hit_inst = w.hit_inst; p.thr = w.thr; p.rad = w.rad; p.rng = w.rng;
     p.sa_o = w.sa_o; p.sa_d = w.sa_d; p.sa_c = w.sa_c; p.sb_o = w.sb_o; p.sb_d = w.sb_d; p.sb_c = w.sb_c;
     p.counters = w.counters; p.work = w.work; p.err = w.err;
+    p.guide = w.guide;
     return p;
 }
 
@@ -734,6 +741,7 @@ void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counte
         else k_trace<false, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p, cur);
         if (timed) VKB_CUDA(cudaEventRecord(c->kernel_events[2 * tot.trace_launches + 1], st));
         tot.trace_launches++;
+        if (!BATCH && b == 0u && p.guide) { k_guides<<<sms * 8, 256, 0, st>>>(p); tot.launches += 1; }
         k_reset_queues<<<1, 1, 0, st>>>(p.counters, cur ^ 1);
         k_shade<BATCH><<<sgrid, 512, 0, st>>>(p, cur);
         if (counted) k_trace_shadow<true, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
@@ -1015,8 +1023,11 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
         if (outs[k]->primary_ids) ids_words += 2 * npix;
         if (!outs[k]->on_device) staged += npix;
     }
-    bool adaptive = false;
+    bool adaptive = false, guides = false;
     for (const auto& job : in) adaptive = adaptive || job.second.adaptive;
+    for (size_t k = 0; k < in.size(); ++k) guides = guides || outs[k]->guide_albedo || outs[k]->guide_normal;
+    if (guides && (in.size() != 1 || cache || adaptive))
+        throw Unsupported{"denoiser guides render one job through vkb_render / vkb_render_view, without adaptive stopping"};
     if (adaptive) {
         // path.slang stops pixels sample by sample against their neighbours' previous
         // sample: one job, one sample per wave, the whole exposure in this call.
@@ -1033,6 +1044,14 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
     capacity = std::max(capacity, max_pix);
     c->wave.reserve(capacity, uint32_t(in.size()));
     c->accum.alloc(std::max<size_t>(1, total_pixels));
+    WaveBuffers wb = c->wave.view();
+    if (guides) {
+        c->guide_slots.alloc(2 * capacity);
+        c->guide_accum.alloc(2 * max_pix);
+        VKB_CUDA(cudaMemsetAsync(c->guide_accum.p, 0, 2 * max_pix * sizeof(float4), st));
+        if (!outs[0]->on_device) c->guide_staging.alloc(2 * max_pix);
+        wb.guide = c->guide_slots.p;
+    }
     if (staged) c->staging.alloc(staged);
     if (ids_words) c->ids.alloc(ids_words);
     std::vector<EngineJob> jobs(in.size());
@@ -1048,10 +1067,25 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
         else { e.out_dev = c->staging.p + stg; stg += e.npix; }
         if (outs[k]->primary_ids) { e.ids_dev = c->ids.p + idw; idw += 2 * size_t(e.npix); }
         if (adaptive) { e.ad_mean = c->ad_mean.p; e.ad_m2 = c->ad_m2.p; e.ad_state = c->ad_state.p; }
+        if (guides) {
+            e.guide_accum = c->guide_accum.p;
+            if (outs[k]->on_device) {
+                e.guide_albedo = reinterpret_cast<float4*>(outs[k]->guide_albedo);
+                e.guide_normal = reinterpret_cast<float4*>(outs[k]->guide_normal);
+            } else {
+                e.guide_albedo = outs[k]->guide_albedo ? c->guide_staging.p : nullptr;
+                e.guide_normal = outs[k]->guide_normal ? c->guide_staging.p + e.npix : nullptr;
+            }
+        }
         paths += uint64_t(e.npix) * e.count;
     }
-    run_engine(c, jobs, c->wave.view(), capacity, flags, true, tot, (flags & VKB_BATCH_FAIR) == 0, cache);
+    run_engine(c, jobs, wb, capacity, flags, true, tot, (flags & VKB_BATCH_FAIR) == 0, cache);
     for (size_t k = 0; k < in.size(); ++k) {
+        if (guides && !outs[k]->on_device) {
+            const size_t bytes = size_t(jobs[k].npix) * sizeof(float4);
+            if (outs[k]->guide_albedo) VKB_CUDA(cudaMemcpyAsync(outs[k]->guide_albedo, jobs[k].guide_albedo, bytes, cudaMemcpyDeviceToHost, st));
+            if (outs[k]->guide_normal) VKB_CUDA(cudaMemcpyAsync(outs[k]->guide_normal, jobs[k].guide_normal, bytes, cudaMemcpyDeviceToHost, st));
+        }
         if (!outs[k]->on_device) VKB_CUDA(cudaMemcpyAsync(outs[k]->rgba, jobs[k].out_dev, size_t(jobs[k].npix) * sizeof(float4), cudaMemcpyDeviceToHost, st));
         if (outs[k]->primary_ids) VKB_CUDA(cudaMemcpyAsync(outs[k]->primary_ids, jobs[k].ids_dev, size_t(jobs[k].npix) * 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     }
@@ -1098,6 +1132,7 @@ vkb_status vkb_close(vkb_ctx* c) {
     if (c->ev1) cudaEventDestroy(c->ev1);
     c->wave.release();
     c->accum.release(); c->staging.release(); c->ids.release(); c->ad_mean.release(); c->ad_m2.release(); c->ad_state.release();
+    c->guide_slots.release(); c->guide_accum.release(); c->guide_staging.release();
     c->lut.release(); c->filter.release();
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -1921,21 +1956,13 @@ constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(VKB_NOALLOC_SCRATCH_MIB) << 20;
 // Every GPU that loads this library holds this array until the process exits.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
-// Device address of g_noalloc_scratch per device ordinal, looked up once with that
-// device current (the host-side symbol is only a stand-in, never a device address).
-constexpr int NOALLOC_MAX_DEVICES = 64;
-unsigned char* g_noalloc_base[NOALLOC_MAX_DEVICES] = {};
-std::mutex g_noalloc_mutex;
-
-unsigned char* noalloc_scratch(int device) {
-    if (device < 0 || device >= NOALLOC_MAX_DEVICES) throw ArgError{"device ordinal beyond the no-alloc table"};
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_base[device]) {
-        void* p = nullptr;
-        VKB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        g_noalloc_base[device] = static_cast<unsigned char*>(p);
-    }
-    return g_noalloc_base[device];
+// Device address of g_noalloc_scratch on the current device, looked up on every call
+// (the host-side symbol is only a stand-in, never a device address; a per-process cache
+// would go stale if the caller reset the device and its context were recreated).
+unsigned char* noalloc_scratch() {
+    void* p = nullptr;
+    VKB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    return static_cast<unsigned char*>(p);
 }
 
 struct Carver {
@@ -1957,10 +1984,11 @@ extern "C" vkb_status vkb_render_noalloc(vkb_scene* s, const vkb_profile* pf, vk
     return guarded([&] {
         validate_profile(pf);
         if (pf->adaptive) throw Unsupported{"adaptive stopping renders through vkb_render"};
+        if (out->guide_albedo || out->guide_normal) throw Unsupported{"denoiser guides render through vkb_render"};
         uint32_t count = pf->sample_count ? pf->sample_count : pf->samples - pf->first_sample;
         vkb_ctx* c = s->ctx;
         VKB_CUDA(cudaSetDevice(c->device));
-        unsigned char* base = noalloc_scratch(c->device);
+        unsigned char* base = noalloc_scratch();
         cudaStream_t st = c->stream;
         const uint32_t W = s->camera.width, H = s->camera.height, npix = W * H;
         // Fixed part: counters, error word, traversal counters, job table, accumulator,
@@ -2010,7 +2038,8 @@ extern "C" vkb_status vkb_render_noalloc(vkb_scene* s, const vkb_profile* pf, vk
         if (out->primary_ids) VKB_CUDA(cudaMemcpyAsync(out->primary_ids, ids, size_t(npix) * 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         VKB_CUDA(cudaStreamSynchronize(st));
         s->launches += tot.launches;
-        fill_stats(stats, tot, uint64_t(npix) * count, 0.f);
+        c->launches += tot.launches;
+        fill_stats(stats, tot, uint64_t(npix) * count, s->build_ms);
     });
 }
 

@@ -313,6 +313,29 @@ __device__ __forceinline__ float3 direct_diffuse(const Lut& l, const Closure& c,
     float3 albedo = c.specular_color * dielectric_albedo(l, fmaxf(dot(n, view), 0.0001f), c.specular_roughness, dielectric_ior(c));
     return (c.base_color * c.base_weight) * (1.f - c.base_metalness) * (f3(1.f) - albedo) / PI_F;
 }
+// Denoiser guide albedo of a camera hit (path.slang:1549-1571): the response to a uniform
+// white world from surface_radiance_at (surface_lighting.slang:260-300) -- diffuse =
+// direct_diffuse * pi, reflected = specular_reflectance(specular_response(c, view),
+// brdf_moments(nv, roughness)) (bsdf_response.slang:47-77) -- about the closure's own
+// normal, clamped to [0, 1] (closure weight 1: one closure, opaque).
+__device__ __forceinline__ float3 guide_albedo(const Lut& l, const Closure& c, float3 view) {
+    const float3 n = c.n;
+    const float nv = fmaxf(dot(n, view), 0.0001f);
+    const float4 m = brdf_texel(l, nv, c.specular_roughness);
+    const float3 diffuse = direct_diffuse(l, c, n, view) * PI_F;
+    const float f0 = fresnel(1.f, dielectric_ior(c));
+    const float grazing = f0 != 0.f ? m.y : 0.f;
+    float3 reflected = (f3(f0) * m.x + f3(grazing)) * c.specular_color;
+    if (c.base_metalness > 0.f) {
+        const float3 metal = c.base_color * c.base_weight;
+        const float3 corr = metal_edge_correction(metal, c.specular_color);
+        const float3 comp = metal_compensation(l, c, n, view);
+        const float3 mr = (f3(1.f) + comp) * c.specular_weight * vmax(metal * m.x + f3(m.y) - corr * m.z, f3(0.f));
+        reflected = lerp3(reflected, mr, c.base_metalness);
+    }
+    const float3 a = diffuse + reflected;
+    return f3(clampf(a.x, 0.f, 1.f), clampf(a.y, 0.f, 1.f), clampf(a.z, 0.f, 1.f));
+}
 // bsdf.slang:242-250.
 __device__ __forceinline__ Prepared transport_prepare(const Lut& l, const Closure& c, float3 view, float3 smooth, float3 geometric) {
     Prepared pr;

@@ -440,6 +440,9 @@ struct Job {
     uint32_t adaptive, adaptive_min;
     float adaptive_threshold;
     float4* ad_mean; float4* ad_m2; uint32_t* ad_state;
+    // Denoiser guides (path.slang:1549-1571,1956-1963), single-job renders only: per-pixel
+    // sums (albedo + coverage, normal) in sample order and the mean planes written at resolve.
+    float4* guide_accum; float4* guide_albedo; float4* guide_normal;
 };
 constexpr uint32_t AD_STOPPED = 4u;
 // Radiance-cache hooks of a wave.  mode 1 (query): a path reaching vertex `vertex`
@@ -474,6 +477,7 @@ struct PathParams {
     unsigned long long* work;  // instrumented traversal: closest nodes, tris, instances, blas nodes; shadow nodes, tris, blas nodes
     uint32_t* err;
     CacheParams cache;
+    float4* guide;        // guide renders: the camera hit's guide albedo and normal per path slot (2 float4)
 };
 constexpr uint32_t META_NONFINITE = 0x80000000u;
 constexpr uint32_t SH_TRACE_A = 1u, SH_HAS_B = 2u, SH_TRACE_B = 4u, SH_DIRECT = 8u;
@@ -1062,6 +1066,35 @@ __global__ void k_adaptive_decide(PathParams p) {
 }
 // Zero the next ray queue and the shadow queue before a shade pass.
 __global__ void k_reset_queues(uint32_t* counters, int nxt) { counters[nxt] = 0u; counters[2] = 0u; counters[11] = 0u; counters[12] = 0u; }
+// Denoiser guides of this wave's camera hits (path.slang:1549-1571): per path slot the
+// hit's guide albedo (w = 1: coverage) and shading normal, zero on a miss.  Runs between
+// the bounce-0 closest-hit trace and the shade pass of single-job guide renders.
+__global__ void k_guides(PathParams p) {
+    const uint32_t n = p.counters[0];
+    const Job& J = p.job0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 rd = p.ray_d[0][i], hh = p.hit[i];
+        const uint32_t slot = __float_as_uint(rd.w);
+        float4 ga = make_float4(0.f, 0.f, 0.f, 0.f), gn = ga;
+        if (hh.x >= 0.f) {
+            const uint32_t inst = p.hit_inst[i];
+            const float3 dir = f3(rd.x, rd.y, rd.z);
+            const Surface s = hit_surface(J, inst, __float_as_uint(hh.w), hh.y, hh.z, dir);
+            const vkb_material& mt = J.materials[__ldg(&J.inst_info[inst]).y];
+            Closure c;
+            c.base_color = get3(mt.base_color); c.base_weight = mt.base_weight; c.base_metalness = mt.base_metalness;
+            c.specular_color = get3(mt.specular_color); c.specular_weight = mt.specular_weight;
+            c.specular_roughness = mt.specular_roughness; c.specular_ior = mt.specular_ior; c.optical_ior = 0.f;
+            c.n = s.geometric;
+            boundary_closure_air(c);
+            const float3 a = guide_albedo(p.lut, c, -dir);
+            ga = make_float4(a.x, a.y, a.z, 1.f);
+            gn = make_float4(c.n.x, c.n.y, c.n.z, 0.f);
+        }
+        p.guide[2 * size_t(slot)] = ga;
+        p.guide[2 * size_t(slot) + 1] = gn;
+    }
+}
 // resolve.slang:162-191: add this wave's finished samples to each job's accumulator,
 // one sample at a time in sample order (any wave size gives the same sums).
 template <bool BATCH>
@@ -1096,6 +1129,25 @@ __global__ void k_accumulate(PathParams p) {
                 J.ad_mean[pixel] = nm;
                 J.ad_m2[pixel] = m2;
             }
+        } else if (!BATCH && J.guide_accum) {
+            // Guide renders: the guides of a dropped sample are zero too (path.slang:1946-1950).
+            float4 ga = J.guide_accum[2 * pixel], gn = J.guide_accum[2 * pixel + 1];
+            for (uint32_t k = 0; k < J.wave_samples; ++k) {
+                uint32_t slot = J.slot_base + k * J.npix + pixel;
+                float4 T = p.thr[slot], R = p.rad[slot];
+                dl += __float_as_uint(R.w);
+                float3 v = f3(R.x, R.y, R.z) * J.env.exposure;
+                const bool drop = (__float_as_uint(T.w) & META_NONFINITE) || !finite3(v);
+                if (drop) { v = f3(0.f); dp++; }
+                sum.x += v.x; sum.y += v.y; sum.z += v.z; sum.w += 1.f;
+                if (!drop) {
+                    const float4 a = p.guide[2 * size_t(slot)], nn = p.guide[2 * size_t(slot) + 1];
+                    ga.x += a.x; ga.y += a.y; ga.z += a.z; ga.w += a.w;
+                    gn.x += nn.x; gn.y += nn.y; gn.z += nn.z;
+                }
+            }
+            J.guide_accum[2 * pixel] = ga;
+            J.guide_accum[2 * pixel + 1] = gn;
         } else
         for (uint32_t k = 0; k < J.wave_samples; ++k) {
             uint32_t slot = J.slot_base + k * J.npix + pixel;
@@ -1120,6 +1172,11 @@ __global__ void k_resolve(PathParams p, uint32_t total_pixels) {
         float4 a = J.accum[i];
         float inv = a.w > 0.f ? 1.f / a.w : 0.f;
         J.out[i] = make_float4(a.x * inv, a.y * inv, a.z * inv, a.w > 0.f ? 1.f : 0.f);
+        if (!BATCH && J.guide_accum) {
+            const float4 ga = J.guide_accum[2 * i], gn = J.guide_accum[2 * i + 1];
+            if (J.guide_albedo) J.guide_albedo[i] = make_float4(ga.x * inv, ga.y * inv, ga.z * inv, ga.w * inv);
+            if (J.guide_normal) J.guide_normal[i] = make_float4(gn.x * inv, gn.y * inv, gn.z * inv, 0.f);
+        }
     }
 }
 // Test entry: sampler groups for arbitrary (pixel, index, group).
