@@ -591,6 +591,9 @@ def main():
     paths_per_step = npix * prof.samples
     r = Renderer(local)
     s = r.install(sc)
+    info0 = s.info()
+    install = {k: info0[k] for k in ("install_ms", "blas_host_ms", "upload_ms", "tlas_ms", "scene_bytes", "num_triangles",
+                                     "num_instances")}
     stream = torch.cuda.ExternalStream(r.stream, device=torch.device("cuda", local))
     dev_frames = [torch.from_numpy(f).to(f"cuda:{local}") for f in frames]
     pinned = [torch.from_numpy(f).pin_memory() for f in frames]
@@ -695,6 +698,7 @@ def main():
                     "d2h_bytes_per_step": int(npix * 16)},
             "gpu_launches": int(launches),
             "tlas": tlas,
+            "install": install,
             "clocks": clocks.summary(),
             "work": {k: counted[k] for k in ("extension_rays", "shadow_rays", "nodes_visited", "triangles_tested",
                                              "instances_entered", "blas_nodes_visited", "shadow_nodes_visited", "shadow_triangles_tested",

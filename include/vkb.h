@@ -316,6 +316,12 @@ typedef struct vkb_scene_info_t {
     uint64_t motion_bytes;     /* changed object bytes accumulated since the last rebuild */
     float build_ms;            /* device time of the last TLAS build or refit */
     uint32_t reserved;
+    /* Install cost (Renderer::install + Rays::new, lib.rs:1322-1470, rt.rs:1098-1289) of
+     * vkb_scene_create (of vkb_scene_fork for a fork): */
+    float install_ms;          /* wall time of the whole call */
+    float blas_host_ms;        /* of which the host binned-SAH builds and 4-wide collapses of every BLAS */
+    float upload_ms;           /* of which the host->device copies (meshes, BLAS, records, instances) */
+    float tlas_ms;             /* of which the first TLAS build (device time) */
 } vkb_scene_info_t;
 vkb_status vkb_scene_info(vkb_scene* scene, vkb_scene_info_t* out);
 

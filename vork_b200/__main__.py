@@ -1,7 +1,8 @@
 """`python -m vork_b200 render scene.json --out image.png`: the std/path route of
 `vork render scene.json --profile std/path --out x.png` for the supported scene subset
 (scene_json.py): load, install, path-trace on the GPU, display transform (std/standard),
-PNG.  `--linear out.npy` also keeps the linear RGBA mean."""
+PNG.  `--linear out.npy` also keeps the linear RGBA mean; `--exr out.exr` writes it as a
+float OpenEXR (png_output.rs:291-366), with the denoiser guide planes when `--guides`."""
 from __future__ import annotations
 
 import argparse
@@ -9,7 +10,7 @@ import sys
 
 import numpy as np
 
-from . import Profile, Renderer, display, scene_json
+from . import Profile, Renderer, display, exr, scene_json
 
 
 def render_command(argv=None) -> int:
@@ -26,16 +27,21 @@ def render_command(argv=None) -> int:
     ap.add_argument("--gamma", type=float, default=1.0)
     ap.add_argument("--bits", type=int, default=8, choices=[8, 16])
     ap.add_argument("--linear", default=None, help="also save the linear RGBA mean (.npy)")
+    ap.add_argument("--exr", default=None, help="also write the linear RGBA mean as a float OpenEXR")
+    ap.add_argument("--guides", action="store_true", help="with --exr: add the denoiser guide planes")
+    ap.add_argument("--exr-compression", default="zip", choices=sorted(exr.COMPRESSION))
     ap.add_argument("--device", type=int, default=0)
     a = ap.parse_args(argv)
     sc = scene_json.load(a.scene, a.width, a.height)
     prof = Profile.reference_transport(a.depth, a.samples, seed=a.seed) if a.depth else Profile(samples=a.samples, seed=a.seed)
     with Renderer(a.device) as r, r.install(sc) as s:
-        res = s.render(prof)
+        res = s.render(prof, guides=bool(a.exr and a.guides))
         codes = display.display(r, res.image, a.display, a.exposure, a.gamma, bits=a.bits)
     display.write_png(a.out, codes, a.display)
     if a.linear:
         np.save(a.linear, res.image)
+    if a.exr:
+        exr.write_exr(a.exr, exr.channels_of(res.image, res.guide_albedo, res.guide_normal), compression=a.exr_compression)
     st = res.stats
     print(f"{a.out}: {sc.camera.width}x{sc.camera.height}, {a.samples} spp, {st['paths'] / max(st['render_ms'], 1e-6) / 1e3:.1f} M paths/s",
           file=sys.stderr)

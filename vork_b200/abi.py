@@ -127,7 +127,8 @@ class VkbServerStatus(C.Structure):
 class VkbSceneInfo(C.Structure):
     _fields_ = [("num_instances", C.c_uint64), ("num_triangles", C.c_uint64), ("scene_bytes", C.c_uint64),
                 ("tlas_rebuilds", C.c_uint64), ("tlas_refits", C.c_uint64), ("motion_bytes", C.c_uint64),
-                ("build_ms", C.c_float), ("reserved", C.c_uint32)]
+                ("build_ms", C.c_float), ("reserved", C.c_uint32), ("install_ms", C.c_float), ("blas_host_ms", C.c_float),
+                ("upload_ms", C.c_float), ("tlas_ms", C.c_float)]
 
 
 # Every symbol include/vkb.h declares, with its ctypes signature.

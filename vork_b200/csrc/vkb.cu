@@ -489,6 +489,7 @@ struct vkb_scene {
     // tree and owns only its instances and TLAS; a base counts its live forks.
     vkb_scene* base = nullptr;
     uint32_t forks = 0;
+    float install_ms = 0.f, blas_host_ms = 0.f, upload_ms = 0.f, tlas_ms = 0.f;   // install cost
 };
 
 namespace {
@@ -1144,6 +1145,8 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
     *out = nullptr;
     vkb_scene* s = new vkb_scene();
     s->ctx = ctx;
+    const auto t_start = std::chrono::steady_clock::now();
+    double blas_host = 0.0;
     vkb_status st = guarded([&] {
         validate_desc(d);
         VKB_CUDA(cudaSetDevice(ctx->device));
@@ -1189,6 +1192,7 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         for (auto& mi : s->mesh_info) max_tris = std::max(max_tris, mi.num_triangles);
         s->tri_lo.alloc(std::max(1u, max_tris)); s->tri_hi.alloc(std::max(1u, max_tris));
         VKB_CUDA(cudaEventRecord(s->ev0, str));
+        const auto t_blas = std::chrono::steady_clock::now();
         std::vector<Bvh4Node> all_nodes;
         std::vector<float4> all_tris(std::max<size_t>(1, size_t(nt) * 3)), all_nrm(std::max<size_t>(1, size_t(nt) * 3));
         for (uint32_t m = 0; m < d->num_meshes; ++m) {
@@ -1228,6 +1232,7 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
             }
         }
         if (all_nodes.empty()) all_nodes.emplace_back();
+        blas_host = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_blas).count();
         s->blas4.alloc(all_nodes.size());
         VKB_CUDA(cudaMemcpyAsync(s->blas4.p, all_nodes.data(), all_nodes.size() * sizeof(Bvh4Node), cudaMemcpyHostToDevice, str));
         VKB_CUDA(cudaMemcpyAsync(s->blas_tris.p, all_tris.data(), all_tris.size() * sizeof(float4), cudaMemcpyHostToDevice, str));
@@ -1264,7 +1269,11 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         float blas_ms = 0.f;
         VKB_CUDA(cudaEventElapsedTime(&blas_ms, s->ev0, s->ev1));
         build_tlas(s);
+        s->tlas_ms = s->build_ms;
         s->build_ms += blas_ms;
+        s->install_ms = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
+        s->blas_host_ms = float(blas_host);
+        s->upload_ms = std::max(0.f, s->install_ms - s->blas_host_ms - s->tlas_ms);
     });
     if (st != VKB_OK) { vkb_scene_destroy(s); return st; }
     *out = s;
@@ -1277,6 +1286,7 @@ vkb_status vkb_scene_fork(vkb_scene* b, vkb_scene** out) {
     *out = nullptr;
     vkb_scene* s = new vkb_scene();
     s->ctx = b->ctx;
+    const auto t_start = std::chrono::steady_clock::now();
     vkb_status st = guarded([&] {
         VKB_CUDA(cudaSetDevice(b->ctx->device));
         cudaStream_t str = b->ctx->stream;
@@ -1308,6 +1318,9 @@ vkb_status vkb_scene_fork(vkb_scene* b, vkb_scene** out) {
         s->tlas_leaves.alloc(std::max(1u, n));
         s->tlas_codes.alloc(std::max(1u, n));
         build_tlas(s);
+        s->tlas_ms = s->build_ms;
+        s->install_ms = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
+        s->upload_ms = std::max(0.f, s->install_ms - s->tlas_ms);
     });
     if (st != VKB_OK) { vkb_scene_destroy(s); return st; }
     *out = s;
@@ -1531,6 +1544,7 @@ vkb_status vkb_scene_info(vkb_scene* s, vkb_scene_info_t* out) {
     dev += s->tlas_nodes.n * sizeof(BvhNode) + s->tlas4.n * sizeof(Bvh4Node) + s->tlas_odd.n + s->tlas_leaves.n * sizeof(TlasLeaf) + (s->o2w.n + s->w2o.n) * sizeof(float4);
     out->scene_bytes = dev;
     out->build_ms = s->build_ms;
+    out->install_ms = s->install_ms; out->blas_host_ms = s->blas_host_ms; out->upload_ms = s->upload_ms; out->tlas_ms = s->tlas_ms;
     return VKB_OK;
 }
 
