@@ -420,6 +420,24 @@ def cache_block(r, s, sc, frames, warmup: int, steps: int, errors: bool = True, 
         conv = k.render(Profile.reference_transport(depth, 256, seed=3)).image[..., :3]
         out["error_vs_plain_ref"] = {"ref_spp": ref_spp, "cached_16spp": _errors(last_cached, ref, h16),
                                      "plain_16spp": _errors(last_plain, ref, h16), "cached_256spp": _errors(conv, ref, h16)}
+        # Time to image at equal error: the fewest samples per pixel whose 16x16-block
+        # relative RMSE against the reference is <= 1%, and the device time it takes (the
+        # cached side adds this frame's training round).
+        tti = {}
+        for name, fn in (("plain", lambda spp: s.render(Profile.reference_transport(depth, spp, seed=5))),
+                         ("cached", lambda spp: k.render(Profile.reference_transport(depth, spp, seed=5)))):
+            row = None
+            for spp in (8, 12, 16, 24, 32, 48, 64, 96, 128):
+                res = fn(spp)
+                e = _errors(res.image[..., :3], ref, h16)
+                if e["rel_rmse_16x16_blocks"] <= 0.01:
+                    ms = res.stats["render_ms"] + (out["per_frame_ms"]["train"] if name == "cached" else 0.0)
+                    row = {"spp": spp, "ms": ms, **e}
+                    break
+            tti[name] = row
+        if tti["plain"] and tti["cached"]:
+            tti["speedup"] = tti["plain"]["ms"] / tti["cached"]["ms"]
+        out["time_to_1pct_block_rmse"] = tti
         # FP64 oracle on the 64x64 centre crop of the last frame (plain path tracing, 64 spp).
         try:
             import dataclasses

@@ -744,7 +744,7 @@ void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counte
         tot.trace_launches++;
         if (!BATCH && b == 0u && p.guide) { k_guides<<<sms * 8, 256, 0, st>>>(p); tot.launches += 1; }
         k_reset_queues<<<1, 1, 0, st>>>(p.counters, cur ^ 1);
-        k_shade<BATCH><<<sgrid, 512, 0, st>>>(p, cur);
+        k_shade<BATCH><<<sgrid, SHADE_BLOCK, 0, st>>>(p, cur);
         if (counted) k_trace_shadow<true, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
         else k_trace_shadow<false, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
     }

@@ -851,8 +851,15 @@ __device__ __noinline__ void cache_append(const PathParams& p, float3 world, flo
 // (a plain by-value parameter that is referenced gets copied to a 736-byte local frame
 // per thread); one block of 512 per SM (128 registers, a small spill) measured faster
 // than 3 blocks of 128 at 158 registers, 4 blocks of 128 and 2 blocks of 256.
+#ifndef VKB_SHADE_BLOCK
+#define VKB_SHADE_BLOCK 512
+#endif
+#ifndef VKB_SHADE_MIN_BLOCKS
+#define VKB_SHADE_MIN_BLOCKS 1
+#endif
+constexpr int SHADE_BLOCK = VKB_SHADE_BLOCK;
 template <bool BATCH>
-__global__ void __launch_bounds__(512, 1) k_shade(const __grid_constant__ PathParams p, int cur) {
+__global__ void __launch_bounds__(VKB_SHADE_BLOCK, VKB_SHADE_MIN_BLOCKS) k_shade(const __grid_constant__ PathParams p, int cur) {
     const int nxt = cur ^ 1;
     uint32_t n = p.counters[cur];
     uint32_t loop_end = (n + blockDim.x - 1) / blockDim.x * blockDim.x;  // whole warps stay in the loop for ballots
