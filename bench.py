@@ -354,11 +354,11 @@ def _errors(img, ref, h16):
             "rel_rmse_16x16_blocks": float(np.sqrt(np.mean((blocks(img) - br) ** 2)) / br.mean())}
 
 
-def cache_block(r, s, sc, frames, warmup: int, steps: int, errors: bool = True, ref_spp: int = 1024) -> dict:
+def cache_block(r, s, sc, frames, warmup: int, steps: int, errors: bool = True, ref_spp: int = 1024, pretrain: int = 16) -> dict:
     """Learned radiance cache on the large scene, 16 spp, depth 8: per frame the TLAS is
     rebuilt, the cache takes one online training round (2^16 records, 4 Adam steps) and
     renders through it (paths stop at vertex 2); against plain 16-spp renders of the same
-    frames.  Error of both against the plain tracer at `ref_spp` of the last frame, and
+    frames, after `pretrain` untimed training rounds (earlier frames of the sequence).  Error of both against the plain tracer at `ref_spp` of the last frame, and
     of the 64x64 centre crop against the FP64 oracle."""
     import torch
     from vork_b200 import Profile, RadianceCache, abi
@@ -374,6 +374,11 @@ def cache_block(r, s, sc, frames, warmup: int, steps: int, errors: bool = True, 
     cached_ms, plain_ms, train_ms, build_ms, cache_ms, queries = [], [], [], [], 0.0, 0
     train_parts = {"paths_ms": 0.0, "steps_ms": 0.0, "host_ms": 0.0}
     rays_cached = rays_plain = 0
+    # An animated sequence trains the cache every frame; before the measured frames it has
+    # seen `pretrain` rounds (untimed), as it would have after that many earlier frames.
+    s.update_instances_device(dev_frames[0].data_ptr(), n_inst, 1)
+    for i in range(pretrain):
+        k.train(Profile.reference_transport(depth, 1, seed=500 + i))
     with ClockSampler(r.device) as clocks:
         for i in range(warmup + steps):
             s.update_instances_device(dev_frames[i].data_ptr(), n_inst, 1)

@@ -497,6 +497,17 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
     base = __shfl_sync(mask, base, leader);
     return base + __popc(mask & ((1u << lane) - 1u));
 }
+// Queue append by the threads of a warp that reach it together (one atomic per group).
+__device__ __forceinline__ uint32_t group_append(uint32_t* counter) {
+    namespace cg = cooperative_groups;
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(counter, g.size());
+    return g.shfl(base, 0) + g.thread_rank();
+}
+#ifndef VKB_SHADE_EARLY_APPEND
+#define VKB_SHADE_EARLY_APPEND 0
+#endif
 // The job owning a slot (BATCH) or job 0.
 template <bool BATCH>
 __device__ __forceinline__ uint32_t job_of_slot(const PathParams& p, uint32_t slot) { return BATCH ? __ldg(&p.slot_job[slot]) : 0u; }
@@ -975,6 +986,13 @@ __global__ void __launch_bounds__(VKB_SHADE_BLOCK, VKB_SHADE_MIN_BLOCKS) k_shade
                         sh_d = make_float4(da.x, da.y, da.z, __uint_as_float(slot));
                         sh_c = make_float4(ca.x, ca.y, ca.z, __uint_as_float(flags));
                         if (!trace_a) sh_o = make_float4(0.f, 0.f, 0.f, 0.f);
+#if VKB_SHADE_EARLY_APPEND
+                        {
+                            const uint32_t si = group_append(&p.counters[2]);
+                            p.sa_o[si] = sh_o; p.sa_d[si] = sh_d; p.sa_c[si] = sh_c;
+                            push_shadow = false;
+                        }
+#endif
                         if (has_b) {
                             p.sb_c[slot] = make_float4(cb.x, cb.y, cb.z, 0.f);
                             if (trace_b) { p.sb_o[slot] = make_float4(ob.x, ob.y, ob.z, lb); p.sb_d[slot] = make_float4(db.x, db.y, db.z, 0.f); }
@@ -1007,6 +1025,13 @@ __global__ void __launch_bounds__(VKB_SHADE_BLOCK, VKB_SHADE_MIN_BLOCKS) k_shade
                         new_o = make_float4(o.x, o.y, o.z, FP32_MAX);
                         new_d = make_float4(smp.dir.x, smp.dir.y, smp.dir.z, __uint_as_float(slot));
                         push_ray = true;
+#if VKB_SHADE_EARLY_APPEND
+                        {
+                            const uint32_t ri = group_append(&p.counters[nxt]);
+                            p.ray_o[nxt][ri] = new_o; p.ray_d[nxt][ri] = new_d;
+                            push_ray = false;
+                        }
+#endif
                         meta = (meta & META_NONFINITE) | ((bounce + 1u) & 0xffu) | ((diffuse & 0xffu) << 8) | ((glossy & 0xffu) << 16) | ((event & 0x3fu) << 24);
                     }
                 }
