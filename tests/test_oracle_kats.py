@@ -207,3 +207,27 @@ def test_metal_sampling_preserves_energy_bound(oracle):
             ws.append(w[0] if ev else 0.0)
         assert np.mean(ws) <= 1.02, (rough, np.mean(ws))
         assert np.mean(ws) >= 0.85, (rough, np.mean(ws))
+
+
+def test_guide_planes_of_the_oracle(oracle):
+    # path.slang:1549-1571 restated: a white-world response of a specular-free Lambert
+    # plane is its base colour, its normal the plane's; misses add zero coverage.
+    import numpy as np
+    from vork_b200 import Profile, scene as S
+    g = S.grid((200.0, 200.0), (2, 2))
+    m = S.material((0.8, 0.6, 0.4), 0.5, 0.0)
+    m.specular_weight = 0.0
+    cam = S.look_at((0, 5, 0.001), (0, 0, 0), width=8, height=8, fov_y_degrees=30)
+    sc = S.Scene([g], S.rows_from(1.0, (0, 0, 0))[None], np.zeros(1, np.uint32), np.zeros(1, np.uint32), [m], [], cam,
+                 S.environment((1.0, 0.75, 0.5)))
+    o = oracle.OracleScene(sc)
+    _, _, gd = o.render(Profile.reference_transport(4, 4).c(), fp64=True, guides=True)
+    assert np.allclose(gd[:, :, 0].reshape(-1, 4), [0.8, 0.6, 0.4, 1.0], atol=1e-12)
+    assert np.allclose(gd[:, :, 1].reshape(-1, 4), [0.0, 1.0, 0.0, 0.0], atol=1e-12)
+    # A general scene: albedo in [0, 1], coverage the fraction of hits, unit-or-shorter normals.
+    sc2 = S.spheres_scene(width=48, height=48)
+    _, _, g2 = oracle.OracleScene(sc2, fp64=False).render(Profile.reference_transport(4, 4).c(), fp64=False, guides=True)
+    a, n = g2[:, :, 0], g2[:, :, 1]
+    assert np.all((a[..., :3] >= 0) & (a[..., :3] <= 1)) and np.all((a[..., 3] >= 0) & (a[..., 3] <= 1))
+    assert 0.3 < a[..., 3].mean() < 1.0
+    assert np.all(np.linalg.norm(n[..., :3], axis=-1) <= 1 + 1e-6) and np.all(n[..., 3] == 0)
