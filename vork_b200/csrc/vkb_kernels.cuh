@@ -505,8 +505,12 @@ __device__ __forceinline__ uint32_t group_append(uint32_t* counter) {
     if (g.thread_rank() == 0) base = atomicAdd(counter, g.size());
     return g.shfl(base, 0) + g.thread_rank();
 }
+// Shade appends a new extension ray or shadow entry where it makes it (the threads of a
+// warp that get there together share one atomic) instead of carrying five float4s to a
+// warp-wide append at the end of the loop body: 128 registers with 12/16 B of spill
+// instead of 108/156 B (measured: 618 vs 623 ms per large frame).
 #ifndef VKB_SHADE_EARLY_APPEND
-#define VKB_SHADE_EARLY_APPEND 0
+#define VKB_SHADE_EARLY_APPEND 1
 #endif
 // The job owning a slot (BATCH) or job 0.
 template <bool BATCH>
