@@ -11,7 +11,7 @@ ROOT = Path(__file__).resolve().parent
 CSRC = ROOT / "csrc"
 OUT = ROOT / "_lib" / "libvkb.so"
 SOURCES = [CSRC / "vkb.cu"]
-HEADERS = sorted(CSRC.glob("*.cuh")) + [ROOT.parent / "include" / "vkb.h"]
+HEADERS = sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [ROOT.parent / "include" / "vkb.h"]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared", "-diag-suppress", "177"]

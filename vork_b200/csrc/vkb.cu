@@ -21,10 +21,13 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <thread>
+#include <future>
 #include <string>
 #include <vector>
 
 #include "vkb_kernels.cuh"
+#include "vkb_sah.h"
 #include "vkb_nrc.cuh"
 #include "vkb_display.cuh"
 
@@ -157,110 +160,6 @@ std::vector<LightTreeNode> light_tree(const vkb_light* lights, uint32_t n) {
     if (n) b.go(ids.data(), n, 0xffffffffu);
     return nodes;
 }
-
-// Binned-SAH BLAS over one mesh's triangles (object space), built once at install:
-// BVH2 nodes in the device layout (both child boxes per node), leaves of up to
-// BLAS_LEAF_MAX triangles referenced as ~((first << 2) | (count - 1)), triangles
-// reordered into leaf order.  The per-frame TLAS keeps the GPU LBVH.
-constexpr uint32_t BLAS_LEAF_MAX = VKB_BLAS_LEAF_MAX;
-struct SahBlas {
-    std::vector<BvhNode> nodes;
-    std::vector<uint32_t> order;  // leaf-ordered original triangle ids
-    const float* lo; const float* hi; const float* c;
-    std::vector<uint32_t> ids;
-    struct Box { float lo[3], hi[3]; };
-    static float area(const Box& b) {
-        float x = std::max(b.hi[0] - b.lo[0], 0.f), y = std::max(b.hi[1] - b.lo[1], 0.f), z = std::max(b.hi[2] - b.lo[2], 0.f);
-        return x * y + y * z + z * x;
-    }
-    static void grow(Box& a, const float* l, const float* h) { for (int k = 0; k < 3; ++k) { a.lo[k] = std::min(a.lo[k], l[k]); a.hi[k] = std::max(a.hi[k], h[k]); } }
-    static Box empty() { Box b; for (int k = 0; k < 3; ++k) { b.lo[k] = INFINITY; b.hi[k] = -INFINITY; } return b; }
-    static void set_child(BvhNode& n, int side, const Box& b, int ref) {
-        if (side == 0) { n.a = make_float4(b.lo[0], b.hi[0], b.lo[1], b.hi[1]); n.c.x = b.lo[2]; n.c.y = b.hi[2]; n.d.x = ref; }
-        else { n.b = make_float4(b.lo[0], b.hi[0], b.lo[1], b.hi[1]); n.c.z = b.lo[2]; n.c.w = b.hi[2]; n.d.y = ref; }
-    }
-    // Returns the reference of the subtree over ids[first, first+count) and its box.
-    int build(uint32_t first, uint32_t count, Box& out, int depth) {
-        Box b = empty(), cb = empty();
-        for (uint32_t i = first; i < first + count; ++i) { grow(b, lo + 3 * ids[i], hi + 3 * ids[i]); grow(cb, c + 3 * ids[i], c + 3 * ids[i]); }
-        out = b;
-        const int BINS = 16;
-        float best = INFINITY; int best_axis = -1, best_bin = 0;
-        if (count > 1 && depth < 60) {
-            for (int axis = 0; axis < 3; ++axis) {
-                float l = cb.lo[axis], h = cb.hi[axis];
-                if (!(h > l)) continue;
-                Box bb[BINS]; uint32_t cnt[BINS] = {};
-                for (int k = 0; k < BINS; ++k) bb[k] = empty();
-                float sc = float(BINS) / (h - l);
-                for (uint32_t i = first; i < first + count; ++i) {
-                    int k = std::min(BINS - 1, int((c[3 * ids[i] + axis] - l) * sc));
-                    grow(bb[k], lo + 3 * ids[i], hi + 3 * ids[i]); cnt[k]++;
-                }
-                float la[BINS]; uint32_t lc[BINS];
-                Box acc = empty(); uint32_t ac = 0;
-                for (int k = 0; k < BINS; ++k) { grow(acc, bb[k].lo, bb[k].hi); ac += cnt[k]; la[k] = area(acc); lc[k] = ac; }
-                acc = empty(); ac = 0;
-                for (int k = BINS - 1; k > 0; --k) {
-                    grow(acc, bb[k].lo, bb[k].hi); ac += cnt[k];
-                    if (lc[k - 1] == 0 || ac == 0) continue;
-                    float cost = la[k - 1] * float(lc[k - 1]) + area(acc) * float(ac);
-                    if (cost < best) { best = cost; best_axis = axis; best_bin = k; }
-                }
-            }
-        }
-        float parent = area(b);
-        // SAH with traversal cost 1 and triangle cost 1, relative to the parent's area.
-        bool leaf = count == 1 || (count <= BLAS_LEAF_MAX && (best_axis < 0 || float(count) * parent <= parent + best));
-        if (!leaf && best_axis < 0 && count > BLAS_LEAF_MAX) best_axis = -2;  // degenerate centroids: median split
-        if (leaf) {
-            uint32_t f = uint32_t(order.size());
-            for (uint32_t i = first; i < first + count; ++i) order.push_back(ids[i]);
-            return ~int((f << 2) | (count - 1));
-        }
-        uint32_t mid;
-        if (best_axis >= 0) {
-            float l = cb.lo[best_axis], sc = float(BINS) / (cb.hi[best_axis] - l);
-            auto it = std::partition(ids.begin() + first, ids.begin() + first + count, [&](uint32_t p) {
-                return std::min(BINS - 1, int((c[3 * p + best_axis] - l) * sc)) < best_bin; });
-            mid = uint32_t(it - ids.begin());
-            if (mid == first || mid == first + count) mid = first + count / 2;
-        } else {
-            mid = first + count / 2;
-        }
-        int index = int(nodes.size());
-        nodes.push_back(BvhNode{});
-        Box lb, rb;
-        int lref = build(first, mid - first, lb, depth + 1);
-        int rref = build(mid, first + count - mid, rb, depth + 1);
-        set_child(nodes[index], 0, lb, lref);
-        set_child(nodes[index], 1, rb, rref);
-        nodes[index].d.z = nodes[index].d.w = 0;
-        return index;
-    }
-    void run(uint32_t n, const float* l, const float* h, const float* cent) {
-        lo = l; hi = h; c = cent;
-        ids.resize(n);
-        for (uint32_t i = 0; i < n; ++i) ids[i] = i;
-        nodes.clear(); order.clear();
-        nodes.push_back(BvhNode{});  // root
-        Box b = empty(), cb = empty();
-        for (uint32_t i = 0; i < n; ++i) grow(b, l + 3 * i, h + 3 * i);
-        (void)cb;
-        if (n <= BLAS_LEAF_MAX) {
-            order.assign(ids.begin(), ids.end());
-            set_child(nodes[0], 0, b, ~int(n - 1));
-            set_child(nodes[0], 1, empty(), ~int(n - 1));
-            nodes[0].d.z = nodes[0].d.w = 0;
-            return;
-        }
-        // The root is node 0: build its two halves under it.
-        Box rb;
-        nodes.pop_back();
-        int r = build(0, n, rb, 0);
-        (void)r;  // r == 0: the root node was allocated first
-    }
-};
 
 // Bounding sphere of a mesh about its box centre (c = (lo + hi) / 2 in fp32): the radius
 // is the largest vertex distance, in f64, rounded up to fp32; radius -1 for no vertices.
@@ -1208,10 +1107,13 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
                     lo[3 * t + a] = std::min(v0, std::min(v1, v2)); hi[3 * t + a] = std::max(v0, std::max(v1, v2));
                     cen[3 * t + a] = 0.5f * (lo[3 * t + a] + hi[3 * t + a]);
                 }
-            SahBlas sah;
+            vkb_host::SahBlas sah;
             sah.run(n, lo.data(), hi.data(), cen.data());
             if (sah.nodes.size() > std::max(1u, n > 1 ? n - 1 : 1u)) throw ArgError{"BLAS node count above its bound"};
-            std::vector<Bvh4Node> wide = collapse_blas(sah.nodes);
+            static_assert(sizeof(vkb_host::SahNode) == sizeof(BvhNode), "host SAH nodes have the device layout");
+            std::vector<BvhNode> bin(sah.nodes.size());
+            std::memcpy(bin.data(), sah.nodes.data(), bin.size() * sizeof(BvhNode));
+            std::vector<Bvh4Node> wide = collapse_blas(bin);
             if (all_nodes.size() + wide.size() > size_t(INT32_MAX)) throw ArgError{"BLAS node count above its bound"};
             all_nodes.insert(all_nodes.end(), wide.begin(), wide.end());
             for (uint32_t k = 0; k < n; ++k) {
