@@ -317,14 +317,15 @@ def serve_block(r, requests: int, rates, schedule: str = "srpt", fifo: bool = Tr
     from vork_b200.serving import Server, fifo_load, poisson_load, request_mix
     t_block = time.perf_counter()
     scenes, animations, names, owned = serve_scenes(r, flock_inst, flock)
-    flags = {"srpt": 0, "fair": 4, "packed": 8}[schedule]
+    flags = {"srpt": 0, "aged": 0, "fair": 4, "packed": 8}[schedule]
+    aging = 2e8 if schedule == "aged" else 0.0   # paths per second waited: about the device's rate on these scenes
     out = []
     for i, rate in enumerate(rates):
         reqs = request_mix(requests, len(scenes), seed=i, frames=24, spp_range=(8, 128), bounces=8,
                            pixels_range=(256 * 256, 1920 * 1080))
         row = {"rate": rate}
         with ClockSampler(r.device) as clocks:
-            with Server(r, memory_budget_bytes=160 << 30, max_jobs=256, flags=flags) as srv:
+            with Server(r, memory_budget_bytes=160 << 30, max_jobs=256, flags=flags, aging_paths_per_s=aging) as srv:
                 row["continuous"] = poisson_load(srv, scenes, copy.deepcopy(reqs), rate=rate, seed=i, timeout_s=timeout_s,
                                                  animations=animations)
         row["continuous"]["clocks"] = clocks.summary()
@@ -569,7 +570,7 @@ def main():
     ap.add_argument("--tlas", choices=["lbvh", "ploc"], default="lbvh", help="TLAS builder of the frame scene")
     ap.add_argument("--no-error", action="store_true", help="cache: skip the reference renders (timing/profiling runs)")
     ap.add_argument("--res", default="1920x1080", help="cache: frame resolution (smaller for profiling captures)")
-    ap.add_argument("--schedule", default="srpt", choices=["srpt", "fair", "packed"], help="serve: wave schedule")
+    ap.add_argument("--schedule", default="srpt", choices=["srpt", "aged", "fair", "packed"], help="serve: wave schedule")
     ap.add_argument("--dry-run", action="store_true", help="multi-rank host logic on CPU (gloo), no GPU work")
     ap.add_argument("--no-blocks", action="store_true", help="large: skip the batch/cache/serve blocks after the frame timing")
     ap.add_argument("--block-requests", type=int, default=40, help="large: requests of the serve block")

@@ -286,6 +286,9 @@ typedef struct vkb_server_config {
     uint32_t max_jobs;             /* admitted requests at once (job-table entries) */
     uint32_t flags;                /* VKB_PROFILE_* switches for every wave */
     uint64_t wave_capacity;        /* path slots per wave (0: the context's autotuned value) */
+    double aging_paths_per_s;      /* shortest-remaining-work waves: a request's remaining paths count as
+                                      reduced by this rate times the seconds since its admission, so a
+                                      large request is not overtaken forever (0: pure shortest first) */
 } vkb_server_config;
 typedef struct vkb_server_status {
     uint32_t queued, running, finished;   /* finished: requests completed by this step */

@@ -116,7 +116,8 @@ class VkbTuneResult(C.Structure):
 
 
 class VkbServerConfig(C.Structure):
-    _fields_ = [("memory_budget_bytes", C.c_uint64), ("max_jobs", C.c_uint32), ("flags", C.c_uint32), ("wave_capacity", C.c_uint64)]
+    _fields_ = [("memory_budget_bytes", C.c_uint64), ("max_jobs", C.c_uint32), ("flags", C.c_uint32), ("wave_capacity", C.c_uint64),
+                ("aging_paths_per_s", C.c_double)]
 
 
 class VkbServerStatus(C.Structure):

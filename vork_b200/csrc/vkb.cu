@@ -531,6 +531,7 @@ void validate_camera(const vkb_camera& cam) {
 
 
 // ================================================================ wave engine
+double host_seconds() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
 // One job of a render call: a scene, its profile, and where its mean image goes.
 struct EngineJob {
     vkb_scene* s = nullptr;
@@ -547,6 +548,7 @@ struct EngineJob {
     float4* guide_albedo = nullptr;
     float4* guide_normal = nullptr;
     uint32_t npix = 0, count = 0, done = 0, pixel_base = 0;
+    double admitted_s = 0.0;        // serving: host clock at admission (aging of the shortest-first order)
 };
 struct WaveTotals {
     uint32_t launches = 0, trace_launches = 0, cache_launches = 0;
@@ -687,6 +689,7 @@ struct WaveEngine {
     // BVHs stay in L2 -- batch throughput), or shortest remaining work first (the jobs
     // with the fewest paths left take their samples first -- serving latency).
     bool packed = false, srpt = false;
+    double aging_rate = 0.0;              // shortest-first aging, paths per second waited
     const CacheLaunch* cache = nullptr;   // radiance-cache hooks (single-job renders)
     ~WaveEngine() { for (auto& g : captured) cudaGraphExecDestroy(g.exec); }
     WaveEngine(vkb_ctx* ctx, const WaveBuffers& wb, size_t cap, uint32_t fl, bool use_graphs) : c(ctx), w(wb), capacity(cap), flags(fl), graphs(use_graphs) {
@@ -721,11 +724,16 @@ struct WaveEngine {
         if (srpt) {
             // Shortest remaining work first: every job, in order of the paths it has left
             // (admission order on ties), takes as many samples as still fit.
+            // With aging, the paths left count as reduced by aging_rate x seconds waited.
             std::vector<uint32_t> order;
-            for (uint32_t k = 0; k < njobs; ++k) if (!finished(k)) order.push_back(k);
-            std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-                return uint64_t(jobs[a].count - jobs[a].done) * jobs[a].npix < uint64_t(jobs[b].count - jobs[b].done) * jobs[b].npix;
-            });
+            std::vector<double> key(njobs, 0.0);
+            const double now = aging_rate > 0.0 ? host_seconds() : 0.0;
+            for (uint32_t k = 0; k < njobs; ++k) {
+                if (finished(k)) continue;
+                order.push_back(k);
+                key[k] = double(jobs[k].count - jobs[k].done) * double(jobs[k].npix) - aging_rate * (now - jobs[k].admitted_s);
+            }
+            std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
             for (uint32_t k : order) {
                 EngineJob& e = jobs[k];
                 uint32_t n = uint32_t(std::min<size_t>(e.count - e.done, left / e.npix));
@@ -1695,12 +1703,23 @@ struct vkb_server {
     Wavefront wave;                                   // the server's own queues (renders on the context keep theirs)
     std::unique_ptr<WaveEngine> eng;
     struct Pending { uint64_t id; vkb_scene* s; vkb_profile pf; float* host_out; bool own_camera; vkb_camera cam; };
-    struct Live { uint64_t id; float* host_out; DBuf<float4> accum, out; uint64_t bytes; };
+    // A request's device accumulator and mean image, taken from (and returned to) a pool
+    // keyed by pixel capacity, so steady serving calls neither cudaMalloc nor cudaFree.
+    struct Buffers { float4* accum = nullptr; float4* out = nullptr; size_t npix = 0; };
+    struct Live { uint64_t id; float* host_out; Buffers buf; uint32_t npix; uint64_t bytes; };
     std::deque<Pending> queue;
     std::map<uint64_t, std::unique_ptr<Live>> live;   // admitted, keyed by id
     std::map<uint64_t, int> state;                    // 0 queued, 1 running, 2 done
-    uint64_t next_id = 1, used_bytes = 0, peak_bytes = 0, wave_bytes = 0;
+    uint64_t next_id = 1, used_bytes = 0, peak_bytes = 0, wave_bytes = 0, pool_bytes = 0;
     std::map<vkb_scene*, uint64_t> resident;           // scene -> device bytes
+    std::multimap<size_t, Buffers> pool;               // idle request buffers by pixel capacity
+    // Waves in flight: the event after a wave and the copies of its finished requests' images,
+    // with those requests' ids.  A step enqueues its wave without waiting for the previous
+    // one, so the device always has the next wave queued while the host admits and reaps.
+    struct Completion { cudaEvent_t ev; std::vector<uint64_t> ids; };
+    std::deque<Completion> inflight;
+    std::vector<cudaEvent_t> spare_events;
+    cudaStream_t copy_stream = nullptr;               // device->host copies of finished images
 };
 
 namespace {
@@ -1716,6 +1735,61 @@ uint64_t resident_bytes(const vkb_server* v) {
     uint64_t b = 0;
     for (auto& kv : v->resident) b += kv.second;
     return b;
+}
+constexpr uint64_t SERVER_BYTES_PER_PIXEL = 2 * sizeof(float4);   // accumulator + mean image
+// Buffers for npix pixels: the smallest idle ones that hold them (and are not more than
+// twice as large), else new ones.
+vkb_server::Buffers take_buffers(vkb_server* v, size_t npix) {
+    auto it = v->pool.lower_bound(npix);
+    if (it != v->pool.end() && it->first <= 2 * npix) {
+        vkb_server::Buffers b = it->second;
+        v->pool.erase(it);
+        v->pool_bytes -= b.npix * SERVER_BYTES_PER_PIXEL;
+        return b;
+    }
+    vkb_server::Buffers b;
+    b.npix = npix;
+    VKB_CUDA(cudaMalloc(&b.accum, npix * sizeof(float4)));
+    cudaError_t e = cudaMalloc(&b.out, npix * sizeof(float4));
+    if (e != cudaSuccess) { cudaFree(b.accum); throw CudaError{e, "cudaMalloc(request image)"}; }
+    return b;
+}
+void free_pool(vkb_server* v) {
+    for (auto& kv : v->pool) { cudaFree(kv.second.accum); cudaFree(kv.second.out); }
+    v->pool.clear();
+    v->pool_bytes = 0;
+}
+// Finished requests of the waves whose events have completed (all of them with wait):
+// copy each image to its host buffer on the copy stream (the next wave keeps running),
+// return the buffers to the pool and mark the request done.
+uint32_t reap(vkb_server* v, bool wait_all, bool wait_oldest) {
+    uint32_t done = 0;
+    while (!v->inflight.empty()) {
+        vkb_server::Completion& cpl = v->inflight.front();
+        if (wait_all || (wait_oldest && done == 0)) VKB_CUDA(cudaEventSynchronize(cpl.ev));
+        else {
+            cudaError_t q = cudaEventQuery(cpl.ev);
+            if (q == cudaErrorNotReady) break;
+            if (q != cudaSuccess) throw CudaError{q, "cudaEventQuery(wave)"};
+        }
+        for (uint64_t id : cpl.ids) {
+            vkb_server::Live& l = *v->live[id];
+            VKB_CUDA(cudaMemcpyAsync(l.host_out, l.buf.out, size_t(l.npix) * sizeof(float4), cudaMemcpyDeviceToHost, v->copy_stream));
+        }
+        VKB_CUDA(cudaStreamSynchronize(v->copy_stream));
+        for (uint64_t id : cpl.ids) {
+            vkb_server::Live& l = *v->live[id];
+            v->pool.emplace(l.buf.npix, l.buf);
+            v->pool_bytes += l.buf.npix * SERVER_BYTES_PER_PIXEL;
+            v->used_bytes -= l.bytes;
+            v->live.erase(id);
+            v->state[id] = 2;
+            ++done;
+        }
+        v->spare_events.push_back(cpl.ev);
+        v->inflight.pop_front();
+    }
+    return done;
 }
 }  // namespace
 
@@ -1735,9 +1809,12 @@ vkb_status vkb_server_create(vkb_ctx* c, const vkb_server_config* cfg, vkb_serve
         v->wave_bytes = uint64_t(v->capacity) * 220u + uint64_t(v->max_jobs) * sizeof(Job);
         if (v->budget && v->wave_bytes >= v->budget) throw ArgError{"memory budget below the wavefront's own footprint"};
         v->wave.reserve(v->capacity, v->max_jobs);
+        VKB_CUDA(cudaStreamCreateWithFlags(&v->copy_stream, cudaStreamNonBlocking));
         v->eng = std::make_unique<WaveEngine>(c, v->wave.view(), v->capacity, cfg->flags, true);
         v->eng->packed = (cfg->flags & VKB_BATCH_PACKED) != 0;
         v->eng->srpt = !v->eng->packed && (cfg->flags & VKB_BATCH_FAIR) == 0;
+        if (!(cfg->aging_paths_per_s >= 0.0)) throw ArgError{"aging_paths_per_s must be non-negative"};
+        v->eng->aging_rate = cfg->aging_paths_per_s;
     });
     if (st != VKB_OK) return st;
     *out = v.release();
@@ -1772,65 +1849,82 @@ vkb_status vkb_server_step(vkb_server* v, vkb_server_status* status) {
         vkb_ctx* c = v->c;
         VKB_CUDA(cudaSetDevice(c->device));
         WaveEngine& eng = *v->eng;
+        uint32_t finished = reap(v, false, false);
         // Scenes held under the budget: those of the admitted requests (and a fork's base).
         v->resident.clear();
         for (const EngineJob& e : eng.jobs) {
             v->resident[e.s] = scene_bytes(e.s);
             if (e.s->base) v->resident[e.s->base] = scene_bytes(e.s->base);
         }
-        // Admit at the wave boundary.
+        // Admit at the wave boundary.  Budget: the wavefront, resident scenes, every live
+        // request's buffers and the idle pool (emptied first when a request needs the room).
         while (!v->queue.empty() && eng.jobs.size() < v->max_jobs) {
             auto& q = v->queue.front();
             uint64_t npix = uint64_t(q.cam.width) * q.cam.height;
-            uint64_t need = npix * 32u;
+            uint64_t need = npix * SERVER_BYTES_PER_PIXEL;
             uint64_t scene = v->resident.count(q.s) ? 0u : scene_bytes(q.s);
             if (q.s->base && !v->resident.count(q.s->base)) scene += scene_bytes(q.s->base);
-            if (v->budget && v->wave_bytes + resident_bytes(v) + scene + v->used_bytes + need > v->budget) break;
+            auto held = [&] { return v->wave_bytes + resident_bytes(v) + v->used_bytes + v->pool_bytes; };
+            auto fit = v->pool.lower_bound(npix);
+            uint64_t extra = (fit != v->pool.end() && fit->first <= 2 * npix) ? 0u : need;   // reused buffers add nothing
+            if (v->budget && held() + scene + extra > v->budget && v->pool_bytes) {
+                finished += reap(v, true, false);
+                free_pool(v);
+                extra = need;
+            }
+            if (v->budget && held() + scene + extra > v->budget) break;
             auto live = std::make_unique<vkb_server::Live>();
-            live->id = q.id; live->host_out = q.host_out; live->bytes = need;
-            live->accum.alloc(npix); live->out.alloc(npix);
+            live->id = q.id; live->host_out = q.host_out; live->npix = uint32_t(npix);
+            live->buf = take_buffers(v, npix);
+            live->bytes = live->buf.npix * SERVER_BYTES_PER_PIXEL;
             EngineJob e;
             e.s = q.s; e.pf = q.pf; e.npix = uint32_t(npix);
             e.own_camera = q.own_camera; e.camera = q.cam;
             e.count = q.pf.sample_count ? q.pf.sample_count : q.pf.samples - q.pf.first_sample;
-            e.accum = live->accum.p; e.out_dev = live->out.p;
+            e.accum = live->buf.accum; e.out_dev = live->buf.out;
+            e.admitted_s = host_seconds();
             eng.add(e);
             v->resident[q.s] = scene_bytes(q.s);
             if (q.s->base) v->resident[q.s->base] = scene_bytes(q.s->base);
-            v->used_bytes += need;
-            v->peak_bytes = std::max(v->peak_bytes, v->wave_bytes + resident_bytes(v) + v->used_bytes);
+            v->used_bytes += live->bytes;
+            v->peak_bytes = std::max(v->peak_bytes, held());
             v->state[q.id] = 1;
             v->live[q.id] = std::move(live);
             v->queue.pop_front();
         }
-        uint32_t finished = 0;
         if (!eng.jobs.empty()) {
             eng.step();
-            // Finished jobs: resolve, copy out, release.
-            std::vector<uint64_t> ids;
+            // Requests whose last samples are in this wave: resolve behind it; they are done
+            // once the wave's event has completed and their images are copied (reap).
+            vkb_server::Completion cpl;
             for (size_t k = 0; k < eng.jobs.size(); ++k) {
                 if (!eng.finished(k)) continue;
                 eng.resolve(k);
                 for (auto& kv : v->live)
-                    if (kv.second->out.p == eng.jobs[k].out_dev) {
-                        VKB_CUDA(cudaMemcpyAsync(kv.second->host_out, kv.second->out.p, size_t(eng.jobs[k].npix) * sizeof(float4), cudaMemcpyDeviceToHost, c->stream));
-                        ids.push_back(kv.first);
-                    }
+                    if (kv.second->buf.out == eng.jobs[k].out_dev) cpl.ids.push_back(kv.first);
             }
-            VKB_CUDA(cudaStreamSynchronize(c->stream));
             eng.compact();
-            for (uint64_t id : ids) {
-                v->used_bytes -= v->live[id]->bytes;
-                v->live.erase(id);
-                v->state[id] = 2;
-                ++finished;
+            if (v->spare_events.empty()) {
+                cudaEvent_t ev;
+                VKB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+                v->spare_events.push_back(ev);
             }
+            cpl.ev = v->spare_events.back();
+            v->spare_events.pop_back();
+            VKB_CUDA(cudaEventRecord(cpl.ev, c->stream));
+            v->inflight.push_back(std::move(cpl));
+            // At most two waves in flight: wait for the older one before returning.
+            if (v->inflight.size() > 2) finished += reap(v, false, true);
+        } else if (!v->inflight.empty()) {
+            finished += reap(v, false, true);             // nothing new to run: deliver the oldest
         }
         if (status) {
+            uint32_t completing = 0;
+            for (const auto& cp : v->inflight) completing += uint32_t(cp.ids.size());
             status->queued = uint32_t(v->queue.size());
-            status->running = uint32_t(eng.jobs.size());
+            status->running = uint32_t(eng.jobs.size()) + completing;
             status->finished = finished;
-            status->used_bytes = v->wave_bytes + resident_bytes(v) + v->used_bytes;
+            status->used_bytes = v->wave_bytes + resident_bytes(v) + v->used_bytes + v->pool_bytes;
             status->peak_bytes = v->peak_bytes;
         }
     });
@@ -1840,6 +1934,10 @@ vkb_status vkb_server_poll(vkb_server* v, uint64_t id, int* state) {
     if (!v || !state) return fail(VKB_INVALID_ARG, "null argument");
     auto it = v->state.find(id);
     if (it == v->state.end()) return fail(VKB_INVALID_ARG, "unknown request id");
+    if (it->second == 1) {
+        vkb_status st = guarded([&] { VKB_CUDA(cudaSetDevice(v->c->device)); reap(v, false, false); });
+        if (st != VKB_OK) return st;
+    }
     *state = it->second;
     return VKB_OK;
 }
@@ -1848,7 +1946,12 @@ vkb_status vkb_server_destroy(vkb_server* v) {
     if (!v) return VKB_OK;
     cudaSetDevice(v->c->device);
     cudaStreamSynchronize(v->c->stream);
+    for (auto& cp : v->inflight) cudaEventDestroy(cp.ev);
+    for (cudaEvent_t e : v->spare_events) cudaEventDestroy(e);
+    if (v->copy_stream) { cudaStreamSynchronize(v->copy_stream); cudaStreamDestroy(v->copy_stream); }
+    for (auto& kv : v->live) { cudaFree(kv.second->buf.accum); cudaFree(kv.second->buf.out); }
     v->live.clear();
+    free_pool(v);
     v->eng.reset();
     v->wave.release();
     delete v;

@@ -499,11 +499,11 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
 }
 // Queue append by the threads of a warp that reach it together (one atomic per group).
 __device__ __forceinline__ uint32_t group_append(uint32_t* counter) {
-    namespace cg = cooperative_groups;
-    cg::coalesced_group g = cg::coalesced_threads();
+    const uint32_t mask = __activemask(), lane = threadIdx.x & 31u, leader = __ffs(mask) - 1u;
     uint32_t base = 0;
-    if (g.thread_rank() == 0) base = atomicAdd(counter, g.size());
-    return g.shfl(base, 0) + g.thread_rank();
+    if (lane == leader) base = atomicAdd(counter, uint32_t(__popc(mask)));
+    base = __shfl_sync(mask, base, leader);
+    return base + uint32_t(__popc(mask & ((1u << lane) - 1u)));
 }
 // Shade appends a new extension ray or shadow entry where it makes it (the threads of a
 // warp that get there together share one atomic) instead of carrying five float4s to a

@@ -21,10 +21,12 @@ from . import Profile
 
 
 class Server:
-    def __init__(self, renderer, memory_budget_bytes: int = 160 << 30, max_jobs: int = 64, flags: int = 0, wave_capacity: int = 0):
+    def __init__(self, renderer, memory_budget_bytes: int = 160 << 30, max_jobs: int = 64, flags: int = 0, wave_capacity: int = 0,
+                 aging_paths_per_s: float = 0.0):
         self.r = renderer
         cfg = abi.VkbServerConfig()
         cfg.memory_budget_bytes, cfg.max_jobs, cfg.flags, cfg.wave_capacity = memory_budget_bytes, max_jobs, flags, wave_capacity
+        cfg.aging_paths_per_s = aging_paths_per_s
         h = C.c_void_p()
         abi.check(renderer.lib.vkb_server_create(renderer.h, C.byref(cfg), C.byref(h)))
         self.h = h
