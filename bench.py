@@ -574,7 +574,7 @@ def main():
     ap.add_argument("--dry-run", action="store_true", help="multi-rank host logic on CPU (gloo), no GPU work")
     ap.add_argument("--no-blocks", action="store_true", help="large: skip the batch/cache/serve blocks after the frame timing")
     ap.add_argument("--block-requests", type=int, default=40, help="large: requests of the serve block")
-    ap.add_argument("--block-rate", type=float, default=10.0, help="large: arrival rate of the serve block (req/s)")
+    ap.add_argument("--block-rate", type=float, default=2.0, help="large: arrival rate of the serve block (req/s)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
