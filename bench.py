@@ -9,8 +9,8 @@ image out, both copies inside the timed region.  Multi-GPU (torchrun): every ran
 renders its own frames (weak scaling, no collective on the data path).
 
 At one GPU the same line then carries compact blocks of the other configurations, each
-timed with its own clock record: `batch` (256 batched preview jobs vs sequential plain
-renders), `cache` (the learned radiance cache on the frame scene vs plain, with errors
+timed with its own clock record: `small` (the 256x256 configuration), `batch` (256
+batched preview jobs vs sequential plain renders), `cache` (the learned radiance cache on the frame scene vs plain, with errors
 against a 1024-spp plain render and the FP64 oracle) and `serve` (continuous batching
 vs the plain path served FIFO on one Poisson trace).  `--config batch|cache|serve` runs
 each at full size.
@@ -232,6 +232,41 @@ def clocks_ok(summary: dict) -> bool:
     noted, not rejected)."""
     bad = {"hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown"}
     return not (set(summary.get("reasons") or []) & bad)
+
+
+def small_block(r, frames: int = 30, warmup: int = 5) -> dict:
+    """The small configuration (256x256, 16 spp, depth 4, 64 spheres + 8192-triangle grid,
+    one area light): device time of whole renders into a device image, and end to end
+    with the host image out, over `frames` renders."""
+    import torch
+    from vork_b200 import Profile, abi, scene
+    sc = scene.spheres_scene(seed=0)
+    prof = Profile.reference_transport(4, 16)
+    cam = sc.camera
+    paths = cam.width * cam.height * prof.samples
+    with r.install(sc) as s:
+        stream = torch.cuda.ExternalStream(r.stream, device=torch.device("cuda", r.device))
+        image = torch.empty((cam.height, cam.width, 4), dtype=torch.float32, device=f"cuda:{r.device}")
+        host = torch.empty((cam.height, cam.width, 4), dtype=torch.float32).pin_memory()
+        for _ in range(warmup):
+            s.render(prof, device_ptr=image.data_ptr())
+        torch.cuda.synchronize()
+        with ClockSampler(r.device) as clocks:
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            for _ in range(frames):
+                s.render(prof, device_ptr=image.data_ptr())
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            dev_ms = ev0.elapsed_time(ev1)
+            t0 = time.perf_counter()
+            for _ in range(frames):
+                s.render(prof, out=host.numpy())
+            e2e_s = time.perf_counter() - t0
+    return {"workload": "plain-small: 256x256, 16 spp, depth 4, 64 UV spheres + 8192-tri grid, 1 area light",
+            "value": frames * paths / (dev_ms / 1000.0), "unit": "paths/s", "ms_per_frame": dev_ms / frames,
+            "e2e": {"value": frames * paths / e2e_s, "unit": "paths/s", "d2h_bytes_per_step": int(cam.width * cam.height * 16)},
+            "frames": frames, "clocks": clocks.summary()}
 
 
 def batch_block(r, jobs: int, warmup: int) -> dict:
@@ -737,7 +772,8 @@ def main():
             # The other configurations, compact, each with its own clock record: batched
             # previews (256 jobs), the learned cache on this frame scene, and serving at one
             # arrival rate with the plain FIFO baseline on the same trace.
-            for name, fn in (("batch", lambda: batch_block(r, 256, 1)),
+            for name, fn in (("small", lambda: small_block(r)),
+                             ("batch", lambda: batch_block(r, 256, 1)),
                              ("cache", lambda: cache_block(r, s, sc, frames, 2, 3)),
                              ("serve", lambda: serve_block(r, args.block_requests, [args.block_rate], fifo=True,
                                                            flock_inst=s, flock=flock))):
