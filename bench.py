@@ -234,7 +234,7 @@ def clocks_ok(summary: dict) -> bool:
     return not (set(summary.get("reasons") or []) & bad)
 
 
-def small_block(r, frames: int = 30, warmup: int = 5) -> dict:
+def small_block(r, frames: int = 400, warmup: int = 5) -> dict:
     """The small configuration (256x256, 16 spp, depth 4, 64 spheres + 8192-triangle grid,
     one area light): device time of whole renders into a device image, and end to end
     with the host image out, over `frames` renders."""

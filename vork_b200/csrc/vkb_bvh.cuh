@@ -192,9 +192,6 @@ __device__ __forceinline__ bool tri_test(const RaySpace& r, float3 v0, float3 v1
 #ifndef VKB_BLAS_LEAF_MAX
 #define VKB_BLAS_LEAF_MAX 1
 #endif
-#ifndef VKB_TRACE_FUSE_ENTRY
-#define VKB_TRACE_FUSE_ENTRY 0
-#endif
 static_assert(VKB_BLAS_LEAF_MAX >= 1 && VKB_BLAS_LEAF_MAX <= 4, "leaf counts are stored in two bits");
 
 // tri: the hit triangle's position in BLAS leaf order (global index into blas_tris; its
@@ -257,28 +254,6 @@ struct TraceLane {
         if (++steps >= TRACE_STEP_LIMIT) { atomicOr(err, 2u); return true; }
         bool respace = false;
         float3 so, sd;
-#if VKB_TRACE_FUSE_ENTRY
-        // An instance entry and the visit of its BLAS root in the same step.
-        if (node < 0 && !in_blas) {
-            if (COUNT) count->instances++;
-            const TlasLeaf* lf = s.tlas_leaves + (~node);
-            float4 r0 = __ldg(&lf->w2o[0]), r1 = __ldg(&lf->w2o[1]), r2 = __ldg(&lf->w2o[2]);
-            uint4 info = __ldg(reinterpret_cast<const uint4*>(&lf->instance));
-            const float3 o = ray.origin(), d = ray.dir();
-            so = f3(r0.x * o.x + r0.y * o.y + r0.z * o.z + r0.w, r1.x * o.x + r1.y * o.y + r1.z * o.z + r1.w, r2.x * o.x + r2.y * o.y + r2.z * o.z + r2.w);
-            sd = f3(r0.x * d.x + r0.y * d.y + r0.z * d.z, r1.x * d.x + r1.y * d.y + r1.z * d.z, r2.x * d.x + r2.y * d.y + r2.z * d.z);
-            cur_instance = info.x;
-            nodes = s.blas_nodes + info.y;
-            tri_base = info.z;
-            cull = !ANY && (info.w & LEAF_CULL_BACKFACES);
-            if (sp >= STACK_CAP) { atomicOr(err, 1u); return true; }
-            stk.put(sp, SENTINEL);
-            ++sp;
-            in_blas = true;
-            node = 0;
-            make_space(rs, so, sd);
-        }
-#endif
         if (node >= 0) {
             if (COUNT) { count->nodes++; if (in_blas) count->blas_nodes++; }
             const float4* p = reinterpret_cast<const float4*>(nodes + node);
