@@ -111,6 +111,26 @@ typedef struct vkb_environment {
     uint32_t camera_sees_environment;
 } vkb_environment;
 
+/* Image environment (the image term of path_environment, path.slang:961-983; the
+ * proposal of crates/vork-render/src/environment.rs:573-620 and
+ * shaders/environment_proposal.slang:1-49; environment_next_event, path.slang:1096-1120).
+ * A lat-long linear RGBA image: direction d (after the rotation) maps to
+ * equirect_uv(d) = (atan2(d.z, d.x)/2pi + 1/2, atan2(|d.xz|, d.y)/pi) (vork_prelude.slang:78-85),
+ * texel row 0 at the +y pole, sampled bilinearly, wrapping in longitude
+ * (vork_prelude.slang:306-330).  Radiance of a direction = environment.radiance +
+ * image x strength x color.  With strength > 0 every surface vertex also samples the
+ * environment (next-event estimation from a proposal proportional to the image's 3x3
+ * smoothed, alpha-weighted luminance times texel solid angle), MIS-weighted against the
+ * BSDF, and escaping rays are weighted the other way. */
+typedef struct vkb_environment_image {
+    const float* rgba;         /* width*height*4 (copied at vkb_scene_create) */
+    uint32_t width, height;    /* each >= 1 */
+    float strength;            /* Frame.environment.x: 0 turns the image and its strategy off */
+    float color[3];            /* Frame.environment_color.rgb */
+    float rotation[9];         /* row-major 3x3 R: a world direction d looks up equirect_uv(normalize(d R));
+                                  all zero means the identity */
+} vkb_environment_image;
+
 typedef struct vkb_scene_desc {
     const vkb_mesh* meshes;
     uint32_t num_meshes;
@@ -126,6 +146,7 @@ typedef struct vkb_scene_desc {
     vkb_environment environment;
     uint32_t tlas_builder;            /* VKB_TLAS_LBVH or VKB_TLAS_PLOC (no reference counterpart: the
                                          reference's TLAS is built by the graphics driver) */
+    const vkb_environment_image* environment_image;   /* NULL: the constant environment alone */
 } vkb_scene_desc;
 
 /* TLAS builders, both over the instance boxes in Morton order and both refittable:

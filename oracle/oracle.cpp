@@ -1026,7 +1026,54 @@ template <class R> struct Scene {
     std::vector<TreeNode> tree;
     Bvh<R> tlas;
     vkb_camera cam; vkb_environment env;
+    // Image environment: texels as float (as stored on the device), strength, colour,
+    // rotation (row-major, world direction d -> d R), and the proposal table (cumulative
+    // mass, density) in float as the reference stores it.
+    std::vector<float> env_rgba; uint32_t env_w = 0, env_h = 0; float env_strength = 0, env_color[3] = {0, 0, 0};
+    double env_rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    std::vector<float> env_cdf, env_density;
+    bool env_strategy() const { return env_w > 0 && env_strength > 0; }
 };
+// The proposal of an environment image (crates/vork-render/src/environment.rs:573-620):
+// per texel the 3x3 (1,2,1)^2/16 stencil of alpha-weighted RGB (columns wrap, rows clamp),
+// its Rec.709 luminance times the texel's solid angle, accumulated in f64 row-major and
+// normalised; a black image falls back to the uniform sphere.
+void env_distribution(const float* rgba, uint32_t dw, uint32_t dh, std::vector<float>& cdf, std::vector<float>& density) {
+    std::vector<double> cum(size_t(dw) * dh), lum_of(size_t(dw) * dh);
+    double total = 0;
+    for (uint32_t y = 0; y < dh; ++y) {
+        const double solid = TAU / dw * (std::cos(PI * y / dh) - std::cos(PI * (y + 1) / dh));
+        const int rows[3] = {std::clamp(int(y) - 1, 0, int(dh) - 1), int(y), std::clamp(int(y) + 1, 0, int(dh) - 1)};
+        for (uint32_t x = 0; x < dw; ++x) {
+            const int cols[3] = {(int(x) - 1 + int(dw)) % int(dw), int(x), (int(x) + 1) % int(dw)};
+            double rgb[3] = {0, 0, 0};
+            for (int dy = 0; dy < 3; ++dy)
+                for (int dx = 0; dx < 3; ++dx) {
+                    const size_t at = (size_t(rows[dy]) * dw + cols[dx]) * 4;
+                    const double alpha = double(rgba[at + 3]), wx = dx == 1 ? 2. : 1., wy = dy == 1 ? 2. : 1.;
+                    for (int c = 0; c < 3; ++c) rgb[c] += double(rgba[at + c]) * alpha * wx * wy;
+                }
+            double l = 0;
+            for (int c = 0; c < 3; ++c) l += double(float(LUM[c])) * (rgb[c] / 16.);
+            total += l * solid;
+            cum[size_t(y) * dw + x] = total;
+            lum_of[size_t(y) * dw + x] = l;
+        }
+    }
+    cdf.resize(cum.size()); density.resize(cum.size());
+    if (total > 0) {
+        for (size_t i = 0; i < cum.size(); ++i) { cdf[i] = float(cum[i] / total); density[i] = float(lum_of[i] / total); }
+        cdf.back() = 1.f;
+    } else {
+        for (size_t i = 0; i < cum.size(); ++i) {
+            const uint32_t y = uint32_t(i / dw), x = uint32_t(i % dw);
+            const float row = (1.f - std::cos(float(PI) * float(y) / float(dh))) / 2.f;
+            const float next = (1.f - std::cos(float(PI) * float(y + 1) / float(dh))) / 2.f;
+            cdf[i] = row + (next - row) * (float(x + 1) / float(dw));
+            density[i] = 1.f / (4.f * float(PI));
+        }
+    }
+}
 template <class R> Scene<R>* make_scene(const vkb_scene_desc* d) {
     Scene<R>* s = new Scene<R>();
     s->meshes.resize(d->num_meshes);
@@ -1062,6 +1109,16 @@ template <class R> Scene<R>* make_scene(const vkb_scene_desc* d) {
     s->lights.assign(d->lights, d->lights + d->num_lights);
     s->tree = build_light_tree(d->lights, d->num_lights);
     s->cam = d->camera; s->env = d->environment;
+    if (d->environment_image && d->environment_image->rgba && d->environment_image->width && d->environment_image->height) {
+        const vkb_environment_image& e = *d->environment_image;
+        s->env_w = e.width; s->env_h = e.height; s->env_strength = e.strength;
+        for (int c = 0; c < 3; ++c) s->env_color[c] = e.color[c];
+        s->env_rgba.assign(e.rgba, e.rgba + size_t(e.width) * e.height * 4);
+        bool any = false;
+        for (int k = 0; k < 9; ++k) any = any || e.rotation[k] != 0.f;
+        if (any) for (int k = 0; k < 9; ++k) s->env_rot[k] = double(e.rotation[k]);
+        env_distribution(e.rgba, e.width, e.height, s->env_cdf, s->env_density);
+    }
     return s;
 }
 struct Hit { double t = -1; uint32_t inst = 0xffffffffu, prim = 0xffffffffu; double u = 0, v = 0; };
@@ -1240,6 +1297,90 @@ template <class R> V3<R> clamp_sample(V3<R> v, R limit, uint64_t& dropped) {
     return v * ((limit > 0 && br > limit) ? limit / std::max(br, R(POSITIVE_EPSILON)) : R(1));
 }
 
+// ---------------------------------------------------------------- image environment
+// vork_prelude.slang:78-85.
+template <class R> inline void equirect_uv(V3<R> d, R& u, R& v) {
+    if (d.x == 0 && d.z == 0) { u = R(0.5); v = d.y > 0 ? R(0) : R(1); return; }
+    u = std::atan2(d.z, d.x) / R(TAU) + R(0.5);
+    v = std::atan2(std::sqrt(d.x * d.x + d.z * d.z), d.y) / R(PI);
+}
+// World -> environment (row vector times the rotation) and back (environment_uv,
+// environment_direction: path.slang:985-992).
+template <class R> inline V3<R> env_local(const Scene<R>& s, V3<R> d) {
+    const double* m = s.env_rot;
+    return normalize(V3<R>(d.x * R(m[0]) + d.y * R(m[3]) + d.z * R(m[6]), d.x * R(m[1]) + d.y * R(m[4]) + d.z * R(m[7]),
+                           d.x * R(m[2]) + d.y * R(m[5]) + d.z * R(m[8])));
+}
+template <class R> inline V3<R> env_world(const Scene<R>& s, V3<R> l) {
+    const double* m = s.env_rot;
+    return normalize(V3<R>(R(m[0]) * l.x + R(m[1]) * l.y + R(m[2]) * l.z, R(m[3]) * l.x + R(m[4]) * l.y + R(m[5]) * l.z,
+                           R(m[6]) * l.x + R(m[7]) * l.y + R(m[8]) * l.z));
+}
+template <class R> inline R fracr(R x) { return x - std::floor(x); }
+// environment_radiance, wrap mode 0 (vork_prelude.slang:306-330): bilinear by differences.
+template <class R> V3<R> env_lookup(const Scene<R>& s, R u, R v) {
+    const int w = int(s.env_w), h = int(s.env_h);
+    const R px = fracr(u) * R(w) - R(0.5), py = clampr(v, R(0), R(1)) * R(h) - R(0.5);
+    const int cx = int(std::floor(px)), cy = int(std::floor(py));
+    const R fx = fracr(px), fy = fracr(py);
+    const int x0 = (cx + w) % w, x1 = (x0 + 1) % w, y0 = std::clamp(cy, 0, h - 1), y1 = std::clamp(cy + 1, 0, h - 1);
+    auto at = [&](int x, int y) { const float* t = &s.env_rgba[(size_t(y) * w + x) * 4]; return V3<R>(t[0], t[1], t[2]); };
+    const V3<R> a = at(x0, y0), b = at(x1, y0), c = at(x0, y1), d = at(x1, y1);
+    const V3<R> top = a + (b - a) * fx, bottom = c + (d - c) * fx;
+    return top + (bottom - top) * fy;
+}
+// The environment radiance of a non-camera direction (path.slang:961-983).
+template <class R> V3<R> path_environment(const Scene<R>& s, V3<R> dir) {
+    V3<R> r(s.env.radiance[0], s.env.radiance[1], s.env.radiance[2]);
+    if (s.env_strategy()) {
+        R u, v;
+        equirect_uv(env_local(s, dir), u, v);
+        const V3<R> img = env_lookup(s, u, v);
+        r = r + img * R(s.env_strength) * V3<R>(s.env_color[0], s.env_color[1], s.env_color[2]);
+    }
+    return r;
+}
+// environment_proposal.slang:5-14, 17-24, 29-49.
+template <class R> R env_solid_angle(const Scene<R>& s, uint32_t row) {
+    const R angle = R(PI) / R(s.env_h);
+    return R(TAU) / R(s.env_w) * 2 * std::sin(angle * (R(row) + R(0.5))) * std::sin(R(0.5) * angle);
+}
+template <class R> R env_pdf_local(const Scene<R>& s, V3<R> l) {
+    R u, v;
+    equirect_uv(l, u, v);
+    const uint32_t cx = std::min(uint32_t(fracr(u) * R(s.env_w)), s.env_w - 1), cy = std::min(uint32_t(clampr(v, R(0), R(1)) * R(s.env_h)), s.env_h - 1);
+    const uint32_t index = cy * s.env_w + cx;
+    const R previous = index > 0 ? R(s.env_cdf[index - 1]) : R(0);
+    return (R(s.env_cdf[index]) - previous) / env_solid_angle(s, cy);
+}
+inline uint32_t env_cdf_search(const std::vector<float>& cdf, uint32_t first, uint32_t stride, uint32_t count, float base, float target) {
+    uint32_t low = 0, high = count - 1;
+    while (low < high) {
+        const uint32_t mid = (low + high) / 2;
+        if (cdf[first + mid * stride] - base <= target) low = mid + 1; else high = mid;
+    }
+    return low;
+}
+template <class R> V3<R> env_sample_local(const Scene<R>& s, float ux, float uy, R& pdf) {
+    const std::vector<float>& cdf = s.env_cdf;
+    const uint32_t w = s.env_w, h = s.env_h;
+    const uint32_t row = env_cdf_search(cdf, w - 1, w, h, 0.f, uy);
+    const float row_start = row > 0 ? cdf[row * w - 1] : 0.f;
+    const float row_mass = cdf[(row + 1) * w - 1] - row_start;
+    const float target = std::min(ux * row_mass, std::nextafter(row_mass, -INFINITY));
+    const uint32_t column = env_cdf_search(cdf, row * w, 1, w, row_start, target);
+    const uint32_t at = row * w + column;
+    const float previous = (at > 0 ? cdf[at - 1] : 0.f) - row_start;
+    const R fraction = (R(target) - R(previous)) / (R(cdf[at]) - R(row_start) - R(previous));
+    const R height = (R(uy) - R(row_start)) / R(row_mass);
+    const R phi = R(TAU) * ((R(column) + fraction) / R(w) - R(0.5));
+    const R cosine = lerp(std::cos(R(PI) * R(row) / R(h)), std::cos(R(PI) * R(row + 1) / R(h)), height);
+    const R sine = std::sqrt(std::max(1 - cosine * cosine, R(0)));
+    pdf = (R(cdf[at]) - (at > 0 ? R(cdf[at - 1]) : R(0))) / env_solid_angle(s, row);
+    return V3<R>(sine * std::cos(phi), cosine, sine * std::sin(phi));
+}
+template <class R> R environment_density(const Scene<R>& s, V3<R> dir) { return env_pdf_local(s, env_local(s, dir)); }
+
 template <class R> struct Ctx {
     const Scene<R>& s;
     const vkb_profile& prof;
@@ -1355,6 +1496,7 @@ template <class R> V3<R> integrate(Ctx<R>& cx, uint32_t px, uint32_t py, uint32_
     camera_ray<R>(s.cam, px, py, cs, origin, dir, cam_tmax);
     V3<R> throughput(1, 1, 1), radiance;
     uint32_t ray_event = VKB_RAY_CAMERA, diffuse = 0, glossy = 0, groups = 0;
+    R previous_pdf = 0;                                                   // path.slang:1326,1699
     bool nonfinite = false;
     uint64_t dropped = 0;
     const uint32_t B = pf.bounces[0];
@@ -1368,7 +1510,7 @@ template <class R> V3<R> integrate(Ctx<R>& cx, uint32_t px, uint32_t py, uint32_
             V3<R> sky;
             if (ray_event == VKB_RAY_CAMERA && !s.env.camera_sees_environment) sky = V3<R>(s.env.background[0], s.env.background[1], s.env.background[2]);
             else {
-                sky = V3<R>(s.env.radiance[0], s.env.radiance[1], s.env.radiance[2]);
+                sky = path_environment(s, dir);
                 if (ray_event == VKB_RAY_CAMERA)
                     for (const vkb_light& l : s.lights) {
                         LightV<R> L = light_values<R>(l);
@@ -1376,7 +1518,10 @@ template <class R> V3<R> integrate(Ctx<R>& cx, uint32_t px, uint32_t py, uint32_
                         sky = sky + emitter_eval(L, V3<R>(), dir).radiance;
                     }
             }
-            radiance = radiance + clamp_sample(throughput * sky, limit, dropped);
+            // path.slang:1463: an escape after a BSDF sample is weighed against the
+            // environment strategy.
+            const R mis = (s.env_strategy() && previous_pdf > 0) ? mis_power(previous_pdf, environment_density(s, dir)) : R(1);
+            radiance = radiance + clamp_sample(throughput * sky * mis, limit, dropped);
             break;
         }
         float sc[4];
@@ -1402,6 +1547,34 @@ template <class R> V3<R> integrate(Ctx<R>& cx, uint32_t px, uint32_t py, uint32_
         BsdfSample<R> smp = transport_sample(c, view, R(sc[0]), R(sc[1]), R(sc[2]), pr);
         if (!finite3(smp.dir) || !finite3(smp.weight) || !std::isfinite(smp.pdf)) { nonfinite = true; break; }
         radiance = radiance + clamp_sample(throughput * next_event(cx, hs, c, view, pr, smp, sm, rng, groups), limit, dropped);
+        if (s.env_strategy()) {
+            // environment_next_event (path.slang:1096-1120): a proposal direction, the
+            // diffuse and specular responses MIS-weighted against continuing there
+            // (continuation_mask, path.slang:1003-1010), one visibility ray to infinity.
+            uint32_t cont = 0;
+            if (bounce < B) {
+                if (diffuse < pf.bounces[1]) cont |= VKB_RAY_DIFFUSE;
+                if (glossy < pf.bounces[2] && (diffuse == 0 || (pf.caustics & 1u))) cont |= VKB_RAY_SPECULAR;
+            }
+            float eu[4];
+            vertex_group(sm, 3, eu);                                      // path_environment
+            R epdf = 0;
+            const V3<R> edir = env_world(s, env_sample_local(s, eu[0], eu[1], epdf));
+            V3<R> env_value;
+            if (epdf > 0) {
+                for (uint32_t event : {uint32_t(VKB_RAY_DIFFUSE), uint32_t(VKB_RAY_SPECULAR)}) {
+                    if (!event_hemisphere(event, edir, hs.face, hs.geometric)) continue;
+                    const V3<R> emitted = path_environment(s, edir);
+                    if (maxc(emitted) <= 0) continue;
+                    const V3<R> response = eval_mask(c, view, edir, event, pr);
+                    if (maxc(response) <= 0) continue;
+                    const R bsdf_pdf = (cont & event) ? pdf_mask(c, view, edir, event, pr) : R(0);
+                    env_value = env_value + emitted * response * (mis_power(epdf, bsdf_pdf) / epdf);
+                }
+                if (any_nonzero(env_value) && occluded(cx, path_origin(hs, edir), edir, R(FP32_MAX))) env_value = V3<R>();
+            }
+            radiance = radiance + clamp_sample(throughput * env_value, limit, dropped);
+        }
         if (bounce == B) break;
         uint32_t event = smp.event;
         ray_event = event;
@@ -1421,6 +1594,7 @@ template <class R> V3<R> integrate(Ctx<R>& cx, uint32_t px, uint32_t py, uint32_
         }
         dir = smp.dir;
         origin = path_origin(hs, dir);
+        previous_pdf = smp.pdf;
         bounce++;
     }
     cx.dropped_light += dropped;
@@ -1761,6 +1935,31 @@ void oracle_trace(void* h, int fp64, uint32_t n, const float* rays7, int any, fl
         else hit = trace(*static_cast<Scene<float>*>(o->s32), V3<float>(r[0], r[1], r[2]), V3<float>(r[3], r[4], r[5]), r[6], any != 0);
         out_t[i] = float(hit.t); out_ids[2 * i] = hit.inst; out_ids[2 * i + 1] = hit.prim;
         out_uv[2 * i] = float(hit.u); out_uv[2 * i + 1] = float(hit.v);
+    }
+}
+// Image environment probes: n proposal samples (u2 pairs) -> world directions and pdfs;
+// the proposal pdf and the radiance of n world directions.
+void oracle_env_sample(void* h, int fp64, uint32_t n, const float* u2, float* dir3, float* pdf) {
+    OracleScene* o = static_cast<OracleScene*>(h);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (fp64) {
+            const Scene<double>& s = *static_cast<Scene<double>*>(o->s64);
+            double p; V3<double> d = env_world(s, env_sample_local(s, u2[2 * i], u2[2 * i + 1], p));
+            dir3[3 * i] = float(d.x); dir3[3 * i + 1] = float(d.y); dir3[3 * i + 2] = float(d.z); pdf[i] = float(p);
+        } else {
+            const Scene<float>& s = *static_cast<Scene<float>*>(o->s32);
+            float p; V3<float> d = env_world(s, env_sample_local(s, u2[2 * i], u2[2 * i + 1], p));
+            dir3[3 * i] = d.x; dir3[3 * i + 1] = d.y; dir3[3 * i + 2] = d.z; pdf[i] = p;
+        }
+    }
+}
+void oracle_env_eval(void* h, uint32_t n, const float* dir3, float* pdf, float* rgb) {
+    const Scene<double>& s = *static_cast<Scene<double>*>(static_cast<OracleScene*>(h)->s64);
+    for (uint32_t i = 0; i < n; ++i) {
+        V3<double> d = normalize(V3<double>(dir3[3 * i], dir3[3 * i + 1], dir3[3 * i + 2]));
+        if (pdf) pdf[i] = float(environment_density(s, d));
+        V3<double> r = path_environment(s, d);
+        rgb[3 * i] = float(r.x); rgb[3 * i + 1] = float(r.y); rgb[3 * i + 2] = float(r.z);
     }
 }
 // Camera rays of sample `index` for a crop, as path_camera_ray builds them (rays7 layout).

@@ -56,6 +56,8 @@ def lib():
         l.oracle_instance_boxes.argtypes = [P, f32p, f32p]
         l.oracle_blas_morton.argtypes = [P, C.c_uint32, u32p]
         l.oracle_set_lut.argtypes = [f32p]
+        l.oracle_env_sample.argtypes = [P, C.c_int, C.c_uint32, f32p, f32p, f32p]
+        l.oracle_env_eval.argtypes = [P, C.c_uint32, f32p, f32p, f32p]
         _lib = l
     return _lib
 
@@ -174,6 +176,20 @@ class OracleScene:
         with ThreadPoolExecutor(threads) as ex:
             list(ex.map(lambda a: chunk(a, min(n, a + step)), range(0, n, step)))
         return t, ids, uv
+
+    def env_sample(self, u2, fp64=True):
+        """Proposal samples of the image environment: (directions (n,3), pdfs (n,))."""
+        u = np.ascontiguousarray(u2, np.float32).reshape(-1, 2)
+        d = np.zeros((len(u), 3), np.float32); p = np.zeros(len(u), np.float32)
+        lib().oracle_env_sample(self.h, 1 if fp64 else 0, len(u), _p(u, C.c_float), _p(d, C.c_float), _p(p, C.c_float))
+        return d, p
+
+    def env_eval(self, dirs):
+        """(proposal pdf, radiance) of world directions under the image environment."""
+        d = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
+        p = np.zeros(len(d), np.float32); rgb = np.zeros((len(d), 3), np.float32)
+        lib().oracle_env_eval(self.h, len(d), _p(d, C.c_float), _p(p, C.c_float), _p(rgb, C.c_float))
+        return p, rgb
 
     def camera_rays(self, profile, index, x0=0, y0=0, w=None, h=None):
         cam = self.scene.camera

@@ -51,12 +51,18 @@ class VkbEnvironment(C.Structure):
                 ("camera_sees_environment", C.c_uint32)]
 
 
+class VkbEnvironmentImage(C.Structure):
+    _fields_ = [("rgba", C.POINTER(C.c_float)), ("width", C.c_uint32), ("height", C.c_uint32), ("strength", C.c_float),
+                ("color", C.c_float * 3), ("rotation", C.c_float * 9)]
+
+
 class VkbSceneDesc(C.Structure):
     _fields_ = [("meshes", C.POINTER(VkbMesh)), ("num_meshes", C.c_uint32), ("num_instances", C.c_uint32),
                 ("instance_rows", C.POINTER(C.c_float)), ("instance_mesh", C.POINTER(C.c_uint32)),
                 ("instance_material", C.POINTER(C.c_uint32)), ("materials", C.POINTER(VkbMaterial)),
                 ("num_materials", C.c_uint32), ("lights", C.POINTER(VkbLight)), ("num_lights", C.c_uint32),
-                ("camera", VkbCamera), ("environment", VkbEnvironment), ("tlas_builder", C.c_uint32)]
+                ("camera", VkbCamera), ("environment", VkbEnvironment), ("tlas_builder", C.c_uint32),
+                ("environment_image", C.POINTER(VkbEnvironmentImage))]
 
 
 class VkbProfile(C.Structure):

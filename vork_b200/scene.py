@@ -261,6 +261,7 @@ class Scene:
     environment: abi.VkbEnvironment
     name: str = "scene"
     tlas_builder: int = abi.TLAS_LBVH
+    env_image: "EnvironmentImage | None" = None
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -301,8 +302,52 @@ class Scene:
         d.camera = self.camera
         d.environment = self.environment
         d.tlas_builder = self.tlas_builder
+        if self.env_image is not None:
+            img = np.ascontiguousarray(self.env_image.rgba, np.float32)
+            e = abi.VkbEnvironmentImage()
+            e.rgba = abi.fptr(img)
+            e.height, e.width = int(img.shape[0]), int(img.shape[1])
+            e.strength = float(self.env_image.strength)
+            e.color[:] = [float(v) for v in self.env_image.color]
+            e.rotation[:] = [float(v) for v in np.asarray(self.env_image.rotation, np.float64).reshape(9)]
+            keep += [img, e]
+            d.environment_image = C.pointer(e)
         self._keep = keep
         return d
+
+
+@dataclass
+class EnvironmentImage:
+    """A lat-long linear RGBA environment (row 0 at the +y pole) with its strength,
+    colour and 3x3 rotation (a world direction d looks up normalize(d R))."""
+    rgba: np.ndarray
+    strength: float = 1.0
+    color: tuple = (1.0, 1.0, 1.0)
+    rotation: np.ndarray = field(default_factory=lambda: np.eye(3))
+
+
+def sky_image(width: int = 256, height: int = 128, sun_dir=(0.4, 0.8, 0.45), sun_radiance: float = 400.0,
+              sun_radius_deg: float = 3.0, seed: int = 0) -> np.ndarray:
+    """A procedural lat-long sky: a blue-to-white gradient, a warm ground, seeded
+    low-frequency cloud noise and a small bright disc around `sun_dir`."""
+    rng = np.random.default_rng(seed)
+    v = (np.arange(height) + 0.5) / height
+    u = (np.arange(width) + 0.5) / width
+    theta = np.pi * v[:, None]
+    phi = 2 * np.pi * (u[None, :] - 0.5)
+    d = np.stack([np.sin(theta) * np.cos(phi), np.cos(theta) * np.ones_like(phi), np.sin(theta) * np.sin(phi)], -1)
+    up = np.clip(d[..., 1], -1, 1)
+    sky = np.where(up[..., None] > 0, (1 - up[..., None]) * np.array([0.9, 0.95, 1.0]) + up[..., None] * np.array([0.25, 0.45, 0.9]),
+                   np.array([0.3, 0.25, 0.2]) * (1 + up[..., None]))
+    noise = rng.random((8, 16))
+    ny = np.minimum((v * 8).astype(int), 7)[:, None]
+    nx = np.minimum((u * 16).astype(int), 15)[None, :]
+    sky = sky * (0.8 + 0.4 * noise[ny, nx])[..., None]
+    s = np.asarray(sun_dir, np.float64); s /= np.linalg.norm(s)
+    disc = np.einsum("hwc,c->hw", d, s) > np.cos(np.radians(sun_radius_deg))
+    sky[disc] = sun_radiance * np.array([1.0, 0.93, 0.85])
+    rgba = np.concatenate([sky, np.ones(sky.shape[:2] + (1,))], -1)
+    return rgba.astype(np.float32)
 
 
 def environment(radiance=(0.0, 0.0, 0.0), exposure=1.0, background=(0.0, 0.0, 0.0), camera_sees=True) -> abi.VkbEnvironment:
