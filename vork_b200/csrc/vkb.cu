@@ -296,6 +296,8 @@ struct WaveBuffers {
     unsigned long long* work = nullptr;
     Job* jobs = nullptr;
     float4* guide = nullptr;   // guide renders: 2 float4 per path slot
+    float4 *sc_o = nullptr, *sc_d = nullptr, *sc_c = nullptr;   // image-environment waves: the third shadow ray
+    float* prev_pdf = nullptr;
 };
 // The context's own wavefront storage (grown on demand, reused by every render).
 struct Wavefront {
@@ -304,9 +306,19 @@ struct Wavefront {
     DBuf<uint2> rng;
     DBuf<unsigned long long> work;
     DBuf<Job> jobs;
+    DBuf<float4> sc_o, sc_d, sc_c;     // image-environment waves only (allocated on first need)
+    DBuf<float> prev_pdf;
     uint64_t generation = 0;  // bumps when a buffer moves (captured graphs refer to the old ones)
+    // The third shadow ray and previous pdf of every slot, for waves with an image environment.
+    void reserve_env(size_t slots) {
+        if (slots > sc_o.n) {
+            sc_o.alloc(slots); sc_d.alloc(slots); sc_c.alloc(slots); prev_pdf.alloc(slots);
+            generation++;
+        }
+    }
     WaveBuffers view() const {
         WaveBuffers w;
+        w.sc_o = sc_o.p; w.sc_d = sc_d.p; w.sc_c = sc_c.p; w.prev_pdf = prev_pdf.p;
         w.capacity = ray_o0.n; w.job_capacity = uint32_t(jobs.n);
         w.ray_o0 = ray_o0.p; w.ray_d0 = ray_d0.p; w.ray_o1 = ray_o1.p; w.ray_d1 = ray_d1.p; w.hit = hit.p; w.thr = thr.p; w.rad = rad.p;
         w.sa_o = sa_o.p; w.sa_d = sa_d.p; w.sa_c = sa_c.p; w.sb_o = sb_o.p; w.sb_d = sb_d.p; w.sb_c = sb_c.p;
@@ -318,14 +330,16 @@ struct Wavefront {
             DBuf<float4>* f4[] = {&ray_o0, &ray_d0, &ray_o1, &ray_d1, &hit, &thr, &rad, &sa_o, &sa_d, &sa_c, &sb_o, &sb_d, &sb_c};
             for (auto* b : f4) b->alloc(slots);
             hit_inst.alloc(slots); slot_job.alloc(slots); rng.alloc(slots);
+            if (sc_o.p) reserve_env(slots);
             generation++;
         }
         if (!counters.p) { counters.alloc(16); err.alloc(1); work.alloc(8); generation++; }
         if (njobs > jobs.n) { jobs.alloc(std::max<size_t>(njobs, 16)); generation++; }
     }
     void release() {
-        DBuf<float4>* f4[] = {&ray_o0, &ray_d0, &ray_o1, &ray_d1, &hit, &thr, &rad, &sa_o, &sa_d, &sa_c, &sb_o, &sb_d, &sb_c};
+        DBuf<float4>* f4[] = {&ray_o0, &ray_d0, &ray_o1, &ray_d1, &hit, &thr, &rad, &sa_o, &sa_d, &sa_c, &sb_o, &sb_d, &sb_c, &sc_o, &sc_d, &sc_c};
         for (auto* b : f4) b->release();
+        prev_pdf.release();
         hit_inst.release(); slot_job.release(); rng.release(); counters.release(); err.release(); work.release(); jobs.release();
     }
 };
@@ -389,6 +403,12 @@ struct vkb_scene {
     vkb_scene* base = nullptr;
     uint32_t forks = 0;
     float install_ms = 0.f, blas_host_ms = 0.f, upload_ms = 0.f, tlas_ms = 0.f;   // install cost
+    // Image environment (env_w == 0: none): texels, proposal, strength x colour, rotation.
+    DBuf<float4> env_img;
+    DBuf<float2> env_dist;
+    uint32_t env_w = 0, env_h = 0;
+    float env_scale[3] = {0.f, 0.f, 0.f};
+    float env_rot[9] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};
 };
 
 namespace {
@@ -419,6 +439,49 @@ SceneView scene_view(const vkb_scene* s) {
     v.blas_nodes = s->blas4.p; v.blas_tris = s->blas_tris.p;
     v.num_instances = s->num_instances;
     return v;
+}
+
+// The proposal of an environment image (crates/vork-render/src/environment.rs:573-620):
+// per texel the 3x3 (1,2,1)^2/16 stencil of alpha-weighted RGB (columns wrap, rows clamp),
+// its Rec.709 luminance times the texel's solid angle, accumulated in f64 row-major and
+// normalised to (cumulative mass, density) in f32; a black image gets the uniform sphere.
+std::vector<float2> env_proposal(const float* rgba, uint32_t dw, uint32_t dh) {
+    const double PI_D = 3.141592653589793, TAU_D = 2.0 * PI_D;
+    const float lum[3] = {0.2126f, 0.7152f, 0.0722f};
+    std::vector<double> cum(size_t(dw) * dh), dens(size_t(dw) * dh);
+    double total = 0.0;
+    for (uint32_t y = 0; y < dh; ++y) {
+        const double solid = TAU_D / dw * (std::cos(PI_D * y / dh) - std::cos(PI_D * (y + 1) / dh));
+        const int rows[3] = {std::max(int(y) - 1, 0), int(y), std::min(int(y) + 1, int(dh) - 1)};
+        for (uint32_t x = 0; x < dw; ++x) {
+            const int cols[3] = {(int(x) - 1 + int(dw)) % int(dw), int(x), (int(x) + 1) % int(dw)};
+            double rgb[3] = {0.0, 0.0, 0.0};
+            for (int dy = 0; dy < 3; ++dy)
+                for (int dx = 0; dx < 3; ++dx) {
+                    const size_t at = (size_t(rows[dy]) * dw + cols[dx]) * 4;
+                    const double w = double(rgba[at + 3]) * (dx == 1 ? 2.0 : 1.0) * (dy == 1 ? 2.0 : 1.0);
+                    for (int c = 0; c < 3; ++c) rgb[c] += double(rgba[at + c]) * w;
+                }
+            double l = 0.0;
+            for (int c = 0; c < 3; ++c) l += double(lum[c]) * (rgb[c] / 16.0);
+            total += l * solid;
+            cum[size_t(y) * dw + x] = total;
+            dens[size_t(y) * dw + x] = l;
+        }
+    }
+    std::vector<float2> out(cum.size());
+    if (total > 0.0) {
+        for (size_t i = 0; i < cum.size(); ++i) out[i] = make_float2(float(cum[i] / total), float(dens[i] / total));
+        out.back().x = 1.f;
+    } else {
+        for (size_t i = 0; i < cum.size(); ++i) {
+            const uint32_t y = uint32_t(i / dw), x = uint32_t(i % dw);
+            const float row = (1.f - std::cos(float(PI_D) * float(y) / float(dh))) / 2.f;
+            const float next = (1.f - std::cos(float(PI_D) * float(y + 1) / float(dh))) / 2.f;
+            out[i] = make_float2(row + (next - row) * (float(x + 1) / float(dw)), 1.f / (4.f * float(PI_D)));
+        }
+    }
+    return out;
 }
 
 // Instance rows -> w2o, world boxes, TLAS and its leaf records.  The TLAS is the
@@ -519,6 +582,13 @@ void validate_desc(const vkb_scene_desc* d) {
     }
     if (d->camera.width == 0 || d->camera.height == 0) throw ArgError{"camera resolution is zero"};
     if (d->tlas_builder > VKB_TLAS_PLOC) throw ArgError{"unknown TLAS builder"};
+    if (const vkb_environment_image* e = d->environment_image) {
+        if (!e->rgba || e->width == 0 || e->height == 0) throw ArgError{"environment image has no texels"};
+        if (uint64_t(e->width) * e->height > (uint64_t(1) << 26)) throw ArgError{"environment image above 2^26 texels"};
+        if (!(e->strength >= 0.f) || !std::isfinite(e->strength)) throw ArgError{"environment strength must be finite and non-negative"};
+        for (size_t i = 0; i < size_t(e->width) * e->height * 4; ++i)
+            if (!std::isfinite(e->rgba[i]) || e->rgba[i] < 0.f) throw ArgError{"environment image texels must be finite and non-negative"};
+    }
 }
 
 
@@ -593,6 +663,9 @@ Job make_job(const EngineJob& e) {
     j.adaptive_min = pf.adaptive_min_samples ? pf.adaptive_min_samples : std::max(16u, uint32_t(std::sqrt(float(pf.samples))));
     j.ad_mean = e.ad_mean; j.ad_m2 = e.ad_m2; j.ad_state = e.ad_state;
     j.guide_accum = e.guide_accum; j.guide_albedo = e.guide_albedo; j.guide_normal = e.guide_normal;
+    j.env_img = s->env_img.p; j.env_dist = s->env_dist.p; j.env_w = s->env_w; j.env_h = s->env_h;
+    for (int k = 0; k < 3; ++k) j.env_scale[k] = s->env_scale[k];
+    for (int k = 0; k < 9; ++k) j.env_rot[k] = s->env_rot[k];
     return j;
 }
 
@@ -605,6 +678,7 @@ PathParams path_params(const vkb_ctx* c, const WaveBuffers& w, uint32_t njobs) {
     p.sa_o = w.sa_o; p.sa_d = w.sa_d; p.sa_c = w.sa_c; p.sb_o = w.sb_o; p.sb_d = w.sb_d; p.sb_c = w.sb_c;
     p.counters = w.counters; p.work = w.work; p.err = w.err;
     p.guide = w.guide;
+    p.sc_o = w.sc_o; p.sc_d = w.sc_d; p.sc_c = w.sc_c; p.prev_pdf = w.prev_pdf;
     return p;
 }
 
@@ -622,7 +696,7 @@ struct CacheLaunch {
 // mode records events around every closest-hit trace.
 template <bool BATCH>
 void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counted, bool timed, WaveTotals& tot,
-                  const CacheLaunch* cache = nullptr) {
+                  const CacheLaunch* cache = nullptr, bool env = false) {
     cudaStream_t st = c->stream;
     const int sms = c->sms, tgrid = sms * c->trace_blocks_per_sm, sgrid = sms * c->trace_blocks_per_sm;
     const bool adaptive = !BATCH && p.job0.adaptive;
@@ -645,9 +719,17 @@ void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counte
         tot.trace_launches++;
         if (!BATCH && b == 0u && p.guide) { k_guides<<<sms * 8, 256, 0, st>>>(p); tot.launches += 1; }
         k_reset_queues<<<1, 1, 0, st>>>(p.counters, cur ^ 1);
-        k_shade<BATCH><<<sgrid, SHADE_BLOCK, 0, st>>>(p, cur);
-        if (counted) k_trace_shadow<true, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
-        else k_trace_shadow<false, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
+        // Waves with an image environment run the kernels that sample it (a third shadow
+        // ray per vertex); the others keep the plain ones.
+        if (env) {
+            k_shade<BATCH, true><<<sgrid, SHADE_BLOCK, 0, st>>>(p, cur);
+            if (counted) k_trace_shadow<true, BATCH, true><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
+            else k_trace_shadow<false, BATCH, true><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
+        } else {
+            k_shade<BATCH, false><<<sgrid, SHADE_BLOCK, 0, st>>>(p, cur);
+            if (counted) k_trace_shadow<true, BATCH, false><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
+            else k_trace_shadow<false, BATCH, false><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
+        }
     }
     if (cache && cache->dev.mode == 1u) {
         if (timed) {
@@ -810,13 +892,16 @@ struct WaveEngine {
         VKB_CUDA(cudaMemcpyAsync(w.counters + 7, wave_counts, sizeof(wave_counts), cudaMemcpyHostToDevice, st));
         PathParams p = path_params(c, w, wave_jobs);
         p.job0 = wave_table[0];
+        bool env = false;
+        for (const Job& j : wave_table) env = env || j.env_w != 0u;
+        if (env && !w.sc_o) throw InternalError{"image-environment wave without its shadow buffers"};
         if (cache) {
             if (batch) throw ArgError{"radiance-cache renders take one job"};
             p.cache = cache->dev;
         }
         if (use_graph) {
             uint64_t key = (uint64_t(bounces) << 1) | 1u;
-            key = key * 1315423911ull + (counted ? 7u : 3u);
+            key = key * 1315423911ull + (counted ? 7u : 3u) + (env ? 11u : 0u);
             key = key * 40503ull + wave_jobs;
             key = key * 97ull + uint64_t(c->trace_blocks_per_sm);
             cudaGraphExec_t exec = nullptr;
@@ -825,7 +910,7 @@ struct WaveEngine {
                 cudaGraph_t g;
                 VKB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
                 WaveTotals scratch;
-                wave_kernels<true>(c, p, bounces, counted, false, scratch);
+                wave_kernels<true>(c, p, bounces, counted, false, scratch, nullptr, env);
                 VKB_CUDA(cudaStreamEndCapture(st, &g));
                 VKB_CUDA(cudaGraphInstantiate(&exec, g, 0));
                 VKB_CUDA(cudaGraphDestroy(g));
@@ -835,9 +920,9 @@ struct WaveEngine {
             tot.launches += 3 + 4 * (bounces + 1);
             tot.trace_launches += bounces + 1;
         } else if (batch) {
-            wave_kernels<true>(c, p, bounces, counted, timed, tot);
+            wave_kernels<true>(c, p, bounces, counted, timed, tot, nullptr, env);
         } else {
-            wave_kernels<false>(c, p, bounces, counted, timed, tot, cache);
+            wave_kernels<false>(c, p, bounces, counted, timed, tot, cache, env);
         }
         VKB_CUDA(cudaGetLastError());
         return true;
@@ -951,6 +1036,8 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
     if (in.size() == 1 && wave_samples_hint) capacity = max_pix * wave_samples_hint;
     capacity = std::max(capacity, max_pix);
     c->wave.reserve(capacity, uint32_t(in.size()));
+    for (const auto& job : in)
+        if (job.first->env_w) { c->wave.reserve_env(std::max(capacity, c->wave.ray_o0.n)); break; }
     c->accum.alloc(std::max<size_t>(1, total_pixels));
     WaveBuffers wb = c->wave.view();
     if (guides) {
@@ -1160,6 +1247,19 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         s->tree.upload(tree.data(), tree.size(), str);
         s->camera = d->camera;
         s->env = d->environment;
+        if (const vkb_environment_image* e = d->environment_image) {
+            if (e->strength > 0.f) {
+                s->env_w = e->width; s->env_h = e->height;
+                for (int c = 0; c < 3; ++c) s->env_scale[c] = e->strength * e->color[c];
+                bool any = false;
+                for (int k = 0; k < 9; ++k) any = any || e->rotation[k] != 0.f;
+                if (any) for (int k = 0; k < 9; ++k) s->env_rot[k] = e->rotation[k];
+                s->env_img.upload(reinterpret_cast<const float4*>(e->rgba), size_t(e->width) * e->height, str);
+                std::vector<float2> dist = env_proposal(e->rgba, e->width, e->height);
+                s->env_dist.upload(dist.data(), dist.size(), str);
+                VKB_CUDA(cudaStreamSynchronize(str));
+            }
+        }
         // Instances + TLAS.
         uint32_t n = d->num_instances;
         s->inst_mesh.assign(d->instance_mesh, d->instance_mesh + n);
@@ -1210,6 +1310,8 @@ vkb_status vkb_scene_fork(vkb_scene* b, vkb_scene** out) {
         s->vpos = b->vpos; s->vnrm = b->vnrm; s->blas_tris = b->blas_tris; s->tri_nrm = b->tri_nrm;
         s->indices = b->indices; s->meshes = b->meshes; s->blas4 = b->blas4;
         s->d_materials = b->d_materials; s->d_lights = b->d_lights; s->tree = b->tree;
+        s->env_img = b->env_img; s->env_dist = b->env_dist; s->env_w = b->env_w; s->env_h = b->env_h;
+        std::copy(b->env_scale, b->env_scale + 3, s->env_scale); std::copy(b->env_rot, b->env_rot + 9, s->env_rot);
         s->base = b;
         b->forks++;
         // Owned: the base's current instance rows and records, and a TLAS over them.
@@ -1252,8 +1354,11 @@ vkb_status vkb_scene_destroy(vkb_scene* s) {
         s->d_materials.p = nullptr; s->d_materials.n = 0;
         s->d_lights.p = nullptr; s->d_lights.n = 0;
         s->tree.p = nullptr; s->tree.n = 0;
+        s->env_img.p = nullptr; s->env_img.n = 0;
+        s->env_dist.p = nullptr; s->env_dist.n = 0;
         s->base->forks--;
     }
+    s->env_img.release(); s->env_dist.release();
     DBuf<float4>* f4[] = {&s->vpos, &s->vnrm, &s->blas_tris, &s->tri_nrm, &s->o2w, &s->o2w_next, &s->w2o, &s->inst_lo, &s->inst_hi, &s->tri_lo, &s->tri_hi};
     for (auto* b : f4) b->release();
     s->changed.release();
@@ -1873,6 +1978,13 @@ vkb_status vkb_server_step(vkb_server* v, vkb_server_status* status) {
                 extra = need;
             }
             if (v->budget && held() + scene + extra > v->budget) break;
+            if (q.s->env_w && !v->wave.sc_o.p) {
+                // The first request with an image environment: the wavefront's third shadow
+                // ray and previous-pdf buffers (52 B per path slot), for every later wave.
+                v->wave.reserve_env(v->capacity);
+                v->wave_bytes += uint64_t(v->capacity) * 52u;
+                eng.w = v->wave.view();
+            }
             auto live = std::make_unique<vkb_server::Live>();
             live->id = q.id; live->host_out = q.host_out; live->npix = uint32_t(npix);
             live->buf = take_buffers(v, npix);
@@ -2004,6 +2116,7 @@ extern "C" vkb_status vkb_render_noalloc(vkb_scene* s, const vkb_profile* pf, vk
         validate_profile(pf);
         if (pf->adaptive) throw Unsupported{"adaptive stopping renders through vkb_render"};
         if (out->guide_albedo || out->guide_normal) throw Unsupported{"denoiser guides render through vkb_render"};
+        if (s->env_w) throw Unsupported{"image environments render through vkb_render"};
         uint32_t count = pf->sample_count ? pf->sample_count : pf->samples - pf->first_sample;
         vkb_ctx* c = s->ctx;
         VKB_CUDA(cudaSetDevice(c->device));

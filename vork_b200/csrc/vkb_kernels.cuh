@@ -443,6 +443,12 @@ struct Job {
     // Denoiser guides (path.slang:1549-1571,1956-1963), single-job renders only: per-pixel
     // sums (albedo + coverage, normal) in sample order and the mean planes written at resolve.
     float4* guide_accum; float4* guide_albedo; float4* guide_normal;
+    // Image environment (env_w == 0: none): RGBA texels, the proposal (cumulative mass,
+    // density), strength x colour, and the rotation (world d -> d R, row-major).
+    const float4* env_img; const float2* env_dist;
+    uint32_t env_w, env_h;
+    float env_scale[3];
+    float env_rot[9];
 };
 constexpr uint32_t AD_STOPPED = 4u;
 // Radiance-cache hooks of a wave.  mode 1 (query): a path reaching vertex `vertex`
@@ -478,9 +484,91 @@ struct PathParams {
     uint32_t* err;
     CacheParams cache;
     float4* guide;        // guide renders: the camera hit's guide albedo and normal per path slot (2 float4)
+    // Image-environment waves: each slot's environment shadow ray (origin+tmax, direction,
+    // contribution) and the pdf of the BSDF sample that made its current ray.
+    float4* sc_o; float4* sc_d; float4* sc_c; float* prev_pdf;
 };
 constexpr uint32_t META_NONFINITE = 0x80000000u;
-constexpr uint32_t SH_TRACE_A = 1u, SH_HAS_B = 2u, SH_TRACE_B = 4u, SH_DIRECT = 8u;
+constexpr uint32_t SH_TRACE_A = 1u, SH_HAS_B = 2u, SH_TRACE_B = 4u, SH_DIRECT = 8u, SH_HAS_C = 16u;
+
+// ---------------------------------------------------------------- image environment
+// vork_prelude.slang:78-85.
+__device__ __forceinline__ float2 equirect_uv(float3 d) {
+    if (d.x == 0.f && d.z == 0.f) return make_float2(0.5f, d.y > 0.f ? 0.f : 1.f);
+    return make_float2(atan2f(d.z, d.x) / TAU_F + 0.5f, atan2f(sqrtf(d.x * d.x + d.z * d.z), d.y) / PI_F);
+}
+// World -> environment (row vector times the rotation) and back (path.slang:985-992).
+__device__ __forceinline__ float3 env_local(const Job& J, float3 d) {
+    const float* m = J.env_rot;
+    return normalize(f3(d.x * m[0] + d.y * m[3] + d.z * m[6], d.x * m[1] + d.y * m[4] + d.z * m[7], d.x * m[2] + d.y * m[5] + d.z * m[8]));
+}
+__device__ __forceinline__ float3 env_world(const Job& J, float3 l) {
+    const float* m = J.env_rot;
+    return normalize(f3(m[0] * l.x + m[1] * l.y + m[2] * l.z, m[3] * l.x + m[4] * l.y + m[5] * l.z, m[6] * l.x + m[7] * l.y + m[8] * l.z));
+}
+__device__ __forceinline__ float fracf(float x) { return x - floorf(x); }
+// environment_radiance, wrap mode 0 (vork_prelude.slang:306-330): bilinear by differences.
+__device__ float3 env_lookup(const Job& J, float2 uv) {
+    const int w = int(J.env_w), h = int(J.env_h);
+    const float px = fracf(uv.x) * float(w) - 0.5f, py = clampf(uv.y, 0.f, 1.f) * float(h) - 0.5f;
+    const int cx = int(floorf(px)), cy = int(floorf(py));
+    const float fx = fracf(px), fy = fracf(py);
+    const int x0 = (cx + w) % w, x1 = (x0 + 1) % w, y0 = min(max(cy, 0), h - 1), y1 = min(max(cy + 1, 0), h - 1);
+    const float4 a = __ldg(J.env_img + y0 * w + x0), b = __ldg(J.env_img + y0 * w + x1);
+    const float4 c = __ldg(J.env_img + y1 * w + x0), d = __ldg(J.env_img + y1 * w + x1);
+    const float3 top = f3(a.x, a.y, a.z) + (f3(b.x, b.y, b.z) - f3(a.x, a.y, a.z)) * fx;
+    const float3 bottom = f3(c.x, c.y, c.z) + (f3(d.x, d.y, d.z) - f3(c.x, c.y, c.z)) * fx;
+    return top + (bottom - top) * fy;
+}
+// Radiance of a direction: the constant environment plus the image term (path.slang:961-983).
+__device__ __forceinline__ float3 env_radiance(const Job& J, float3 dir) {
+    float3 r = get3(J.env.radiance);
+    if (J.env_w) {
+        const float3 img = env_lookup(J, equirect_uv(env_local(J, dir)));
+        r = r + f3(img.x * J.env_scale[0], img.y * J.env_scale[1], img.z * J.env_scale[2]);
+    }
+    return r;
+}
+// environment_proposal.slang:5-14, 17-24, 29-49.
+__device__ __forceinline__ float env_solid_angle(const Job& J, uint32_t row) {
+    const float angle = PI_F / float(J.env_h);
+    return TAU_F / float(J.env_w) * 2.f * sinf(angle * (float(row) + 0.5f)) * sinf(0.5f * angle);
+}
+__device__ float env_density(const Job& J, float3 dir) {
+    const float2 uv = equirect_uv(env_local(J, dir));
+    const uint32_t cx = min(uint32_t(fracf(uv.x) * float(J.env_w)), J.env_w - 1u);
+    const uint32_t cy = min(uint32_t(clampf(uv.y, 0.f, 1.f) * float(J.env_h)), J.env_h - 1u);
+    const uint32_t index = cy * J.env_w + cx;
+    const float previous = index > 0u ? __ldg(&J.env_dist[index - 1u].x) : 0.f;
+    return (__ldg(&J.env_dist[index].x) - previous) / env_solid_angle(J, cy);
+}
+__device__ __forceinline__ uint32_t env_cdf_search(const float2* dist, uint32_t first, uint32_t stride, uint32_t count, float base, float target) {
+    uint32_t low = 0u, high = count - 1u;
+    while (low < high) {
+        const uint32_t mid = (low + high) >> 1;
+        if (__ldg(&dist[first + mid * stride].x) - base <= target) low = mid + 1u; else high = mid;
+    }
+    return low;
+}
+__device__ float3 env_sample(const Job& J, float ux, float uy, float& pdf) {
+    const float2* cdf = J.env_dist;
+    const uint32_t w = J.env_w, h = J.env_h;
+    const uint32_t row = env_cdf_search(cdf, w - 1u, w, h, 0.f, uy);
+    const float row_start = row > 0u ? __ldg(&cdf[row * w - 1u].x) : 0.f;
+    const float row_mass = __ldg(&cdf[(row + 1u) * w - 1u].x) - row_start;
+    const float target = fminf(ux * row_mass, __uint_as_float(__float_as_uint(row_mass) - 1u));
+    const uint32_t column = env_cdf_search(cdf, row * w, 1u, w, row_start, target);
+    const uint32_t at = row * w + column;
+    const float at_mass = __ldg(&cdf[at].x), before = at > 0u ? __ldg(&cdf[at - 1u].x) : 0.f;
+    const float previous = before - row_start;
+    const float fraction = (target - previous) / (at_mass - row_start - previous);
+    const float height = (uy - row_start) / row_mass;
+    const float phi = TAU_F * ((float(column) + fraction) / float(w) - 0.5f);
+    const float cosine = lerpf(cosf(PI_F * float(row) / float(h)), cosf(PI_F * float(row + 1u) / float(h)), height);
+    const float sine = sqrtf(fmaxf(1.f - cosine * cosine, 0.f));
+    pdf = (at_mass - before) / env_solid_angle(J, row);
+    return env_world(J, f3(sine * cosf(phi), cosine, sine * sinf(phi)));
+}
 
 __device__ __forceinline__ float filter_offset(const float* table, float u) {
     float x = clampf(u, 0.f, 1.f) * float(FILTER_INTERVALS);
@@ -677,7 +765,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace(Pat
 // Shadow entries with lane refill (as k_trace): a lane carries one entry through its
 // ray A, then its ray B (the second estimator's, when present and traced), then adds
 // the unoccluded contributions to the slot's radiance.
-template <bool COUNT, bool BATCH>
+template <bool COUNT, bool BATCH, bool ENV>
 __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace_shadow(PathParams p) {
     VKB_STACK_DECL
     const uint32_t n = p.counters[2];
@@ -693,9 +781,15 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace_sha
         if (ph == 0u) {
             if ((flags & SH_TRACE_A) && L.start(BATCH ? p.jobs[job].sv : p.job0.sv, RayRef{p.sa_o, p.sa_d, e}, p.sa_o[e].w)) { phase = 0u; rid = e; return true; }
         }
-        if ((flags & SH_HAS_B) && (flags & SH_TRACE_B)) {
+        if (ph <= 1u && (flags & SH_HAS_B) && (flags & SH_TRACE_B)) {
             const uint32_t slot = __float_as_uint(p.sa_d[e].w);
             if (L.start(BATCH ? p.jobs[job].sv : p.job0.sv, RayRef{p.sb_o, p.sb_d, slot}, p.sb_o[slot].w)) { phase = 1u; rid = slot; return true; }
+        }
+        if constexpr (ENV) {
+            if (flags & SH_HAS_C) {
+                const uint32_t slot = __float_as_uint(p.sa_d[e].w);
+                if (L.start(BATCH ? p.jobs[job].sv : p.job0.sv, RayRef{p.sc_o, p.sc_d, slot}, p.sc_o[slot].w)) { phase = 2u; rid = slot; return true; }
+            }
         }
         return false;
     };
@@ -710,7 +804,15 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace_sha
         const float4 r = p.rad[slot];
         uint32_t dropped = __float_as_uint(r.w);
         const Job& J = BATCH ? p.jobs[job] : p.job0;
-        const float3 add = clamp_sample(total, (flags & SH_DIRECT) ? J.clamp_direct : J.clamp_indirect, dropped);
+        const float limit = (flags & SH_DIRECT) ? J.clamp_direct : J.clamp_indirect;
+        float3 add = clamp_sample(total, limit, dropped);
+        if constexpr (ENV) {
+            // The environment estimate is clamped on its own (path.slang:1661).
+            if ((flags & SH_HAS_C) && !(occ & 4u)) {
+                const float4 cc = p.sc_c[slot];
+                add = add + clamp_sample(f3(cc.x, cc.y, cc.z), limit, dropped);
+            }
+        }
         p.rad[slot] = make_float4(r.x + add.x, r.y + add.y, r.z + add.z, __uint_as_float(dropped));
         e = NONE;
     };
@@ -745,8 +847,9 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace_sha
             else done = L.step(p.job0.sv, ray, p.err, &tc, stk);
         }
         if (done) {
-            if (L.found) occ |= phase ? 2u : 1u;
-            if (phase != 0u || !begin(1u)) finish();
+            if (L.found) occ |= 1u << phase;
+            if constexpr (ENV) { if (phase == 2u || !begin(phase + 1u)) finish(); }
+            else { if (phase != 0u || !begin(1u)) finish(); }
         }
     }
     if (COUNT) {
@@ -893,7 +996,7 @@ __device__ __noinline__ void cache_append(const PathParams& p, float3 world, flo
 #define VKB_SHADE_MIN_BLOCKS 1
 #endif
 constexpr int SHADE_BLOCK = VKB_SHADE_BLOCK;
-template <bool BATCH>
+template <bool BATCH, bool ENV>
 __global__ void __launch_bounds__(VKB_SHADE_BLOCK, VKB_SHADE_MIN_BLOCKS) k_shade(const __grid_constant__ PathParams p, int cur) {
     const int nxt = cur ^ 1;
     uint32_t n = p.counters[cur];
@@ -929,13 +1032,19 @@ __global__ void __launch_bounds__(VKB_SHADE_BLOCK, VKB_SHADE_MIN_BLOCKS) k_shade
                 float3 sky;
                 if (ray_event == VKB_RAY_CAMERA && !J.env.camera_sees_environment) sky = get3(J.env.background);
                 else {
-                    sky = get3(J.env.radiance);
+                    sky = ENV ? env_radiance(J, dir) : get3(J.env.radiance);
                     if (ray_event == VKB_RAY_CAMERA)
                         for (uint32_t l = 0; l < J.num_lights; ++l) {
                             const vkb_light& L = J.lights[l];
                             if (L.position[3] != 0.f || !(L.shadow_offsets[0] & VKB_RAY_CAMERA)) continue;
                             sky = sky + emitter_eval(L, f3(0.f), dir).radiance;
                         }
+                }
+                if (ENV && J.env_w && bounce > 0u) {
+                    // path.slang:1463: an escape after a BSDF sample, weighed against the
+                    // environment strategy.
+                    const float prev = p.prev_pdf[slot];
+                    if (prev > 0.f) sky = sky * mis_power(prev, env_density(J, dir));
                 }
                 rad = rad + clamp_sample(thr * sky, limit, dropped);
             } else {
@@ -1002,10 +1111,48 @@ __global__ void __launch_bounds__(VKB_SHADE_BLOCK, VKB_SHADE_MIN_BLOCKS) k_shade
                             }
                         }
                     }
+                    // environment_next_event (path.slang:1096-1120): a proposal direction,
+                    // the diffuse and specular responses MIS-weighted against continuing
+                    // there (continuation_mask, path.slang:1003-1010), one visibility ray
+                    // to infinity; clamped on its own.
+                    bool trace_c = false;
+                    if (ENV && J.env_w) {
+                        uint32_t cont = 0u;
+                        if (bounce < J.bounces[0]) {
+                            if (diffuse < J.bounces[1]) cont |= VKB_RAY_DIFFUSE;
+                            if (glossy < J.bounces[2] && (diffuse == 0u || (J.caustics & 1u))) cont |= VKB_RAY_SPECULAR;
+                        }
+                        const float4 eu = sample_group(pseed, sidx, J.sample_mask, vertex_group(vtx, 3));   // path_environment
+                        float epdf = 0.f;
+                        const float3 edir = env_sample(J, eu.x, eu.y, epdf);
+                        float3 ev = f3(0.f);
+                        if (epdf > 0.f) {
+                            const float3 emitted = env_radiance(J, edir);
+                            if (maxc(emitted) > 0.f) {
+                                #pragma unroll
+                                for (int k = 0; k < 2; ++k) {
+                                    const uint32_t event = k == 0 ? VKB_RAY_DIFFUSE : VKB_RAY_SPECULAR;
+                                    if (!event_hemisphere(event, edir, s.face, s.geometric)) continue;
+                                    const float3 response = eval_mask(c, view, edir, event, pr);
+                                    if (maxc(response) <= 0.f) continue;
+                                    const float bpdf = (cont & event) ? pdf_mask(c, view, edir, event, pr) : 0.f;
+                                    ev = ev + emitted * response * (mis_power(epdf, bpdf) / epdf);
+                                }
+                            }
+                        }
+                        if (any_nonzero(ev)) {
+                            const float3 oc = path_origin(s, edir), cc = thr * ev;
+                            p.sc_o[slot] = make_float4(oc.x, oc.y, oc.z, FP32_MAX);
+                            p.sc_d[slot] = make_float4(edir.x, edir.y, edir.z, 0.f);
+                            p.sc_c[slot] = make_float4(cc.x, cc.y, cc.z, 0.f);
+                            trace_c = true;
+                        }
+                    }
                     float3 ca = thr * va, cb = thr * vb;
-                    if (trace_a || trace_b) {
+                    if (trace_a || trace_b || trace_c) {
                         push_shadow = true;
-                        uint32_t flags = (trace_a ? SH_TRACE_A : 0u) | (has_b ? SH_HAS_B : 0u) | (trace_b ? SH_TRACE_B : 0u) | (bounce == 0 ? SH_DIRECT : 0u);
+                        uint32_t flags = (trace_a ? SH_TRACE_A : 0u) | (has_b ? SH_HAS_B : 0u) | (trace_b ? SH_TRACE_B : 0u) | (bounce == 0 ? SH_DIRECT : 0u) |
+                                         (trace_c ? SH_HAS_C : 0u);
                         sh_o = make_float4(oa.x, oa.y, oa.z, la);
                         sh_d = make_float4(da.x, da.y, da.z, __uint_as_float(slot));
                         sh_c = make_float4(ca.x, ca.y, ca.z, __uint_as_float(flags));
@@ -1049,6 +1196,7 @@ __global__ void __launch_bounds__(VKB_SHADE_BLOCK, VKB_SHADE_MIN_BLOCKS) k_shade
                         new_o = make_float4(o.x, o.y, o.z, FP32_MAX);
                         new_d = make_float4(smp.dir.x, smp.dir.y, smp.dir.z, __uint_as_float(slot));
                         push_ray = true;
+                        if (ENV) p.prev_pdf[slot] = smp.pdf;
 #if VKB_SHADE_EARLY_APPEND
                         {
 #if VKB_SHADE_OCTANT_APPEND
