@@ -1033,6 +1033,13 @@ template <class R> struct Scene {
     double env_rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     std::vector<float> env_cdf, env_density;
     bool env_strategy() const { return env_w > 0 && env_strength > 0; }
+    // Emissive-mesh sources (emitters.rs:22-44): per instance its source index (~0u: none);
+    // per source its instance and the cumulative triangle count through it; the weight
+    // tree over the padded leaves (float, node 1 the root, leaves from em_leaves on).
+    std::vector<uint32_t> em_inst_source, em_src_inst, em_src_cum;
+    uint32_t em_tris = 0, em_leaves = 0;
+    std::vector<float> em_tree;
+    bool mesh_strategy() const { return !em_src_inst.empty(); }
 };
 // The proposal of an environment image (crates/vork-render/src/environment.rs:573-620):
 // per texel the 3x3 (1,2,1)^2/16 stencil of alpha-weighted RGB (columns wrap, rows clamp),
@@ -1074,6 +1081,152 @@ void env_distribution(const float* rgba, uint32_t dw, uint32_t dh, std::vector<f
         }
     }
 }
+// ---------------------------------------------------------------- emissive meshes
+// A material emits when emission_luminance > 0 and its colour is not black
+// (materials.rs:579-583); every instance drawn with such a material is a source, its
+// triangles counted in instance order (emitters.rs:22-44, opaque materials only).
+inline bool material_emits(const vkb_material& m) {
+    return m.emission_luminance > 0.f && (m.emission_color[0] != 0.f || m.emission_color[1] != 0.f || m.emission_color[2] != 0.f);
+}
+inline uint32_t emitter_leaves(uint32_t count) {                          // emitter_mesh_proposal.slang:12
+    uint32_t l = 1;
+    while (l < count) l <<= 1;
+    return l;
+}
+template <class R> void emitter_sources(Scene<R>& s) {
+    const uint32_t n = uint32_t(s.inst_mesh.size());
+    s.em_inst_source.assign(n, 0xffffffffu);
+    s.em_src_inst.clear(); s.em_src_cum.clear(); s.em_tris = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!material_emits(s.mats[s.inst_mat[i]])) continue;
+        s.em_tris += uint32_t(s.meshes[s.inst_mesh[i]].idx.size() / 3);
+        s.em_inst_source[i] = uint32_t(s.em_src_inst.size());
+        s.em_src_inst.push_back(i);
+        s.em_src_cum.push_back(s.em_tris);
+    }
+    s.em_leaves = s.em_src_inst.empty() ? 0u : emitter_leaves(s.em_tris);
+}
+// Source triangle -> (source, primitive) by binary search over the cumulative counts
+// (emitter_mesh_proposal.slang:13-22); a triangle past the last source (reachable only
+// through a zero-mass branch) maps to the last source.
+template <class R> void emitter_triangle(const Scene<R>& s, uint32_t triangle, uint32_t& source, uint32_t& primitive) {
+    uint32_t low = 0, high = uint32_t(s.em_src_inst.size());
+    while (low < high) {
+        const uint32_t mid = (low + high) / 2;
+        if (triangle < s.em_src_cum[mid]) high = mid; else low = mid + 1;
+    }
+    source = std::min(low, uint32_t(s.em_src_inst.size()) - 1u);
+    primitive = triangle - (source == 0 ? 0u : s.em_src_cum[source - 1]);
+}
+// Current world-space corners of a source triangle: the object corners, the edge vectors
+// and the point at barycentrics (b1, b2) (hit_geometry.slang:121-124, 246-256).
+template <class R> struct EmitterGeometry { V3<R> point, face; R area; };
+template <class R> EmitterGeometry<R> emitter_geometry(const Scene<R>& s, uint32_t inst, uint32_t prim, R b1, R b2) {
+    const MeshData<R>& m = s.meshes[s.inst_mesh[inst]];
+    const Affine<R>& M = s.model[inst];
+    const Affine<R>& I = s.inv[inst];
+    const uint32_t i0 = m.idx[3 * prim], i1 = m.idx[3 * prim + 1], i2 = m.idx[3 * prim + 2];
+    const V3<R> P[3] = {m.pos[i0], m.pos[i1], m.pos[i2]};
+    const V3<R> raw = cross(P[1] - P[0], P[2] - P[0]);
+    const V3<R> fobj = finite_unit_normal(raw, m.has_normals ? m.nrm[i0] : raw);
+    EmitterGeometry<R> g;
+    g.face = finite_unit_normal(I.tvec(fobj), V3<R>(0, 0, 1));
+    g.point = M.point(P[0] * (R(1) - b1 - b2) + P[1] * b1 + P[2] * b2);
+    g.area = length(cross(M.vec(P[1] - P[0]), M.vec(P[2] - P[0]))) * R(0.5);
+    return g;
+}
+// The frame's weight tree (emitter_weights.slang:23-55): leaf = world area x the
+// emission's Rec.709 luminance power (the area alone when that product is not finite),
+// padded leaves 0; an inner node stores the mean of its children.
+template <class R> void emitter_tree(Scene<R>& s) {
+    s.em_tree.assign(s.em_leaves ? 2 * size_t(s.em_leaves) : 0, 0.f);
+    if (!s.em_leaves) return;
+    for (uint32_t t = 0; t < s.em_tris; ++t) {
+        uint32_t src, prim;
+        emitter_triangle(s, t, src, prim);
+        const uint32_t inst = s.em_src_inst[src];
+        float area = float(emitter_geometry(s, inst, prim, R(0), R(0)).area);
+        if (area > 0.f) {
+            const vkb_material& mt = s.mats[s.inst_mat[inst]];
+            const float power = (std::max(mt.emission_color[0], 0.f) * float(LUM[0]) + std::max(mt.emission_color[1], 0.f) * float(LUM[1]) +
+                                 std::max(mt.emission_color[2], 0.f) * float(LUM[2])) * std::max(mt.emission_luminance, 0.f);
+            const float weight = area * power;
+            if (std::isfinite(weight)) area = weight;
+        }
+        s.em_tree[s.em_leaves + t] = area;
+    }
+    for (uint32_t node = s.em_leaves - 1; node >= 1; --node) s.em_tree[node] = 0.5f * s.em_tree[2 * node] + 0.5f * s.em_tree[2 * node + 1];
+}
+// Ratio of sibling masses under a shared power-of-two scale (emitter_mesh_proposal.slang:25-35).
+inline float emitter_left_probability(float left, float right) {
+    uint32_t bits;
+    const float top = std::max(left, right);
+    std::memcpy(&bits, &top, 4);
+    const int exponent = int((bits >> 23) & 255u) - 127;
+    const uint32_t sb = uint32_t(127 - exponent / 2) << 23;
+    float scale;
+    std::memcpy(&scale, &sb, 4);
+    left *= scale; right *= scale;
+    if (left >= right) return left > 0.f ? 1.f / (1.f + right / left) : 0.f;
+    const float ratio = left / right;
+    return ratio / (1.f + ratio);
+}
+constexpr float MESH_SOURCE_UNIFORM_MIX = 0.5f;   // registry.rs MESH_SOURCE_UNIFORM_MIX
+// The product of the branch probabilities from the leaf up, mixed half and half with the
+// uniform choice over all source triangles (emitter_mesh_proposal.slang:37-57).
+template <class R> float emitter_probability(const Scene<R>& s, uint32_t inst, uint32_t prim) {
+    if (!s.mesh_strategy() || s.em_inst_source[inst] == 0xffffffffu || !(s.em_tree[1] > 0.f)) return 0.f;
+    const uint32_t src = s.em_inst_source[inst];
+    uint32_t node = s.em_leaves + prim + (src == 0 ? 0u : s.em_src_cum[src - 1]);
+    float probability = 1.f;
+    bool zero = false;
+    while (node > 1) {
+        const uint32_t parent = node / 2;
+        const float left = s.em_tree[2 * parent], right = s.em_tree[2 * parent + 1];
+        if (std::max(left, right) <= 0.f) { zero = true; break; }
+        const float p = emitter_left_probability(left, right);
+        probability *= (node & 1u) ? 1.f - p : p;
+        node = parent;
+    }
+    const float weighted = zero ? 0.f : probability;
+    return (1.f - MESH_SOURCE_UNIFORM_MIX) * weighted + MESH_SOURCE_UNIFORM_MIX / float(s.em_tris);
+}
+// emitter_mesh_sample (emitter_mesh_proposal.slang:59-83): u = path_triangle (the vertex's
+// group 2 as .zxy): x picks the triangle, y the radius, z the strategy and the split.
+template <class R> bool emitter_sample(const Scene<R>& s, const float u[3], uint32_t& inst, uint32_t& prim, float& b1, float& b2) {
+    const float top = 0x1.fffffep-1f;
+    float choice = std::min(u[0], top);
+    uint32_t node = 1;
+    if (!(s.em_tree[1] > 0.f)) return false;
+    const bool uniform = u[2] < MESH_SOURCE_UNIFORM_MIX;
+    const float point = (u[2] - (uniform ? 0.f : MESH_SOURCE_UNIFORM_MIX)) / (uniform ? MESH_SOURCE_UNIFORM_MIX : 1.f - MESH_SOURCE_UNIFORM_MIX);
+    if (uniform) node = s.em_leaves + std::min(uint32_t(choice * float(s.em_tris)), s.em_tris - 1u);
+    else
+        while (node < s.em_leaves) {
+            const float p = emitter_left_probability(s.em_tree[2 * node], s.em_tree[2 * node + 1]);
+            if (choice < p) { choice /= p; node *= 2; }
+            else { choice = (choice - p) / (1.f - p); node = 2 * node + 1; }
+            choice = std::min(choice, top);
+        }
+    uint32_t src;
+    emitter_triangle(s, node - s.em_leaves, src, prim);
+    inst = s.em_src_inst[src];
+    const float radius = std::sqrt(u[1]);
+    b1 = radius * (1.f - point);
+    b2 = radius - b1;
+    return true;
+}
+// emitter_mesh_pdf x the triangle's probability (path.slang:996-1002, emitter_mesh_proposal.slang:86-92):
+// the solid-angle density at `from` of the point on a source triangle.
+template <class R> R mesh_pdf(const Scene<R>& s, uint32_t inst, uint32_t prim, R area, V3<R> from, V3<R> point, V3<R> face) {
+    if (!s.mesh_strategy() || s.em_inst_source[inst] == 0xffffffffu) return 0;
+    const V3<R> delta = point - from;
+    const R squared = dot(delta, delta);
+    const R cosine = std::fabs(dot(face, normalize(delta)));
+    const R density = area > 0 && cosine > 0 ? squared / (area * cosine) : R(0);
+    return density * R(emitter_probability(s, inst, prim));
+}
+
 template <class R> Scene<R>* make_scene(const vkb_scene_desc* d) {
     Scene<R>* s = new Scene<R>();
     s->meshes.resize(d->num_meshes);
@@ -1119,6 +1272,8 @@ template <class R> Scene<R>* make_scene(const vkb_scene_desc* d) {
         if (any) for (int k = 0; k < 9; ++k) s->env_rot[k] = double(e.rotation[k]);
         env_distribution(e.rgba, e.width, e.height, s->env_cdf, s->env_density);
     }
+    emitter_sources(*s);
+    emitter_tree(*s);
     return s;
 }
 struct Hit { double t = -1; uint32_t inst = 0xffffffffu, prim = 0xffffffffu; double u = 0, v = 0; };
@@ -1497,6 +1652,7 @@ template <class R> V3<R> integrate(Ctx<R>& cx, uint32_t px, uint32_t py, uint32_
     V3<R> throughput(1, 1, 1), radiance;
     uint32_t ray_event = VKB_RAY_CAMERA, diffuse = 0, glossy = 0, groups = 0;
     R previous_pdf = 0;                                                   // path.slang:1326,1699
+    V3<R> previous_world = origin;
     bool nonfinite = false;
     uint64_t dropped = 0;
     const uint32_t B = pf.bounces[0];
@@ -1542,6 +1698,17 @@ template <class R> V3<R> integrate(Ctx<R>& cx, uint32_t px, uint32_t py, uint32_
             guide[0] = a.x; guide[1] = a.y; guide[2] = a.z; guide[3] = 1;
             guide[4] = c.n.x; guide[5] = c.n.y; guide[6] = c.n.z; guide[7] = 0;
         }
+        if (material_emits(mt) && ((mt.flags & 2u) || hs.entering)) {
+            // Surface emission (path.slang:1580-1591) on the side the material covers,
+            // weighed against the mesh strategy after a BSDF sample.
+            const V3<R> emitted = V3<R>(mt.emission_color[0], mt.emission_color[1], mt.emission_color[2]) * R(mt.emission_luminance);
+            R mis = 1;
+            if (previous_pdf > 0) {
+                const R area = emitter_geometry(s, h.inst, h.prim, R(0), R(0)).area;
+                mis = mis_power(previous_pdf, mesh_pdf(s, h.inst, h.prim, area, previous_world, hs.world, hs.face));
+            }
+            radiance = radiance + clamp_sample(throughput * emitted * mis, limit, dropped);
+        }
         V3<R> iface = dot(hs.geometric, view) > 0 ? hs.geometric : hs.face;
         Prepared<R> pr = transport_prepare(c, view, hs.geometric, iface);
         BsdfSample<R> smp = transport_sample(c, view, R(sc[0]), R(sc[1]), R(sc[2]), pr);
@@ -1575,6 +1742,51 @@ template <class R> V3<R> integrate(Ctx<R>& cx, uint32_t px, uint32_t py, uint32_
             }
             radiance = radiance + clamp_sample(throughput * env_value, limit, dropped);
         }
+        if (s.mesh_strategy()) {
+            // mesh_next_event (path.slang:1121-1167), constant emission: a point on a source
+            // triangle, the diffuse and specular responses MIS-weighted against continuing
+            // there, one visibility ray between the offset end points; clamped on its own.
+            uint32_t cont = 0;
+            if (bounce < B) {
+                if (diffuse < pf.bounces[1]) cont |= VKB_RAY_DIFFUSE;
+                if (glossy < pf.bounces[2] && (diffuse == 0 || (pf.caustics & 1u))) cont |= VKB_RAY_SPECULAR;
+            }
+            float g[4];
+            vertex_group(sm, 2, g);                                       // path_triangle (.zxy)
+            const float u[3] = {g[2], g[0], g[1]};
+            uint32_t ei, ep; float b1, b2;
+            V3<R> mesh_value;
+            if (emitter_sample(s, u, ei, ep, b1, b2)) {
+                const EmitterGeometry<R> eg = emitter_geometry(s, ei, ep, R(b1), R(b2));
+                const V3<R> delta = eg.point - hs.world;
+                const R distance = length(delta);
+                if (distance > 0) {
+                    const V3<R> axis = delta / distance;
+                    const R pdf = mesh_pdf(s, ei, ep, eg.area, hs.world, eg.point, eg.face);
+                    const vkb_material& em = s.mats[s.inst_mat[ei]];
+                    const bool entering = dot(eg.face, axis) < 0;
+                    const V3<R> emitted = V3<R>(em.emission_color[0], em.emission_color[1], em.emission_color[2]) * R(em.emission_luminance);
+                    if (pdf > 0 && ((em.flags & 2u) || entering) && maxc(emitted) > 0) {
+                        const V3<R> start = path_origin(hs, axis);
+                        const V3<R> end = surface_ray_origin(eg.point, position_error(s, ei, eg.point), entering ? eg.face : -eg.face, -axis);
+                        const V3<R> connection = end - start;
+                        const R extent = length(connection);
+                        V3<R> response;
+                        if (extent > 0)
+                            for (uint32_t event : {uint32_t(VKB_RAY_DIFFUSE), uint32_t(VKB_RAY_SPECULAR)}) {
+                                if (!event_hemisphere(event, axis, hs.face, hs.geometric)) continue;
+                                const V3<R> f = eval_mask(c, view, axis, event, pr);
+                                if (maxc(f) <= 0) continue;
+                                const R bsdf_pdf = (cont & event) ? pdf_mask(c, view, axis, event, pr) : R(0);
+                                response = response + f * mis_power(pdf, bsdf_pdf);
+                            }
+                        if (any_nonzero(response) && occluded(cx, start, connection / extent, extent)) response = V3<R>();
+                        mesh_value = response * emitted / pdf;
+                    }
+                }
+            }
+            radiance = radiance + clamp_sample(throughput * mesh_value, limit, dropped);
+        }
         if (bounce == B) break;
         uint32_t event = smp.event;
         ray_event = event;
@@ -1595,6 +1807,7 @@ template <class R> V3<R> integrate(Ctx<R>& cx, uint32_t px, uint32_t py, uint32_
         dir = smp.dir;
         origin = path_origin(hs, dir);
         previous_pdf = smp.pdf;
+        previous_world = hs.world;
         bounce++;
     }
     cx.dropped_light += dropped;
@@ -1952,6 +2165,27 @@ void oracle_env_sample(void* h, int fp64, uint32_t n, const float* u2, float* di
             dir3[3 * i] = d.x; dir3[3 * i + 1] = d.y; dir3[3 * i + 2] = d.z; pdf[i] = p;
         }
     }
+}
+// Emissive-mesh proposal of the fp32 scene: the weight tree (2 x leaves floats), source
+// samples (instance, primitive, barycentrics, probability) and triangle probabilities.
+uint32_t oracle_mesh_tree(void* h, float* out) {
+    const Scene<float>& s = *static_cast<Scene<float>*>(static_cast<OracleScene*>(h)->s32);
+    if (out) std::copy(s.em_tree.begin(), s.em_tree.end(), out);
+    return s.em_leaves;
+}
+uint32_t oracle_mesh_triangles(void* h) { return static_cast<Scene<float>*>(static_cast<OracleScene*>(h)->s32)->em_tris; }
+void oracle_mesh_sample(void* h, uint32_t n, const float* u3, uint32_t* inst, uint32_t* prim, float* bary2, float* probability) {
+    const Scene<float>& s = *static_cast<Scene<float>*>(static_cast<OracleScene*>(h)->s32);
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t a = 0xffffffffu, b = 0xffffffffu; float b1 = 0.f, b2 = 0.f;
+        const bool ok = s.mesh_strategy() && emitter_sample(s, u3 + 3 * i, a, b, b1, b2);
+        inst[i] = a; prim[i] = b; bary2[2 * i] = b1; bary2[2 * i + 1] = b2;
+        probability[i] = ok ? emitter_probability(s, a, b) : 0.f;
+    }
+}
+void oracle_mesh_probability(void* h, uint32_t n, const uint32_t* inst, const uint32_t* prim, float* out) {
+    const Scene<float>& s = *static_cast<Scene<float>*>(static_cast<OracleScene*>(h)->s32);
+    for (uint32_t i = 0; i < n; ++i) out[i] = emitter_probability(s, inst[i], prim[i]);
 }
 void oracle_env_eval(void* h, uint32_t n, const float* dir3, float* pdf, float* rgb) {
     const Scene<double>& s = *static_cast<Scene<double>*>(static_cast<OracleScene*>(h)->s64);

@@ -58,6 +58,12 @@ def lib():
         l.oracle_set_lut.argtypes = [f32p]
         l.oracle_env_sample.argtypes = [P, C.c_int, C.c_uint32, f32p, f32p, f32p]
         l.oracle_env_eval.argtypes = [P, C.c_uint32, f32p, f32p, f32p]
+        l.oracle_mesh_tree.argtypes = [P, f32p]
+        l.oracle_mesh_tree.restype = C.c_uint32
+        l.oracle_mesh_triangles.argtypes = [P]
+        l.oracle_mesh_triangles.restype = C.c_uint32
+        l.oracle_mesh_sample.argtypes = [P, C.c_uint32, f32p, u32p, u32p, f32p, f32p]
+        l.oracle_mesh_probability.argtypes = [P, C.c_uint32, u32p, u32p, f32p]
         _lib = l
     return _lib
 
@@ -190,6 +196,31 @@ class OracleScene:
         p = np.zeros(len(d), np.float32); rgb = np.zeros((len(d), 3), np.float32)
         lib().oracle_env_eval(self.h, len(d), _p(d, C.c_float), _p(p, C.c_float), _p(rgb, C.c_float))
         return p, rgb
+
+    def mesh_tree(self):
+        """The emissive-mesh weight tree (2 x leaves floats, node 1 the root) and its leaf count."""
+        leaves = lib().oracle_mesh_tree(self.h, None)
+        out = np.zeros(2 * leaves, np.float32)
+        if leaves:
+            lib().oracle_mesh_tree(self.h, _p(out, C.c_float))
+        return out, leaves
+
+    def mesh_triangles(self):
+        return int(lib().oracle_mesh_triangles(self.h))
+
+    def mesh_sample(self, u3):
+        """Source samples for uniforms u (n,3): (instance, primitive, barycentrics (n,2), probability)."""
+        u = np.ascontiguousarray(u3, np.float32).reshape(-1, 3)
+        n = len(u)
+        inst = np.zeros(n, np.uint32); prim = np.zeros(n, np.uint32); b = np.zeros((n, 2), np.float32); pr = np.zeros(n, np.float32)
+        lib().oracle_mesh_sample(self.h, n, _p(u, C.c_float), _p(inst, C.c_uint32), _p(prim, C.c_uint32), _p(b, C.c_float), _p(pr, C.c_float))
+        return inst, prim, b, pr
+
+    def mesh_probability(self, inst, prim):
+        i = np.ascontiguousarray(inst, np.uint32); q = np.ascontiguousarray(prim, np.uint32)
+        out = np.zeros(len(i), np.float32)
+        lib().oracle_mesh_probability(self.h, len(i), _p(i, C.c_uint32), _p(q, C.c_uint32), _p(out, C.c_float))
+        return out
 
     def camera_rays(self, profile, index, x0=0, y0=0, w=None, h=None):
         cam = self.scene.camera

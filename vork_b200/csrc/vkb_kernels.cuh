@@ -842,7 +842,10 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace_sha
         }
         bool done = false;
         if (e != NONE) {
-            const RayRef ray{phase ? p.sb_o : p.sa_o, phase ? p.sb_d : p.sa_d, rid};
+            // The traversal re-reads its ray (instance entry, return to world space):
+            // phase 0 the light ray A, 1 the light ray B, 2 the environment ray.
+            RayRef ray{phase ? p.sb_o : p.sa_o, phase ? p.sb_d : p.sa_d, rid};
+            if constexpr (ENV) { if (phase == 2u) ray = RayRef{p.sc_o, p.sc_d, rid}; }
             if constexpr (BATCH) done = L.step(p.jobs[job].sv, ray, p.err, &tc, stk);
             else done = L.step(p.job0.sv, ray, p.err, &tc, stk);
         }

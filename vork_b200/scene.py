@@ -176,6 +176,17 @@ def material(base_color=(0.8, 0.8, 0.8), roughness=0.3, metalness=0.0, double_si
     return m
 
 
+def emissive(color=(1.0, 1.0, 1.0), luminance=1.0, double_sided=False) -> abi.VkbMaterial:
+    """A black surface emitting colour x luminance (OpenPBR emission_color, emission_luminance)
+    on its front side, or on both sides when double sided."""
+    m = material((0.0, 0.0, 0.0), 1.0, 0.0, double_sided)
+    m.base_weight = 0.0
+    m.specular_weight = 0.0
+    m.emission_luminance = float(luminance)
+    m.emission_color[:] = [float(v) for v in color]
+    return m
+
+
 ALL_RAYS = abi.RAY_CAMERA | abi.RAY_SHADOW | abi.RAY_DIFFUSE | abi.RAY_SPECULAR | abi.RAY_TRANSMISSION | abi.RAY_VOLUME
 
 
@@ -394,6 +405,34 @@ def spheres_scene(num_spheres: int = 64, seed: int = 0, width: int = 256, height
 
 
 # ----------------------------------------------------------------------------- plain method, large
+def lamp_scene(width: int = 128, height: int = 96, seed: int = 0, lamps: int = 3, spheres: int = 8, double_sided=False):
+    """A floor with diffuse and glossy spheres lit by emissive quads facing down and one
+    small emissive sphere (no analytic lights, black world): every light comes through
+    surface emission and the mesh next-event strategy."""
+    rng = np.random.default_rng(seed)
+    meshes = [grid((12.0, 12.0), (4, 4)), grid((1.0, 1.0), (2, 2)), uv_sphere(1.0)]
+    rows, mesh_ids, mat_ids = [rows_from(1.0, (0.0, 0.0, 0.0))], [0], [0]
+    materials = [material((0.75, 0.75, 0.75), 0.8, 0.0)]
+    for k in range(lamps):
+        w, d = rng.uniform(0.6, 1.8, 2)
+        r = np.zeros((3, 4), np.float32)
+        r[0, 0], r[1, 1], r[2, 2] = w, -1.0, -d          # scale in x/z, flipped to face -Y (det > 0)
+        r[:, 3] = (rng.uniform(-3.5, 3.5), rng.uniform(2.5, 4.0), rng.uniform(-3.5, 3.5))
+        rows.append(r); mesh_ids.append(1); mat_ids.append(len(materials))
+        materials.append(emissive(tuple(rng.uniform(0.4, 1.0, 3)), float(rng.uniform(4.0, 20.0)), double_sided))
+    rows.append(rows_from(0.3, (rng.uniform(-2.0, 2.0), 1.2, rng.uniform(-2.0, 2.0))))
+    mesh_ids.append(2); mat_ids.append(len(materials))
+    materials.append(emissive((1.0, 0.6, 0.3), 30.0))
+    for k in range(spheres):
+        rad = float(rng.uniform(0.3, 0.8))
+        rows.append(rows_from(rad, (rng.uniform(-4.0, 4.0), rad, rng.uniform(-4.0, 4.0))))
+        mesh_ids.append(2); mat_ids.append(len(materials))
+        materials.append(material(tuple(rng.uniform(0.2, 0.9, 3)), float(rng.uniform(0.1, 0.7)), float(k % 3 == 0)))
+    cam = look_at((0.0, 5.5, 9.0), (0.0, 0.8, 0.0), width=width, height=height, fov_y_degrees=50)
+    return Scene(meshes, np.stack(rows).astype(np.float32), np.asarray(mesh_ids, np.uint32), np.asarray(mat_ids, np.uint32),
+                 materials, [], cam, environment((0.0, 0.0, 0.0)), name="lamps")
+
+
 def value_noise_heights(cells: int, size: float, seed: int = 0, amplitude: float = 30.0, octaves: int = 6) -> np.ndarray:
     """(cells+1)^2 heights of seeded fBm value noise (smoothstep-interpolated lattice values)."""
     rng = np.random.default_rng(seed)
