@@ -69,7 +69,13 @@ typedef struct vkb_material {
     float specular_color[3];
     float specular_roughness;
     float specular_ior;
-    float emission_luminance;  /* must be 0: emissive meshes are outside the built subset */
+    /* Emission: radiance emission_color x emission_luminance on the front side (both sides
+     * when double sided), finite and >= 0.  Every instance drawn with emission_luminance > 0
+     * and a non-black colour is a mesh light source: its triangles are sampled by the mesh
+     * next-event strategy (area x luminance power, half uniform; emitters.rs:22-44,
+     * emitter_mesh_proposal.slang) and its hits are weighed against it by MIS
+     * (path.slang:1121-1167,1580-1591). */
+    float emission_luminance;
     float emission_color[3];
     uint32_t flags;            /* bit 1: double sided (registry FLAG_DOUBLE_SIDED) */
 } vkb_material;

@@ -296,8 +296,10 @@ struct WaveBuffers {
     unsigned long long* work = nullptr;
     Job* jobs = nullptr;
     float4* guide = nullptr;   // guide renders: 2 float4 per path slot
-    float4 *sc_o = nullptr, *sc_d = nullptr, *sc_c = nullptr;   // image-environment waves: the third shadow ray
-    float* prev_pdf = nullptr;
+    // Waves with an image environment or emissive meshes: the environment and mesh shadow
+    // rays of every slot and its previous vertex + BSDF pdf.
+    float4 *sc_o = nullptr, *sc_d = nullptr, *sc_c = nullptr, *sd_o = nullptr, *sd_d = nullptr, *sd_c = nullptr;
+    float4* prev = nullptr;
 };
 // The context's own wavefront storage (grown on demand, reused by every render).
 struct Wavefront {
@@ -306,19 +308,20 @@ struct Wavefront {
     DBuf<uint2> rng;
     DBuf<unsigned long long> work;
     DBuf<Job> jobs;
-    DBuf<float4> sc_o, sc_d, sc_c;     // image-environment waves only (allocated on first need)
-    DBuf<float> prev_pdf;
+    DBuf<float4> sc_o, sc_d, sc_c, sd_o, sd_d, sd_c, prev;   // EXT waves only (allocated on first need)
     uint64_t generation = 0;  // bumps when a buffer moves (captured graphs refer to the old ones)
-    // The third shadow ray and previous pdf of every slot, for waves with an image environment.
-    void reserve_env(size_t slots) {
+    // The environment and mesh shadow rays and the previous vertex of every slot, for waves
+    // with an image environment or emissive meshes (112 B per slot).
+    void reserve_ext(size_t slots) {
         if (slots > sc_o.n) {
-            sc_o.alloc(slots); sc_d.alloc(slots); sc_c.alloc(slots); prev_pdf.alloc(slots);
+            DBuf<float4>* f4[] = {&sc_o, &sc_d, &sc_c, &sd_o, &sd_d, &sd_c, &prev};
+            for (auto* b : f4) b->alloc(slots);
             generation++;
         }
     }
     WaveBuffers view() const {
         WaveBuffers w;
-        w.sc_o = sc_o.p; w.sc_d = sc_d.p; w.sc_c = sc_c.p; w.prev_pdf = prev_pdf.p;
+        w.sc_o = sc_o.p; w.sc_d = sc_d.p; w.sc_c = sc_c.p; w.sd_o = sd_o.p; w.sd_d = sd_d.p; w.sd_c = sd_c.p; w.prev = prev.p;
         w.capacity = ray_o0.n; w.job_capacity = uint32_t(jobs.n);
         w.ray_o0 = ray_o0.p; w.ray_d0 = ray_d0.p; w.ray_o1 = ray_o1.p; w.ray_d1 = ray_d1.p; w.hit = hit.p; w.thr = thr.p; w.rad = rad.p;
         w.sa_o = sa_o.p; w.sa_d = sa_d.p; w.sa_c = sa_c.p; w.sb_o = sb_o.p; w.sb_d = sb_d.p; w.sb_c = sb_c.p;
@@ -330,16 +333,16 @@ struct Wavefront {
             DBuf<float4>* f4[] = {&ray_o0, &ray_d0, &ray_o1, &ray_d1, &hit, &thr, &rad, &sa_o, &sa_d, &sa_c, &sb_o, &sb_d, &sb_c};
             for (auto* b : f4) b->alloc(slots);
             hit_inst.alloc(slots); slot_job.alloc(slots); rng.alloc(slots);
-            if (sc_o.p) reserve_env(slots);
+            if (sc_o.p) reserve_ext(slots);
             generation++;
         }
         if (!counters.p) { counters.alloc(16); err.alloc(1); work.alloc(8); generation++; }
         if (njobs > jobs.n) { jobs.alloc(std::max<size_t>(njobs, 16)); generation++; }
     }
     void release() {
-        DBuf<float4>* f4[] = {&ray_o0, &ray_d0, &ray_o1, &ray_d1, &hit, &thr, &rad, &sa_o, &sa_d, &sa_c, &sb_o, &sb_d, &sb_c, &sc_o, &sc_d, &sc_c};
+        DBuf<float4>* f4[] = {&ray_o0, &ray_d0, &ray_o1, &ray_d1, &hit, &thr, &rad, &sa_o, &sa_d, &sa_c, &sb_o, &sb_d, &sb_c,
+                              &sc_o, &sc_d, &sc_c, &sd_o, &sd_d, &sd_c, &prev};
         for (auto* b : f4) b->release();
-        prev_pdf.release();
         hit_inst.release(); slot_job.release(); rng.release(); counters.release(); err.release(); work.release(); jobs.release();
     }
 };
@@ -409,6 +412,12 @@ struct vkb_scene {
     uint32_t env_w = 0, env_h = 0;
     float env_scale[3] = {0.f, 0.f, 0.f};
     float env_rot[9] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};
+    // Emissive meshes (em_tris == 0: none): the source topology (shared with forks) and
+    // the weight tree (each scene's own: it follows its instance rows).
+    DBuf<uint32_t> em_inst_source;
+    DBuf<uint2> em_sources;
+    DBuf<float> em_tree;
+    uint32_t em_count = 0, em_tris = 0, em_leaves = 0;
 };
 
 namespace {
@@ -487,6 +496,7 @@ std::vector<float2> env_proposal(const float* rgba, uint32_t dw, uint32_t dh) {
 // Instance rows -> w2o, world boxes, TLAS and its leaf records.  The TLAS is the
 // Karras LBVH or a PLOC tree over the instance boxes in Morton order (the scene's
 // tlas_builder); both keep parent links for refits.
+void build_emitter_tree(vkb_scene* s);
 void build_tlas(vkb_scene* s) {
     cudaStream_t st = s->ctx->stream;
     int sms = s->ctx->sms;
@@ -516,9 +526,53 @@ void build_tlas(vkb_scene* s) {
     VKB_CUDA(cudaMemcpyAsync(s->tlas_codes.p, s->scratch.codes.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     VKB_CUDA(cudaMemcpyAsync(s->tlas_order.p, s->scratch.ids_sorted.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     s->tlas_rebuilds++;
+    build_emitter_tree(s);
     VKB_CUDA(cudaEventRecord(s->ev1, st));
     VKB_CUDA(cudaEventSynchronize(s->ev1));
     VKB_CUDA(cudaEventElapsedTime(&s->build_ms, s->ev0, s->ev1));
+}
+
+// The mesh-source weight tree at the scene's current instance rows: the leaves, the
+// large inner levels one launch each, the top levels (<= 1024 nodes) in one block.
+void build_emitter_tree(vkb_scene* s) {
+    if (!s->em_tris) return;
+    cudaStream_t st = s->ctx->stream;
+    const int sms = s->ctx->sms;
+    Job j{};
+    j.o2w = s->o2w.p; j.w2o = s->w2o.p; j.inst_info = s->inst_info.p; j.meshes = s->meshes.p; j.materials = s->d_materials.p;
+    j.em_inst_source = s->em_inst_source.p; j.em_sources = s->em_sources.p; j.indices = s->indices.p; j.vpos = s->vpos.p;
+    j.em_count = s->em_count; j.em_tris = s->em_tris; j.em_leaves = s->em_leaves;
+    k_em_leaves<<<grid_for(s->em_leaves, 256, sms), 256, 0, st>>>(j, s->em_tree.p);
+    s->launches++;
+    uint32_t first = s->em_leaves / 2u;
+    for (; first > 1024u; first >>= 1) { k_em_reduce<<<grid_for(first, 256, sms), 256, 0, st>>>(s->em_tree.p, first); s->launches++; }
+    if (first >= 1u) { k_em_reduce_top<<<1, 1024, 0, st>>>(s->em_tree.p, first); s->launches++; }
+    VKB_CUDA(cudaGetLastError());
+}
+// Emissive-mesh sources (emitters.rs:22-44): every instance drawn with a material whose
+// emission_luminance > 0 and colour is not black, its triangles counted in instance order.
+void emitter_topology(vkb_scene* s, cudaStream_t str) {
+    std::vector<uint32_t> inst_source(s->num_instances, 0xffffffffu);
+    std::vector<uint2> sources;
+    uint64_t tris = 0;
+    for (uint32_t i = 0; i < s->num_instances; ++i) {
+        const vkb_material& m = s->materials[s->inst_mat[i]];
+        if (!(m.emission_luminance > 0.f && (m.emission_color[0] != 0.f || m.emission_color[1] != 0.f || m.emission_color[2] != 0.f))) continue;
+        const uint32_t nt = s->mesh_info[s->inst_mesh[i]].num_triangles;
+        if (!nt) continue;
+        tris += nt;
+        if (tris > (uint64_t(1) << 30)) throw Unsupported{"more than 2^30 emissive triangles"};
+        inst_source[i] = uint32_t(sources.size());
+        sources.push_back(make_uint2(i, uint32_t(tris)));
+    }
+    if (sources.empty()) return;
+    s->em_count = uint32_t(sources.size());
+    s->em_tris = uint32_t(tris);
+    s->em_leaves = 1u;
+    while (s->em_leaves < s->em_tris) s->em_leaves <<= 1;
+    s->em_inst_source.upload(inst_source.data(), inst_source.size(), str);
+    s->em_sources.upload(sources.data(), sources.size(), str);
+    s->em_tree.alloc(2 * size_t(s->em_leaves));
 }
 
 // Refit the TLAS in place: new instance boxes and world->object rows, same topology.
@@ -541,6 +595,7 @@ void refit_tlas(vkb_scene* s) {
     k_collapse4<<<grid_for(ni, 256, sms), 256, 0, st>>>(ni, s->tlas_nodes.p, s->tlas_odd.p, s->tlas4.p);
     s->launches += 4;
     VKB_CUDA(cudaGetLastError());
+    build_emitter_tree(s);
     VKB_CUDA(cudaEventRecord(s->ev1, st));
     VKB_CUDA(cudaEventSynchronize(s->ev1));
     VKB_CUDA(cudaEventElapsedTime(&s->build_ms, s->ev0, s->ev1));
@@ -574,8 +629,12 @@ void validate_desc(const vkb_scene_desc* d) {
         if (d->instance_mesh[i] >= d->num_meshes) throw ArgError{"instance mesh index out of range"};
         if (d->instance_material[i] >= d->num_materials) throw ArgError{"instance material index out of range"};
     }
-    for (uint32_t m = 0; m < d->num_materials; ++m)
-        if (d->materials[m].emission_luminance != 0.f) throw Unsupported{"emissive materials are outside the built subset"};
+    for (uint32_t m = 0; m < d->num_materials; ++m) {
+        const vkb_material& mt = d->materials[m];
+        if (!(mt.emission_luminance >= 0.f) || !std::isfinite(mt.emission_luminance)) throw ArgError{"emission luminance must be finite and non-negative"};
+        for (int k = 0; k < 3; ++k)
+            if (!std::isfinite(mt.emission_color[k])) throw ArgError{"emission colour must be finite"};
+    }
     for (uint32_t l = 0; l < d->num_lights; ++l) {
         float k = d->lights[l].position[3];
         if (!(k == 0.f || k == 1.f || k == 2.f || k == 3.f)) throw ArgError{"light kind must be 0..3"};
@@ -666,6 +725,9 @@ Job make_job(const EngineJob& e) {
     j.env_img = s->env_img.p; j.env_dist = s->env_dist.p; j.env_w = s->env_w; j.env_h = s->env_h;
     for (int k = 0; k < 3; ++k) j.env_scale[k] = s->env_scale[k];
     for (int k = 0; k < 9; ++k) j.env_rot[k] = s->env_rot[k];
+    j.em_inst_source = s->em_inst_source.p; j.em_sources = s->em_sources.p; j.em_tree = s->em_tree.p;
+    j.indices = s->indices.p; j.vpos = s->vpos.p;
+    j.em_count = s->em_count; j.em_tris = s->em_tris; j.em_leaves = s->em_leaves;
     return j;
 }
 
@@ -678,7 +740,7 @@ PathParams path_params(const vkb_ctx* c, const WaveBuffers& w, uint32_t njobs) {
     p.sa_o = w.sa_o; p.sa_d = w.sa_d; p.sa_c = w.sa_c; p.sb_o = w.sb_o; p.sb_d = w.sb_d; p.sb_c = w.sb_c;
     p.counters = w.counters; p.work = w.work; p.err = w.err;
     p.guide = w.guide;
-    p.sc_o = w.sc_o; p.sc_d = w.sc_d; p.sc_c = w.sc_c; p.prev_pdf = w.prev_pdf;
+    p.sc_o = w.sc_o; p.sc_d = w.sc_d; p.sc_c = w.sc_c; p.sd_o = w.sd_o; p.sd_d = w.sd_d; p.sd_c = w.sd_c; p.prev = w.prev;
     return p;
 }
 
@@ -696,7 +758,7 @@ struct CacheLaunch {
 // mode records events around every closest-hit trace.
 template <bool BATCH>
 void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counted, bool timed, WaveTotals& tot,
-                  const CacheLaunch* cache = nullptr, bool env = false) {
+                  const CacheLaunch* cache = nullptr, bool ext = false) {
     cudaStream_t st = c->stream;
     const int sms = c->sms, tgrid = sms * c->trace_blocks_per_sm, sgrid = sms * c->trace_blocks_per_sm;
     const bool adaptive = !BATCH && p.job0.adaptive;
@@ -719,9 +781,9 @@ void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counte
         tot.trace_launches++;
         if (!BATCH && b == 0u && p.guide) { k_guides<<<sms * 8, 256, 0, st>>>(p); tot.launches += 1; }
         k_reset_queues<<<1, 1, 0, st>>>(p.counters, cur ^ 1);
-        // Waves with an image environment run the kernels that sample it (a third shadow
-        // ray per vertex); the others keep the plain ones.
-        if (env) {
+        // Waves with an image environment or emissive meshes run the kernels with their
+        // strategies (two more shadow rays per vertex); the others keep the plain ones.
+        if (ext) {
             k_shade<BATCH, true><<<sgrid, SHADE_BLOCK, 0, st>>>(p, cur);
             if (counted) k_trace_shadow<true, BATCH, true><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
             else k_trace_shadow<false, BATCH, true><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
@@ -892,16 +954,16 @@ struct WaveEngine {
         VKB_CUDA(cudaMemcpyAsync(w.counters + 7, wave_counts, sizeof(wave_counts), cudaMemcpyHostToDevice, st));
         PathParams p = path_params(c, w, wave_jobs);
         p.job0 = wave_table[0];
-        bool env = false;
-        for (const Job& j : wave_table) env = env || j.env_w != 0u;
-        if (env && !w.sc_o) throw InternalError{"image-environment wave without its shadow buffers"};
+        bool ext = false;
+        for (const Job& j : wave_table) ext = ext || j.env_w != 0u || j.em_tris != 0u;
+        if (ext && !w.sc_o) throw InternalError{"environment or emissive-mesh wave without its shadow buffers"};
         if (cache) {
             if (batch) throw ArgError{"radiance-cache renders take one job"};
             p.cache = cache->dev;
         }
         if (use_graph) {
             uint64_t key = (uint64_t(bounces) << 1) | 1u;
-            key = key * 1315423911ull + (counted ? 7u : 3u) + (env ? 11u : 0u);
+            key = key * 1315423911ull + (counted ? 7u : 3u) + (ext ? 11u : 0u);
             key = key * 40503ull + wave_jobs;
             key = key * 97ull + uint64_t(c->trace_blocks_per_sm);
             cudaGraphExec_t exec = nullptr;
@@ -910,7 +972,7 @@ struct WaveEngine {
                 cudaGraph_t g;
                 VKB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
                 WaveTotals scratch;
-                wave_kernels<true>(c, p, bounces, counted, false, scratch, nullptr, env);
+                wave_kernels<true>(c, p, bounces, counted, false, scratch, nullptr, ext);
                 VKB_CUDA(cudaStreamEndCapture(st, &g));
                 VKB_CUDA(cudaGraphInstantiate(&exec, g, 0));
                 VKB_CUDA(cudaGraphDestroy(g));
@@ -920,9 +982,9 @@ struct WaveEngine {
             tot.launches += 3 + 4 * (bounces + 1);
             tot.trace_launches += bounces + 1;
         } else if (batch) {
-            wave_kernels<true>(c, p, bounces, counted, timed, tot, nullptr, env);
+            wave_kernels<true>(c, p, bounces, counted, timed, tot, nullptr, ext);
         } else {
-            wave_kernels<false>(c, p, bounces, counted, timed, tot, cache, env);
+            wave_kernels<false>(c, p, bounces, counted, timed, tot, cache, ext);
         }
         VKB_CUDA(cudaGetLastError());
         return true;
@@ -1037,7 +1099,7 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
     capacity = std::max(capacity, max_pix);
     c->wave.reserve(capacity, uint32_t(in.size()));
     for (const auto& job : in)
-        if (job.first->env_w) { c->wave.reserve_env(std::max(capacity, c->wave.ray_o0.n)); break; }
+        if (job.first->env_w || job.first->em_tris) { c->wave.reserve_ext(std::max(capacity, c->wave.ray_o0.n)); break; }
     c->accum.alloc(std::max<size_t>(1, total_pixels));
     WaveBuffers wb = c->wave.view();
     if (guides) {
@@ -1275,6 +1337,7 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         s->tlas_odd.alloc(std::max(1u, n > 1 ? n - 1 : 1u));
         s->tlas_leaves.alloc(std::max(1u, n));
         s->tlas_codes.alloc(std::max(1u, n));
+        emitter_topology(s, str);
         VKB_CUDA(cudaStreamSynchronize(str));
         float blas_ms = 0.f;
         VKB_CUDA(cudaEventElapsedTime(&blas_ms, s->ev0, s->ev1));
@@ -1312,6 +1375,9 @@ vkb_status vkb_scene_fork(vkb_scene* b, vkb_scene** out) {
         s->d_materials = b->d_materials; s->d_lights = b->d_lights; s->tree = b->tree;
         s->env_img = b->env_img; s->env_dist = b->env_dist; s->env_w = b->env_w; s->env_h = b->env_h;
         std::copy(b->env_scale, b->env_scale + 3, s->env_scale); std::copy(b->env_rot, b->env_rot + 9, s->env_rot);
+        s->em_inst_source = b->em_inst_source; s->em_sources = b->em_sources;
+        s->em_count = b->em_count; s->em_tris = b->em_tris; s->em_leaves = b->em_leaves;
+        if (s->em_leaves) s->em_tree.alloc(2 * size_t(s->em_leaves));
         s->base = b;
         b->forks++;
         // Owned: the base's current instance rows and records, and a TLAS over them.
@@ -1356,9 +1422,12 @@ vkb_status vkb_scene_destroy(vkb_scene* s) {
         s->tree.p = nullptr; s->tree.n = 0;
         s->env_img.p = nullptr; s->env_img.n = 0;
         s->env_dist.p = nullptr; s->env_dist.n = 0;
+        s->em_inst_source.p = nullptr; s->em_inst_source.n = 0;
+        s->em_sources.p = nullptr; s->em_sources.n = 0;
         s->base->forks--;
     }
     s->env_img.release(); s->env_dist.release();
+    s->em_inst_source.release(); s->em_sources.release(); s->em_tree.release();
     DBuf<float4>* f4[] = {&s->vpos, &s->vnrm, &s->blas_tris, &s->tri_nrm, &s->o2w, &s->o2w_next, &s->w2o, &s->inst_lo, &s->inst_hi, &s->tri_lo, &s->tri_hi};
     for (auto* b : f4) b->release();
     s->changed.release();
@@ -1557,6 +1626,7 @@ vkb_status vkb_scene_info(vkb_scene* s, vkb_scene_info_t* out) {
     size_t dev = 0;
     dev += s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas4.n * sizeof(Bvh4Node) + (s->blas_tris.n + s->tri_nrm.n) * sizeof(float4);
     dev += s->tlas_nodes.n * sizeof(BvhNode) + s->tlas4.n * sizeof(Bvh4Node) + s->tlas_odd.n + s->tlas_leaves.n * sizeof(TlasLeaf) + (s->o2w.n + s->w2o.n) * sizeof(float4);
+    dev += s->env_img.n * sizeof(float4) + s->env_dist.n * sizeof(float2) + s->em_inst_source.n * 4 + s->em_sources.n * sizeof(uint2) + s->em_tree.n * sizeof(float);
     out->scene_bytes = dev;
     out->build_ms = s->build_ms;
     out->install_ms = s->install_ms; out->blas_host_ms = s->blas_host_ms; out->upload_ms = s->upload_ms; out->tlas_ms = s->tlas_ms;
@@ -1831,10 +1901,11 @@ namespace {
 // Device bytes a scene holds itself (a fork: its instances and TLAS only).
 uint64_t scene_bytes(const vkb_scene* s) {
     uint64_t own = s->tlas_nodes.n * sizeof(BvhNode) + s->tlas4.n * sizeof(Bvh4Node) + s->tlas_odd.n + s->tlas_leaves.n * sizeof(TlasLeaf) +
-                   (s->o2w.n + s->w2o.n) * sizeof(float4) + s->inst_info.n * sizeof(uint4);
+                   (s->o2w.n + s->w2o.n) * sizeof(float4) + s->inst_info.n * sizeof(uint4) + s->em_tree.n * sizeof(float);
     if (s->base) return own;
     return own + s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas4.n * sizeof(Bvh4Node) +
-           (s->blas_tris.n + s->tri_nrm.n) * sizeof(float4);
+           (s->blas_tris.n + s->tri_nrm.n) * sizeof(float4) + s->env_img.n * sizeof(float4) + s->env_dist.n * sizeof(float2) +
+           s->em_inst_source.n * 4 + s->em_sources.n * sizeof(uint2);
 }
 uint64_t resident_bytes(const vkb_server* v) {
     uint64_t b = 0;
@@ -1972,17 +2043,20 @@ vkb_status vkb_server_step(vkb_server* v, vkb_server_status* status) {
             auto held = [&] { return v->wave_bytes + resident_bytes(v) + v->used_bytes + v->pool_bytes; };
             auto fit = v->pool.lower_bound(npix);
             uint64_t extra = (fit != v->pool.end() && fit->first <= 2 * npix) ? 0u : need;   // reused buffers add nothing
-            if (v->budget && held() + scene + extra > v->budget && v->pool_bytes) {
+            // The first request with an image environment or emissive meshes: the
+            // wavefront's environment and mesh shadow rays and previous vertices (112 B per
+            // path slot), kept for every later wave.
+            const bool ext = (q.s->env_w || q.s->em_tris) && !v->wave.sc_o.p;
+            const uint64_t ext_bytes = ext ? uint64_t(v->capacity) * 112u : 0u;
+            if (v->budget && held() + scene + extra + ext_bytes > v->budget && v->pool_bytes) {
                 finished += reap(v, true, false);
                 free_pool(v);
                 extra = need;
             }
-            if (v->budget && held() + scene + extra > v->budget) break;
-            if (q.s->env_w && !v->wave.sc_o.p) {
-                // The first request with an image environment: the wavefront's third shadow
-                // ray and previous-pdf buffers (52 B per path slot), for every later wave.
-                v->wave.reserve_env(v->capacity);
-                v->wave_bytes += uint64_t(v->capacity) * 52u;
+            if (v->budget && held() + scene + extra + ext_bytes > v->budget) break;
+            if (ext) {
+                v->wave.reserve_ext(v->capacity);
+                v->wave_bytes += ext_bytes;
                 eng.w = v->wave.view();
             }
             auto live = std::make_unique<vkb_server::Live>();
@@ -2116,7 +2190,7 @@ extern "C" vkb_status vkb_render_noalloc(vkb_scene* s, const vkb_profile* pf, vk
         validate_profile(pf);
         if (pf->adaptive) throw Unsupported{"adaptive stopping renders through vkb_render"};
         if (out->guide_albedo || out->guide_normal) throw Unsupported{"denoiser guides render through vkb_render"};
-        if (s->env_w) throw Unsupported{"image environments render through vkb_render"};
+        if (s->env_w || s->em_tris) throw Unsupported{"image environments and emissive meshes render through vkb_render"};
         uint32_t count = pf->sample_count ? pf->sample_count : pf->samples - pf->first_sample;
         vkb_ctx* c = s->ctx;
         VKB_CUDA(cudaSetDevice(c->device));

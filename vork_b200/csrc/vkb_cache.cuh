@@ -260,7 +260,7 @@ vkb_status vkb_cache_train(vkb_cache* k, const vkb_profile* pf, vkb_cache_stats*
         k->rec_count.alloc(1); k->records.alloc(size_t(cap) * 4); k->targets.alloc(size_t(cap) * 3);
         VKB_CUDA(cudaMemsetAsync(k->rec_flag.p, 0, size_t(cap) * sizeof(uint32_t), st));
         c->wave.reserve(e.npix, 1);
-        if (s->env_w) c->wave.reserve_env(c->wave.ray_o0.n);
+        if (s->env_w || s->em_tris) c->wave.reserve_ext(c->wave.ray_o0.n);
         CacheLaunch cl;
         cl.dev.mode = 2; cl.dev.vertex = 0; cl.dev.capacity = cap; cl.dev.vmax = vmax;
         cl.dev.box_lo = k->box_lo; cl.dev.box_scale = k->box_scale;

@@ -449,6 +449,13 @@ struct Job {
     uint32_t env_w, env_h;
     float env_scale[3];
     float env_rot[9];
+    // Emissive meshes (em_tris == 0: none): per instance its source (~0u: none), per source
+    // its instance and the cumulative triangle count through it, the weight tree (node 1
+    // the root, leaves from em_leaves on), and the meshes' own index order (indices
+    // relative to the mesh's vertices) for the corners of a sampled triangle.
+    const uint32_t* em_inst_source; const uint2* em_sources; const float* em_tree;
+    const uint32_t* indices; const float4* vpos;
+    uint32_t em_count, em_tris, em_leaves;
 };
 constexpr uint32_t AD_STOPPED = 4u;
 // Radiance-cache hooks of a wave.  mode 1 (query): a path reaching vertex `vertex`
@@ -484,12 +491,15 @@ struct PathParams {
     uint32_t* err;
     CacheParams cache;
     float4* guide;        // guide renders: the camera hit's guide albedo and normal per path slot (2 float4)
-    // Image-environment waves: each slot's environment shadow ray (origin+tmax, direction,
-    // contribution) and the pdf of the BSDF sample that made its current ray.
-    float4* sc_o; float4* sc_d; float4* sc_c; float* prev_pdf;
+    // Waves with an image environment or emissive meshes: each slot's environment and
+    // mesh shadow rays (origin+tmax, direction, contribution), and the vertex and pdf of
+    // the BSDF sample that made its current ray (xyz, w).
+    float4* sc_o; float4* sc_d; float4* sc_c;
+    float4* sd_o; float4* sd_d; float4* sd_c;
+    float4* prev;
 };
 constexpr uint32_t META_NONFINITE = 0x80000000u;
-constexpr uint32_t SH_TRACE_A = 1u, SH_HAS_B = 2u, SH_TRACE_B = 4u, SH_DIRECT = 8u, SH_HAS_C = 16u;
+constexpr uint32_t SH_TRACE_A = 1u, SH_HAS_B = 2u, SH_TRACE_B = 4u, SH_DIRECT = 8u, SH_HAS_C = 16u, SH_HAS_D = 32u;
 
 // ---------------------------------------------------------------- image environment
 // vork_prelude.slang:78-85.
@@ -765,7 +775,9 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace(Pat
 // Shadow entries with lane refill (as k_trace): a lane carries one entry through its
 // ray A, then its ray B (the second estimator's, when present and traced), then adds
 // the unoccluded contributions to the slot's radiance.
-template <bool COUNT, bool BATCH, bool ENV>
+// EXT: waves with an image environment or emissive meshes, whose entries may carry an
+// environment ray (phase 2) and a mesh ray (phase 3) after the light rays A and B.
+template <bool COUNT, bool BATCH, bool EXT>
 __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace_shadow(PathParams p) {
     VKB_STACK_DECL
     const uint32_t n = p.counters[2];
@@ -785,10 +797,13 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace_sha
             const uint32_t slot = __float_as_uint(p.sa_d[e].w);
             if (L.start(BATCH ? p.jobs[job].sv : p.job0.sv, RayRef{p.sb_o, p.sb_d, slot}, p.sb_o[slot].w)) { phase = 1u; rid = slot; return true; }
         }
-        if constexpr (ENV) {
-            if (flags & SH_HAS_C) {
-                const uint32_t slot = __float_as_uint(p.sa_d[e].w);
+        if constexpr (EXT) {
+            const uint32_t slot = __float_as_uint(p.sa_d[e].w);
+            if (ph <= 2u && (flags & SH_HAS_C)) {
                 if (L.start(BATCH ? p.jobs[job].sv : p.job0.sv, RayRef{p.sc_o, p.sc_d, slot}, p.sc_o[slot].w)) { phase = 2u; rid = slot; return true; }
+            }
+            if (flags & SH_HAS_D) {
+                if (L.start(BATCH ? p.jobs[job].sv : p.job0.sv, RayRef{p.sd_o, p.sd_d, slot}, p.sd_o[slot].w)) { phase = 3u; rid = slot; return true; }
             }
         }
         return false;
@@ -806,11 +821,15 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace_sha
         const Job& J = BATCH ? p.jobs[job] : p.job0;
         const float limit = (flags & SH_DIRECT) ? J.clamp_direct : J.clamp_indirect;
         float3 add = clamp_sample(total, limit, dropped);
-        if constexpr (ENV) {
-            // The environment estimate is clamped on its own (path.slang:1661).
+        if constexpr (EXT) {
+            // The environment and mesh estimates are clamped on their own (path.slang:1660-1661).
             if ((flags & SH_HAS_C) && !(occ & 4u)) {
                 const float4 cc = p.sc_c[slot];
                 add = add + clamp_sample(f3(cc.x, cc.y, cc.z), limit, dropped);
+            }
+            if ((flags & SH_HAS_D) && !(occ & 8u)) {
+                const float4 dc = p.sd_c[slot];
+                add = add + clamp_sample(f3(dc.x, dc.y, dc.z), limit, dropped);
             }
         }
         p.rad[slot] = make_float4(r.x + add.x, r.y + add.y, r.z + add.z, __uint_as_float(dropped));
@@ -843,15 +862,18 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace_sha
         bool done = false;
         if (e != NONE) {
             // The traversal re-reads its ray (instance entry, return to world space):
-            // phase 0 the light ray A, 1 the light ray B, 2 the environment ray.
+            // phase 0 the light ray A, 1 the light ray B, 2 the environment ray, 3 the mesh ray.
             RayRef ray{phase ? p.sb_o : p.sa_o, phase ? p.sb_d : p.sa_d, rid};
-            if constexpr (ENV) { if (phase == 2u) ray = RayRef{p.sc_o, p.sc_d, rid}; }
+            if constexpr (EXT) {
+                if (phase == 2u) ray = RayRef{p.sc_o, p.sc_d, rid};
+                else if (phase == 3u) ray = RayRef{p.sd_o, p.sd_d, rid};
+            }
             if constexpr (BATCH) done = L.step(p.jobs[job].sv, ray, p.err, &tc, stk);
             else done = L.step(p.job0.sv, ray, p.err, &tc, stk);
         }
         if (done) {
             if (L.found) occ |= 1u << phase;
-            if constexpr (ENV) { if (phase == 2u || !begin(phase + 1u)) finish(); }
+            if constexpr (EXT) { if (phase == 3u || !begin(phase + 1u)) finish(); }
             else { if (phase != 0u || !begin(1u)) finish(); }
         }
     }
@@ -862,11 +884,29 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace_sha
     }
 }
 
-struct Surface { float3 world, face, geometric, error, shadow_xyz; float shadow_cone; };
+struct Surface { float3 world, face, geometric, error, shadow_xyz; float shadow_cone; bool entering; };
 __device__ __forceinline__ float3 tvec(const float4 I[3], float3 x) {
     return f3(I[0].x * x.x + I[1].x * x.y + I[2].x * x.z, I[0].y * x.x + I[1].y * x.y + I[2].y * x.z, I[0].z * x.x + I[1].z * x.y + I[2].z * x.z);
 }
 __device__ __forceinline__ float3 mvec(const float4 M[3], float3 x) { return f3(M[0].x * x.x + M[0].y * x.y + M[0].z * x.z, M[1].x * x.x + M[1].y * x.y + M[1].z * x.z, M[2].x * x.x + M[2].y * x.y + M[2].z * x.z); }
+// surface_position_error: the rounding bound of a world point on an instance of mesh m.
+__device__ __forceinline__ float3 position_error(const MeshInfo& m, const float4 M[3], const float4 I[3], float3 world) {
+    float3 lo = f3(m.lo[0], m.lo[1], m.lo[2]), hi = f3(m.hi[0], m.hi[1], m.hi[2]);
+    float3 mag = vmax(vabs(lo), vabs(hi));
+    float extent = maxc(vabs(hi - lo));
+    float3 aw = vabs(world);
+    float3 iw = f3(fabsf(I[0].x) * aw.x + fabsf(I[0].y) * aw.y + fabsf(I[0].z) * aw.z + fabsf(I[0].w),
+                   fabsf(I[1].x) * aw.x + fabsf(I[1].y) * aw.y + fabsf(I[1].z) * aw.z + fabsf(I[1].w),
+                   fabsf(I[2].x) * aw.x + fabsf(I[2].y) * aw.y + fabsf(I[2].z) * aw.z + fabsf(I[2].w));
+    const float g7 = fp32_gamma7();
+    float3 local = (mag + f3(extent) + iw) * g7;
+    float e[3];
+    for (int r = 0; r < 3; ++r) {
+        float4 row = M[r];
+        e[r] = fabsf(row.x) * local.x + fabsf(row.y) * local.y + fabsf(row.z) * local.z + g7 * (fabsf(row.x) * mag.x + fabsf(row.y) * mag.y + fabsf(row.z) * mag.z + fabsf(row.w));
+    }
+    return f3(e[0], e[1], e[2]);
+}
 // hit_geometry.slang:64-138,174-205; hit.slang:86-114; surface.slang:290-333; material.slang:69-79.
 // The triangle's corners come from the BLAS leaf-order copies (positions in blas_tris,
 // normals in tri_nrm, the index buffer's vertex order), so they need no index lookup
@@ -913,22 +953,8 @@ __device__ __forceinline__ Surface hit_surface(const Job& p, uint32_t inst, uint
     s.shadow_xyz = smooth * fmaxf(envelope, 0.5f * quadratic);
     s.shadow_cone = cone;
     s.face = entering ? face : -face;
-    // surface_position_error.
-    float3 lo = f3(m.lo[0], m.lo[1], m.lo[2]), hi = f3(m.hi[0], m.hi[1], m.hi[2]);
-    float3 mag = vmax(vabs(lo), vabs(hi));
-    float extent = maxc(vabs(hi - lo));
-    float3 aw = vabs(s.world);
-    float3 iw = f3(fabsf(I[0].x) * aw.x + fabsf(I[0].y) * aw.y + fabsf(I[0].z) * aw.z + fabsf(I[0].w),
-                   fabsf(I[1].x) * aw.x + fabsf(I[1].y) * aw.y + fabsf(I[1].z) * aw.z + fabsf(I[1].w),
-                   fabsf(I[2].x) * aw.x + fabsf(I[2].y) * aw.y + fabsf(I[2].z) * aw.z + fabsf(I[2].w));
-    const float g7 = fp32_gamma7();
-    float3 local = (mag + f3(extent) + iw) * g7;
-    float e[3];
-    for (int r = 0; r < 3; ++r) {
-        float4 row = M[r];
-        e[r] = fabsf(row.x) * local.x + fabsf(row.y) * local.y + fabsf(row.z) * local.z + g7 * (fabsf(row.x) * mag.x + fabsf(row.y) * mag.y + fabsf(row.z) * mag.z + fabsf(row.w));
-    }
-    s.error = f3(e[0], e[1], e[2]);
+    s.entering = entering;
+    s.error = position_error(m, M, I, s.world);
     return s;
 }
 // path.slang:771-784 with vork_prelude.slang:340-345.
@@ -942,6 +968,140 @@ __device__ __forceinline__ float3 path_origin(const Surface& s, float3 dir) {
     }
     return surface_ray_origin(base, s.error, reflection ? s.geometric : s.face, dir);
 }
+// ---------------------------------------------------------------- emissive meshes
+// Ratio of sibling masses under a shared power-of-two scale (emitter_mesh_proposal.slang:25-35).
+__device__ __forceinline__ float em_left_probability(float left, float right) {
+    const int exponent = int((__float_as_uint(fmaxf(left, right)) >> 23) & 255u) - 127;
+    const float scale = __uint_as_float(uint32_t(127 - exponent / 2) << 23);
+    left *= scale; right *= scale;
+    if (left >= right) return left > 0.f ? 1.f / (1.f + right / left) : 0.f;
+    const float ratio = left / right;
+    return ratio / (1.f + ratio);
+}
+constexpr float MESH_SOURCE_UNIFORM_MIX = 0.5f;
+// Source triangle -> (source, primitive) over the cumulative counts (emitter_mesh_proposal.slang:13-22);
+// past the last source (only through a zero-mass branch) it stays on the last one.
+__device__ __forceinline__ void em_triangle(const Job& J, uint32_t triangle, uint32_t& src, uint32_t& prim) {
+    uint32_t low = 0u, high = J.em_count;
+    while (low < high) {
+        const uint32_t mid = (low + high) >> 1;
+        if (triangle < __ldg(&J.em_sources[mid].y)) high = mid; else low = mid + 1u;
+    }
+    src = min(low, J.em_count - 1u);
+    prim = triangle - (src == 0u ? 0u : __ldg(&J.em_sources[src - 1u].y));
+}
+// The branch probabilities from the leaf up, mixed half and half with the uniform choice
+// (emitter_mesh_proposal.slang:37-57); 0 for a triangle that is not a source.
+__device__ float em_probability(const Job& J, uint32_t inst, uint32_t prim) {
+    const uint32_t src = __ldg(&J.em_inst_source[inst]);
+    if (src == 0xffffffffu || !(__ldg(&J.em_tree[1]) > 0.f)) return 0.f;
+    uint32_t node = J.em_leaves + prim + (src == 0u ? 0u : __ldg(&J.em_sources[src - 1u].y));
+    float probability = 1.f;
+    while (node > 1u) {
+        const uint32_t parent = node >> 1;
+        const float left = __ldg(&J.em_tree[2u * parent]), right = __ldg(&J.em_tree[2u * parent + 1u]);
+        if (fmaxf(left, right) <= 0.f) { probability = 0.f; break; }
+        const float q = em_left_probability(left, right);
+        probability *= (node & 1u) ? 1.f - q : q;
+        node = parent;
+    }
+    return (1.f - MESH_SOURCE_UNIFORM_MIX) * probability + MESH_SOURCE_UNIFORM_MIX / float(J.em_tris);
+}
+// emitter_mesh_sample (emitter_mesh_proposal.slang:59-83); u = path_triangle (group 2 as .zxy).
+__device__ bool em_sample(const Job& J, float ux, float uy, float uz, uint32_t& inst, uint32_t& prim, float& b1, float& b2) {
+    const float top = __uint_as_float(0x3f7fffffu);
+    float choice = fminf(ux, top);
+    if (!(__ldg(&J.em_tree[1]) > 0.f)) return false;
+    const bool uniform = uz < MESH_SOURCE_UNIFORM_MIX;
+    const float point = (uz - (uniform ? 0.f : MESH_SOURCE_UNIFORM_MIX)) / (uniform ? MESH_SOURCE_UNIFORM_MIX : 1.f - MESH_SOURCE_UNIFORM_MIX);
+    uint32_t node = 1u;
+    if (uniform) node = J.em_leaves + min(uint32_t(choice * float(J.em_tris)), J.em_tris - 1u);
+    else
+        while (node < J.em_leaves) {
+            const float q = em_left_probability(__ldg(&J.em_tree[2u * node]), __ldg(&J.em_tree[2u * node + 1u]));
+            if (choice < q) { choice /= q; node *= 2u; }
+            else { choice = (choice - q) / (1.f - q); node = 2u * node + 1u; }
+            choice = fminf(choice, top);
+        }
+    uint32_t src;
+    em_triangle(J, node - J.em_leaves, src, prim);
+    inst = __ldg(&J.em_sources[src].x);
+    const float radius = sqrtf(uy);
+    b1 = radius * (1.f - point);
+    b2 = radius - b1;
+    return true;
+}
+// World point at (b1, b2), face normal and area of a source triangle in the mesh's own
+// index order (hit_geometry.slang:116-124,246-256).
+struct EmGeometry { float3 point, face, error; float area; };
+__device__ EmGeometry em_geometry(const Job& J, uint32_t inst, uint32_t prim, float b1, float b2) {
+    const MeshInfo& m = J.meshes[__ldg(&J.inst_info[inst]).x];
+    const float4 M[3] = {__ldg(&J.o2w[3 * inst]), __ldg(&J.o2w[3 * inst + 1]), __ldg(&J.o2w[3 * inst + 2])};
+    const float4 I[3] = {__ldg(&J.w2o[3 * inst]), __ldg(&J.w2o[3 * inst + 1]), __ldg(&J.w2o[3 * inst + 2])};
+    const uint32_t* ix = J.indices + m.index_offset + 3u * prim;
+    const float4* vp = J.vpos + m.vertex_offset;
+    const float4 q0 = __ldg(vp + __ldg(ix)), q1 = __ldg(vp + __ldg(ix + 1)), q2 = __ldg(vp + __ldg(ix + 2));
+    const float3 P0 = f3(q0.x, q0.y, q0.z), P1 = f3(q1.x, q1.y, q1.z), P2 = f3(q2.x, q2.y, q2.z);
+    const float3 raw = cross(P1 - P0, P2 - P0);
+    // A degenerate face (whose vertex-normal fallback the hit uses) has no area, hence no
+    // probability and no contribution, so the face's own cross product stands in for it.
+    EmGeometry g;
+    g.face = finite_unit_normal(tvec(I, finite_unit_normal(raw, raw)), f3(0.f, 0.f, 1.f));
+    g.point = mvec(M, P0 * (1.f - b1 - b2) + P1 * b1 + P2 * b2) + f3(M[0].w, M[1].w, M[2].w);
+    g.area = length(cross(mvec(M, P1 - P0), mvec(M, P2 - P0))) * 0.5f;
+    g.error = position_error(m, M, I, g.point);
+    return g;
+}
+// Solid-angle density at `from` of a point on a source triangle, times the triangle's
+// probability (path.slang:996-1002, emitter_mesh_proposal.slang:86-92).
+__device__ __forceinline__ float mesh_pdf(const Job& J, uint32_t inst, uint32_t prim, float area, float3 from, float3 point, float3 face) {
+    const float3 delta = point - from;
+    const float squared = dot(delta, delta);
+    const float cosine = fabsf(dot(face, normalize(delta)));
+    const float density = area > 0.f && cosine > 0.f ? squared / (area * cosine) : 0.f;
+    return density * em_probability(J, inst, prim);
+}
+
+// The frame's mesh-source weights (emitter_weights.slang:23-47): leaf t = world area x the
+// emission's Rec.709 luminance power of source triangle t (the area alone when that
+// product is not finite), 0 on the padded leaves.  J carries the topology and geometry.
+__global__ void k_em_leaves(const __grid_constant__ Job J, float* tree) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < J.em_leaves; t += gridDim.x * blockDim.x) {
+        float area = 0.f;
+        if (t < J.em_tris) {
+            uint32_t src, prim;
+            em_triangle(J, t, src, prim);
+            const uint32_t inst = __ldg(&J.em_sources[src].x);
+            area = em_geometry(J, inst, prim, 0.f, 0.f).area;
+            if (area > 0.f) {
+                const vkb_material& m = J.materials[__ldg(&J.inst_info[inst]).y];
+                const float power = (fmaxf(m.emission_color[0], 0.f) * LUM_R + fmaxf(m.emission_color[1], 0.f) * LUM_G +
+                                     fmaxf(m.emission_color[2], 0.f) * LUM_B) * fmaxf(m.emission_luminance, 0.f);
+                const float weight = area * power;
+                if (isfinite(weight)) area = weight;
+            }
+        }
+        tree[J.em_leaves + t] = area;
+    }
+}
+// Inner nodes [first, 2 first): the mean of their two children (emitter_weights.slang:48-55).
+__global__ void k_em_reduce(float* tree, uint32_t first) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < first; i += gridDim.x * blockDim.x) {
+        const uint32_t node = first + i;
+        tree[node] = 0.5f * tree[2u * node] + 0.5f * tree[2u * node + 1u];
+    }
+}
+// The levels from `first` up to the root in one block (a barrier between levels).
+__global__ void k_em_reduce_top(float* tree, uint32_t first) {
+    for (uint32_t level = first; level >= 1u; level >>= 1) {
+        for (uint32_t i = threadIdx.x; i < level; i += blockDim.x) {
+            const uint32_t node = level + i;
+            tree[node] = 0.5f * tree[2u * node] + 0.5f * tree[2u * node + 1u];
+        }
+        __syncthreads();
+    }
+}
+
 __device__ __forceinline__ float3 light_threshold(float3 value, float threshold, uint32_t& rng) {
     float importance = maxc(value);
     if (importance < threshold && threshold > 0.f) {
@@ -999,7 +1159,9 @@ __device__ __noinline__ void cache_append(const PathParams& p, float3 world, flo
 #define VKB_SHADE_MIN_BLOCKS 1
 #endif
 constexpr int SHADE_BLOCK = VKB_SHADE_BLOCK;
-template <bool BATCH, bool ENV>
+// EXT: waves with an image environment or emissive meshes (their strategies and the
+// per-slot previous vertex); the plain instantiation carries none of it.
+template <bool BATCH, bool EXT>
 __global__ void __launch_bounds__(VKB_SHADE_BLOCK, VKB_SHADE_MIN_BLOCKS) k_shade(const __grid_constant__ PathParams p, int cur) {
     const int nxt = cur ^ 1;
     uint32_t n = p.counters[cur];
@@ -1035,7 +1197,7 @@ __global__ void __launch_bounds__(VKB_SHADE_BLOCK, VKB_SHADE_MIN_BLOCKS) k_shade
                 float3 sky;
                 if (ray_event == VKB_RAY_CAMERA && !J.env.camera_sees_environment) sky = get3(J.env.background);
                 else {
-                    sky = ENV ? env_radiance(J, dir) : get3(J.env.radiance);
+                    sky = EXT ? env_radiance(J, dir) : get3(J.env.radiance);
                     if (ray_event == VKB_RAY_CAMERA)
                         for (uint32_t l = 0; l < J.num_lights; ++l) {
                             const vkb_light& L = J.lights[l];
@@ -1043,10 +1205,10 @@ __global__ void __launch_bounds__(VKB_SHADE_BLOCK, VKB_SHADE_MIN_BLOCKS) k_shade
                             sky = sky + emitter_eval(L, f3(0.f), dir).radiance;
                         }
                 }
-                if (ENV && J.env_w && bounce > 0u) {
+                if (EXT && J.env_w && bounce > 0u) {
                     // path.slang:1463: an escape after a BSDF sample, weighed against the
                     // environment strategy.
-                    const float prev = p.prev_pdf[slot];
+                    const float prev = p.prev[slot].w;
                     if (prev > 0.f) sky = sky * mis_power(prev, env_density(J, dir));
                 }
                 rad = rad + clamp_sample(thr * sky, limit, dropped);
@@ -1062,6 +1224,25 @@ __global__ void __launch_bounds__(VKB_SHADE_BLOCK, VKB_SHADE_MIN_BLOCKS) k_shade
                 c.n = s.geometric;
                 boundary_closure_air(c);
                 float3 view = -dir;
+                if (EXT && mt.emission_luminance > 0.f && ((mt.flags & 2u) || s.entering)) {
+                    // Surface emission (path.slang:1580-1591) on the side the material covers,
+                    // weighed against the mesh strategy after a BSDF sample.
+                    const float3 emitted = get3(mt.emission_color) * mt.emission_luminance;
+                    float mis = 1.f;
+                    if (bounce > 0u && J.em_tris) {
+                        const float4 pv = p.prev[slot];
+                        if (pv.w > 0.f) {
+                            const uint32_t tri = __float_as_uint(hh.w);
+                            const float4* tp = J.sv.blas_tris + 3u * size_t(tri);
+                            const float4 q0 = __ldg(tp), q1 = __ldg(tp + 1), q2 = __ldg(tp + 2);
+                            const float4 M[3] = {__ldg(&J.o2w[3 * inst]), __ldg(&J.o2w[3 * inst + 1]), __ldg(&J.o2w[3 * inst + 2])};
+                            const float3 e1 = mvec(M, f3(q1.x - q0.x, q1.y - q0.y, q1.z - q0.z)), e2 = mvec(M, f3(q2.x - q0.x, q2.y - q0.y, q2.z - q0.z));
+                            const float area = length(cross(e1, e2)) * 0.5f;
+                            mis = mis_power(pv.w, mesh_pdf(J, inst, __float_as_uint(q0.w), area, f3(pv.x, pv.y, pv.z), s.world, s.face));
+                        }
+                    }
+                    rad = rad + clamp_sample(thr * emitted * mis, limit, dropped);
+                }
                 // Radiance cache: record this vertex, and at the query vertex stop the path
                 // here (the query kernel adds thr x the cached outgoing radiance).
                 const bool cache_query = p.cache.mode == 1u && bounce >= p.cache.vertex;
@@ -1118,13 +1299,13 @@ __global__ void __launch_bounds__(VKB_SHADE_BLOCK, VKB_SHADE_MIN_BLOCKS) k_shade
                     // the diffuse and specular responses MIS-weighted against continuing
                     // there (continuation_mask, path.slang:1003-1010), one visibility ray
                     // to infinity; clamped on its own.
-                    bool trace_c = false;
-                    if (ENV && J.env_w) {
-                        uint32_t cont = 0u;
-                        if (bounce < J.bounces[0]) {
-                            if (diffuse < J.bounces[1]) cont |= VKB_RAY_DIFFUSE;
-                            if (glossy < J.bounces[2] && (diffuse == 0u || (J.caustics & 1u))) cont |= VKB_RAY_SPECULAR;
-                        }
+                    bool trace_c = false, trace_d = false;
+                    uint32_t cont = 0u;
+                    if (EXT && bounce < J.bounces[0]) {
+                        if (diffuse < J.bounces[1]) cont |= VKB_RAY_DIFFUSE;
+                        if (glossy < J.bounces[2] && (diffuse == 0u || (J.caustics & 1u))) cont |= VKB_RAY_SPECULAR;
+                    }
+                    if (EXT && J.env_w) {
                         const float4 eu = sample_group(pseed, sidx, J.sample_mask, vertex_group(vtx, 3));   // path_environment
                         float epdf = 0.f;
                         const float3 edir = env_sample(J, eu.x, eu.y, epdf);
@@ -1151,11 +1332,55 @@ __global__ void __launch_bounds__(VKB_SHADE_BLOCK, VKB_SHADE_MIN_BLOCKS) k_shade
                             trace_c = true;
                         }
                     }
+                    if (EXT && J.em_tris) {
+                        // mesh_next_event (path.slang:1121-1167), constant emission: a point on a
+                        // source triangle, the diffuse and specular responses MIS-weighted against
+                        // continuing there, one visibility ray between the offset end points.
+                        const float4 g = sample_group(pseed, sidx, J.sample_mask, vertex_group(vtx, 2));   // path_triangle
+                        uint32_t ei, ep; float b1, b2;
+                        if (em_sample(J, g.z, g.x, g.y, ei, ep, b1, b2)) {
+                            const EmGeometry eg = em_geometry(J, ei, ep, b1, b2);
+                            const float3 delta = eg.point - s.world;
+                            const float distance = length(delta);
+                            if (distance > 0.f) {
+                                const float3 axis = delta / distance;
+                                const float mpdf = mesh_pdf(J, ei, ep, eg.area, s.world, eg.point, eg.face);
+                                const vkb_material& em = J.materials[__ldg(&J.inst_info[ei]).y];
+                                const bool front = dot(eg.face, axis) < 0.f;
+                                const float3 emitted = get3(em.emission_color) * em.emission_luminance;
+                                if (mpdf > 0.f && ((em.flags & 2u) || front) && maxc(emitted) > 0.f) {
+                                    const float3 start = path_origin(s, axis);
+                                    const float3 end = surface_ray_origin(eg.point, eg.error, front ? eg.face : -eg.face, -axis);
+                                    const float3 connection = end - start;
+                                    const float extent = length(connection);
+                                    float3 response = f3(0.f);
+                                    if (extent > 0.f) {
+                                        #pragma unroll
+                                        for (int k = 0; k < 2; ++k) {
+                                            const uint32_t event = k == 0 ? VKB_RAY_DIFFUSE : VKB_RAY_SPECULAR;
+                                            if (!event_hemisphere(event, axis, s.face, s.geometric)) continue;
+                                            const float3 f = eval_mask(c, view, axis, event, pr);
+                                            if (maxc(f) <= 0.f) continue;
+                                            const float bpdf = (cont & event) ? pdf_mask(c, view, axis, event, pr) : 0.f;
+                                            response = response + f * mis_power(mpdf, bpdf);
+                                        }
+                                    }
+                                    if (any_nonzero(response)) {
+                                        const float3 md = thr * (response * emitted / mpdf), cdir = connection / extent;
+                                        p.sd_o[slot] = make_float4(start.x, start.y, start.z, extent);
+                                        p.sd_d[slot] = make_float4(cdir.x, cdir.y, cdir.z, 0.f);
+                                        p.sd_c[slot] = make_float4(md.x, md.y, md.z, 0.f);
+                                        trace_d = true;
+                                    }
+                                }
+                            }
+                        }
+                    }
                     float3 ca = thr * va, cb = thr * vb;
-                    if (trace_a || trace_b || trace_c) {
+                    if (trace_a || trace_b || trace_c || trace_d) {
                         push_shadow = true;
                         uint32_t flags = (trace_a ? SH_TRACE_A : 0u) | (has_b ? SH_HAS_B : 0u) | (trace_b ? SH_TRACE_B : 0u) | (bounce == 0 ? SH_DIRECT : 0u) |
-                                         (trace_c ? SH_HAS_C : 0u);
+                                         (trace_c ? SH_HAS_C : 0u) | (trace_d ? SH_HAS_D : 0u);
                         sh_o = make_float4(oa.x, oa.y, oa.z, la);
                         sh_d = make_float4(da.x, da.y, da.z, __uint_as_float(slot));
                         sh_c = make_float4(ca.x, ca.y, ca.z, __uint_as_float(flags));
@@ -1199,7 +1424,7 @@ __global__ void __launch_bounds__(VKB_SHADE_BLOCK, VKB_SHADE_MIN_BLOCKS) k_shade
                         new_o = make_float4(o.x, o.y, o.z, FP32_MAX);
                         new_d = make_float4(smp.dir.x, smp.dir.y, smp.dir.z, __uint_as_float(slot));
                         push_ray = true;
-                        if (ENV) p.prev_pdf[slot] = smp.pdf;
+                        if (EXT) p.prev[slot] = make_float4(s.world.x, s.world.y, s.world.z, smp.pdf);
 #if VKB_SHADE_EARLY_APPEND
                         {
 #if VKB_SHADE_OCTANT_APPEND
