@@ -603,6 +603,7 @@ def main():
     ap.add_argument("--rates", default="1,5,20,50", help="serve: Poisson arrival rates (req/s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tlas", choices=["lbvh", "ploc"], default="lbvh", help="TLAS builder of the frame scene")
+    ap.add_argument("--blas", choices=["4", "8"], default="4", help="BLAS nodes: 4-wide FP32 planes or compressed 8-wide")
     ap.add_argument("--no-error", action="store_true", help="cache: skip the reference renders (timing/profiling runs)")
     ap.add_argument("--res", default="1920x1080", help="cache: frame resolution (smaller for profiling captures)")
     ap.add_argument("--schedule", default="srpt", choices=["srpt", "aged", "fair", "packed"], help="serve: wave schedule")
@@ -644,6 +645,7 @@ def main():
 
     sc, flock, prof, cfg = workload(args.config, seed=rank)
     sc.tlas_builder = abi.TLAS_PLOC if args.tlas == "ploc" else abi.TLAS_LBVH
+    sc.blas_format = abi.BLAS_WIDE8 if args.blas == "8" else abi.BLAS_WIDE4
     frames = frames_for(sc, flock, args.warmup + args.steps)
     cam = sc.camera
     npix = cam.width * cam.height
@@ -697,6 +699,7 @@ def main():
     launches = s.launch_count - launches0
     tlas = {"builder": ("PLOC (radius 16)" if args.tlas == "ploc" else "Karras LBVH") + " over 30-bit Morton order (bit 30: boxes wider than a quarter of the centroid spread, split at the root), rebuilt every frame",
             "build_ms_per_frame": build_ms / args.steps,
+            "blas_nodes": "compressed 8-wide (80 B)" if args.blas == "8" else "4-wide FP32 planes (128 B)",
             **s.tlas_stats()}
     elapsed_ms = max_over_ranks(elapsed_ms, dist, f"cuda:{local}")
     value = world * args.steps * paths_per_step / (elapsed_ms / 1000.0)

@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define VKB_ABI_VERSION 5u
+#define VKB_ABI_VERSION 6u
 
 /* Error model: FailureKind exit categories of crates/vork-render/src/failure.rs:21-100,
  * reduced to what a render call can report. */
@@ -153,7 +153,15 @@ typedef struct vkb_scene_desc {
     uint32_t tlas_builder;            /* VKB_TLAS_LBVH or VKB_TLAS_PLOC (no reference counterpart: the
                                          reference's TLAS is built by the graphics driver) */
     const vkb_environment_image* environment_image;   /* NULL: the constant environment alone */
+    uint32_t blas_format;             /* VKB_BLAS_WIDE4 (default) or VKB_BLAS_WIDE8 */
 } vkb_scene_desc;
+
+/* BLAS node formats (the TLAS is 4-wide in both): 4-wide FP32 child planes (one 128-byte
+ * line per node), or compressed 8-wide nodes (80 bytes: child boxes as bytes on a per-node
+ * grid; Ylitie, Karras & Laine, HPG 2017).  Scenes of the two formats render alone or in
+ * batches of their own format; the server takes 4-wide scenes. */
+#define VKB_BLAS_WIDE4 0u
+#define VKB_BLAS_WIDE8 1u
 
 /* TLAS builders, both over the instance boxes in Morton order and both refittable:
  * Karras LBVH (fast build, siblings adjacent in memory) or PLOC (lower surface area

@@ -90,9 +90,12 @@ int main(int argc, char** argv) {
         uint32_t bits;
         std::memcpy(&bits, &nd.h.w, 4);
         const uint32_t imask = bits >> 24, internal = uint32_t(__builtin_popcount(imask));
+        // Every reference stays inside the arrays: children below the node count, leaves
+        // below the triangle count, internal slots first.
+        if (nd.b.z < 1 || nd.b.z > 8 || imask != (1u << internal) - 1u || nd.b.x + internal > w8.nodes.size() ||
+            nd.b.y + (nd.b.z - internal) > n) { std::printf("FAIL references of node %u\n", ni); return 1; }
         for (int k = 0; k < 8; ++k) {
-            const bool used = decode(nd, 0, k, false) <= decode(nd, 0, k, true);
-            if (!used) continue;
+            if (uint32_t(k) >= nd.b.z) continue;
             double blo[3], bhi[3];
             for (int a = 0; a < 3; ++a) { blo[a] = decode(nd, a, k, false); bhi[a] = decode(nd, a, k, true); }
             // Triangles under the slot.
@@ -106,7 +109,7 @@ int main(int argc, char** argv) {
                     std::memcpy(&cb, &c.h.w, 4);
                     const uint32_t cm = cb >> 24, ci = uint32_t(__builtin_popcount(cm));
                     for (int j = 0; j < 8; ++j) {
-                        if (!(decode(c, 0, j, false) <= decode(c, 0, j, true))) continue;
+                        if (uint32_t(j) >= c.b.z) continue;
                         if (cm >> j & 1u) sub.push_back(c.b.x + uint32_t(j));
                         else under.push_back(c.b.y + uint32_t(j) - ci);
                     }
@@ -143,7 +146,7 @@ int main(int argc, char** argv) {
             uint32_t bits;
             std::memcpy(&bits, &nd.h.w, 4);
             const uint32_t imask = bits >> 24, internal = uint32_t(__builtin_popcount(imask));
-            for (int k = 0; k < 8; ++k) {
+            for (int k = 0; k < int(nd.b.z); ++k) {
                 double t0 = 0, t1 = wbest;
                 for (int a = 0; a < 3; ++a) {
                     const double l = decode(nd, a, k, false), h = decode(nd, a, k, true);

@@ -28,6 +28,7 @@
 
 #include "vkb_kernels.cuh"
 #include "vkb_sah.h"
+#include "vkb_wide8.h"
 #include "vkb_nrc.cuh"
 #include "vkb_display.cuh"
 
@@ -390,6 +391,8 @@ struct vkb_scene {
     DBuf<MeshInfo> meshes;
     DBuf<BvhNode> tlas_nodes;                 // binary TLAS (built, refitted; SAH statistics)
     DBuf<Bvh4Node> blas4, tlas4;              // 4-wide traversal nodes (TLAS sparse: index = binary node)
+    DBuf<Bvh8Node> blas8;                     // compressed 8-wide BLAS nodes (VKB_BLAS_WIDE8 scenes; blas4 then unused)
+    uint32_t blas_format = VKB_BLAS_WIDE4;
     DBuf<uint8_t> tlas_odd;                   // depth parity of the binary TLAS nodes
     DBuf<TlasLeaf> tlas_leaves;
     DBuf<vkb_material> d_materials;
@@ -446,6 +449,7 @@ SceneView scene_view(const vkb_scene* s) {
     SceneView v;
     v.tlas_nodes = s->tlas4.p; v.tlas_leaves = s->tlas_leaves.p;
     v.blas_nodes = s->blas4.p; v.blas_tris = s->blas_tris.p;
+    v.blas8 = s->blas8.p;   // null unless the scene was built with compressed 8-wide BLASes
     v.num_instances = s->num_instances;
     return v;
 }
@@ -641,6 +645,7 @@ void validate_desc(const vkb_scene_desc* d) {
     }
     if (d->camera.width == 0 || d->camera.height == 0) throw ArgError{"camera resolution is zero"};
     if (d->tlas_builder > VKB_TLAS_PLOC) throw ArgError{"unknown TLAS builder"};
+    if (d->blas_format > VKB_BLAS_WIDE8) throw ArgError{"unknown BLAS format"};
     if (const vkb_environment_image* e = d->environment_image) {
         if (!e->rgba || e->width == 0 || e->height == 0) throw ArgError{"environment image has no texels"};
         if (uint64_t(e->width) * e->height > (uint64_t(1) << 26)) throw ArgError{"environment image above 2^26 texels"};
@@ -756,9 +761,21 @@ struct CacheLaunch {
 // The kernels of one wave: camera, then per bounce closest-hit trace, shade, shadow trace;
 // then the radiance-cache queries, if any; then accumulation.  Timed
 // mode records events around every closest-hit trace.
+// The closest-hit and shadow traces of one bounce, instantiated for the counters (COUNT),
+// the EXT shadow entries and the BLAS format (W8: compressed 8-wide).
+template <bool BATCH, bool W8>
+void launch_trace(bool counted, int grid, cudaStream_t st, const PathParams& p, int cur) {
+    if (counted) k_trace<true, BATCH, W8><<<grid, TRACE_BLOCK, 0, st>>>(p, cur);
+    else k_trace<false, BATCH, W8><<<grid, TRACE_BLOCK, 0, st>>>(p, cur);
+}
+template <bool BATCH, bool EXT, bool W8>
+void launch_shadow(bool counted, int grid, cudaStream_t st, const PathParams& p) {
+    if (counted) k_trace_shadow<true, BATCH, EXT, W8><<<grid, TRACE_BLOCK, 0, st>>>(p);
+    else k_trace_shadow<false, BATCH, EXT, W8><<<grid, TRACE_BLOCK, 0, st>>>(p);
+}
 template <bool BATCH>
 void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counted, bool timed, WaveTotals& tot,
-                  const CacheLaunch* cache = nullptr, bool ext = false) {
+                  const CacheLaunch* cache = nullptr, bool ext = false, bool w8 = false) {
     cudaStream_t st = c->stream;
     const int sms = c->sms, tgrid = sms * c->trace_blocks_per_sm, sgrid = sms * c->trace_blocks_per_sm;
     const bool adaptive = !BATCH && p.job0.adaptive;
@@ -775,8 +792,8 @@ void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counte
             }
             VKB_CUDA(cudaEventRecord(c->kernel_events[2 * tot.trace_launches], st));
         }
-        if (counted) k_trace<true, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p, cur);
-        else k_trace<false, BATCH><<<tgrid, TRACE_BLOCK, 0, st>>>(p, cur);
+        if (w8) launch_trace<BATCH, true>(counted, tgrid, st, p, cur);
+        else launch_trace<BATCH, false>(counted, tgrid, st, p, cur);
         if (timed) VKB_CUDA(cudaEventRecord(c->kernel_events[2 * tot.trace_launches + 1], st));
         tot.trace_launches++;
         if (!BATCH && b == 0u && p.guide) { k_guides<<<sms * 8, 256, 0, st>>>(p); tot.launches += 1; }
@@ -785,12 +802,12 @@ void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counte
         // strategies (two more shadow rays per vertex); the others keep the plain ones.
         if (ext) {
             k_shade<BATCH, true><<<sgrid, SHADE_BLOCK, 0, st>>>(p, cur);
-            if (counted) k_trace_shadow<true, BATCH, true><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
-            else k_trace_shadow<false, BATCH, true><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
+            if (w8) launch_shadow<BATCH, true, true>(counted, tgrid, st, p);
+            else launch_shadow<BATCH, true, false>(counted, tgrid, st, p);
         } else {
             k_shade<BATCH, false><<<sgrid, SHADE_BLOCK, 0, st>>>(p, cur);
-            if (counted) k_trace_shadow<true, BATCH, false><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
-            else k_trace_shadow<false, BATCH, false><<<tgrid, TRACE_BLOCK, 0, st>>>(p);
+            if (w8) launch_shadow<BATCH, false, true>(counted, tgrid, st, p);
+            else launch_shadow<BATCH, false, false>(counted, tgrid, st, p);
         }
     }
     if (cache && cache->dev.mode == 1u) {
@@ -955,7 +972,11 @@ struct WaveEngine {
         PathParams p = path_params(c, w, wave_jobs);
         p.job0 = wave_table[0];
         bool ext = false;
-        for (const Job& j : wave_table) ext = ext || j.env_w != 0u || j.em_tris != 0u;
+        const bool w8 = wave_table[0].sv.blas8 != nullptr;
+        for (const Job& j : wave_table) {
+            ext = ext || j.env_w != 0u || j.em_tris != 0u;
+            if ((j.sv.blas8 != nullptr) != w8) throw ArgError{"the jobs of one wave share a BLAS format"};
+        }
         if (ext && !w.sc_o) throw InternalError{"environment or emissive-mesh wave without its shadow buffers"};
         if (cache) {
             if (batch) throw ArgError{"radiance-cache renders take one job"};
@@ -963,7 +984,7 @@ struct WaveEngine {
         }
         if (use_graph) {
             uint64_t key = (uint64_t(bounces) << 1) | 1u;
-            key = key * 1315423911ull + (counted ? 7u : 3u) + (ext ? 11u : 0u);
+            key = key * 1315423911ull + (counted ? 7u : 3u) + (ext ? 11u : 0u) + (w8 ? 17u : 0u);
             key = key * 40503ull + wave_jobs;
             key = key * 97ull + uint64_t(c->trace_blocks_per_sm);
             cudaGraphExec_t exec = nullptr;
@@ -972,7 +993,7 @@ struct WaveEngine {
                 cudaGraph_t g;
                 VKB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
                 WaveTotals scratch;
-                wave_kernels<true>(c, p, bounces, counted, false, scratch, nullptr, ext);
+                wave_kernels<true>(c, p, bounces, counted, false, scratch, nullptr, ext, w8);
                 VKB_CUDA(cudaStreamEndCapture(st, &g));
                 VKB_CUDA(cudaGraphInstantiate(&exec, g, 0));
                 VKB_CUDA(cudaGraphDestroy(g));
@@ -982,9 +1003,9 @@ struct WaveEngine {
             tot.launches += 3 + 4 * (bounces + 1);
             tot.trace_launches += bounces + 1;
         } else if (batch) {
-            wave_kernels<true>(c, p, bounces, counted, timed, tot, nullptr, ext);
+            wave_kernels<true>(c, p, bounces, counted, timed, tot, nullptr, ext, w8);
         } else {
-            wave_kernels<false>(c, p, bounces, counted, timed, tot, cache, ext);
+            wave_kernels<false>(c, p, bounces, counted, timed, tot, cache, ext, w8);
         }
         VKB_CUDA(cudaGetLastError());
         return true;
@@ -1078,6 +1099,9 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
         if (outs[k]->primary_ids) ids_words += 2 * npix;
         if (!outs[k]->on_device) staged += npix;
     }
+    for (const auto& job : in)
+        if ((job.first->blas8.p != nullptr) != (in[0].first->blas8.p != nullptr))
+            throw ArgError{"the scenes of one batch share a BLAS format"};
     bool adaptive = false, guides = false;
     for (const auto& job : in) adaptive = adaptive || job.second.adaptive;
     for (size_t k = 0; k < in.size(); ++k) guides = guides || outs[k]->guide_albedo || outs[k]->guide_normal;
@@ -1213,6 +1237,8 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         s->num_meshes = d->num_meshes;
         s->num_instances = d->num_instances;
         s->tlas_builder = d->tlas_builder;
+        s->blas_format = d->blas_format;
+        const bool wide8 = s->blas_format == VKB_BLAS_WIDE8;
         // Concatenate meshes.
         uint32_t nv = 0, nt = 0;
         s->mesh_info.resize(d->num_meshes);
@@ -1250,12 +1276,13 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         VKB_CUDA(cudaEventRecord(s->ev0, str));
         const auto t_blas = std::chrono::steady_clock::now();
         std::vector<Bvh4Node> all_nodes;
+        std::vector<Bvh8Node> all_nodes8;
         std::vector<float4> all_tris(std::max<size_t>(1, size_t(nt) * 3)), all_nrm(std::max<size_t>(1, size_t(nt) * 3));
         for (uint32_t m = 0; m < d->num_meshes; ++m) {
             MeshInfo& mi = s->mesh_info[m];
             const vkb_mesh& me = d->meshes[m];
             uint32_t n = mi.num_triangles;
-            mi.node_offset = uint32_t(all_nodes.size());
+            mi.node_offset = uint32_t(wide8 ? all_nodes8.size() : all_nodes.size());
             if (n == 0) continue;
             std::vector<float> lo(3 * size_t(n)), hi(3 * size_t(n)), cen(3 * size_t(n));
             for (uint32_t t = 0; t < n; ++t)
@@ -1268,13 +1295,26 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
             sah.run(n, lo.data(), hi.data(), cen.data());
             if (sah.nodes.size() > std::max(1u, n > 1 ? n - 1 : 1u)) throw ArgError{"BLAS node count above its bound"};
             static_assert(sizeof(vkb_host::SahNode) == sizeof(BvhNode), "host SAH nodes have the device layout");
-            std::vector<BvhNode> bin(sah.nodes.size());
-            std::memcpy(bin.data(), sah.nodes.data(), bin.size() * sizeof(BvhNode));
-            std::vector<Bvh4Node> wide = collapse_blas(bin);
-            if (all_nodes.size() + wide.size() > size_t(INT32_MAX)) throw ArgError{"BLAS node count above its bound"};
-            all_nodes.insert(all_nodes.end(), wide.begin(), wide.end());
+            // Leaf position k of this mesh's BLAS -> its original triangle.
+            std::vector<uint32_t> leaf_tri(sah.order);
+            if (wide8) {
+                static_assert(sizeof(vkb_host::Wide8Node) == sizeof(Bvh8Node), "host 8-wide nodes have the device layout");
+                vkb_host::Wide8Blas w8;
+                w8.run(sah.nodes, n);
+                if (all_nodes8.size() + w8.nodes.size() > size_t(INT32_MAX)) throw ArgError{"BLAS node count above its bound"};
+                const size_t at = all_nodes8.size();
+                all_nodes8.resize(at + w8.nodes.size());
+                std::memcpy(all_nodes8.data() + at, w8.nodes.data(), w8.nodes.size() * sizeof(Bvh8Node));
+                for (uint32_t k = 0; k < n; ++k) leaf_tri[k] = sah.order[w8.order[k]];
+            } else {
+                std::vector<BvhNode> bin(sah.nodes.size());
+                std::memcpy(bin.data(), sah.nodes.data(), bin.size() * sizeof(BvhNode));
+                std::vector<Bvh4Node> wide = collapse_blas(bin);
+                if (all_nodes.size() + wide.size() > size_t(INT32_MAX)) throw ArgError{"BLAS node count above its bound"};
+                all_nodes.insert(all_nodes.end(), wide.begin(), wide.end());
+            }
             for (uint32_t k = 0; k < n; ++k) {
-                uint32_t t = sah.order[k];
+                uint32_t t = leaf_tri[k];
                 const float* p0 = me.positions + 3 * me.indices[3 * t];
                 const float* p1 = me.positions + 3 * me.indices[3 * t + 1];
                 const float* p2 = me.positions + 3 * me.indices[3 * t + 2];
@@ -1291,6 +1331,10 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
             }
         }
         if (all_nodes.empty()) all_nodes.emplace_back();
+        if (wide8) {
+            if (all_nodes8.empty()) all_nodes8.emplace_back();
+            s->blas8.upload(all_nodes8.data(), all_nodes8.size(), str);
+        }
         blas_host = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_blas).count();
         s->blas4.alloc(all_nodes.size());
         VKB_CUDA(cudaMemcpyAsync(s->blas4.p, all_nodes.data(), all_nodes.size() * sizeof(Bvh4Node), cudaMemcpyHostToDevice, str));
@@ -1371,7 +1415,7 @@ vkb_status vkb_scene_fork(vkb_scene* b, vkb_scene** out) {
         s->tree_nodes = b->tree_nodes; s->tlas_builder = b->tlas_builder;
         // Shared, read-only: geometry, BLASes, materials, lights, light tree.
         s->vpos = b->vpos; s->vnrm = b->vnrm; s->blas_tris = b->blas_tris; s->tri_nrm = b->tri_nrm;
-        s->indices = b->indices; s->meshes = b->meshes; s->blas4 = b->blas4;
+        s->indices = b->indices; s->meshes = b->meshes; s->blas4 = b->blas4; s->blas8 = b->blas8; s->blas_format = b->blas_format;
         s->d_materials = b->d_materials; s->d_lights = b->d_lights; s->tree = b->tree;
         s->env_img = b->env_img; s->env_dist = b->env_dist; s->env_w = b->env_w; s->env_h = b->env_h;
         std::copy(b->env_scale, b->env_scale + 3, s->env_scale); std::copy(b->env_rot, b->env_rot + 9, s->env_rot);
@@ -1417,6 +1461,7 @@ vkb_status vkb_scene_destroy(vkb_scene* s) {
         s->indices.p = nullptr; s->indices.n = 0;
         s->meshes.p = nullptr; s->meshes.n = 0;
         s->blas4.p = nullptr; s->blas4.n = 0;
+        s->blas8.p = nullptr; s->blas8.n = 0;
         s->d_materials.p = nullptr; s->d_materials.n = 0;
         s->d_lights.p = nullptr; s->d_lights.n = 0;
         s->tree.p = nullptr; s->tree.n = 0;
@@ -1433,7 +1478,7 @@ vkb_status vkb_scene_destroy(vkb_scene* s) {
     s->changed.release();
     s->indices.release(); s->tlas_codes.release();
     s->tlas_order.release(); s->tlas_leaf_parent.release(); s->tlas_node_parent.release(); s->tlas_counters.release(); s->inst_info.release(); s->meshes.release();
-    s->blas4.release(); s->tlas4.release(); s->tlas_odd.release(); s->tlas_nodes.release(); s->tlas_leaves.release(); s->d_materials.release(); s->d_lights.release();
+    s->blas4.release(); s->blas8.release(); s->tlas4.release(); s->tlas_odd.release(); s->tlas_nodes.release(); s->tlas_leaves.release(); s->d_materials.release(); s->d_lights.release();
     s->tree.release();
     s->scratch.codes.release(); s->scratch.codes_sorted.release(); s->scratch.ids.release(); s->scratch.ids_sorted.release();
     s->scratch.leaf_parent.release(); s->scratch.node_parent.release(); s->scratch.counters.release(); s->scratch.bounds.release(); s->scratch.cub_temp.release();
@@ -1624,7 +1669,8 @@ vkb_status vkb_scene_info(vkb_scene* s, vkb_scene_info_t* out) {
     out->tlas_refits = s->tlas_refits;
     out->motion_bytes = s->motion_bytes;
     size_t dev = 0;
-    dev += s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas4.n * sizeof(Bvh4Node) + (s->blas_tris.n + s->tri_nrm.n) * sizeof(float4);
+    dev += s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas4.n * sizeof(Bvh4Node) + s->blas8.n * sizeof(Bvh8Node) +
+           (s->blas_tris.n + s->tri_nrm.n) * sizeof(float4);
     dev += s->tlas_nodes.n * sizeof(BvhNode) + s->tlas4.n * sizeof(Bvh4Node) + s->tlas_odd.n + s->tlas_leaves.n * sizeof(TlasLeaf) + (s->o2w.n + s->w2o.n) * sizeof(float4);
     dev += s->env_img.n * sizeof(float4) + s->env_dist.n * sizeof(float2) + s->em_inst_source.n * 4 + s->em_sources.n * sizeof(uint2) + s->em_tree.n * sizeof(float);
     out->scene_bytes = dev;
@@ -1821,7 +1867,8 @@ vkb_status vkb_debug_trace(vkb_scene* s, uint32_t n, const float* rays7, float* 
         r.upload(rays4.data(), rays4.size(), st);
         t.alloc(n); uv.alloc(size_t(n) * 2); ids.alloc(size_t(n) * 2); err.alloc(1);
         VKB_CUDA(cudaMemsetAsync(err.p, 0, sizeof(uint32_t), st));
-        if (n) k_debug_trace<<<grid_for(n, 128, s->ctx->sms), 128, 0, st>>>(scene_view(s), n, r.p, t.p, ids.p, uv.p, err.p);
+        if (n && s->blas8.p) k_debug_trace<true><<<grid_for(n, 128, s->ctx->sms), 128, 0, st>>>(scene_view(s), n, r.p, t.p, ids.p, uv.p, err.p);
+        else if (n) k_debug_trace<false><<<grid_for(n, 128, s->ctx->sms), 128, 0, st>>>(scene_view(s), n, r.p, t.p, ids.p, uv.p, err.p);
         if (n) {
             VKB_CUDA(cudaMemcpyAsync(out_t, t.p, n * sizeof(float), cudaMemcpyDeviceToHost, st));
             VKB_CUDA(cudaMemcpyAsync(out_ids, ids.p, size_t(n) * 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -1849,7 +1896,8 @@ vkb_status vkb_debug_occluded(vkb_scene* s, uint32_t n, const float* rays7, uint
         occ.alloc(n); err.alloc(1);
         VKB_CUDA(cudaMemsetAsync(err.p, 0, sizeof(uint32_t), st));
         if (n) {
-            k_debug_occluded<<<grid_for(n, 128, s->ctx->sms), 128, 0, st>>>(scene_view(s), n, r.p, occ.p, err.p);
+            if (s->blas8.p) k_debug_occluded<true><<<grid_for(n, 128, s->ctx->sms), 128, 0, st>>>(scene_view(s), n, r.p, occ.p, err.p);
+            else k_debug_occluded<false><<<grid_for(n, 128, s->ctx->sms), 128, 0, st>>>(scene_view(s), n, r.p, occ.p, err.p);
             VKB_CUDA(cudaMemcpyAsync(out_occluded, occ.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         }
         uint32_t e = 0;
@@ -1903,7 +1951,7 @@ uint64_t scene_bytes(const vkb_scene* s) {
     uint64_t own = s->tlas_nodes.n * sizeof(BvhNode) + s->tlas4.n * sizeof(Bvh4Node) + s->tlas_odd.n + s->tlas_leaves.n * sizeof(TlasLeaf) +
                    (s->o2w.n + s->w2o.n) * sizeof(float4) + s->inst_info.n * sizeof(uint4) + s->em_tree.n * sizeof(float);
     if (s->base) return own;
-    return own + s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas4.n * sizeof(Bvh4Node) +
+    return own + s->vpos.n * sizeof(float4) + s->vnrm.n * sizeof(float4) + s->indices.n * 4 + s->blas4.n * sizeof(Bvh4Node) + s->blas8.n * sizeof(Bvh8Node) +
            (s->blas_tris.n + s->tri_nrm.n) * sizeof(float4) + s->env_img.n * sizeof(float4) + s->env_dist.n * sizeof(float2) +
            s->em_inst_source.n * 4 + s->em_sources.n * sizeof(uint2);
 }
@@ -2004,6 +2052,7 @@ vkb_status vkb_server_submit_view(vkb_server* v, vkb_scene* s, const vkb_camera*
         validate_profile(pf);
         if (cam) validate_camera(*cam);
         if (pf->adaptive) throw Unsupported{"adaptive stopping renders through vkb_render"};
+        if (s->blas8.p) throw Unsupported{"compressed 8-wide BLAS scenes render through vkb_render and vkb_render_batch"};
         const vkb_camera& c = cam ? *cam : s->camera;
         uint64_t need = uint64_t(c.width) * c.height * 32u;
         const uint64_t sb = scene_bytes(s) + (s->base ? scene_bytes(s->base) : 0u);

@@ -31,6 +31,15 @@ struct alignas(16) BvhNode { float4 a, b, c; int4 d; };
 struct alignas(16) Bvh4Node { float4 plane[6]; int4 child; int4 pad; };
 static_assert(sizeof(Bvh4Node) == 128, "one 128-byte line per 4-wide node");
 
+// Compressed 8-wide BLAS node, 80 bytes (the layout of vkb_host::Wide8Node, built on the
+// host in vkb_wide8.h): child boxes as bytes on the node's grid (origin + q * 2^(e-127)
+// per axis, rounded outward), internal children from child_base in the first slots, leaf
+// triangles from leaf_base in the next ones, unused slots (lo 255 > hi 0) last.
+//   h = (origin.xyz, bits: ex | ey << 8 | ez << 16 | internal-slot mask << 24)
+//   b = (child_base, leaf_base, used slots, -);  q[a] = (lo bytes 0-3, lo 4-7, hi 0-3, hi 4-7) of axis a
+struct alignas(16) Bvh8Node { float4 h; uint4 b; uint4 q[3]; };
+static_assert(sizeof(Bvh8Node) == 80, "80-byte compressed 8-wide node");
+
 // One TLAS leaf, in Morton order: the instance's world->object rows and what its BLAS needs.
 struct alignas(16) TlasLeaf { float4 w2o[3]; uint32_t instance, node_offset, tri_offset, flags; };
 constexpr uint32_t LEAF_CULL_BACKFACES = 1u;
@@ -55,6 +64,9 @@ struct MeshInfo {
 constexpr int SMEM_STACK = VKB_SMEM_STACK;
 constexpr int SPILL_STACK = VKB_SPILL_STACK;
 constexpr int STACK_CAP = SMEM_STACK + SPILL_STACK;
+// An 8-wide BLAS visit pushes up to seven children: its traversals get a deeper local part.
+constexpr int SPILL_STACK8 = 104;
+constexpr int STACK_CAP8 = SMEM_STACK + SPILL_STACK8;
 constexpr int TRACE_BLOCK = 128;
 struct TraceStack {
     int* r;
@@ -158,6 +170,23 @@ __device__ __forceinline__ int slot_child(const int4& c, uint32_t key) {
     const int lo = odd ? c.y : c.x, hi = odd ? c.w : c.z;
     return (key & 2u) ? hi : lo;
 }
+// Byte k (0-3) of w as a float: a byte permute builds 2^23 + byte, an exact subtract removes 2^23.
+__device__ __forceinline__ float byte_f(uint32_t w, uint32_t k) {
+    return __uint_as_float(__byte_perm(w, 0x4b000000u, k | 0x7440u)) - 8388608.f;
+}
+// Far-first key of an 8-wide slot (three slot bits).
+__device__ __forceinline__ uint32_t far_key8(uint32_t key) {
+    return key == 0xffffffffu ? key : ((0x7ffffff8u - (key & ~7u)) | (key & 7u));
+}
+// Batcher's odd-even merge network for eight keys (19 exchanges), ascending.
+__device__ __forceinline__ void sort8(uint32_t (&k)[8]) {
+    key_order(k[0], k[1]); key_order(k[2], k[3]); key_order(k[4], k[5]); key_order(k[6], k[7]);
+    key_order(k[0], k[2]); key_order(k[1], k[3]); key_order(k[4], k[6]); key_order(k[5], k[7]);
+    key_order(k[1], k[2]); key_order(k[5], k[6]);
+    key_order(k[0], k[4]); key_order(k[1], k[5]); key_order(k[2], k[6]); key_order(k[3], k[7]);
+    key_order(k[2], k[4]); key_order(k[3], k[5]);
+    key_order(k[1], k[2]); key_order(k[3], k[4]); key_order(k[5], k[6]);
+}
 // Watertight ray/triangle test. cull: accept front faces only (counter-clockwise
 // winding seen from the ray origin).  Returns t and barycentrics of vertices 1, 2.
 __device__ __forceinline__ bool tri_test(const RaySpace& r, float3 v0, float3 v1, float3 v2, bool cull, float tbest, float& t, float& b1, float& b2) {
@@ -220,6 +249,7 @@ struct SceneView {
     const Bvh4Node* tlas_nodes;
     const TlasLeaf* tlas_leaves;
     const Bvh4Node* blas_nodes;
+    const Bvh8Node* blas8;       // compressed 8-wide BLAS nodes (scenes built with VKB_BLAS_WIDE8)
     const float4* blas_tris;     // 3 per triangle (Morton order within a mesh); v0.w = original triangle id
     uint32_t num_instances;
 };
@@ -230,14 +260,16 @@ struct TraceCount { uint32_t nodes = 0, tris = 0, instances = 0, blas_nodes = 0;
 // Traversal state of one ray: closest hit (ANY == false) or first hit (ANY == true) over
 // the two-level BVH, advanced one step (a 4-wide node, an instance entry, a BLAS leaf,
 // then a pop) at a time.  Error: overflow/step-limit exits set *err and end the ray with
-// the best hit so far.
-template <bool ANY, bool COUNT = false>
+// the best hit so far.  W8: the BLASes are compressed 8-wide (the TLAS stays 4-wide).
+template <bool ANY, bool COUNT = false, bool W8 = false>
 struct TraceLane {
+    static constexpr int CAP = W8 ? STACK_CAP8 : STACK_CAP;
     RaySpace rs;
     float tbest;
     int node, sp;
     bool found, in_blas, cull;
     const Bvh4Node* nodes;
+    const Bvh8Node* nodes8;
     uint32_t tri_base, cur_instance, steps;
     HitRecord hit;
 
@@ -254,7 +286,57 @@ struct TraceLane {
         if (++steps >= TRACE_STEP_LIMIT) { atomicOr(err, 2u); return true; }
         bool respace = false;
         float3 so, sd;
-        if (node >= 0) {
+        if (W8 && in_blas && node >= 0) {
+            // A compressed 8-wide BLAS node: decode the eight slots' planes on the ray's
+            // grid (t = q * 2^e / d + (origin - o) / d), sort the hit slots' keys, descend
+            // into the first and push the rest (farthest first).
+            if (COUNT) { count->nodes++; count->blas_nodes++; }
+            const float4* p = reinterpret_cast<const float4*>(nodes8 + node);
+            const float4 h = __ldg(p);
+            const uint4 b = __ldg(reinterpret_cast<const uint4*>(p + 1));
+            const uint4 qx = __ldg(reinterpret_cast<const uint4*>(p + 2));
+            const uint4 qy = __ldg(reinterpret_cast<const uint4*>(p + 3));
+            const uint4 qz = __ldg(reinterpret_cast<const uint4*>(p + 4));
+            const uint32_t bits = __float_as_uint(h.w);
+            const float ax = __uint_as_float((bits & 0xffu) << 23) * rs.idir.x;
+            const float ay = __uint_as_float(((bits >> 8) & 0xffu) << 23) * rs.idir.y;
+            const float az = __uint_as_float(((bits >> 16) & 0xffu) << 23) * rs.idir.z;
+            const float bx = fmaf(h.x, rs.idir.x, -rs.ood.x), by = fmaf(h.y, rs.idir.y, -rs.ood.y), bz = fmaf(h.z, rs.idir.z, -rs.ood.z);
+            const bool nx = rs.idir.x < 0.f, ny = rs.idir.y < 0.f, nz = rs.idir.z < 0.f;
+            const uint32_t nx0 = nx ? qx.z : qx.x, nx1 = nx ? qx.w : qx.y, fx0 = nx ? qx.x : qx.z, fx1 = nx ? qx.y : qx.w;
+            const uint32_t ny0 = ny ? qy.z : qy.x, ny1 = ny ? qy.w : qy.y, fy0 = ny ? qy.x : qy.z, fy1 = ny ? qy.y : qy.w;
+            const uint32_t nz0 = nz ? qz.z : qz.x, nz1 = nz ? qz.w : qz.y, fz0 = nz ? qz.x : qz.z, fz1 = nz ? qz.y : qz.w;
+            uint32_t key[8];
+            #pragma unroll
+            for (uint32_t k = 0; k < 8u; ++k) {
+                const uint32_t sel = k & 3u;
+                const float tn = max3f(fmaf(byte_f(k < 4u ? nx0 : nx1, sel), ax, bx), fmaf(byte_f(k < 4u ? ny0 : ny1, sel), ay, by),
+                                       fmaxf(fmaf(byte_f(k < 4u ? nz0 : nz1, sel), az, bz), 0.f));
+                const float tf = min3f(fmaf(byte_f(k < 4u ? fx0 : fx1, sel), ax, bx), fmaf(byte_f(k < 4u ? fy0 : fy1, sel), ay, by),
+                                       fminf(fmaf(byte_f(k < 4u ? fz0 : fz1, sel), az, bz), tbest));
+                // Unused slots are skipped by the count: their inverted boxes could still pass
+                // the widened test on a ray from very far away.
+                key[k] = (k < b.z && tn <= tf * 1.00000024f) ? ((__float_as_uint(tn) & ~7u) | k) : 0xffffffffu;
+                if (ANY) key[k] = far_key8(key[k]);
+            }
+            sort8(key);
+            if (key[0] != 0xffffffffu) {
+                const uint32_t imask = bits >> 24, internal = uint32_t(__popc(imask));
+                auto child = [&](uint32_t kk) -> int {
+                    const uint32_t slot = kk & 7u;
+                    return ((imask >> slot) & 1u) ? int(b.x + slot) : ~int((b.y + slot - internal) << 2);
+                };
+                int pushes = 0;
+                #pragma unroll
+                for (int i = 1; i < 8; ++i) pushes += key[i] != 0xffffffffu ? 1 : 0;
+                if (sp + pushes > CAP) { atomicOr(err, 1u); return true; }
+                #pragma unroll
+                for (int i = 7; i >= 1; --i)
+                    if (key[i] != 0xffffffffu) { stk.put(sp, child(key[i])); ++sp; }
+                node = child(key[0]);
+                return false;
+            }
+        } else if (node >= 0) {
             if (COUNT) { count->nodes++; if (in_blas) count->blas_nodes++; }
             const float4* p = reinterpret_cast<const float4*>(nodes + node);
             const uint32_t sx = __float_as_uint(rs.idir.x) >> 31, sy = __float_as_uint(rs.idir.y) >> 31, sz = __float_as_uint(rs.idir.z) >> 31;
@@ -279,7 +361,7 @@ struct TraceLane {
                         if (k2 != 0xffffffffu) { stk.r[sp * TRACE_BLOCK] = slot_child(ch, k2); ++sp; }
                         stk.r[sp * TRACE_BLOCK] = slot_child(ch, k1); ++sp;
                     } else {
-                        if (sp + pushes > STACK_CAP) { atomicOr(err, 1u); return true; }
+                        if (sp + pushes > CAP) { atomicOr(err, 1u); return true; }
                         if (k3 != 0xffffffffu) { stk.put(sp, slot_child(ch, k3)); ++sp; }
                         if (k2 != 0xffffffffu) { stk.put(sp, slot_child(ch, k2)); ++sp; }
                         stk.put(sp, slot_child(ch, k1)); ++sp;
@@ -297,10 +379,11 @@ struct TraceLane {
             so = f3(r0.x * o.x + r0.y * o.y + r0.z * o.z + r0.w, r1.x * o.x + r1.y * o.y + r1.z * o.z + r1.w, r2.x * o.x + r2.y * o.y + r2.z * o.z + r2.w);
             sd = f3(r0.x * d.x + r0.y * d.y + r0.z * d.z, r1.x * d.x + r1.y * d.y + r1.z * d.z, r2.x * d.x + r2.y * d.y + r2.z * d.z);
             cur_instance = info.x;
-            nodes = s.blas_nodes + info.y;
+            if (W8) nodes8 = s.blas8 + info.y;
+            else nodes = s.blas_nodes + info.y;
             tri_base = info.z;
             cull = !ANY && (info.w & LEAF_CULL_BACKFACES);
-            if (sp >= STACK_CAP) { atomicOr(err, 1u); return true; }
+            if (sp >= CAP) { atomicOr(err, 1u); return true; }
             stk.put(sp, SENTINEL);
             ++sp;
             in_blas = true;
@@ -343,10 +426,10 @@ struct TraceLane {
     }
 };
 
-template <bool ANY, bool COUNT = false>
+template <bool ANY, bool COUNT = false, bool W8 = false>
 __device__ __forceinline__ bool trace_ray(const SceneView& s, RayRef ray, float tmax, HitRecord& hit, uint32_t* err,
                                           TraceCount* count, TraceStack stk) {
-    TraceLane<ANY, COUNT> L;
+    TraceLane<ANY, COUNT, W8> L;
     if (!L.start(s, ray, tmax)) return false;
     while (!L.step(s, ray, err, count, stk)) {}
     hit = L.hit;

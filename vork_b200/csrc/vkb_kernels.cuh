@@ -695,16 +695,18 @@ __device__ __forceinline__ void flush_count(unsigned long long* dst, uint32_t v)
 #ifndef VKB_TRACE_MIN_BLOCKS
 #define VKB_TRACE_MIN_BLOCKS 8
 #endif
-template <bool ANY, bool COUNT>
+template <bool ANY, bool COUNT, bool W8 = false>
 __device__ __forceinline__ bool trace_any(const SceneView& sv, RayRef ray, float tmax, HitRecord& h, uint32_t* err, TraceCount* tc,
                                           TraceStack stk) {
-    return trace_ray<ANY, COUNT>(sv, ray, tmax, h, err, tc, stk);
+    return trace_ray<ANY, COUNT, W8>(sv, ray, tmax, h, err, tc, stk);
 }
-// This thread's column of the block's shared-memory traversal stack.
-#define VKB_STACK_DECL                                                                                   \
+// This thread's column of the block's shared-memory traversal stack (W8: the deeper local
+// part of the 8-wide BLAS traversal).
+#define VKB_STACK_DECL_W(W8)                                                                             \
     __shared__ int stack_r_[SMEM_STACK * TRACE_BLOCK];                                                  \
-    int stack_spill_[SPILL_STACK > 0 ? SPILL_STACK : 1];                                                \
+    int stack_spill_[(W8) ? SPILL_STACK8 : (SPILL_STACK > 0 ? SPILL_STACK : 1)];                         \
     TraceStack stk{stack_r_ + threadIdx.x, stack_spill_};
+#define VKB_STACK_DECL VKB_STACK_DECL_W(false)
 // Lanes of a warp refill together once at most this many are still tracing.
 #ifndef VKB_TRACE_REFILL
 #define VKB_TRACE_REFILL 20
@@ -716,14 +718,14 @@ static_assert(VKB_TRACE_REFILL >= 1 && VKB_TRACE_REFILL <= 31, "refill threshold
 // does not run on with a few long rays while its other lanes wait (measured: a warp's
 // lanes otherwise spend ~60% of its steps idle behind its longest ray).  Refilling
 // each lane as soon as it finishes is slower: the refill code then runs on single lanes.
-template <bool COUNT, bool BATCH>
+template <bool COUNT, bool BATCH, bool W8 = false>
 __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace(PathParams p, int cur) {
-    VKB_STACK_DECL
+    VKB_STACK_DECL_W(W8)
     const uint32_t n = p.counters[cur];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.counters[3], n);
     const uint32_t lane = threadIdx.x & 31u;
     TraceCount tc;
-    TraceLane<false, COUNT> L;
+    TraceLane<false, COUNT, W8> L;
     constexpr uint32_t NONE = 0xffffffffu;
     uint32_t ray = NONE, job = 0;
     bool drained = false;
@@ -777,14 +779,14 @@ __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace(Pat
 // the unoccluded contributions to the slot's radiance.
 // EXT: waves with an image environment or emissive meshes, whose entries may carry an
 // environment ray (phase 2) and a mesh ray (phase 3) after the light rays A and B.
-template <bool COUNT, bool BATCH, bool EXT>
+template <bool COUNT, bool BATCH, bool EXT, bool W8 = false>
 __global__ void __launch_bounds__(TRACE_BLOCK, VKB_TRACE_MIN_BLOCKS) k_trace_shadow(PathParams p) {
-    VKB_STACK_DECL
+    VKB_STACK_DECL_W(W8)
     const uint32_t n = p.counters[2];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.counters[4], n);
     const uint32_t lane = threadIdx.x & 31u;
     TraceCount tc;
-    TraceLane<true, COUNT> L;
+    TraceLane<true, COUNT, W8> L;
     constexpr uint32_t NONE = 0xffffffffu;
     uint32_t e = NONE, rid = 0, phase = 0, occ = 0, job = 0;
     // Starts entry e's next ray from phase ph on; false when the entry has no ray left.
@@ -1625,11 +1627,12 @@ __global__ void k_sampler_groups(uint32_t n, const uint32_t* px, const uint32_t*
     }
 }
 // Test entry: closest hits of arbitrary world rays.
+template <bool W8>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_debug_trace(SceneView sv, uint32_t n, const float4* rays, float* t, uint32_t* ids, float* uv, uint32_t* err) {
-    VKB_STACK_DECL
+    VKB_STACK_DECL_W(W8)
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         HitRecord h;
-        bool f = trace_any<false, false>(sv, RayRef{rays, rays + n, i}, rays[i].w, h, err, nullptr, stk);
+        bool f = trace_any<false, false, W8>(sv, RayRef{rays, rays + n, i}, rays[i].w, h, err, nullptr, stk);
         t[i] = f ? h.t : -1.f;
         ids[2 * i] = f ? h.inst : 0xffffffffu; ids[2 * i + 1] = f ? __float_as_uint(__ldg(&sv.blas_tris[3u * size_t(h.tri)]).w) : 0xffffffffu;
         uv[2 * i] = f ? h.u : 0.f; uv[2 * i + 1] = f ? h.v : 0.f;
@@ -1637,11 +1640,12 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_debug_trace(SceneView sv, uint3
 }
 // Occlusion of n world rays by the shadow rays' any-hit traversal (first hit ends the
 // walk, no back-face culling): occluded[i] = 1 when anything lies within (0, tmax).
+template <bool W8>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_debug_occluded(SceneView sv, uint32_t n, const float4* rays, uint32_t* occluded, uint32_t* err) {
-    VKB_STACK_DECL
+    VKB_STACK_DECL_W(W8)
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         HitRecord h;
-        occluded[i] = trace_any<true, false>(sv, RayRef{rays, rays + n, i}, rays[i].w, h, err, nullptr, stk) ? 1u : 0u;
+        occluded[i] = trace_any<true, false, W8>(sv, RayRef{rays, rays + n, i}, rays[i].w, h, err, nullptr, stk) ? 1u : 0u;
     }
 }
 

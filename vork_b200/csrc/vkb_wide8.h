@@ -17,11 +17,11 @@ namespace vkb_host {
 
 // h = (origin.x, origin.y, origin.z, bits: ex | ey << 8 | ez << 16 | internal-slot mask << 24),
 //     e the biased exponent of the axis step 2^(e - 127);
-// b = (child_base, leaf_base, 0, 0): the internal children take the first slots and
-//     are stored in slot order from child_base; the leaf children (one triangle each)
+// b = (child_base, leaf_base, used slots, 0): the internal children take the first slots
+//     and are stored in slot order from child_base; the leaf children (one triangle each)
 //     take the next slots, their triangles in slot order from leaf_base;
 // q[a] = (lo bytes of slots 0-3, lo 4-7, hi 0-3, hi 4-7) of axis a; an unused slot
-//     (always after the used ones) has lo 255 > hi 0, which every ray misses.
+//     (after the used ones) has lo 255 > hi 0, and the traversal skips it by the count.
 struct alignas(16) Wide8Node { float4 h; uint4 b; uint4 q[3]; };
 static_assert(sizeof(Wide8Node) == 80, "80-byte compressed 8-wide node");
 
@@ -128,7 +128,7 @@ struct Wide8Blas {
             float hb;
             std::memcpy(&hb, &bits, 4);
             node.h = make_float4(origin[0], origin[1], origin[2], hb);
-            node.b = make_uint4(child_base, leaf_base, 0u, 0u);
+            node.b = make_uint4(child_base, leaf_base, uint32_t(count), 0u);
             auto pack = [&](int row, int half) {
                 return qb[row][4 * half] | (qb[row][4 * half + 1] << 8) | (qb[row][4 * half + 2] << 16) | (qb[row][4 * half + 3] << 24);
             };

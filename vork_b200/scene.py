@@ -273,6 +273,7 @@ class Scene:
     name: str = "scene"
     tlas_builder: int = abi.TLAS_LBVH
     env_image: "EnvironmentImage | None" = None
+    blas_format: int = abi.BLAS_WIDE4
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -313,6 +314,7 @@ class Scene:
         d.camera = self.camera
         d.environment = self.environment
         d.tlas_builder = self.tlas_builder
+        d.blas_format = self.blas_format
         if self.env_image is not None:
             img = np.ascontiguousarray(self.env_image.rgba, np.float32)
             e = abi.VkbEnvironmentImage()
