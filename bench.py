@@ -725,7 +725,8 @@ def main():
         traffic = dram_gbs = None
         prof_note = ROOT / "profiles" / "trace_closest_traffic.json"
         if prof_note.exists() and args.config in ("large", "profile"):
-            # ncu capture of a smaller case of the same scene, scaled by rays per launch.
+            # ncu capture of every closest-hit launch of one timed frame of this workload
+            # (DRAM bytes per ray, times this run's rays per launch).
             tr = json.loads(prof_note.read_text())
             rays_per_launch = counted["extension_rays"] / max(1, counted["trace_launches"])
             traffic = tr["traffic_bytes_per_ray"] * rays_per_launch
