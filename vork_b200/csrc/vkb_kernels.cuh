@@ -1256,47 +1256,10 @@ __global__ void __launch_bounds__(VKB_SHADE_BLOCK, VKB_SHADE_MIN_BLOCKS) k_shade
                 if (!finite3(smp.dir) || !finite3(smp.weight) || !isfinite(smp.pdf)) {
                     meta |= META_NONFINITE;
                 } else {
-                    // next_event (path.slang:851-951): one analytic light, two estimators.
-                    float3 va = f3(0.f), vb = f3(0.f);
-                    bool trace_a = false, has_b = false, trace_b = false;
-                    float3 oa, da, ob, db; float la = 0.f, lb = 0.f;
-                    if (J.num_lights > 0) {
-                        float4 u = sample_group(pseed, sidx, J.sample_mask, vertex_group(vtx, 1));   // path_light
-                        float probability;
-                        uint32_t li = tree_pick(J.tree, J.tree_nodes, s.world, u.z, u.w, probability);
-                        if (probability > 0.f && li < J.num_lights) {
-                            const vkb_light& L = J.lights[li];
-                            uint32_t contribution = L.shadow_offsets[VKB_LIGHT_CONTRIBUTION_WORD];
-                            bool shadowed = (L.shadow_offsets[VKB_LIGHT_RAY_WORD] & VKB_LIGHT_RAY_SHADOWED) != 0u;
-                            if ((contribution & VKB_LIGHT_LINK_ALL) || L.shadow_offsets[VKB_LIGHT_LINK_WORD]) {
-                                LightSample src = emitter_sample(L, s.world, u.x, u.y);
-                                float3 power = src.delta ? src.radiance : (src.pdf > 0.f ? src.radiance / src.pdf : f3(0.f));
-                                va = analytic_mis_response(c, view, src.dir, s.face, contribution, src.pdf, pr) * power / probability;
-                                va = light_threshold(va, J.light_threshold, rng);
-                                if (any_nonzero(va) && shadowed) {
-                                    oa = path_origin(s, src.dir);
-                                    ray_connection(oa, s.world, src.dir, src.distance, da, la);
-                                    trace_a = true;
-                                }
-                                bool continuation = (contribution & smp.event) && event_hemisphere(smp.event, smp.dir, s.face, s.geometric);
-                                if (continuation && dot(smp.dir, smp.dir) > 0.f) {
-                                    EmitterEval e = emitter_eval(L, s.world, smp.dir);
-                                    if (e.pdf > 0.f) {
-                                        float w = smp.pdf > 0.f ? mis_power(smp.pdf, e.pdf) : 1.f;
-                                        vb = light_threshold(smp.weight * e.radiance * (w / probability), J.light_threshold, rng);
-                                        if (any_nonzero(vb)) {
-                                            has_b = true;
-                                            if (shadowed) {
-                                                ob = path_origin(s, smp.dir);
-                                                ray_connection(ob, s.world, smp.dir, e.distance, db, lb);
-                                                trace_b = true;
-                                            }
-                                        }
-                                    }
-                                }
-                            }
-                        }
-                    }
+                    // The image-environment and mesh strategies first: their shadow rays go
+                    // to the slot's own buffers at once, so nothing of theirs stays live
+                    // across the analytic estimate (the sample groups and the order of the
+                    // sums in the shadow kernel do not depend on this order).
                     // environment_next_event (path.slang:1096-1120): a proposal direction,
                     // the diffuse and specular responses MIS-weighted against continuing
                     // there (continuation_mask, path.slang:1003-1010), one visibility ray
@@ -1373,6 +1336,47 @@ __global__ void __launch_bounds__(VKB_SHADE_BLOCK, VKB_SHADE_MIN_BLOCKS) k_shade
                                         p.sd_d[slot] = make_float4(cdir.x, cdir.y, cdir.z, 0.f);
                                         p.sd_c[slot] = make_float4(md.x, md.y, md.z, 0.f);
                                         trace_d = true;
+                                    }
+                                }
+                            }
+                        }
+                    }
+                    // next_event (path.slang:851-951): one analytic light, two estimators.
+                    float3 va = f3(0.f), vb = f3(0.f);
+                    bool trace_a = false, has_b = false, trace_b = false;
+                    float3 oa, da, ob, db; float la = 0.f, lb = 0.f;
+                    if (J.num_lights > 0) {
+                        float4 u = sample_group(pseed, sidx, J.sample_mask, vertex_group(vtx, 1));   // path_light
+                        float probability;
+                        uint32_t li = tree_pick(J.tree, J.tree_nodes, s.world, u.z, u.w, probability);
+                        if (probability > 0.f && li < J.num_lights) {
+                            const vkb_light& L = J.lights[li];
+                            uint32_t contribution = L.shadow_offsets[VKB_LIGHT_CONTRIBUTION_WORD];
+                            bool shadowed = (L.shadow_offsets[VKB_LIGHT_RAY_WORD] & VKB_LIGHT_RAY_SHADOWED) != 0u;
+                            if ((contribution & VKB_LIGHT_LINK_ALL) || L.shadow_offsets[VKB_LIGHT_LINK_WORD]) {
+                                LightSample src = emitter_sample(L, s.world, u.x, u.y);
+                                float3 power = src.delta ? src.radiance : (src.pdf > 0.f ? src.radiance / src.pdf : f3(0.f));
+                                va = analytic_mis_response(c, view, src.dir, s.face, contribution, src.pdf, pr) * power / probability;
+                                va = light_threshold(va, J.light_threshold, rng);
+                                if (any_nonzero(va) && shadowed) {
+                                    oa = path_origin(s, src.dir);
+                                    ray_connection(oa, s.world, src.dir, src.distance, da, la);
+                                    trace_a = true;
+                                }
+                                bool continuation = (contribution & smp.event) && event_hemisphere(smp.event, smp.dir, s.face, s.geometric);
+                                if (continuation && dot(smp.dir, smp.dir) > 0.f) {
+                                    EmitterEval e = emitter_eval(L, s.world, smp.dir);
+                                    if (e.pdf > 0.f) {
+                                        float w = smp.pdf > 0.f ? mis_power(smp.pdf, e.pdf) : 1.f;
+                                        vb = light_threshold(smp.weight * e.radiance * (w / probability), J.light_threshold, rng);
+                                        if (any_nonzero(vb)) {
+                                            has_b = true;
+                                            if (shadowed) {
+                                                ob = path_origin(s, smp.dir);
+                                                ray_connection(ob, s.world, smp.dir, e.distance, db, lb);
+                                                trace_b = true;
+                                            }
+                                        }
                                     }
                                 }
                             }
