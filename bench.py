@@ -604,6 +604,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tlas", choices=["lbvh", "ploc"], default="lbvh", help="TLAS builder of the frame scene")
     ap.add_argument("--blas", choices=["4", "8"], default="4", help="BLAS nodes: 4-wide FP32 planes or compressed 8-wide")
+    ap.add_argument("--serial-waves", action="store_true", help="large: one wave after another on one stream (no overlap)")
+    ap.add_argument("--wave-samples", type=int, default=0, help="large: samples per wave (0: as many as the wavefront holds)")
     ap.add_argument("--no-error", action="store_true", help="cache: skip the reference renders (timing/profiling runs)")
     ap.add_argument("--res", default="1920x1080", help="cache: frame resolution (smaller for profiling captures)")
     ap.add_argument("--schedule", default="srpt", choices=["srpt", "aged", "fair", "packed"], help="serve: wave schedule")
@@ -660,7 +662,12 @@ def main():
     pinned = [torch.from_numpy(f).pin_memory() for f in frames]
     image = torch.empty((cam.height, cam.width, 4), dtype=torch.float32, device=f"cuda:{local}")
     host_image = torch.empty((cam.height, cam.width, 4), dtype=torch.float32).pin_memory()
-    timed_prof = prof.__class__(**{**prof.__dict__, "flags": abi.PROFILE_TIME_KERNELS})
+    serial = abi.PROFILE_SERIAL_WAVES if args.serial_waves else 0
+    prof = prof.__class__(**{**prof.__dict__, "flags": serial, "wave_samples": args.wave_samples})
+    # Kernel durations for the roofline come from one more frame with events around every
+    # closest-hit launch and its waves one after another: with overlapped waves an event
+    # pair would also count the other stream's kernels sharing the SMs.
+    kernel_prof = prof.__class__(**{**prof.__dict__, "flags": abi.PROFILE_TIME_KERNELS | abi.PROFILE_SERIAL_WAVES})
     n_inst = frames[0].shape[0]
 
     def step(i, p):
@@ -676,7 +683,7 @@ def main():
     for i in range(args.warmup):
         step(i, prof)
     # One instrumented render (untimed) for the roofline's algorithmic bytes.
-    counted = s.render(prof.__class__(**{**prof.__dict__, "flags": abi.PROFILE_COUNT_TRAVERSAL}), device_ptr=image.data_ptr()).stats
+    counted = s.render(prof.__class__(**{**prof.__dict__, "flags": abi.PROFILE_COUNT_TRAVERSAL | serial}), device_ptr=image.data_ptr()).stats
 
     sync()
     launches0 = s.launch_count
@@ -688,15 +695,16 @@ def main():
     with ClockSampler(local) as clocks:
         ev0.record(stream)
         for k in range(args.steps):
-            st = step(args.warmup + k, timed_prof).stats
-            trace_ms += st["trace_ms"]
-            trace_launches += st["trace_launches"]
+            st = step(args.warmup + k, prof).stats
             latencies.append(st["render_ms"] + st["build_ms"])
             build_ms += st["build_ms"]
         ev1.record(stream)
         sync()
     elapsed_ms = ev0.elapsed_time(ev1)
     launches = s.launch_count - launches0
+    # The kernel-timing frame (untimed; the last frame's rows again).
+    kt = step(args.warmup + args.steps - 1, kernel_prof).stats
+    trace_ms, trace_launches = kt["trace_ms"] * args.steps, kt["trace_launches"] * args.steps
     tlas = {"builder": ("PLOC (radius 16)" if args.tlas == "ploc" else "Karras LBVH") + " over 30-bit Morton order (bit 30: boxes wider than a quarter of the centroid spread, split at the root), rebuilt every frame",
             "build_ms_per_frame": build_ms / args.steps,
             "blas_nodes": "compressed 8-wide (80 B)" if args.blas == "8" else "4-wide FP32 planes (128 B)",
@@ -738,6 +746,7 @@ def main():
             "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded generator; no dataset)",
             "config": {**cfg, "global_batch": paths_per_step * world, "parallelism": f"replicas x{world}",
+                       "waves": "one stream" if args.serial_waves else "alternating between two streams (overlapped)",
                        "l2_flush": "inputs > L2: 1M-instance TLAS + 2M-tri BLAS + 1.1 GB of wavefront queues per frame"},
             "latency_ms": {"p50": float(np.percentile(latencies, 50)), "p99": float(np.percentile(latencies, 99))},
             # Against HBM (the only roofline family this integer/pointer-chasing kernel has);

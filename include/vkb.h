@@ -191,6 +191,11 @@ typedef struct vkb_profile {
 /* Measurement switches of vkb_profile.flags (no reference counterpart: timing hooks). */
 #define VKB_PROFILE_TIME_KERNELS 1u        /* CUDA events around every closest-hit trace launch */
 #define VKB_PROFILE_COUNT_TRAVERSAL 2u     /* instrumented traversal: node and triangle visits */
+#define VKB_PROFILE_SERIAL_WAVES 16u       /* one wave after another on one stream (default: the
+                                              waves of a single-job render alternate between two
+                                              streams and wavefronts, so one wave's sparse last
+                                              bounces overlap the next wave's first ones; the
+                                              image is the same either way) */
 /* Wave scheduling of several jobs (vkb_render_batch flags / vkb_server_config.flags):
  * batches pack each job's remaining samples before the next job (throughput: fewer
  * scenes per wave keep their BVHs in L2) unless VKB_BATCH_FAIR; servers give the waves to

@@ -55,6 +55,16 @@ def test_lamp_scene_matches_fp32_oracle(renderer, oracle, mixed):
     assert min(fracs) > 0.95, fracs
 
 
+def test_overlapped_waves_of_a_lamp_scene_equal_serial_waves(renderer):
+    from vork_b200 import abi
+    sc = S.lamp_scene(width=64, height=48, seed=8)
+    sc.env_image = S.EnvironmentImage(S.sky_image(32, 16, sun_radiance=10.0), strength=0.3)
+    with renderer.install(sc) as s:
+        a = s.render(Profile.reference_transport(4, 6, wave_samples=1)).image
+        b = s.render(Profile.reference_transport(4, 6, wave_samples=1, flags=abi.PROFILE_SERIAL_WAVES)).image
+    assert np.array_equal(a, b)
+
+
 def test_weight_tree_follows_instance_updates(renderer):
     # Moving and scaling the lamps (a TLAS rebuild) re-derives the weight tree: the render
     # equals a fresh install of the moved scene.

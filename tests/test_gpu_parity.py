@@ -221,6 +221,17 @@ def test_deterministic_across_waves_and_runs(renderer, small_scene):
         assert np.allclose((h0 + h1) / 2, a, rtol=1e-5, atol=1e-6)
 
 
+def test_overlapped_waves_equal_serial_waves(renderer, small_scene):
+    # Waves of one render alternate between two streams and wavefronts; the accumulation
+    # keeps wave order, so the image and the counts equal one wave after another.
+    with renderer.install(small_scene) as s:
+        a = s.render(_small_profile(8, wave_samples=1))
+        b = s.render(_small_profile(8, wave_samples=1, flags=abi.PROFILE_SERIAL_WAVES))
+    assert np.array_equal(a.image, b.image)
+    for k in ("extension_rays", "shadow_rays", "dropped_path_samples", "dropped_light_samples", "traversal_overflows"):
+        assert a.stats[k] == b.stats[k], k
+
+
 def test_update_instances_equals_fresh_install(renderer, small_scene):
     moved = S.spheres_scene()
     moved.instance_rows = small_scene.instance_rows.copy()

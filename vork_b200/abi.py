@@ -90,7 +90,7 @@ DISPLAY_SRGB, DISPLAY_P3, DISPLAY_REC2100_PQ, DISPLAY_REC2100_HLG = 0, 1, 2, 3
 class VkbDisplayParams(C.Structure):
     _fields_ = [("display", C.c_uint32), ("exposure", C.c_float), ("gamma", C.c_float), ("peak_luminance", C.c_float),
                 ("reference_white", C.c_float), ("bits", C.c_uint32), ("unassociate", C.c_uint32), ("reserved", C.c_uint32)]
-PROFILE_TIME_KERNELS, PROFILE_COUNT_TRAVERSAL = 1, 2
+PROFILE_TIME_KERNELS, PROFILE_COUNT_TRAVERSAL, PROFILE_SERIAL_WAVES = 1, 2, 16
 BATCH_FAIR, BATCH_PACKED = 4, 8
 TLAS_LBVH, TLAS_PLOC = 0, 1
 BLAS_WIDE4, BLAS_WIDE8 = 0, 1

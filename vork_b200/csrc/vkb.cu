@@ -367,6 +367,11 @@ struct vkb_ctx {
     DBuf<float4> ad_mean, ad_m2;              // adaptive stopping: per-pixel moments
     DBuf<uint32_t> ad_state;                  // and parity/stop bits
     DBuf<float4> guide_slots, guide_accum, guide_staging;   // denoiser-guide renders
+    // Overlapped waves of single-job renders: a second stream and wavefront; consecutive
+    // waves alternate between the two, their accumulations kept in wave order by events.
+    cudaStream_t stream2 = nullptr;
+    Wavefront wave2;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr, acc_ev[2] = {nullptr, nullptr};
 };
 
 struct vkb_scene {
@@ -773,10 +778,13 @@ void launch_shadow(bool counted, int grid, cudaStream_t st, const PathParams& p)
     if (counted) k_trace_shadow<true, BATCH, EXT, W8><<<grid, TRACE_BLOCK, 0, st>>>(p);
     else k_trace_shadow<false, BATCH, EXT, W8><<<grid, TRACE_BLOCK, 0, st>>>(p);
 }
+// st: the wave's stream; acc_wait / acc_done: events that order the accumulation after
+// the previous wave's and mark this one's (overlapped waves), or null.
 template <bool BATCH>
 void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counted, bool timed, WaveTotals& tot,
-                  const CacheLaunch* cache = nullptr, bool ext = false, bool w8 = false) {
-    cudaStream_t st = c->stream;
+                  const CacheLaunch* cache = nullptr, bool ext = false, bool w8 = false, cudaStream_t st = nullptr,
+                  cudaEvent_t acc_wait = nullptr, cudaEvent_t acc_done = nullptr) {
+    if (!st) st = c->stream;
     const int sms = c->sms, tgrid = sms * c->trace_blocks_per_sm, sgrid = sms * c->trace_blocks_per_sm;
     const bool adaptive = !BATCH && p.job0.adaptive;
     if (adaptive) k_adaptive_decide<<<grid_for(p.job0.npix, 256, sms), 256, 0, st>>>(p);
@@ -825,7 +833,9 @@ void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counte
         tot.cache_launches++;
         tot.launches += 1;
     }
+    if (acc_wait) VKB_CUDA(cudaStreamWaitEvent(st, acc_wait, 0));
     k_accumulate<BATCH><<<sms * 8, 256, 0, st>>>(p);
+    if (acc_done) VKB_CUDA(cudaEventRecord(acc_done, st));
     tot.launches += 3 + 4 * (bounces + 1) + (adaptive ? 1 : 0);
 }
 
@@ -837,6 +847,9 @@ void wave_kernels(vkb_ctx* c, const PathParams& p, uint32_t bounces, bool counte
 struct WaveEngine {
     vkb_ctx* c;
     WaveBuffers w;
+    WaveBuffers w2;                     // overlapped waves: the second wavefront (on c->stream2)
+    bool overlap = false;
+    uint32_t waves = 0;
     size_t capacity;
     uint32_t flags;
     bool graphs;
@@ -874,7 +887,12 @@ struct WaveEngine {
     }
     // One wave; false when no job has work left.
     bool step() {
-        cudaStream_t st = c->stream;
+        // Overlapped waves alternate between the two wavefronts and streams.
+        const bool second = overlap && (waves & 1u);
+        const WaveBuffers& w = second ? this->w2 : this->w;
+        cudaStream_t st = second ? c->stream2 : c->stream;
+        cudaEvent_t acc_wait = (overlap && waves > 0) ? c->acc_ev[(waves - 1) & 1u] : nullptr;
+        cudaEvent_t acc_done = overlap ? c->acc_ev[waves & 1u] : nullptr;
         const uint32_t njobs = uint32_t(jobs.size());
         if (njobs == 0) return false;
         if (njobs > w.job_capacity) throw ArgError{"more active jobs than the job table holds"};
@@ -1003,11 +1021,12 @@ struct WaveEngine {
             tot.launches += 3 + 4 * (bounces + 1);
             tot.trace_launches += bounces + 1;
         } else if (batch) {
-            wave_kernels<true>(c, p, bounces, counted, timed, tot, nullptr, ext, w8);
+            wave_kernels<true>(c, p, bounces, counted, timed, tot, nullptr, ext, w8, st, acc_wait, acc_done);
         } else {
-            wave_kernels<false>(c, p, bounces, counted, timed, tot, cache, ext, w8);
+            wave_kernels<false>(c, p, bounces, counted, timed, tot, cache, ext, w8, st, acc_wait, acc_done);
         }
         VKB_CUDA(cudaGetLastError());
+        ++waves;
         return true;
     }
     // Mean image of job k into its out_dev.
@@ -1024,7 +1043,22 @@ struct WaveEngine {
         VKB_CUDA(cudaMemcpyAsync(tot.counters, w.counters, sizeof(tot.counters), cudaMemcpyDeviceToHost, st));
         VKB_CUDA(cudaMemcpyAsync(tot.work, w.work, sizeof(tot.work), cudaMemcpyDeviceToHost, st));
         VKB_CUDA(cudaMemcpyAsync(&tot.err, w.err, sizeof(tot.err), cudaMemcpyDeviceToHost, st));
+        uint32_t counters2[16] = {};
+        unsigned long long work2[8] = {};
+        uint32_t err2 = 0;
+        if (overlap) {
+            // c->stream has joined c->stream2: the second wavefront's totals are final.
+            VKB_CUDA(cudaMemcpyAsync(counters2, w2.counters, sizeof(counters2), cudaMemcpyDeviceToHost, st));
+            VKB_CUDA(cudaMemcpyAsync(work2, w2.work, sizeof(work2), cudaMemcpyDeviceToHost, st));
+            VKB_CUDA(cudaMemcpyAsync(&err2, w2.err, sizeof(err2), cudaMemcpyDeviceToHost, st));
+        }
         VKB_CUDA(cudaStreamSynchronize(st));
+        if (overlap) {
+            static_assert(sizeof(tot.counters) == sizeof(counters2) && sizeof(tot.work) == sizeof(work2), "per-wavefront totals");
+            for (int k = 0; k < 16; ++k) tot.counters[k] += counters2[k];
+            for (int k = 0; k < 8; ++k) tot.work[k] += work2[k];
+            tot.err |= err2;
+        }
         tot.render_ms = ms_since_ev0;
         if (flags & VKB_PROFILE_TIME_KERNELS)
             for (uint32_t k = 0; k < tot.trace_launches; ++k) {
@@ -1042,14 +1076,31 @@ struct WaveEngine {
 };
 
 // Run `jobs` to completion on the wavefront `w` and resolve each into its out_dev.
+// w2 (non-null: overlapped waves): the second wavefront, used on c->stream2.
 void run_engine(vkb_ctx* c, std::vector<EngineJob>& jobs, const WaveBuffers& w, size_t capacity, uint32_t flags, bool graphs, WaveTotals& tot,
-                bool packed = false, const CacheLaunch* cache = nullptr) {
+                bool packed = false, const CacheLaunch* cache = nullptr, const WaveBuffers* w2 = nullptr) {
     WaveEngine eng(c, w, capacity, flags, graphs);
     eng.packed = packed;
     eng.cache = cache;
     for (auto& e : jobs) eng.add(e);
+    if (w2) {
+        eng.overlap = true;
+        eng.w2 = *w2;
+        VKB_CUDA(cudaMemsetAsync(w2->counters, 0, 16 * sizeof(uint32_t), c->stream));
+        VKB_CUDA(cudaMemsetAsync(w2->err, 0, sizeof(uint32_t), c->stream));
+        VKB_CUDA(cudaMemsetAsync(w2->work, 0, 8 * sizeof(unsigned long long), c->stream));
+    }
     VKB_CUDA(cudaEventRecord(c->ev0, c->stream));
+    if (w2) {
+        // c->stream2 starts after everything queued so far (scene builds, cleared accumulators).
+        VKB_CUDA(cudaEventRecord(c->fork_ev, c->stream));
+        VKB_CUDA(cudaStreamWaitEvent(c->stream2, c->fork_ev, 0));
+    }
     while (eng.step()) {}
+    if (w2) {
+        VKB_CUDA(cudaEventRecord(c->join_ev, c->stream2));
+        VKB_CUDA(cudaStreamWaitEvent(c->stream, c->join_ev, 0));
+    }
     VKB_CUDA(cudaEventRecord(c->ev1, c->stream));
     for (size_t k = 0; k < eng.jobs.size(); ++k) eng.resolve(k);
     VKB_CUDA(cudaEventSynchronize(c->ev1));
@@ -1160,7 +1211,17 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
         }
         paths += uint64_t(e.npix) * e.count;
     }
-    run_engine(c, jobs, wb, capacity, flags, true, tot, (flags & VKB_BATCH_FAIR) == 0, cache);
+    // A single job of more than one wave overlaps its waves on two streams (not with the
+    // adaptive, guide or radiance-cache hooks, which read one wave's results in the next).
+    const bool overlap = in.size() == 1 && !adaptive && !guides && !cache && !(flags & VKB_PROFILE_SERIAL_WAVES) &&
+                         uint64_t(jobs[0].npix) * jobs[0].count > capacity;
+    WaveBuffers wb2;
+    if (overlap) {
+        c->wave2.reserve(capacity, 1u);
+        if (in[0].first->env_w || in[0].first->em_tris) c->wave2.reserve_ext(std::max(capacity, c->wave2.ray_o0.n));
+        wb2 = c->wave2.view();
+    }
+    run_engine(c, jobs, wb, capacity, flags, true, tot, (flags & VKB_BATCH_FAIR) == 0, cache, overlap ? &wb2 : nullptr);
     for (size_t k = 0; k < in.size(); ++k) {
         if (guides && !outs[k]->on_device) {
             const size_t bytes = size_t(jobs[k].npix) * sizeof(float4);
@@ -1189,8 +1250,13 @@ vkb_status vkb_open(int device, vkb_ctx** out) {
         VKB_CUDA(cudaSetDevice(device));
         VKB_CUDA(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
         VKB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        VKB_CUDA(cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
         VKB_CUDA(cudaEventCreate(&c->ev0));
         VKB_CUDA(cudaEventCreate(&c->ev1));
+        VKB_CUDA(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
+        VKB_CUDA(cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming));
+        VKB_CUDA(cudaEventCreateWithFlags(&c->acc_ev[0], cudaEventDisableTiming));
+        VKB_CUDA(cudaEventCreateWithFlags(&c->acc_ev[1], cudaEventDisableTiming));
         c->lut.alloc(size_t(BRDF_SIZE) * BRDF_HEIGHT);
         k_bake_lut<<<dim3(1, BRDF_HEIGHT), BRDF_SIZE, 0, c->stream>>>(c->lut.p);
         VKB_CUDA(cudaGetLastError());
@@ -1207,15 +1273,20 @@ vkb_status vkb_close(vkb_ctx* c) {
     if (!c) return VKB_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->stream2) cudaStreamSynchronize(c->stream2);
+    for (cudaEvent_t e : {c->fork_ev, c->join_ev, c->acc_ev[0], c->acc_ev[1]})
+        if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : c->kernel_events) cudaEventDestroy(e);
     for (cudaEvent_t e : c->cache_events) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     c->wave.release();
+    c->wave2.release();
     c->accum.release(); c->staging.release(); c->ids.release(); c->ad_mean.release(); c->ad_m2.release(); c->ad_state.release();
     c->guide_slots.release(); c->guide_accum.release(); c->guide_staging.release();
     c->lut.release(); c->filter.release();
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->stream2) cudaStreamDestroy(c->stream2);
     delete c;
     return VKB_OK;
 }
