@@ -189,7 +189,8 @@ typedef struct vkb_profile {
 } vkb_profile;
 
 /* Measurement switches of vkb_profile.flags (no reference counterpart: timing hooks). */
-#define VKB_PROFILE_TIME_KERNELS 1u        /* CUDA events around every closest-hit trace launch */
+#define VKB_PROFILE_TIME_KERNELS 1u        /* CUDA events around every closest-hit trace launch
+                                              (its waves then run one after another) */
 #define VKB_PROFILE_COUNT_TRAVERSAL 2u     /* instrumented traversal: node and triangle visits */
 #define VKB_PROFILE_SERIAL_WAVES 16u       /* one wave after another on one stream (default: the
                                               waves of a single-job render alternate between two

@@ -1213,7 +1213,10 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
     }
     // A single job of more than one wave overlaps its waves on two streams (not with the
     // adaptive, guide or radiance-cache hooks, which read one wave's results in the next).
-    const bool overlap = in.size() == 1 && !adaptive && !guides && !cache && !(flags & VKB_PROFILE_SERIAL_WAVES) &&
+    // Timed renders keep one stream too: an event pair around a kernel would also count the
+    // other stream's kernels sharing the SMs.
+    const bool overlap = in.size() == 1 && !adaptive && !guides && !cache &&
+                         !(flags & (VKB_PROFILE_SERIAL_WAVES | VKB_PROFILE_TIME_KERNELS)) &&
                          uint64_t(jobs[0].npix) * jobs[0].count > capacity;
     WaveBuffers wb2;
     if (overlap) {
