@@ -274,7 +274,7 @@ def batch_block(r, jobs: int, warmup: int) -> dict:
     wave, wave shape from the autotuner) against one plain render per job in sequence;
     per-job images are bit-identical between the arms (the test suite checks that)."""
     import torch
-    from vork_b200 import Profile, scene
+    from vork_b200 import Profile, abi, scene
     t_block = time.perf_counter()
     items = [(r.install(sc), Profile.reference_transport(depth, spp)) for sc, spp, depth in scene.preview_jobs(jobs, seed=0)]
     paths = sum(i.scene.camera.width * i.scene.camera.height * p.samples for i, p in items)
@@ -298,6 +298,9 @@ def batch_block(r, jobs: int, warmup: int) -> dict:
         t0 = time.perf_counter()
         r.render_batch(items, flags=4, outs=outs)  # fair scheduling (one sample of every job per wave)
         fair_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        r.render_batch(items, flags=abi.PROFILE_SERIAL_WAVES, outs=outs)  # waves one after another, graphs replayed
+        serial_s = time.perf_counter() - t0
     for inst, _ in items:
         inst.close()
     return {"workload": f"batched previews: {len(items)} jobs, resolution log-uniform 128^2..1024^2, spp U{{4..32}}, depth U{{4..8}}, "
@@ -305,6 +308,7 @@ def batch_block(r, jobs: int, warmup: int) -> dict:
             "paths": paths, "value": paths / batch_s, "unit": "paths/s", "makespan_ms": 1000 * batch_s,
             "sequential": {"value": paths / seq_s, "unit": "paths/s", "makespan_ms": 1000 * seq_s},
             "fair_schedule": {"value": paths / fair_s, "unit": "paths/s", "makespan_ms": 1000 * fair_s},
+            "one_stream": {"value": paths / serial_s, "unit": "paths/s", "makespan_ms": 1000 * serial_s},
             "speedup_vs_sequential": seq_s / batch_s,
             "autotune": {k: tune[k] for k in ("best_capacity", "best_blocks_per_sm", "best_ms")},
             "gpu_launches": st["kernel_launches"], "clocks": clocks.summary(), "block_wall_s": time.perf_counter() - t_block}

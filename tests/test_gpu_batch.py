@@ -50,3 +50,22 @@ def test_autotune_picks_a_candidate_and_keeps_results(renderer):
     finally:
         for inst, _ in items:
             inst.close()
+
+
+def test_overlapped_batch_waves_equal_one_stream(renderer):
+    # Jobs of 2^25 paths and more take several waves of the default 32 Mi-slot wavefront:
+    # their waves alternate between two streams, and every image equals the one-stream run.
+    from vork_b200 import abi
+    items = []
+    for k, (side, spp) in enumerate([(1024, 16), (768, 24), (512, 40)]):
+        sc = S.spheres_scene(num_spheres=16, seed=20 + k, width=side, height=side, grid_cells=8)
+        items.append((renderer.install(sc), Profile.reference_transport(4, spp)))
+    try:
+        a, sa = renderer.render_batch(items)
+        b, sb = renderer.render_batch(items, flags=abi.PROFILE_SERIAL_WAVES)
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+        assert sa["extension_rays"] == sb["extension_rays"] and sa["shadow_rays"] == sb["shadow_rays"]
+    finally:
+        for inst, _ in items:
+            inst.close()

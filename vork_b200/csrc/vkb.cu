@@ -983,7 +983,9 @@ struct WaveEngine {
         }
         const uint32_t wave_jobs = uint32_t(wave_table.size());
         const bool batch = wave_jobs > 1;
-        const bool use_graph = graphs && batch && !timed;
+        // Overlapped waves launch directly: a captured graph would bake in one stream's
+        // events and buffers, and the second stream hides the launch gaps a graph saves.
+        const bool use_graph = graphs && batch && !timed && !overlap;
         uint32_t wave_counts[2] = {n_paths, total_pixels};
         VKB_CUDA(cudaMemcpyAsync(w.jobs, wave_table.data(), wave_jobs * sizeof(Job), cudaMemcpyHostToDevice, st));
         VKB_CUDA(cudaMemcpyAsync(w.counters + 7, wave_counts, sizeof(wave_counts), cudaMemcpyHostToDevice, st));
@@ -1211,17 +1213,22 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
         }
         paths += uint64_t(e.npix) * e.count;
     }
-    // A single job of more than one wave overlaps its waves on two streams (not with the
+    // Renders of more than one wave overlap their waves on two streams (not with the
     // adaptive, guide or radiance-cache hooks, which read one wave's results in the next).
     // Timed renders keep one stream too: an event pair around a kernel would also count the
     // other stream's kernels sharing the SMs.
-    const bool overlap = in.size() == 1 && !adaptive && !guides && !cache &&
-                         !(flags & (VKB_PROFILE_SERIAL_WAVES | VKB_PROFILE_TIME_KERNELS)) &&
-                         uint64_t(jobs[0].npix) * jobs[0].count > capacity;
+    uint64_t all_paths = 0;
+    bool any_ext = false;
+    for (size_t k = 0; k < jobs.size(); ++k) {
+        all_paths += uint64_t(jobs[k].npix) * jobs[k].count;
+        any_ext = any_ext || in[k].first->env_w || in[k].first->em_tris;
+    }
+    const bool overlap = !adaptive && !guides && !cache && !(flags & (VKB_PROFILE_SERIAL_WAVES | VKB_PROFILE_TIME_KERNELS)) &&
+                         all_paths > capacity;
     WaveBuffers wb2;
     if (overlap) {
-        c->wave2.reserve(capacity, 1u);
-        if (in[0].first->env_w || in[0].first->em_tris) c->wave2.reserve_ext(std::max(capacity, c->wave2.ray_o0.n));
+        c->wave2.reserve(capacity, uint32_t(in.size()));
+        if (any_ext) c->wave2.reserve_ext(std::max(capacity, c->wave2.ray_o0.n));
         wb2 = c->wave2.view();
     }
     run_engine(c, jobs, wb, capacity, flags, true, tot, (flags & VKB_BATCH_FAIR) == 0, cache, overlap ? &wb2 : nullptr);
