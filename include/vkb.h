@@ -182,7 +182,9 @@ typedef struct vkb_profile {
     float clamp_indirect;      /* clamp.y (0 = off) */
     float light_threshold;     /* adaptive.z: stochastic light-sample kill */
     uint32_t adaptive;         /* 1: adaptive stopping (path.slang:1792-1837), vkb_render of a whole exposure only */
-    uint32_t wave_samples;     /* samples per wavefront wave (0 = automatic; 1 with adaptive stopping) */
+    uint32_t wave_samples;     /* samples per wavefront wave (0 = automatic: as many as up to 64 Mi path
+                                  slots hold for one render, the context's capacity in a batch; 1 with
+                                  adaptive stopping) */
     uint32_t flags;            /* VKB_PROFILE_* measurement switches (0 for production renders) */
     float adaptive_threshold;  /* adaptive.x: relative standard error to stop at (0 = 0.01) */
     uint32_t adaptive_min_samples; /* sampling.w: samples before stopping (0 = max(16, sqrt(samples))) */

@@ -349,6 +349,7 @@ struct Wavefront {
 };
 struct GraphEntry { uint64_t key; cudaGraphExec_t exec; };
 
+constexpr size_t SINGLE_JOB_WAVE_SLOTS = size_t(64) << 20;   // 14.8 GB of queues per wavefront when full
 struct vkb_ctx {
     int device = 0;
     int sms = 148;
@@ -1171,8 +1172,17 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
         c->ad_mean.alloc(max_pix); c->ad_m2.alloc(max_pix); c->ad_state.alloc(max_pix);
         VKB_CUDA(cudaMemsetAsync(c->ad_state.p, 0, max_pix * sizeof(uint32_t), st));
     }
+    // Path slots per wave: the context's (autotuned) capacity for batches; for one job the
+    // profile's samples per wave, else up to 64 Mi slots, but no more than the job's paths
+    // (measured on 1080p, 64-spp flock frames with overlapped waves: 2 waves of 32 samples
+    // 218.1 vs 4 of 16 215.8 M paths/s on some frames, equal on others; one wave of 64: 217.2).
     size_t capacity = c->wave_capacity;
-    if (in.size() == 1 && wave_samples_hint) capacity = max_pix * wave_samples_hint;
+    if (in.size() == 1) {
+        const uint64_t job_paths = uint64_t(max_pix) * (in[0].second.sample_count ? in[0].second.sample_count
+                                                                                   : in[0].second.samples - in[0].second.first_sample);
+        capacity = wave_samples_hint ? max_pix * wave_samples_hint
+                                     : size_t(std::min<uint64_t>(std::max<size_t>(capacity, SINGLE_JOB_WAVE_SLOTS), job_paths));
+    }
     capacity = std::max(capacity, max_pix);
     c->wave.reserve(capacity, uint32_t(in.size()));
     for (const auto& job : in)
