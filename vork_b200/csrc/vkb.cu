@@ -851,6 +851,13 @@ struct WaveEngine {
     WaveBuffers w2;                     // overlapped waves: the second wavefront (on c->stream2)
     bool overlap = false;
     uint32_t waves = 0;
+    cudaEvent_t* acc_ev = nullptr;      // overlapped waves: the accumulation-order events (default: the context's)
+    cudaStream_t last_stream = nullptr; // the stream of the latest wave
+    // A long-lived engine (the server's) clears admitted jobs' accumulators on the stream of
+    // the next wave instead of the context's stream, which may still be running the other
+    // stream's work: a later wave's accumulation waits for that wave's by the event chain.
+    bool defer_clears = false;
+    std::vector<std::pair<float4*, size_t>> pending_clears;
     size_t capacity;
     uint32_t flags;
     bool graphs;
@@ -874,7 +881,8 @@ struct WaveEngine {
         VKB_CUDA(cudaMemsetAsync(w.work, 0, 8 * sizeof(unsigned long long), st));
     }
     void add(EngineJob e) {
-        VKB_CUDA(cudaMemsetAsync(e.accum, 0, size_t(e.npix) * sizeof(float4), c->stream));
+        if (defer_clears) pending_clears.push_back({e.accum, size_t(e.npix)});
+        else VKB_CUDA(cudaMemsetAsync(e.accum, 0, size_t(e.npix) * sizeof(float4), c->stream));
         jobs.push_back(e);
         table.push_back(make_job(jobs.back()));
     }
@@ -892,8 +900,9 @@ struct WaveEngine {
         const bool second = overlap && (waves & 1u);
         const WaveBuffers& w = second ? this->w2 : this->w;
         cudaStream_t st = second ? c->stream2 : c->stream;
-        cudaEvent_t acc_wait = (overlap && waves > 0) ? c->acc_ev[(waves - 1) & 1u] : nullptr;
-        cudaEvent_t acc_done = overlap ? c->acc_ev[waves & 1u] : nullptr;
+        cudaEvent_t* order_ev = acc_ev ? acc_ev : c->acc_ev;
+        cudaEvent_t acc_wait = (overlap && waves > 0) ? order_ev[(waves - 1) & 1u] : nullptr;
+        cudaEvent_t acc_done = overlap ? order_ev[waves & 1u] : nullptr;
         const uint32_t njobs = uint32_t(jobs.size());
         if (njobs == 0) return false;
         if (njobs > w.job_capacity) throw ArgError{"more active jobs than the job table holds"};
@@ -988,6 +997,9 @@ struct WaveEngine {
         // events and buffers, and the second stream hides the launch gaps a graph saves.
         const bool use_graph = graphs && batch && !timed && !overlap;
         uint32_t wave_counts[2] = {n_paths, total_pixels};
+        for (const auto& pc : pending_clears) VKB_CUDA(cudaMemsetAsync(pc.first, 0, pc.second * sizeof(float4), st));
+        pending_clears.clear();
+        last_stream = st;
         VKB_CUDA(cudaMemcpyAsync(w.jobs, wave_table.data(), wave_jobs * sizeof(Job), cudaMemcpyHostToDevice, st));
         VKB_CUDA(cudaMemcpyAsync(w.counters + 7, wave_counts, sizeof(wave_counts), cudaMemcpyHostToDevice, st));
         PathParams p = path_params(c, w, wave_jobs);
@@ -1032,12 +1044,12 @@ struct WaveEngine {
         ++waves;
         return true;
     }
-    // Mean image of job k into its out_dev.
-    void resolve(size_t k) {
+    // Mean image of job k into its out_dev (on `st`, default the context's stream).
+    void resolve(size_t k, cudaStream_t st = nullptr) {
         PathParams p = path_params(c, w, 1);
         p.job0 = table[k];
         p.job0.pixel_base = 0;
-        k_resolve<false><<<grid_for(jobs[k].npix, 256, c->sms), 256, 0, c->stream>>>(p, jobs[k].npix);
+        k_resolve<false><<<grid_for(jobs[k].npix, 256, c->sms), 256, 0, st ? st : c->stream>>>(p, jobs[k].npix);
         tot.launches += 1;
     }
     // Counters, traversal work and device time of everything run so far (synchronises).
@@ -2015,6 +2027,8 @@ struct vkb_server {
     uint32_t max_jobs = 0;
     size_t capacity = 0;
     Wavefront wave;                                   // the server's own queues (renders on the context keep theirs)
+    Wavefront wave2;                                  // overlapped waves: the second wavefront (on the context's stream2)
+    cudaEvent_t acc_ev[2] = {nullptr, nullptr};       // and the events that keep its accumulations in wave order
     std::unique_ptr<WaveEngine> eng;
     struct Pending { uint64_t id; vkb_scene* s; vkb_profile pf; float* host_out; bool own_camera; vkb_camera cam; };
     // A request's device accumulator and mean image, taken from (and returned to) a pool
@@ -2126,6 +2140,26 @@ vkb_status vkb_server_create(vkb_ctx* c, const vkb_server_config* cfg, vkb_serve
         v->wave.reserve(v->capacity, v->max_jobs);
         VKB_CUDA(cudaStreamCreateWithFlags(&v->copy_stream, cudaStreamNonBlocking));
         v->eng = std::make_unique<WaveEngine>(c, v->wave.view(), v->capacity, cfg->flags, true);
+        // Consecutive waves alternate between two wavefronts and streams (as single renders
+        // do) when the budget holds both wavefronts and the flags do not ask for one stream;
+        // the second wavefront counts against the budget like the first, and the accumulator
+        // clears of admitted requests then go with the waves.
+        const uint64_t second = uint64_t(v->capacity) * 220u + uint64_t(v->max_jobs) * sizeof(Job);
+        if (!(cfg->flags & (VKB_PROFILE_SERIAL_WAVES | VKB_PROFILE_TIME_KERNELS)) && (!v->budget || v->wave_bytes + second < v->budget)) {
+            v->wave2.reserve(v->capacity, v->max_jobs);
+            VKB_CUDA(cudaEventCreateWithFlags(&v->acc_ev[0], cudaEventDisableTiming));
+            VKB_CUDA(cudaEventCreateWithFlags(&v->acc_ev[1], cudaEventDisableTiming));
+            WaveBuffers w2 = v->wave2.view();
+            VKB_CUDA(cudaMemsetAsync(w2.counters, 0, 16 * sizeof(uint32_t), c->stream));
+            VKB_CUDA(cudaMemsetAsync(w2.err, 0, sizeof(uint32_t), c->stream));
+            VKB_CUDA(cudaMemsetAsync(w2.work, 0, 8 * sizeof(unsigned long long), c->stream));
+            VKB_CUDA(cudaStreamSynchronize(c->stream));
+            v->eng->overlap = true;
+            v->eng->w2 = w2;
+            v->eng->acc_ev = v->acc_ev;
+            v->eng->defer_clears = true;
+            v->wave_bytes += second;
+        }
         v->eng->packed = (cfg->flags & VKB_BATCH_PACKED) != 0;
         v->eng->srpt = !v->eng->packed && (cfg->flags & VKB_BATCH_FAIR) == 0;
         if (!(cfg->aging_paths_per_s >= 0.0)) throw ArgError{"aging_paths_per_s must be non-negative"};
@@ -2187,7 +2221,7 @@ vkb_status vkb_server_step(vkb_server* v, vkb_server_status* status) {
             // wavefront's environment and mesh shadow rays and previous vertices (112 B per
             // path slot), kept for every later wave.
             const bool ext = (q.s->env_w || q.s->em_tris) && !v->wave.sc_o.p;
-            const uint64_t ext_bytes = ext ? uint64_t(v->capacity) * 112u : 0u;
+            const uint64_t ext_bytes = ext ? uint64_t(v->capacity) * 112u * (eng.overlap ? 2u : 1u) : 0u;
             if (v->budget && held() + scene + extra + ext_bytes > v->budget && v->pool_bytes) {
                 finished += reap(v, true, false);
                 free_pool(v);
@@ -2198,6 +2232,10 @@ vkb_status vkb_server_step(vkb_server* v, vkb_server_status* status) {
                 v->wave.reserve_ext(v->capacity);
                 v->wave_bytes += ext_bytes;
                 eng.w = v->wave.view();
+                if (eng.overlap) {   // ext_bytes counts both wavefronts
+                    v->wave2.reserve_ext(v->capacity);
+                    eng.w2 = v->wave2.view();
+                }
             }
             auto live = std::make_unique<vkb_server::Live>();
             live->id = q.id; live->host_out = q.host_out; live->npix = uint32_t(npix);
@@ -2220,12 +2258,13 @@ vkb_status vkb_server_step(vkb_server* v, vkb_server_status* status) {
         }
         if (!eng.jobs.empty()) {
             eng.step();
-            // Requests whose last samples are in this wave: resolve behind it; they are done
-            // once the wave's event has completed and their images are copied (reap).
+            // Requests whose last samples are in this wave: resolve behind it (on its stream);
+            // they are done once the wave's event has completed and their images are copied (reap).
+            cudaStream_t ws = eng.last_stream ? eng.last_stream : c->stream;
             vkb_server::Completion cpl;
             for (size_t k = 0; k < eng.jobs.size(); ++k) {
                 if (!eng.finished(k)) continue;
-                eng.resolve(k);
+                eng.resolve(k, ws);
                 for (auto& kv : v->live)
                     if (kv.second->buf.out == eng.jobs[k].out_dev) cpl.ids.push_back(kv.first);
             }
@@ -2237,7 +2276,7 @@ vkb_status vkb_server_step(vkb_server* v, vkb_server_status* status) {
             }
             cpl.ev = v->spare_events.back();
             v->spare_events.pop_back();
-            VKB_CUDA(cudaEventRecord(cpl.ev, c->stream));
+            VKB_CUDA(cudaEventRecord(cpl.ev, ws));
             v->inflight.push_back(std::move(cpl));
             // At most two waves in flight: wait for the older one before returning.
             if (v->inflight.size() > 2) finished += reap(v, false, true);
@@ -2272,7 +2311,9 @@ vkb_status vkb_server_destroy(vkb_server* v) {
     if (!v) return VKB_OK;
     cudaSetDevice(v->c->device);
     cudaStreamSynchronize(v->c->stream);
+    cudaStreamSynchronize(v->c->stream2);
     for (auto& cp : v->inflight) cudaEventDestroy(cp.ev);
+    for (cudaEvent_t e : v->acc_ev) if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : v->spare_events) cudaEventDestroy(e);
     if (v->copy_stream) { cudaStreamSynchronize(v->copy_stream); cudaStreamDestroy(v->copy_stream); }
     for (auto& kv : v->live) { cudaFree(kv.second->buf.accum); cudaFree(kv.second->buf.out); }
@@ -2280,6 +2321,7 @@ vkb_status vkb_server_destroy(vkb_server* v) {
     free_pool(v);
     v->eng.reset();
     v->wave.release();
+    v->wave2.release();
     delete v;
     return VKB_OK;
 }
