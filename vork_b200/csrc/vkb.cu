@@ -1187,7 +1187,7 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
     // Path slots per wave: the context's (autotuned) capacity for batches; for one job the
     // profile's samples per wave, else up to 64 Mi slots, but no more than the job's paths
     // (measured on 1080p, 64-spp flock frames with overlapped waves: 2 waves of 32 samples
-    // 218.1 vs 4 of 16 215.8 M paths/s on some frames, equal on others; one wave of 64: 217.2).
+    // 218.1 / 216.3 vs 4 of 16 215.8 / 214.2 M paths/s on two frame ranges; one wave of 64: 217.2).
     size_t capacity = c->wave_capacity;
     if (in.size() == 1) {
         const uint64_t job_paths = uint64_t(max_pix) * (in[0].second.sample_count ? in[0].second.sample_count
@@ -1645,7 +1645,7 @@ vkb_status vkb_render(vkb_scene* s, const vkb_profile* pf, vkb_output* out, vkb_
         if (!hint) {
             uint32_t count = pf->sample_count ? pf->sample_count : pf->samples - pf->first_sample;
             size_t npix = size_t(s->camera.width) * s->camera.height;
-            hint = uint32_t(std::max<size_t>(1, std::min<size_t>(count, c->wave_capacity / std::max<size_t>(1, npix))));
+            hint = uint32_t(std::max<size_t>(1, std::min<size_t>(count, std::max(c->wave_capacity, SINGLE_JOB_WAVE_SLOTS) / std::max<size_t>(1, npix))));
         }
         render_jobs(c, in, outs, pf->flags, hint, tot, paths);
         s->launches += tot.launches;
@@ -1670,7 +1670,7 @@ vkb_status vkb_render_view(vkb_scene* s, const vkb_camera* cam, const vkb_profil
         if (!hint) {
             uint32_t count = pf->sample_count ? pf->sample_count : pf->samples - pf->first_sample;
             size_t npix = size_t(cam->width) * cam->height;
-            hint = uint32_t(std::max<size_t>(1, std::min<size_t>(count, c->wave_capacity / std::max<size_t>(1, npix))));
+            hint = uint32_t(std::max<size_t>(1, std::min<size_t>(count, std::max(c->wave_capacity, SINGLE_JOB_WAVE_SLOTS) / std::max<size_t>(1, npix))));
         }
         render_jobs(c, in, outs, pf->flags, hint, tot, paths, nullptr, &cams);
         s->launches += tot.launches;
