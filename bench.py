@@ -347,7 +347,7 @@ def serve_scenes(r, flock_inst=None, flock=None):
 
 
 def serve_block(r, requests: int, rates, schedule: str = "srpt", fifo: bool = True, flock_inst=None, flock=None,
-                timeout_s: float = 1500.0) -> dict:
+                timeout_s: float = 1500.0, wave_slots: int = 0) -> dict:
     """Serving: Poisson arrivals at each rate of 80% stills / 20% 24-frame sequences (the
     flocks' sequences animated: TLAS rebuilt per frame through a fork), resolution per
     request log-uniform 256x256..1920x1080, spp U{8..128}, depth 8, 160 GB admission
@@ -364,7 +364,8 @@ def serve_block(r, requests: int, rates, schedule: str = "srpt", fifo: bool = Tr
                            pixels_range=(256 * 256, 1920 * 1080))
         row = {"rate": rate}
         with ClockSampler(r.device) as clocks:
-            with Server(r, memory_budget_bytes=160 << 30, max_jobs=256, flags=flags, aging_paths_per_s=aging) as srv:
+            with Server(r, memory_budget_bytes=160 << 30, max_jobs=256, flags=flags, aging_paths_per_s=aging,
+                        wave_capacity=wave_slots) as srv:
                 row["continuous"] = poisson_load(srv, scenes, copy.deepcopy(reqs), rate=rate, seed=i, timeout_s=timeout_s,
                                                  animations=animations)
         row["continuous"]["clocks"] = clocks.summary()
@@ -532,7 +533,8 @@ def run_serve(args, device):
     with Renderer(device) as r:
         sc, flock = scene.flock_scene()
         inst = r.install(sc)
-        blk = serve_block(r, args.requests, rates, args.schedule, fifo=True, flock_inst=inst, flock=flock)
+        blk = serve_block(r, args.requests, rates, args.schedule, fifo=True, flock_inst=inst, flock=flock,
+                          wave_slots=args.serve_wave_slots)
         inst.close()
     best = max(blk["rates"], key=lambda x: x["continuous"]["throughput_paths_s"])
     print(json.dumps(_line(best["continuous"]["throughput_paths_s"], "paths/s", len(rates), 0,
@@ -610,6 +612,7 @@ def main():
     ap.add_argument("--blas", choices=["4", "8"], default="4", help="BLAS nodes: 4-wide FP32 planes or compressed 8-wide")
     ap.add_argument("--serial-waves", action="store_true", help="large: one wave after another on one stream (no overlap)")
     ap.add_argument("--wave-samples", type=int, default=0, help="large: samples per wave (0: as many as the wavefront holds)")
+    ap.add_argument("--serve-wave-slots", type=int, default=0, help="serve: path slots per server wave (0: the context's)")
     ap.add_argument("--no-error", action="store_true", help="cache: skip the reference renders (timing/profiling runs)")
     ap.add_argument("--res", default="1920x1080", help="cache: frame resolution (smaller for profiling captures)")
     ap.add_argument("--schedule", default="srpt", choices=["srpt", "aged", "fair", "packed"], help="serve: wave schedule")
