@@ -610,6 +610,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tlas", choices=["lbvh", "ploc"], default="lbvh", help="TLAS builder of the frame scene")
     ap.add_argument("--blas", choices=["4", "8"], default="4", help="BLAS nodes: 4-wide FP32 planes or compressed 8-wide")
+    ap.add_argument("--blas-builder", choices=["sah", "lbvh", "ploc"], default="sah", help="BLAS build: host SAH or GPU LBVH / PLOC")
     ap.add_argument("--serial-waves", action="store_true", help="large: one wave after another on one stream (no overlap)")
     ap.add_argument("--wave-samples", type=int, default=0, help="large: samples per wave (0: as many as the wavefront holds)")
     ap.add_argument("--serve-wave-slots", type=int, default=0, help="serve: path slots per server wave (0: the context's)")
@@ -655,6 +656,7 @@ def main():
     sc, flock, prof, cfg = workload(args.config, seed=rank)
     sc.tlas_builder = abi.TLAS_PLOC if args.tlas == "ploc" else abi.TLAS_LBVH
     sc.blas_format = abi.BLAS_WIDE8 if args.blas == "8" else abi.BLAS_WIDE4
+    sc.blas_builder = {"sah": abi.BLAS_BUILD_SAH, "lbvh": abi.BLAS_BUILD_LBVH, "ploc": abi.BLAS_BUILD_PLOC}[args.blas_builder]
     frames = frames_for(sc, flock, args.warmup + args.steps)
     cam = sc.camera
     npix = cam.width * cam.height
@@ -715,6 +717,7 @@ def main():
     tlas = {"builder": ("PLOC (radius 16)" if args.tlas == "ploc" else "Karras LBVH") + " over 30-bit Morton order (bit 30: boxes wider than a quarter of the centroid spread, split at the root), rebuilt every frame",
             "build_ms_per_frame": build_ms / args.steps,
             "blas_nodes": "compressed 8-wide (80 B)" if args.blas == "8" else "4-wide FP32 planes (128 B)",
+            "blas_builder": {"sah": "binned SAH on the host threads", "lbvh": "GPU LBVH", "ploc": "GPU PLOC"}[args.blas_builder],
             **s.tlas_stats()}
     elapsed_ms = max_over_ranks(elapsed_ms, dist, f"cuda:{local}")
     value = world * args.steps * paths_per_step / (elapsed_ms / 1000.0)

@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define VKB_ABI_VERSION 6u
+#define VKB_ABI_VERSION 7u
 
 /* Error model: FailureKind exit categories of crates/vork-render/src/failure.rs:21-100,
  * reduced to what a render call can report. */
@@ -154,7 +154,15 @@ typedef struct vkb_scene_desc {
                                          reference's TLAS is built by the graphics driver) */
     const vkb_environment_image* environment_image;   /* NULL: the constant environment alone */
     uint32_t blas_format;             /* VKB_BLAS_WIDE4 (default) or VKB_BLAS_WIDE8 */
+    uint32_t blas_builder;            /* VKB_BLAS_BUILD_SAH (default), _LBVH or _PLOC */
 } vkb_scene_desc;
+
+/* BLAS builders: a binned-SAH tree on the host threads (the trees that trace fastest), or
+ * on the GPU the TLAS's own Morton-ordered builders, LBVH or PLOC (install in milliseconds
+ * for scenes that must start rendering at once; 4-wide nodes only). */
+#define VKB_BLAS_BUILD_SAH 0u
+#define VKB_BLAS_BUILD_LBVH 1u
+#define VKB_BLAS_BUILD_PLOC 2u
 
 /* BLAS node formats (the TLAS is 4-wide in both): 4-wide FP32 child planes (one 128-byte
  * line per node), or compressed 8-wide nodes (80 bytes: child boxes as bytes on a per-node

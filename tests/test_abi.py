@@ -27,7 +27,7 @@ def test_library_builds_and_exports_every_symbol():
     for s in declared_symbols():
         assert hasattr(lib, s), s
     assert set(declared_symbols()) == set(abi.SIGNATURES)
-    assert lib.vkb_abi_version() == 6
+    assert lib.vkb_abi_version() == 7
 
 
 def test_product_package_does_not_import_the_oracle():

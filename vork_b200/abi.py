@@ -62,7 +62,8 @@ class VkbSceneDesc(C.Structure):
                 ("instance_material", C.POINTER(C.c_uint32)), ("materials", C.POINTER(VkbMaterial)),
                 ("num_materials", C.c_uint32), ("lights", C.POINTER(VkbLight)), ("num_lights", C.c_uint32),
                 ("camera", VkbCamera), ("environment", VkbEnvironment), ("tlas_builder", C.c_uint32),
-                ("environment_image", C.POINTER(VkbEnvironmentImage)), ("blas_format", C.c_uint32)]
+                ("environment_image", C.POINTER(VkbEnvironmentImage)), ("blas_format", C.c_uint32),
+                ("blas_builder", C.c_uint32)]
 
 
 class VkbProfile(C.Structure):
@@ -94,6 +95,7 @@ PROFILE_TIME_KERNELS, PROFILE_COUNT_TRAVERSAL, PROFILE_SERIAL_WAVES = 1, 2, 16
 BATCH_FAIR, BATCH_PACKED = 4, 8
 TLAS_LBVH, TLAS_PLOC = 0, 1
 BLAS_WIDE4, BLAS_WIDE8 = 0, 1
+BLAS_BUILD_SAH, BLAS_BUILD_LBVH, BLAS_BUILD_PLOC = 0, 1, 2
 NOALLOC_SCRATCH_MIB = 32
 
 

@@ -399,6 +399,7 @@ struct vkb_scene {
     DBuf<Bvh4Node> blas4, tlas4;              // 4-wide traversal nodes (TLAS sparse: index = binary node)
     DBuf<Bvh8Node> blas8;                     // compressed 8-wide BLAS nodes (VKB_BLAS_WIDE8 scenes; blas4 then unused)
     uint32_t blas_format = VKB_BLAS_WIDE4;
+    uint32_t blas_builder = VKB_BLAS_BUILD_SAH;
     DBuf<uint8_t> tlas_odd;                   // depth parity of the binary TLAS nodes
     DBuf<TlasLeaf> tlas_leaves;
     DBuf<vkb_material> d_materials;
@@ -652,6 +653,9 @@ void validate_desc(const vkb_scene_desc* d) {
     if (d->camera.width == 0 || d->camera.height == 0) throw ArgError{"camera resolution is zero"};
     if (d->tlas_builder > VKB_TLAS_PLOC) throw ArgError{"unknown TLAS builder"};
     if (d->blas_format > VKB_BLAS_WIDE8) throw ArgError{"unknown BLAS format"};
+    if (d->blas_builder > VKB_BLAS_BUILD_PLOC) throw ArgError{"unknown BLAS builder"};
+    if (d->blas_builder != VKB_BLAS_BUILD_SAH && d->blas_format == VKB_BLAS_WIDE8)
+        throw Unsupported{"compressed 8-wide BLASes are collapsed from the host SAH tree"};
     if (const vkb_environment_image* e = d->environment_image) {
         if (!e->rgba || e->width == 0 || e->height == 0) throw ArgError{"environment image has no texels"};
         if (uint64_t(e->width) * e->height > (uint64_t(1) << 26)) throw ArgError{"environment image above 2^26 texels"};
@@ -1323,6 +1327,59 @@ vkb_status vkb_close(vkb_ctx* c) {
     return VKB_OK;
 }
 
+// Every mesh's BLAS on the GPU with the TLAS's builders (Morton order, then Karras LBVH or
+// PLOC), its leaf references in the BLAS encoding, collapsed to 4-wide nodes indexed like
+// the binary nodes (even depths used), and the triangles and normals in leaf order.
+void build_blas_gpu(vkb_scene* s, uint32_t builder, cudaStream_t st) {
+    const int sms = s->ctx->sms;
+    uint32_t total = 0, max_tris = 1;
+    for (auto& mi : s->mesh_info) {
+        mi.node_offset = total;
+        total += mi.num_triangles > 1 ? mi.num_triangles - 1 : 1u;
+        max_tris = std::max(max_tris, mi.num_triangles);
+    }
+    s->blas4.alloc(std::max(1u, total));
+    s->tri_nrm.alloc(std::max<size_t>(1, size_t(s->total_tris) * 3));
+    DBuf<BvhNode> bin;
+    DBuf<uint8_t> odd;
+    DBuf<uint32_t> leaf_parent, node_parent, counters;
+    bin.alloc(max_tris); odd.alloc(max_tris);
+    if (builder == VKB_BLAS_BUILD_PLOC) { leaf_parent.alloc(max_tris); node_parent.alloc(max_tris); counters.alloc(max_tris); }
+    // Every scratch buffer at the largest mesh's size before the first launch: growing one
+    // between meshes would free memory that the previous mesh's kernels, still queued on
+    // this non-blocking stream, read.
+    s->scratch.reserve(max_tris, st);
+    if (builder == VKB_BLAS_BUILD_PLOC) s->ploc.reserve(max_tris, st);
+    VKB_CUDA(cudaStreamSynchronize(st));
+    for (const MeshInfo& mi : s->mesh_info) {
+        const uint32_t n = mi.num_triangles;
+        if (n == 0) continue;
+        const uint32_t* idx = s->indices.p + mi.index_offset;
+        k_tri_boxes<<<grid_for(n, 256, sms), 256, 0, st>>>(n, idx, s->vpos.p + mi.vertex_offset, s->tri_lo.p, s->tri_hi.p);
+        const uint32_t* parents = s->scratch.node_parent.p;
+        if (builder == VKB_BLAS_BUILD_PLOC && n > 1) {
+            morton_sort(n, s->tri_lo.p, s->tri_hi.p, s->scratch, st, sms, s->launches);
+            build_ploc(n, s->tri_lo.p, s->tri_hi.p, bin.p, leaf_parent.p, node_parent.p, counters.p, s->scratch, s->ploc, st, sms, s->launches);
+            parents = node_parent.p;
+        } else {
+            build_lbvh(n, s->tri_lo.p, s->tri_hi.p, bin.p, s->scratch, st, sms, s->launches);
+        }
+        const uint32_t ni = n > 1 ? n - 1 : 1u;
+        k_blas_leaf_refs<<<grid_for(ni, 256, sms), 256, 0, st>>>(ni, bin.p);
+        if (n > 1) k_bvh_parity<<<grid_for(ni, 256, sms), 256, 0, st>>>(ni, parents, odd.p);
+        else VKB_CUDA(cudaMemsetAsync(odd.p, 0, 1, st));
+        k_collapse4<<<grid_for(ni, 256, sms), 256, 0, st>>>(ni, bin.p, odd.p, s->blas4.p + mi.node_offset);
+        k_sorted_tris<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->scratch.ids_sorted.p, idx, s->vpos.p + mi.vertex_offset,
+                                                             s->blas_tris.p + 3 * size_t(mi.tri_offset));
+        k_sorted_nrm<<<grid_for(n, 256, sms), 256, 0, st>>>(n, s->scratch.ids_sorted.p, idx, s->vnrm.p + mi.vertex_offset,
+                                                            s->tri_nrm.p + 3 * size_t(mi.tri_offset));
+        s->launches += 6;
+        VKB_CUDA(cudaGetLastError());
+    }
+    VKB_CUDA(cudaStreamSynchronize(st));
+    bin.release(); odd.release(); leaf_parent.release(); node_parent.release(); counters.release();
+}
+
 vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** out) {
     if (!ctx || !out) return fail(VKB_INVALID_ARG, "null context or output pointer");
     *out = nullptr;
@@ -1341,6 +1398,7 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         s->num_instances = d->num_instances;
         s->tlas_builder = d->tlas_builder;
         s->blas_format = d->blas_format;
+        s->blas_builder = d->blas_builder;
         const bool wide8 = s->blas_format == VKB_BLAS_WIDE8;
         // Concatenate meshes.
         uint32_t nv = 0, nt = 0;
@@ -1378,71 +1436,75 @@ vkb_status vkb_scene_create(vkb_ctx* ctx, const vkb_scene_desc* d, vkb_scene** o
         s->tri_lo.alloc(std::max(1u, max_tris)); s->tri_hi.alloc(std::max(1u, max_tris));
         VKB_CUDA(cudaEventRecord(s->ev0, str));
         const auto t_blas = std::chrono::steady_clock::now();
-        std::vector<Bvh4Node> all_nodes;
-        std::vector<Bvh8Node> all_nodes8;
-        std::vector<float4> all_tris(std::max<size_t>(1, size_t(nt) * 3)), all_nrm(std::max<size_t>(1, size_t(nt) * 3));
-        for (uint32_t m = 0; m < d->num_meshes; ++m) {
-            MeshInfo& mi = s->mesh_info[m];
-            const vkb_mesh& me = d->meshes[m];
-            uint32_t n = mi.num_triangles;
-            mi.node_offset = uint32_t(wide8 ? all_nodes8.size() : all_nodes.size());
-            if (n == 0) continue;
-            std::vector<float> lo(3 * size_t(n)), hi(3 * size_t(n)), cen(3 * size_t(n));
-            for (uint32_t t = 0; t < n; ++t)
-                for (int a = 0; a < 3; ++a) {
-                    float v0 = me.positions[3 * me.indices[3 * t] + a], v1 = me.positions[3 * me.indices[3 * t + 1] + a], v2 = me.positions[3 * me.indices[3 * t + 2] + a];
-                    lo[3 * t + a] = std::min(v0, std::min(v1, v2)); hi[3 * t + a] = std::max(v0, std::max(v1, v2));
-                    cen[3 * t + a] = 0.5f * (lo[3 * t + a] + hi[3 * t + a]);
+        if (s->blas_builder != VKB_BLAS_BUILD_SAH) {
+            build_blas_gpu(s, s->blas_builder, str);
+        } else {
+            std::vector<Bvh4Node> all_nodes;
+            std::vector<Bvh8Node> all_nodes8;
+            std::vector<float4> all_tris(std::max<size_t>(1, size_t(nt) * 3)), all_nrm(std::max<size_t>(1, size_t(nt) * 3));
+            for (uint32_t m = 0; m < d->num_meshes; ++m) {
+                MeshInfo& mi = s->mesh_info[m];
+                const vkb_mesh& me = d->meshes[m];
+                uint32_t n = mi.num_triangles;
+                mi.node_offset = uint32_t(wide8 ? all_nodes8.size() : all_nodes.size());
+                if (n == 0) continue;
+                std::vector<float> lo(3 * size_t(n)), hi(3 * size_t(n)), cen(3 * size_t(n));
+                for (uint32_t t = 0; t < n; ++t)
+                    for (int a = 0; a < 3; ++a) {
+                        float v0 = me.positions[3 * me.indices[3 * t] + a], v1 = me.positions[3 * me.indices[3 * t + 1] + a], v2 = me.positions[3 * me.indices[3 * t + 2] + a];
+                        lo[3 * t + a] = std::min(v0, std::min(v1, v2)); hi[3 * t + a] = std::max(v0, std::max(v1, v2));
+                        cen[3 * t + a] = 0.5f * (lo[3 * t + a] + hi[3 * t + a]);
+                    }
+                vkb_host::SahBlas sah;
+                sah.run(n, lo.data(), hi.data(), cen.data());
+                if (sah.nodes.size() > std::max(1u, n > 1 ? n - 1 : 1u)) throw ArgError{"BLAS node count above its bound"};
+                static_assert(sizeof(vkb_host::SahNode) == sizeof(BvhNode), "host SAH nodes have the device layout");
+                // Leaf position k of this mesh's BLAS -> its original triangle.
+                std::vector<uint32_t> leaf_tri(sah.order);
+                if (wide8) {
+                    static_assert(sizeof(vkb_host::Wide8Node) == sizeof(Bvh8Node), "host 8-wide nodes have the device layout");
+                    vkb_host::Wide8Blas w8;
+                    w8.run(sah.nodes, n);
+                    if (all_nodes8.size() + w8.nodes.size() > size_t(INT32_MAX)) throw ArgError{"BLAS node count above its bound"};
+                    const size_t at = all_nodes8.size();
+                    all_nodes8.resize(at + w8.nodes.size());
+                    std::memcpy(all_nodes8.data() + at, w8.nodes.data(), w8.nodes.size() * sizeof(Bvh8Node));
+                    for (uint32_t k = 0; k < n; ++k) leaf_tri[k] = sah.order[w8.order[k]];
+                } else {
+                    std::vector<BvhNode> bin(sah.nodes.size());
+                    std::memcpy(bin.data(), sah.nodes.data(), bin.size() * sizeof(BvhNode));
+                    std::vector<Bvh4Node> wide = collapse_blas(bin);
+                    if (all_nodes.size() + wide.size() > size_t(INT32_MAX)) throw ArgError{"BLAS node count above its bound"};
+                    all_nodes.insert(all_nodes.end(), wide.begin(), wide.end());
                 }
-            vkb_host::SahBlas sah;
-            sah.run(n, lo.data(), hi.data(), cen.data());
-            if (sah.nodes.size() > std::max(1u, n > 1 ? n - 1 : 1u)) throw ArgError{"BLAS node count above its bound"};
-            static_assert(sizeof(vkb_host::SahNode) == sizeof(BvhNode), "host SAH nodes have the device layout");
-            // Leaf position k of this mesh's BLAS -> its original triangle.
-            std::vector<uint32_t> leaf_tri(sah.order);
+                for (uint32_t k = 0; k < n; ++k) {
+                    uint32_t t = leaf_tri[k];
+                    const float* p0 = me.positions + 3 * me.indices[3 * t];
+                    const float* p1 = me.positions + 3 * me.indices[3 * t + 1];
+                    const float* p2 = me.positions + 3 * me.indices[3 * t + 2];
+                    size_t o = 3 * (size_t(mi.tri_offset) + k);
+                    float tid;
+                    std::memcpy(&tid, &t, sizeof(tid));
+                    all_tris[o] = make_float4(p0[0], p0[1], p0[2], tid);
+                    all_tris[o + 1] = make_float4(p1[0], p1[1], p1[2], 0.f);
+                    all_tris[o + 2] = make_float4(p2[0], p2[1], p2[2], 0.f);
+                    for (int c = 0; c < 3; ++c) {
+                        const float* nv = me.normals ? me.normals + 3 * me.indices[3 * t + c] : nullptr;
+                        all_nrm[o + c] = nv ? make_float4(nv[0], nv[1], nv[2], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+                }
+            }
+            if (all_nodes.empty()) all_nodes.emplace_back();
             if (wide8) {
-                static_assert(sizeof(vkb_host::Wide8Node) == sizeof(Bvh8Node), "host 8-wide nodes have the device layout");
-                vkb_host::Wide8Blas w8;
-                w8.run(sah.nodes, n);
-                if (all_nodes8.size() + w8.nodes.size() > size_t(INT32_MAX)) throw ArgError{"BLAS node count above its bound"};
-                const size_t at = all_nodes8.size();
-                all_nodes8.resize(at + w8.nodes.size());
-                std::memcpy(all_nodes8.data() + at, w8.nodes.data(), w8.nodes.size() * sizeof(Bvh8Node));
-                for (uint32_t k = 0; k < n; ++k) leaf_tri[k] = sah.order[w8.order[k]];
-            } else {
-                std::vector<BvhNode> bin(sah.nodes.size());
-                std::memcpy(bin.data(), sah.nodes.data(), bin.size() * sizeof(BvhNode));
-                std::vector<Bvh4Node> wide = collapse_blas(bin);
-                if (all_nodes.size() + wide.size() > size_t(INT32_MAX)) throw ArgError{"BLAS node count above its bound"};
-                all_nodes.insert(all_nodes.end(), wide.begin(), wide.end());
+                if (all_nodes8.empty()) all_nodes8.emplace_back();
+                s->blas8.upload(all_nodes8.data(), all_nodes8.size(), str);
             }
-            for (uint32_t k = 0; k < n; ++k) {
-                uint32_t t = leaf_tri[k];
-                const float* p0 = me.positions + 3 * me.indices[3 * t];
-                const float* p1 = me.positions + 3 * me.indices[3 * t + 1];
-                const float* p2 = me.positions + 3 * me.indices[3 * t + 2];
-                size_t o = 3 * (size_t(mi.tri_offset) + k);
-                float tid;
-                std::memcpy(&tid, &t, sizeof(tid));
-                all_tris[o] = make_float4(p0[0], p0[1], p0[2], tid);
-                all_tris[o + 1] = make_float4(p1[0], p1[1], p1[2], 0.f);
-                all_tris[o + 2] = make_float4(p2[0], p2[1], p2[2], 0.f);
-                for (int c = 0; c < 3; ++c) {
-                    const float* nv = me.normals ? me.normals + 3 * me.indices[3 * t + c] : nullptr;
-                    all_nrm[o + c] = nv ? make_float4(nv[0], nv[1], nv[2], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-            }
+            blas_host = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_blas).count();
+            s->blas4.alloc(all_nodes.size());
+            VKB_CUDA(cudaMemcpyAsync(s->blas4.p, all_nodes.data(), all_nodes.size() * sizeof(Bvh4Node), cudaMemcpyHostToDevice, str));
+            VKB_CUDA(cudaMemcpyAsync(s->blas_tris.p, all_tris.data(), all_tris.size() * sizeof(float4), cudaMemcpyHostToDevice, str));
+            s->tri_nrm.upload(all_nrm.data(), all_nrm.size(), str);
         }
-        if (all_nodes.empty()) all_nodes.emplace_back();
-        if (wide8) {
-            if (all_nodes8.empty()) all_nodes8.emplace_back();
-            s->blas8.upload(all_nodes8.data(), all_nodes8.size(), str);
-        }
-        blas_host = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_blas).count();
-        s->blas4.alloc(all_nodes.size());
-        VKB_CUDA(cudaMemcpyAsync(s->blas4.p, all_nodes.data(), all_nodes.size() * sizeof(Bvh4Node), cudaMemcpyHostToDevice, str));
-        VKB_CUDA(cudaMemcpyAsync(s->blas_tris.p, all_tris.data(), all_tris.size() * sizeof(float4), cudaMemcpyHostToDevice, str));
-        s->tri_nrm.upload(all_nrm.data(), all_nrm.size(), str);
         VKB_CUDA(cudaStreamSynchronize(str));
         VKB_CUDA(cudaEventRecord(s->ev1, str));
         s->meshes.upload(s->mesh_info.data(), s->mesh_info.size(), str);
@@ -1518,7 +1580,7 @@ vkb_status vkb_scene_fork(vkb_scene* b, vkb_scene** out) {
         s->tree_nodes = b->tree_nodes; s->tlas_builder = b->tlas_builder;
         // Shared, read-only: geometry, BLASes, materials, lights, light tree.
         s->vpos = b->vpos; s->vnrm = b->vnrm; s->blas_tris = b->blas_tris; s->tri_nrm = b->tri_nrm;
-        s->indices = b->indices; s->meshes = b->meshes; s->blas4 = b->blas4; s->blas8 = b->blas8; s->blas_format = b->blas_format;
+        s->indices = b->indices; s->meshes = b->meshes; s->blas4 = b->blas4; s->blas8 = b->blas8; s->blas_format = b->blas_format; s->blas_builder = b->blas_builder;
         s->d_materials = b->d_materials; s->d_lights = b->d_lights; s->tree = b->tree;
         s->env_img = b->env_img; s->env_dist = b->env_dist; s->env_w = b->env_w; s->env_h = b->env_h;
         std::copy(b->env_scale, b->env_scale + 3, s->env_scale); std::copy(b->env_rot, b->env_rot + 9, s->env_rot);

@@ -402,6 +402,23 @@ __global__ void k_sorted_tris(uint32_t n, const uint32_t* sorted_ids, const uint
         tris[3 * k + 2] = make_float4(c.x, c.y, c.z, 0.f);
     }
 }
+// Vertex normals of one mesh's triangles in the same order (zeros where the mesh has none).
+__global__ void k_sorted_nrm(uint32_t n, const uint32_t* sorted_ids, const uint32_t* idx, const float4* nrm, float4* out) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        uint32_t t = sorted_ids[k];
+        out[3 * k] = nrm[idx[3 * t]]; out[3 * k + 1] = nrm[idx[3 * t + 1]]; out[3 * k + 2] = nrm[idx[3 * t + 2]];
+    }
+}
+// A GPU-built BLAS's leaf references in the traversal's BLAS encoding: the binary builders
+// reference leaf k as ~k, the BLAS step reads ~(first << 2 | count - 1) (one triangle each).
+__global__ void k_blas_leaf_refs(uint32_t n_internal, BvhNode* nodes) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_internal; i += gridDim.x * blockDim.x) {
+        int4 d = nodes[i].d;
+        if (d.x < 0) d.x = ~int(uint32_t(~d.x) << 2);
+        if (d.y < 0) d.y = ~int(uint32_t(~d.y) << 2);
+        nodes[i].d = d;
+    }
+}
 __global__ void k_tlas_leaves(uint32_t n, const uint32_t* sorted_ids, const float4* w2o, const uint4* info, const MeshInfo* meshes,
                               const vkb_material* materials, TlasLeaf* leaves) {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {

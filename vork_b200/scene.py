@@ -274,6 +274,7 @@ class Scene:
     tlas_builder: int = abi.TLAS_LBVH
     env_image: "EnvironmentImage | None" = None
     blas_format: int = abi.BLAS_WIDE4
+    blas_builder: int = abi.BLAS_BUILD_SAH
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -315,6 +316,7 @@ class Scene:
         d.environment = self.environment
         d.tlas_builder = self.tlas_builder
         d.blas_format = self.blas_format
+        d.blas_builder = self.blas_builder
         if self.env_image is not None:
             img = np.ascontiguousarray(self.env_image.rgba, np.float32)
             e = abi.VkbEnvironmentImage()
