@@ -347,7 +347,7 @@ def serve_scenes(r, flock_inst=None, flock=None):
 
 
 def serve_block(r, requests: int, rates, schedule: str = "srpt", fifo: bool = True, flock_inst=None, flock=None,
-                timeout_s: float = 1500.0, wave_slots: int = 0) -> dict:
+                timeout_s: float = 1500.0, wave_slots: int = 0, serial: bool = False) -> dict:
     """Serving: Poisson arrivals at each rate of 80% stills / 20% 24-frame sequences (the
     flocks' sequences animated: TLAS rebuilt per frame through a fork), resolution per
     request log-uniform 256x256..1920x1080, spp U{8..128}, depth 8, 160 GB admission
@@ -356,7 +356,8 @@ def serve_block(r, requests: int, rates, schedule: str = "srpt", fifo: bool = Tr
     from vork_b200.serving import Server, fifo_load, poisson_load, request_mix
     t_block = time.perf_counter()
     scenes, animations, names, owned = serve_scenes(r, flock_inst, flock)
-    flags = {"srpt": 0, "aged": 0, "fair": 4, "packed": 8}[schedule]
+    from vork_b200 import abi
+    flags = {"srpt": 0, "aged": 0, "fair": 4, "packed": 8}[schedule] | (abi.PROFILE_SERIAL_WAVES if serial else 0)
     aging = 2e8 if schedule == "aged" else 0.0   # paths per second waited: about the device's rate on these scenes
     out = []
     for i, rate in enumerate(rates):
@@ -534,7 +535,7 @@ def run_serve(args, device):
         sc, flock = scene.flock_scene()
         inst = r.install(sc)
         blk = serve_block(r, args.requests, rates, args.schedule, fifo=True, flock_inst=inst, flock=flock,
-                          wave_slots=args.serve_wave_slots)
+                          wave_slots=args.serve_wave_slots, serial=args.serve_serial)
         inst.close()
     best = max(blk["rates"], key=lambda x: x["continuous"]["throughput_paths_s"])
     print(json.dumps(_line(best["continuous"]["throughput_paths_s"], "paths/s", len(rates), 0,
@@ -614,6 +615,7 @@ def main():
     ap.add_argument("--serial-waves", action="store_true", help="large: one wave after another on one stream (no overlap)")
     ap.add_argument("--wave-samples", type=int, default=0, help="large: samples per wave (0: as many as the wavefront holds)")
     ap.add_argument("--serve-wave-slots", type=int, default=0, help="serve: path slots per server wave (0: the context's)")
+    ap.add_argument("--serve-serial", action="store_true", help="serve: the server's waves on one stream (replayed graphs)")
     ap.add_argument("--no-error", action="store_true", help="cache: skip the reference renders (timing/profiling runs)")
     ap.add_argument("--res", default="1920x1080", help="cache: frame resolution (smaller for profiling captures)")
     ap.add_argument("--schedule", default="srpt", choices=["srpt", "aged", "fair", "packed"], help="serve: wave schedule")

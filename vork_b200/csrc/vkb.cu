@@ -2130,6 +2130,7 @@ uint64_t resident_bytes(const vkb_server* v) {
 constexpr uint64_t SERVER_BYTES_PER_PIXEL = 2 * sizeof(float4);   // accumulator + mean image
 // Buffers for npix pixels: the smallest idle ones that hold them (and are not more than
 // twice as large), else new ones.
+constexpr uint64_t SERVER_DEVICE_RESERVE = uint64_t(1) << 30;   // device memory left to the driver and other users
 vkb_server::Buffers take_buffers(vkb_server* v, size_t npix) {
     auto it = v->pool.lower_bound(npix);
     if (it != v->pool.end() && it->first <= 2 * npix) {
@@ -2290,6 +2291,21 @@ vkb_status vkb_server_step(vkb_server* v, vkb_server_status* status) {
                 extra = need;
             }
             if (v->budget && held() + scene + extra + ext_bytes > v->budget) break;
+            // The budget counts the server's own memory only: a request that needs new
+            // device memory also waits for the device to have it (other renders on the
+            // context hold their own wavefronts), unless nothing else is running.
+            if (extra + ext_bytes > 0) {
+                auto device_free = [] {
+                    size_t f = 0, t = 0;
+                    return cudaMemGetInfo(&f, &t) == cudaSuccess ? uint64_t(f) : ~uint64_t(0);
+                };
+                if (device_free() < extra + ext_bytes + SERVER_DEVICE_RESERVE && v->pool_bytes) {
+                    finished += reap(v, true, false);
+                    free_pool(v);
+                    extra = need;
+                }
+                if (device_free() < extra + ext_bytes + SERVER_DEVICE_RESERVE && (!eng.jobs.empty() || !v->inflight.empty())) break;
+            }
             if (ext) {
                 v->wave.reserve_ext(v->capacity);
                 v->wave_bytes += ext_bytes;
