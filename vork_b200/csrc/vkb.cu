@@ -1240,7 +1240,8 @@ void render_jobs(vkb_ctx* c, const std::vector<std::pair<vkb_scene*, vkb_profile
         paths += uint64_t(e.npix) * e.count;
     }
     // Renders of more than one wave overlap their waves on two streams (not with the
-    // adaptive, guide or radiance-cache hooks, which read one wave's results in the next).
+    // adaptive, guide or radiance-cache hooks: adaptive stopping reads one wave's moments in the
+    // next, the guide and cache hooks fill buffers shared by all waves).
     // Timed renders keep one stream too: an event pair around a kernel would also count the
     // other stream's kernels sharing the SMs.
     uint64_t all_paths = 0;
