@@ -615,6 +615,12 @@ void refit_tlas(vkb_scene* s) {
 
 // rt.rs:1465-1476: accumulate the changed object bytes; rebuild once they reach a
 // quarter of the object buffer, otherwise refit (policy 0).  1 rebuilds, 2 refits.
+// A server wave on the second stream may still read a scene's rows and TLAS: an update on
+// the context's stream starts after it.
+void after_second_stream(vkb_ctx* c) {
+    VKB_CUDA(cudaEventRecord(c->join_ev, c->stream2));
+    VKB_CUDA(cudaStreamWaitEvent(c->stream, c->join_ev, 0));
+}
 void update_tlas(vkb_scene* s, uint64_t changed_bytes, int policy) {
     uint64_t total = uint64_t(s->num_instances) * 48u;
     uint64_t threshold = std::max<uint64_t>(1, (total + 3) / 4);
@@ -1620,6 +1626,7 @@ vkb_status vkb_scene_destroy(vkb_scene* s) {
     if (s->forks) return fail(VKB_INVALID_ARG, "scene has live forks: destroy them first");
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->ctx->stream);
+    cudaStreamSynchronize(s->ctx->stream2);
     if (s->base) {
         // Shared with the base scene: not this fork's to free.
         DBuf<float4>* shared4[] = {&s->vpos, &s->vnrm, &s->blas_tris, &s->tri_nrm};
@@ -1663,6 +1670,7 @@ vkb_status vkb_scene_update_instances(vkb_scene* s, const float* rows, uint32_t 
     if (policy < 0 || policy > 2) return fail(VKB_INVALID_ARG, "policy must be 0, 1 or 2");
     return guarded([&] {
         VKB_CUDA(cudaSetDevice(s->ctx->device));
+        after_second_stream(s->ctx);
         // Changed bytes: rows that differ from the installed ones, counted on the device
         // (the new rows go up once; only the count comes back).
         cudaStream_t st = s->ctx->stream;
@@ -1688,6 +1696,7 @@ vkb_status vkb_scene_update_instances_device(vkb_scene* s, const float* rows, ui
     if (policy < 0 || policy > 2) return fail(VKB_INVALID_ARG, "policy must be 0, 1 or 2");
     return guarded([&] {
         VKB_CUDA(cudaSetDevice(s->ctx->device));
+        after_second_stream(s->ctx);
         VKB_CUDA(cudaMemcpyAsync(s->o2w.p, rows, size_t(n) * 3 * sizeof(float4), cudaMemcpyDeviceToDevice, s->ctx->stream));
         // device rows: every row counts as changed
         update_tlas(s, uint64_t(n) * 48u, policy);
